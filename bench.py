@@ -1,0 +1,340 @@
+"""Benchmark of the per-frame fluid step at 256^3 (plume-family scene).
+
+A step is one frame: particle sourcing + FluidSolver::step (forces,
+divergence, red-black Gauss-Seidel to relative FP64 residual 1e-4 warm-started
+from the previous frame's pressure, gradient, RK3 advection).  Prints one
+JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CUDA build (oracle/_ref) on the
+same scene and particles through its FluidSolver API, with maxIterSolve equal
+to the mean sweep count the plain RBGS step needs here (the reference has no
+residual control).  N > 1 runs independent replicas, one per GPU (the single
+grid does not shard); value is the sum over ranks, timed as the max over
+ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "256³ steps/s: learned warm-start vs plain RBGS at equal residual; HBM GB/s"
+GRID = 256
+SEED = 3
+TOL = 1e-4
+MAX_ITER = 4000
+CHECK_EVERY = 20
+# Sweeps per frame the reference arm runs (maxIterSolve): the mean the plain
+# RBGS step needs on this scene and frame window, measured on a B200.
+REF_EQUAL_WORK_SWEEPS = int(os.environ.get("BLZ_REF_SWEEPS", "400"))
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = [r.split(",") for r in (self.out or "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def step_bytes(W, H, D, sweeps, checks):
+    """Algorithmic HBM bytes of one frame (FP32; velocity read once per pass)."""
+    cT = W * H * D
+    cF = (W + 1) * H * D + W * (H + 1) * D + W * H * (D + 1)
+    forces = 8 * cT + 8 * cF
+    divergence = 4 * cF + 4 * cT
+    rbgs = 12 * cT * sweeps
+    residual = 8 * cT * checks
+    gradient = 4 * cT + 8 * cF
+    advect = 8 * cT + 8 * cF
+    return forces + divergence + rbgs + residual + gradient + advect
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline(scn, parts, mean_sweeps):
+    """FP64 oracle (OpenMP) on a bounded sample of the same frame: the
+    non-solver stages once plus 10 sweeps, extrapolated to the mean sweep
+    count of the GPU run."""
+    from oracle import oracle
+    p = scn.to_params()
+    st = oracle.State(p, np.float64)
+    st.add_source(parts)
+    t0 = time.perf_counter()
+    st.add_source(parts)
+    st.forces(0.0)
+    st.divergence()
+    t1 = time.perf_counter()
+    n_s = 10
+    st.gs_sweeps(n_s)
+    t2 = time.perf_counter()
+    st.residual_norms()
+    st.gradient()
+    st.advect()
+    t3 = time.perf_counter()
+    per_sweep = (t2 - t1) / n_s
+    per_step = (t1 - t0) + (t3 - t2) + per_sweep * mean_sweeps
+    return {"value": 1.0 / per_step, "unit": "steps/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"one {scn.gridRes[0]}^3 frame of the FP64 oracle: non-solver stages timed once, "
+                      f"{n_s} GS sweeps timed and scaled to {mean_sweeps:.0f} sweeps "
+                      f"({per_sweep * 1e3:.1f} ms/sweep, {per_step:.1f} s/step)"}
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from blaze_b200 import FluidSolver, Timer, family_scene
+
+    torch.cuda.set_device(local)
+    scn, parts = family_scene(n=args.grid, seed=SEED + rank, tol=TOL, max_iter=MAX_ITER, check_every=CHECK_EVERY)
+    W, H, D = scn.gridRes
+    stream = torch.cuda.current_stream()
+    tmr = Timer()
+    solver = FluidSolver(tmr, scn, particles=parts, stream=stream.cuda_stream)
+
+    def frame():
+        solver.addSource()
+        st = solver.step(tmr.time)
+        tmr.iter += 1
+        tmr.time += scn.dt
+        return st
+
+    for _ in range(args.warmup):
+        frame()
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    launches0 = solver.kernel_launches()
+    stats = []
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            stats.append(frame())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = solver.kernel_launches() - launches0
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    sweeps = np.array([s["iterations"] for s in stats], float)
+    checks = np.array([s["residual_checks"] for s in stats], float)
+    rel = np.array([s["rel_residual"] for s in stats], float)
+    ms_sweeps = float(sum(s["ms_sweeps"] for s in stats))
+    conv = all(s["converged"] for s in stats)
+
+    e2e_s = None
+    # e2e through the public API with host buffers: per frame the particle
+    # records go host->device (the reference re-reads an animated source every
+    # frame) and the advanced temperature field comes back device->host.
+    if not args.no_e2e:
+        pinned_parts = torch.empty((len(parts), 8), dtype=torch.float32, pin_memory=True)
+        pinned_parts.numpy()[...] = parts
+        t_host = torch.empty(scn.to_params().field_shape("T"), dtype=torch.float32, pin_memory=True)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            solver.setParticles(pinned_parts.numpy())
+            solver.addSource()
+            solver.step(tmr.time)
+            solver.get("T", out=t_host.numpy())
+            tmr.iter += 1
+            tmr.time += scn.dt
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - w0
+    if ws > 1 and e2e_s is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    if rank != 0:
+        return None
+    peak, peak_kind = load_peaks()
+    n_cells = W * H * D
+    half_launches = 2.0 * sweeps.sum()
+    avg_half_ms = ms_sweeps / half_launches if half_launches else float("nan")
+    alg_half = 6.0 * n_cells                      # rhs_c + p_other read, p_c written (4 B each, half the cells)
+    achieved = alg_half / (avg_half_ms * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"rbgs_half_{W}.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    value = ws * args.steps / (ms * 1e-3)
+    alg_bytes = float(np.mean([step_bytes(W, H, D, s, c) for s, c in zip(sweeps, checks)]))
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plume-family {W}^3 scene (seed {SEED}, {scn.extra['sources']} sources, "
+                               f"wind {scn.extra['wind_cells_per_step']:.2f} cells/step), plain RBGS with "
+                               f"free-surface top, warm-started, to FP64 relative residual {TOL:g}",
+                   "grid": [W, H, D], "particles": int(len(parts)), "tol": TOL, "check_every": CHECK_EVERY,
+                   "mean_sweeps": float(sweeps.mean()), "max_rel_residual": float(rel.max()),
+                   "all_converged": conv, "l2": "inputs larger than L2 (0.9 GB of fields per replica)",
+                   "parallelism": f"replicas x{ws}", "learned_warm_start": "not built"},
+        "hbm_gbs_step": alg_bytes / (ms / args.steps * 1e-3) / 1e9,
+        "roofline": {"bound": "hbm", "kernel": "k_rbgs_half", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "alg_bytes_per_launch": alg_half, "avg_launch_ms": avg_half_ms},
+        "e2e": None if e2e_s is None else
+               {"value": ws * args.steps / e2e_s, "unit": "steps/s",
+                "h2d_bytes_per_step": int(parts.nbytes), "d2h_bytes_per_step": int(n_cells * 4)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "stage_ms": {k: float(np.mean([s[k] for s in stats])) for k in
+                     ("ms_forces", "ms_divergence", "ms_solve", "ms_gradient", "ms_advect", "ms_sweeps")},
+    }
+    if not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(scn, parts, float(sweeps.mean()))
+    solver.close()
+    return line
+
+
+def run_reference(args, ws, rank, local):
+    if rank != 0:
+        return None
+    import torch
+    from oracle import ref
+    from blaze_b200 import family_scene, BLZ_BC_REF_COMPAT
+    if not ref.available():
+        return {"impl": "reference", "unavailable": "reference CUDA build (oracle/_ref) not built"}
+    torch.cuda.set_device(local)
+    scn, parts = family_scene(n=args.grid, seed=SEED, tol=0.0, max_iter=REF_EQUAL_WORK_SWEEPS,
+                              bc_mode=BLZ_BC_REF_COMPAT)
+    p = scn.to_params()
+    r = ref.RefSolver(p)
+    it, t = 0, 0.0
+
+    def frame():
+        nonlocal it, t
+        r.set_time(it, t)
+        r.set_particles(parts)
+        r.add_source()
+        r.step()
+        it += 1
+        t += scn.dt
+
+    for _ in range(args.warmup):
+        frame()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            frame()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+    r.close()
+    value = args.steps / wall
+    return {
+        "metric": METRIC, "impl": "reference", "value": value, "unit": "steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plume-family {args.grid}^3 scene (seed {SEED}) through the reference's "
+                               f"own CUDA build (src/FluidSolver.cu, -O3 --use_fast_math, sm_100a), "
+                               f"maxIterSolve={REF_EQUAL_WORK_SWEEPS} (equal sweep count; the reference "
+                               f"has no residual control)", "grid": [args.grid] * 3},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference",
+                         "sample": "the reference's CUDA build on the same B200 (it has no CPU path); "
+                                   "its frame includes the .part file read of an animated source"},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=GRID)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) pass")
+    args = ap.parse_args()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        # rank 0 alone runs the reference; the other ranks exit without work
+        line = run_reference(args, ws, rank, local)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if ws > 1:
+        import torch
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        line = run_reference(args, ws, rank, local) if args.impl == "reference" else run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+    if line is not None and rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

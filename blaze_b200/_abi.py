@@ -1,0 +1,113 @@
+"""ctypes mirror of include/blaze_b200.h (structs, constants, prototypes).
+
+Shared by the product binding (``blaze_b200._lib``) and by the test-side
+oracle binding, which takes the same ``blz_params`` struct.
+"""
+import ctypes as C
+
+BLZ_OK = 0
+BLZ_ERR_CUDA = -1
+BLZ_ERR_ARG = -2
+BLZ_ERR_TIMEOUT = -3
+BLZ_ERR_NAN = -4
+BLZ_ERR_NOCONV = -5
+BLZ_ERR_ALLOC = -6
+BLZ_ERR_STATE = -7
+
+BLZ_BC_REF_COMPAT = 0
+BLZ_BC_FREE_SURFACE = 1
+BLZ_GS_RB3D = 0
+BLZ_GS_PLANE = 1
+
+FIELD_T, FIELD_U, FIELD_V, FIELD_W, FIELD_P, FIELD_RHS = range(6)
+FIELD_NAMES = {"T": FIELD_T, "U": FIELD_U, "V": FIELD_V, "W": FIELD_W, "P": FIELD_P, "RHS": FIELD_RHS}
+
+
+class BlzParams(C.Structure):
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int), ("depth", C.c_int),
+        ("dx", C.c_float), ("dt", C.c_float),
+        ("domain_min", C.c_float * 3), ("domain_max", C.c_float * 3),
+        ("closed_bounds", C.c_int * 6),
+        ("density", C.c_float), ("gravity", C.c_float), ("buoyancy", C.c_float),
+        ("cooling_rate", C.c_float), ("vorticity_conf", C.c_float), ("drag", C.c_float),
+        ("wind_dir", C.c_int),
+        ("wind_amp", C.c_float), ("wind_speed", C.c_float),
+        ("wind_turb_amp", C.c_float), ("wind_turb_scale", C.c_float),
+        ("turbulence_amp", C.c_float), ("turbulence_scale", C.c_float),
+        ("turb_mask_temp_ramp", C.c_float * 2), ("turb_mask_vel_ramp", C.c_float * 2),
+        ("max_iter", C.c_int), ("tol", C.c_double), ("check_every", C.c_int),
+        ("bc_mode", C.c_int), ("gs_order", C.c_int), ("reset_pressure", C.c_int),
+        ("max_particles", C.c_int), ("temporal_block", C.c_int),
+    ]
+
+    def dims(self):
+        return self.width, self.height, self.depth
+
+    def field_shape(self, f):
+        """numpy shape (z, y, x) of a field in the reference layout."""
+        W, H, D = self.dims()
+        if isinstance(f, str):
+            f = FIELD_NAMES[f]
+        return {FIELD_T: (D, H, W), FIELD_U: (D, H, W + 1), FIELD_V: (D, H + 1, W),
+                FIELD_W: (D + 1, H, W), FIELD_P: (D, H, W), FIELD_RHS: (D, H, W)}[f]
+
+    def copy(self):
+        p = BlzParams()
+        C.pointer(p)[0] = self
+        return p
+
+    def as_dict(self):
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+class BlzStepStats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int), ("converged", C.c_int),
+        ("residual", C.c_double), ("rhs_norm", C.c_double), ("rel_residual", C.c_double),
+        ("ms_source", C.c_float), ("ms_forces", C.c_float), ("ms_divergence", C.c_float),
+        ("ms_solve", C.c_float), ("ms_gradient", C.c_float), ("ms_advect", C.c_float),
+        ("ms_total", C.c_float), ("ms_sweeps", C.c_float), ("residual_checks", C.c_int),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+# Every entry point declared in include/blaze_b200.h, with its ctypes signature.
+_P = C.POINTER
+EXPORTS = {
+    "blz_default_params": (C.c_int, [_P(BlzParams)]),
+    "blz_create": (C.c_int, [_P(BlzParams), _P(C.c_void_p)]),
+    "blz_destroy": (C.c_int, [C.c_void_p]),
+    "blz_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "blz_set_particles": (C.c_int, [C.c_void_p, _P(C.c_float), C.c_int]),
+    "blz_add_source": (C.c_int, [C.c_void_p]),
+    "blz_step": (C.c_int, [C.c_void_p, C.c_float, _P(BlzStepStats)]),
+    "blz_forces": (C.c_int, [C.c_void_p, C.c_float]),
+    "blz_project": (C.c_int, [C.c_void_p, _P(BlzStepStats)]),
+    "blz_divergence": (C.c_int, [C.c_void_p]),
+    "blz_solve": (C.c_int, [C.c_void_p, _P(BlzStepStats)]),
+    "blz_gradient": (C.c_int, [C.c_void_p]),
+    "blz_advect": (C.c_int, [C.c_void_p]),
+    "blz_residual": (C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double)]),
+    "blz_get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "blz_set_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "blz_field_size": (C.c_size_t, [C.c_void_p, C.c_int]),
+    "blz_field_ptr": (C.c_void_p, [C.c_void_p, C.c_int]),
+    "blz_perlin": (C.c_int, [_P(C.c_float), C.c_int, C.c_float, C.c_int, _P(C.c_float)]),
+    "blz_kernel_launches": (C.c_longlong, [C.c_void_p]),
+    "blz_last_error": (C.c_char_p, [C.c_void_p]),
+}
+
+
+def bind(lib, exports=EXPORTS):
+    for name, (res, args) in exports.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib

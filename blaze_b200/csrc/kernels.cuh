@@ -1,0 +1,83 @@
+// kernels.cuh — host-side launchers of the fluid-step kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace blz {
+
+// Parameters of the force stages, resolved on the host once per step.
+struct ForceParams {
+    int   vort_on, buoy_on, wind_on;
+    float conf, tiny;                 // tiny = 1e-20f * (1/(dx*dt)), FluidSolver.cu:226
+    float beta, grav;
+    int   wind_along_x;               // wind_dir <= 1
+    float wind_dir_sign;              // +1 for dirs 0 and 2, else -1
+    float wind_amp, wind_turb_amp, wind_freq, wind_offset;
+    float turb_amp, turb_freq, turb_offset;
+    float tr0, tr1, vr0, vr1;
+};
+
+struct SolveParams {
+    float scale;                      // rho dx^2 / dt (FluidSolver.cu:530)
+    double scale_d;                   // the same in FP64 (residual only)
+    OpenFaces open;
+    int dirichlet;                    // BLZ_BC_FREE_SURFACE
+};
+
+// Launch shape for kernels over the union of the face ranges
+// [0,W] x [0,H] x [0,D].
+dim3 face_block();
+dim3 face_grid(const Geom &g);
+
+// -- sourcing ---------------------------------------------------------------
+void launch_splat(const Geom &g, const float *rec8, int n, float *accT, float *accU, float *accV,
+                  float *accW, cudaStream_t st);
+void launch_source_apply(const Geom &g, const int box[3][2], float *front, float *acc, int field,
+                         cudaStream_t st);
+
+// -- forces -------------------------------------------------------------------
+void launch_scale(float *a, size_t n, float s, cudaStream_t st);
+void launch_vort_omega(const Geom &g, const float *U, const float *V, const float *W, float *ox,
+                       float *oy, float *oz, cudaStream_t st);
+void launch_vort_force(const Geom &g, const float *U, const float *V, const float *W,
+                       const float *ox, const float *oy, const float *oz, const ForceParams &fp,
+                       float *fx, float *fy, float *fz, cudaStream_t st);
+void launch_face_forces(const Geom &g, float *U, float *V, float *W, const float *T,
+                        const float *fx, const float *fy, const float *fz, const ForceParams &fp,
+                        cudaStream_t st);
+void launch_turb_noise(const Geom &g, const float *T, const float *U, const float *V,
+                       const float *W, float *nU, float *nV, float *nW, const ForceParams &fp,
+                       cudaStream_t st);
+void launch_turb_apply(const Geom &g, float *U, float *V, float *W, const float *nU,
+                       const float *nV, const float *nW, const ForceParams &fp, cudaStream_t st);
+
+// -- projection ---------------------------------------------------------------
+void launch_divergence(const Geom &g, const float *U, const float *V, const float *W,
+                       const OpenFaces &o, float *rhs_r, float *rhs_b, cudaStream_t st);
+void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
+                        const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
+                        long long *launches);
+void launch_plane_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
+                         const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
+                         long long *launches);
+// Writes partial sums to `partials` (2 doubles per block) and the totals
+// {||r||^2, ||b||^2} to out2.  Returns the number of launches (2).
+int  launch_residual(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
+                     const float *p_r, const float *p_b, double *partials, int max_partials,
+                     double *out2, cudaStream_t st);
+int  residual_blocks(const Geom &g);
+void launch_gradient(const Geom &g, const SolveParams &sp, float dt_over_rho_dx, const float *p_r,
+                     const float *p_b, float *U, float *V, float *W, cudaStream_t st);
+// Packed <-> natural layout.
+void launch_pack(const Geom &g, const float *nat, float *red, float *black, cudaStream_t st);
+void launch_unpack(const Geom &g, const float *red, const float *black, float *nat,
+                   cudaStream_t st);
+
+void launch_perlin(const float *pos3, int n, float scale, int seed, float *out, cudaStream_t st);
+
+// -- advection ------------------------------------------------------------------
+void launch_advect(const Geom &g, const float *T, const float *U, const float *V, const float *W,
+                   float *Tn, float *Un, float *Vn, float *Wn, cudaStream_t st);
+
+} // namespace blz

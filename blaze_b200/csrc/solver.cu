@@ -1,0 +1,561 @@
+// solver.cu — the C ABI of libblaze_b200.so: solver object, step
+// orchestration and field access (reference src/FluidSolver.cu:671-955).
+//
+// Ownership follows the reference's FluidSolver: the solver owns every device
+// buffer; parameters are copied at creation.  All work is ordered on one
+// stream (library owned unless the caller sets one).  Errors are returned as
+// BLZ_ERR_* codes with a message; nothing here exits the process.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+using namespace blz;
+
+struct blz_solver {
+    blz_params P{};
+    Geom g{};
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    float *T[2]{}, *U[2]{}, *V[2]{}, *W[2]{};
+    int cur = 0;                                // front = [cur]
+    float *p_r = nullptr, *p_b = nullptr, *rhs_r = nullptr, *rhs_b = nullptr;
+    float *scratch = nullptr;                   // 6 T-sized arrays (vorticity)
+    float *acc[4]{};                            // splat accumulators, kept zero
+    float *parts = nullptr;
+    int n_parts = 0, cap_parts = 0;
+    int box[4][3][2]{};                         // per-field apply box [lo, hi)
+    double *partials = nullptr;
+    int n_partials = 0;
+    double *d_norm2 = nullptr, *h_norm2 = nullptr;
+    cudaEvent_t ev[8]{};
+    long long launches = 0;
+    std::string err;
+};
+
+static thread_local std::string g_thread_err;
+
+static int fail(blz_solver *s, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (s) s->err = buf;
+    g_thread_err = buf;
+    return code;
+}
+
+#define CK(s, x)                                                                            \
+    do {                                                                                    \
+        cudaError_t e_ = (x);                                                               \
+        if (e_ != cudaSuccess)                                                              \
+            return fail((s), BLZ_ERR_CUDA, "%s failed: %s", #x, cudaGetErrorString(e_));    \
+    } while (0)
+
+#define CKL(s)                                                                              \
+    do {                                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                                \
+        if (e_ != cudaSuccess)                                                              \
+            return fail((s), BLZ_ERR_CUDA, "kernel launch failed (%s:%d): %s", __FILE__,   \
+                        __LINE__, cudaGetErrorString(e_));                                  \
+    } while (0)
+
+static size_t n_of(const blz_params &P, int f) {
+    const size_t W = P.width, H = P.height, D = P.depth;
+    switch (f) {
+    case BLZ_FIELD_T: case BLZ_FIELD_P: case BLZ_FIELD_RHS: return W * H * D;
+    case BLZ_FIELD_U: return (W + 1) * H * D;
+    case BLZ_FIELD_V: return W * (H + 1) * D;
+    case BLZ_FIELD_W: return W * H * (D + 1);
+    default: return 0;
+    }
+}
+
+static OpenFaces open_faces(const blz_params &P) {
+    return {!P.closed_bounds[0], !P.closed_bounds[1], !P.closed_bounds[3],
+            !P.closed_bounds[2], !P.closed_bounds[4], !P.closed_bounds[5]};
+}
+
+static SolveParams solve_params(const blz_params &P) {
+    SolveParams sp{};
+    sp.scale = (P.density * P.dx * P.dx) / P.dt;          // FluidSolver.cu:530
+    sp.scale_d = (double)P.density * (double)P.dx * (double)P.dx / (double)P.dt;
+    sp.open = open_faces(P);
+    sp.dirichlet = P.bc_mode == BLZ_BC_FREE_SURFACE;
+    return sp;
+}
+
+extern "C" {
+
+int blz_default_params(blz_params *p) {
+    if (!p) return fail(nullptr, BLZ_ERR_ARG, "null params");
+    std::memset(p, 0, sizeof *p);
+    p->width = p->height = p->depth = 64;
+    p->dx = 1.0f / 64.0f;
+    p->dt = 1.0f / 24.0f;
+    p->domain_max[0] = p->domain_max[1] = p->domain_max[2] = 1.0f;
+    for (int i = 0; i < 6; ++i) p->closed_bounds[i] = 1;
+    p->density = 0.1f;
+    p->gravity = -9.8f;
+    p->wind_turb_scale = 1.0f;
+    p->turbulence_scale = 1.0f;
+    p->turb_mask_temp_ramp[0] = 1e30f; p->turb_mask_temp_ramp[1] = 2e30f;
+    p->turb_mask_vel_ramp[0] = -1.0f; p->turb_mask_vel_ramp[1] = 0.0f;
+    p->max_iter = 200;
+    p->tol = 0.0;
+    p->check_every = 10;
+    p->bc_mode = BLZ_BC_REF_COMPAT;
+    p->gs_order = BLZ_GS_RB3D;
+    p->reset_pressure = 0;
+    p->max_particles = 1 << 16;
+    return BLZ_OK;
+}
+
+const char *blz_last_error(const blz_solver *s) { return s ? s->err.c_str() : g_thread_err.c_str(); }
+
+long long blz_kernel_launches(const blz_solver *s) { return s ? s->launches : 0; }
+
+size_t blz_field_size(const blz_solver *s, int field) { return s ? n_of(s->P, field) : 0; }
+
+static void release(blz_solver *s) {
+    if (!s) return;
+    for (int b = 0; b < 2; ++b) { cudaFree(s->T[b]); cudaFree(s->U[b]); cudaFree(s->V[b]); cudaFree(s->W[b]); }
+    cudaFree(s->p_r); cudaFree(s->p_b); cudaFree(s->rhs_r); cudaFree(s->rhs_b);
+    cudaFree(s->scratch);
+    for (auto *a : s->acc) cudaFree(a);
+    cudaFree(s->parts); cudaFree(s->partials); cudaFree(s->d_norm2);
+    if (s->h_norm2) cudaFreeHost(s->h_norm2);
+    for (auto &e : s->ev) if (e) cudaEventDestroy(e);
+    if (s->own_stream && s->st) cudaStreamDestroy(s->st);
+}
+
+int blz_create(const blz_params *p, blz_solver **out) {
+    if (!p || !out) return fail(nullptr, BLZ_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (p->width < 4 || p->height < 4 || p->depth < 4)
+        return fail(nullptr, BLZ_ERR_ARG, "grid dims must be >= 4 (got %d x %d x %d)", p->width, p->height, p->depth);
+    if (p->width & 1)
+        return fail(nullptr, BLZ_ERR_ARG, "width must be even for the colour-packed solve (got %d)", p->width);
+    if ((long long)p->width * p->height * p->depth > (1LL << 31))
+        return fail(nullptr, BLZ_ERR_ARG, "grid too large for 32-bit packed indexing");
+    if (!(p->dx > 0.0f) || !(p->dt > 0.0f) || !(p->density > 0.0f))
+        return fail(nullptr, BLZ_ERR_ARG, "dx, dt and density must be positive");
+    if (p->max_iter < 0 || p->check_every < 0 || p->max_particles < 0)
+        return fail(nullptr, BLZ_ERR_ARG, "negative max_iter, check_every or max_particles");
+    if (p->bc_mode != BLZ_BC_REF_COMPAT && p->bc_mode != BLZ_BC_FREE_SURFACE)
+        return fail(nullptr, BLZ_ERR_ARG, "bad bc_mode %d", p->bc_mode);
+    if (p->gs_order != BLZ_GS_RB3D && p->gs_order != BLZ_GS_PLANE)
+        return fail(nullptr, BLZ_ERR_ARG, "bad gs_order %d", p->gs_order);
+
+    blz_solver *s = new blz_solver();
+    s->P = *p;
+    Geom &g = s->g;
+    g.W = p->width; g.H = p->height; g.D = p->depth;
+    g.dx = p->dx; g.dt = p->dt; g.inv_dx = 1.0f / p->dx;
+    for (int c = 0; c < 3; ++c) {
+        g.dmin[c] = p->domain_min[c];
+        g.dsize[c] = p->domain_max[c] - p->domain_min[c];
+    }
+    auto bail = [&](int code) { release(s); delete s; return code; };
+    cudaError_t e = cudaGetDevice(&s->device);
+    if (e != cudaSuccess) { int r = fail(s, BLZ_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e)); return bail(r); }
+    auto alloc = [&](float **ptr, size_t n) -> bool {
+        if (cudaMalloc(ptr, n * sizeof(float)) != cudaSuccess) return false;
+        return cudaMemset(*ptr, 0, n * sizeof(float)) == cudaSuccess;
+    };
+    const size_t nT = n_of(*p, 0), nU = n_of(*p, 1), nV = n_of(*p, 2), nW = n_of(*p, 3);
+    bool ok = true;
+    for (int b = 0; b < 2 && ok; ++b)
+        ok = alloc(&s->T[b], nT) && alloc(&s->U[b], nU) && alloc(&s->V[b], nV) && alloc(&s->W[b], nW);
+    ok = ok && alloc(&s->p_r, nT / 2) && alloc(&s->p_b, nT / 2) && alloc(&s->rhs_r, nT / 2) && alloc(&s->rhs_b, nT / 2);
+    ok = ok && alloc(&s->scratch, 6 * nT);
+    ok = ok && alloc(&s->acc[0], nT) && alloc(&s->acc[1], nU) && alloc(&s->acc[2], nV) && alloc(&s->acc[3], nW);
+    s->cap_parts = std::max(p->max_particles, 1);
+    ok = ok && alloc(&s->parts, 8 * (size_t)s->cap_parts);
+    s->n_partials = residual_blocks(g);
+    ok = ok && cudaMalloc(&s->partials, 2 * sizeof(double) * s->n_partials) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->d_norm2, 2 * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&s->h_norm2, 2 * sizeof(double)) == cudaSuccess;
+    if (!ok) { cudaGetLastError(); int r = fail(s, BLZ_ERR_ALLOC, "device allocation failed for %dx%dx%d", g.W, g.H, g.D); return bail(r); }
+    for (auto &ev : s->ev)
+        if (cudaEventCreate(&ev) != cudaSuccess) { int r = fail(s, BLZ_ERR_CUDA, "cudaEventCreate failed"); return bail(r); }
+    if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+        int r = fail(s, BLZ_ERR_CUDA, "cudaStreamCreate failed");
+        return bail(r);
+    }
+    s->own_stream = true;
+    if (cudaDeviceSynchronize() != cudaSuccess) { int r = fail(s, BLZ_ERR_CUDA, "initial synchronize failed"); return bail(r); }
+    *out = s;
+    return BLZ_OK;
+}
+
+int blz_destroy(blz_solver *s) {
+    if (!s) return BLZ_OK;
+    if (s->st) cudaStreamSynchronize(s->st);
+    release(s);
+    delete s;
+    return BLZ_OK;
+}
+
+int blz_set_stream(blz_solver *s, void *stream) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    CK(s, cudaStreamSynchronize(s->st));
+    if (s->own_stream) cudaStreamDestroy(s->st);
+    if (stream) { s->st = (cudaStream_t)stream; s->own_stream = false; }
+    else {
+        CK(s, cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+        s->own_stream = true;
+    }
+    return BLZ_OK;
+}
+
+// The index box a particle can touch in one field, with the splat kernel's
+// formulas (Grid.h:319-324), widened by one cell.
+static void particle_box(const blz_params &P, const float *r, int f, int out[3][2]) {
+    const float ox[4] = {0.5f, 0.0f, 0.5f, 0.5f}, oy[4] = {0.5f, 0.5f, 0.0f, 0.5f}, oz[4] = {0.5f, 0.5f, 0.5f, 0.0f};
+    const int w = P.width + (f == 1), h = P.height + (f == 2), d = P.depth + (f == 3);
+    const double rad = r[6] / 2.0, dx = P.dx;
+    const double dsy = (double)P.domain_max[1] - P.domain_min[1];
+    double lo[3] = {(r[0] - rad - P.domain_min[0]) / dx - ox[f], (dsy - (r[1] + rad - P.domain_min[1])) / dx - oy[f],
+                    (r[2] - rad - P.domain_min[2]) / dx - oz[f]};
+    double hi[3] = {(r[0] + rad - P.domain_min[0]) / dx - ox[f], (dsy - (r[1] - rad - P.domain_min[1])) / dx - oy[f],
+                    (r[2] + rad - P.domain_min[2]) / dx - oz[f]};
+    const int n[3] = {w, h, d};
+    for (int a = 0; a < 3; ++a) {
+        const double l = std::fmax(std::fmin(lo[a], 1e9), -1e9), u = std::fmax(std::fmin(hi[a], 1e9), -1e9);
+        out[a][0] = std::max((int)std::floor(l) - 1, 0);
+        out[a][1] = std::min((int)std::floor(u) + 2, n[a]);
+    }
+}
+
+int blz_set_particles(blz_solver *s, const float *rec8, int n) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    if (n < 0 || (n > 0 && !rec8)) return fail(s, BLZ_ERR_ARG, "bad particle array (n=%d)", n);
+    if (n > s->cap_parts) return fail(s, BLZ_ERR_ARG, "%d particles exceed max_particles=%d", n, s->cap_parts);
+    for (int f = 0; f < 4; ++f)
+        for (int a = 0; a < 3; ++a) { s->box[f][a][0] = 1 << 30; s->box[f][a][1] = -1; }
+    const float half_dx = s->P.dx / 2.0f;
+    for (int p = 0; p < n; ++p) {
+        const float *r = rec8 + 8 * (size_t)p;
+        for (int c = 0; c < 8; ++c)
+            if (!std::isfinite(r[c])) return fail(s, BLZ_ERR_NAN, "particle %d has a non-finite value", p);
+        if (!(r[6] > half_dx)) continue;
+        for (int f = 0; f < 4; ++f) {
+            int b[3][2];
+            particle_box(s->P, r, f, b);
+            for (int a = 0; a < 3; ++a) {
+                s->box[f][a][0] = std::min(s->box[f][a][0], b[a][0]);
+                s->box[f][a][1] = std::max(s->box[f][a][1], b[a][1]);
+            }
+        }
+    }
+    if (n > 0) CK(s, cudaMemcpyAsync(s->parts, rec8, 8 * sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, s->st));
+    CK(s, cudaStreamSynchronize(s->st));
+    s->n_parts = n;
+    return BLZ_OK;
+}
+
+int blz_add_source(blz_solver *s) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    if (s->n_parts <= 0) return BLZ_OK;
+    const int c = s->cur;
+    launch_splat(s->g, s->parts, s->n_parts, s->acc[0], s->acc[1], s->acc[2], s->acc[3], s->st);
+    CKL(s);
+    float *front[4] = {s->T[c], s->U[c], s->V[c], s->W[c]};
+    s->launches += 1;
+    for (int f = 0; f < 4; ++f) {
+        if (s->box[f][0][1] <= s->box[f][0][0]) continue;
+        launch_source_apply(s->g, s->box[f], front[f], s->acc[f], f, s->st);
+        CKL(s);
+        s->launches += 1;
+    }
+    return BLZ_OK;
+}
+
+static ForceParams force_params(const blz_solver *s, float time) {
+    const blz_params &P = s->P;
+    ForceParams fp{};
+    fp.vort_on = std::fabs(P.vorticity_conf) > 0.0f;
+    fp.buoy_on = std::fabs(P.buoyancy) > 0.0f;
+    fp.wind_on = P.wind_amp > 0.0f;
+    fp.conf = P.vorticity_conf;
+    fp.tiny = 1e-20f * (1.0f / (P.dx * P.dt));
+    fp.beta = P.buoyancy;
+    fp.grav = P.gravity;
+    fp.wind_along_x = P.wind_dir <= 1;
+    fp.wind_dir_sign = (P.wind_dir == 0 || P.wind_dir == 2) ? 1.0f : -1.0f;
+    fp.wind_amp = P.wind_amp;
+    fp.wind_turb_amp = P.wind_turb_amp;
+    fp.wind_freq = 1.0f / P.wind_turb_scale;
+    const float avg_dom = ((P.domain_max[0] - P.domain_min[0]) + (P.domain_max[1] - P.domain_min[1]) +
+                           (P.domain_max[2] - P.domain_min[2])) / 3.0f;
+    fp.wind_offset = std::fmod(time * avg_dom * P.wind_speed, 25000.0f);       // FluidSolver.cu:353-354
+    fp.turb_amp = P.turbulence_amp;
+    fp.turb_freq = 1.0f / P.turbulence_scale;
+    const float avg_grid = (float)(P.width + P.height + P.depth) / 3.0f;
+    fp.turb_offset = std::fmod(time * avg_grid, 25000.0f);                      // FluidSolver.cu:305-306
+    fp.tr0 = P.turb_mask_temp_ramp[0]; fp.tr1 = P.turb_mask_temp_ramp[1];
+    fp.vr0 = P.turb_mask_vel_ramp[0]; fp.vr1 = P.turb_mask_vel_ramp[1];
+    return fp;
+}
+
+int blz_forces(blz_solver *s, float time) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    const blz_params &P = s->P;
+    const Geom &g = s->g;
+    const int c = s->cur, b = c ^ 1;
+    float *T = s->T[c], *U = s->U[c], *V = s->V[c], *W = s->W[c];
+    const size_t nT = n_of(P, 0);
+    if (std::fabs(P.cooling_rate) > 0.0f) {                                     // FluidSolver.cu:868-872
+        launch_scale(T, nT, 1.0f - P.dt * P.cooling_rate, s->st); CKL(s); s->launches++;
+    }
+    if (P.drag > 0.0f) {                                                        // FluidSolver.cu:878-882
+        const float k = 1.0f - P.dt * P.drag;
+        launch_scale(U, n_of(P, 1), k, s->st); CKL(s);
+        launch_scale(V, n_of(P, 2), k, s->st); CKL(s);
+        launch_scale(W, n_of(P, 3), k, s->st); CKL(s);
+        s->launches += 3;
+    }
+    const ForceParams fp = force_params(s, time);
+    float *om = s->scratch, *vf = s->scratch + 3 * nT;
+    if (fp.vort_on) {
+        launch_vort_omega(g, U, V, W, om, om + nT, om + 2 * nT, s->st); CKL(s);
+        launch_vort_force(g, U, V, W, om, om + nT, om + 2 * nT, fp, vf, vf + nT, vf + 2 * nT, s->st); CKL(s);
+        s->launches += 2;
+    }
+    if (fp.vort_on || fp.buoy_on || fp.wind_on) {
+        launch_face_forces(g, U, V, W, T, vf, vf + nT, vf + 2 * nT, fp, s->st); CKL(s);
+        s->launches++;
+    }
+    if (P.turbulence_amp > 0.0f) {                                              // FluidSolver.cu:925-934
+        launch_turb_noise(g, T, U, V, W, s->U[b], s->V[b], s->W[b], fp, s->st); CKL(s);
+        launch_turb_apply(g, U, V, W, s->U[b], s->V[b], s->W[b], fp, s->st); CKL(s);
+        s->launches += 2;
+    }
+    return BLZ_OK;
+}
+
+int blz_divergence(blz_solver *s) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    const int c = s->cur;
+    launch_divergence(s->g, s->U[c], s->V[c], s->W[c], open_faces(s->P), s->rhs_r, s->rhs_b, s->st);
+    CKL(s);
+    s->launches++;
+    return BLZ_OK;
+}
+
+static int residual_sync(blz_solver *s, double *r, double *b) {
+    const SolveParams sp = solve_params(s->P);
+    s->launches += launch_residual(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->partials, s->n_partials,
+                                   s->d_norm2, s->st);
+    CKL(s);
+    CK(s, cudaMemcpyAsync(s->h_norm2, s->d_norm2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(s, cudaStreamSynchronize(s->st));
+    *r = std::sqrt(s->h_norm2[0]);
+    *b = std::sqrt(s->h_norm2[1]);
+    return BLZ_OK;
+}
+
+static int sweeps(blz_solver *s, int n) {
+    const SolveParams sp = solve_params(s->P);
+    if (s->P.gs_order == BLZ_GS_PLANE)
+        launch_plane_sweeps(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, s->st, &s->launches);
+    else
+        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, s->st, &s->launches);
+    CKL(s);
+    return BLZ_OK;
+}
+
+int blz_solve(blz_solver *s, blz_step_stats *st) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    const blz_params &P = s->P;
+    const size_t half = n_of(P, 0) / 2;
+    if (P.reset_pressure) {
+        CK(s, cudaMemsetAsync(s->p_r, 0, half * sizeof(float), s->st));
+        CK(s, cudaMemsetAsync(s->p_b, 0, half * sizeof(float), s->st));
+    }
+    int done = 0, rc, checks = 0;
+    double r = 0.0, b = 0.0;
+    bool have = false;
+    float ms_sweeps = 0.0f;
+    // Sweep batches are bracketed by events; their elapsed time is read after
+    // the residual check's synchronisation, so timing adds no stall.
+    auto timed_sweeps = [&](int n) -> int {
+        CK(s, cudaEventRecord(s->ev[6], s->st));
+        int e = sweeps(s, n);
+        if (e != BLZ_OK) return e;
+        CK(s, cudaEventRecord(s->ev[7], s->st));
+        return BLZ_OK;
+    };
+    auto add_elapsed = [&]() {
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, s->ev[6], s->ev[7]) == cudaSuccess) ms_sweeps += t;
+    };
+    if (P.tol <= 0.0) {
+        if ((rc = timed_sweeps(P.max_iter)) != BLZ_OK) return rc;
+        done = P.max_iter;
+    } else {
+        const int chunk = std::max(1, P.check_every);
+        if ((rc = residual_sync(s, &r, &b)) != BLZ_OK) return rc;
+        ++checks;
+        while (done < P.max_iter && !(b == 0.0 || r / b <= P.tol)) {
+            const int n = std::min(chunk, P.max_iter - done);
+            if ((rc = timed_sweeps(n)) != BLZ_OK) return rc;
+            done += n;
+            if ((rc = residual_sync(s, &r, &b)) != BLZ_OK) return rc;
+            ++checks;
+            add_elapsed();
+        }
+        have = true;
+    }
+    if (st) {
+        if (!have) {
+            if ((rc = residual_sync(s, &r, &b)) != BLZ_OK) return rc;
+            ++checks;
+            if (done > 0) add_elapsed();
+        }
+        st->iterations = done;
+        st->residual = r;
+        st->rhs_norm = b;
+        st->rel_residual = b > 0.0 ? r / b : 0.0;
+        st->converged = P.tol <= 0.0 || b == 0.0 || r / b <= P.tol;
+        st->ms_sweeps = ms_sweeps;
+        st->residual_checks = checks;
+        if (!std::isfinite(r)) return fail(s, BLZ_ERR_NAN, "non-finite residual after %d sweeps", done);
+    }
+    return BLZ_OK;
+}
+
+int blz_gradient(blz_solver *s) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    const int c = s->cur;
+    const float sc = s->P.dt / (s->P.density * s->P.dx);                       // FluidSolver.cu:612
+    launch_gradient(s->g, solve_params(s->P), sc, s->p_r, s->p_b, s->U[c], s->V[c], s->W[c], s->st);
+    CKL(s);
+    s->launches++;
+    return BLZ_OK;
+}
+
+int blz_project(blz_solver *s, blz_step_stats *st) {
+    int rc;
+    if ((rc = blz_divergence(s)) != BLZ_OK) return rc;
+    if ((rc = blz_solve(s, st)) != BLZ_OK) return rc;
+    return blz_gradient(s);
+}
+
+int blz_advect(blz_solver *s) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    const int c = s->cur, b = c ^ 1;
+    launch_advect(s->g, s->T[c], s->U[c], s->V[c], s->W[c], s->T[b], s->U[b], s->V[b], s->W[b], s->st);
+    CKL(s);
+    s->launches++;
+    s->cur = b;                                                                 // swap_grids_kernel
+    return BLZ_OK;
+}
+
+int blz_step(blz_solver *s, float time, blz_step_stats *st) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    int rc;
+    CK(s, cudaEventRecord(s->ev[0], s->st));
+    if ((rc = blz_forces(s, time)) != BLZ_OK) return rc;
+    CK(s, cudaEventRecord(s->ev[1], s->st));
+    if ((rc = blz_divergence(s)) != BLZ_OK) return rc;
+    CK(s, cudaEventRecord(s->ev[2], s->st));
+    if ((rc = blz_solve(s, st)) != BLZ_OK) return rc;
+    CK(s, cudaEventRecord(s->ev[3], s->st));
+    if ((rc = blz_gradient(s)) != BLZ_OK) return rc;
+    CK(s, cudaEventRecord(s->ev[4], s->st));
+    if ((rc = blz_advect(s)) != BLZ_OK) return rc;
+    CK(s, cudaEventRecord(s->ev[5], s->st));
+    if (st) {
+        CK(s, cudaEventSynchronize(s->ev[5]));
+        auto ms = [&](int a, int b) { float t = 0.f; cudaEventElapsedTime(&t, s->ev[a], s->ev[b]); return t; };
+        st->ms_source = 0.0f;
+        st->ms_forces = ms(0, 1);
+        st->ms_divergence = ms(1, 2);
+        st->ms_solve = ms(2, 3);
+        st->ms_gradient = ms(3, 4);
+        st->ms_advect = ms(4, 5);
+        st->ms_total = ms(0, 5);
+    }
+    return BLZ_OK;
+}
+
+int blz_residual(blz_solver *s, double *res, double *bn) {
+    if (!s || !res || !bn) return fail(s, BLZ_ERR_ARG, "null argument");
+    return residual_sync(s, res, bn);
+}
+
+int blz_perlin(const float *pos3, int n, float scale, int seed, float *out) {
+    if (n < 0 || (n > 0 && (!pos3 || !out))) return fail(nullptr, BLZ_ERR_ARG, "bad perlin arguments");
+    if (n == 0) return BLZ_OK;
+    float *d = nullptr;
+    CK(nullptr, cudaMalloc(&d, sizeof(float) * 4 * (size_t)n));
+    cudaError_t e = cudaMemcpy(d, pos3, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        launch_perlin(d, n, scale, seed, d + 3 * (size_t)n, nullptr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 3 * (size_t)n, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(nullptr, BLZ_ERR_CUDA, "blz_perlin: %s", cudaGetErrorString(e));
+    return BLZ_OK;
+}
+
+static float *front_of(blz_solver *s, int f) {
+    const int c = s->cur;
+    switch (f) {
+    case BLZ_FIELD_T: return s->T[c];
+    case BLZ_FIELD_U: return s->U[c];
+    case BLZ_FIELD_V: return s->V[c];
+    case BLZ_FIELD_W: return s->W[c];
+    default: return nullptr;
+    }
+}
+
+void *blz_field_ptr(blz_solver *s, int field) { return s ? (void *)front_of(s, field) : nullptr; }
+
+int blz_get_field(blz_solver *s, int f, float *dst, int on_device) {
+    if (!s || !dst) return fail(s, BLZ_ERR_ARG, "null argument");
+    const size_t n = n_of(s->P, f);
+    if (!n) return fail(s, BLZ_ERR_ARG, "bad field %d", f);
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const float *src = front_of(s, f);
+    if (f == BLZ_FIELD_P || f == BLZ_FIELD_RHS) {
+        float *tmp = s->scratch;
+        launch_unpack(s->g, f == BLZ_FIELD_P ? s->p_r : s->rhs_r, f == BLZ_FIELD_P ? s->p_b : s->rhs_b, tmp, s->st);
+        CKL(s);
+        s->launches++;
+        src = tmp;
+    }
+    CK(s, cudaMemcpyAsync(dst, src, n * sizeof(float), kind, s->st));
+    CK(s, cudaStreamSynchronize(s->st));
+    return BLZ_OK;
+}
+
+int blz_set_field(blz_solver *s, int f, const float *src, int on_device) {
+    if (!s || !src) return fail(s, BLZ_ERR_ARG, "null argument");
+    const size_t n = n_of(s->P, f);
+    if (!n) return fail(s, BLZ_ERR_ARG, "bad field %d", f);
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (f == BLZ_FIELD_P || f == BLZ_FIELD_RHS) {
+        float *tmp = s->scratch;
+        CK(s, cudaMemcpyAsync(tmp, src, n * sizeof(float), kind, s->st));
+        launch_pack(s->g, tmp, f == BLZ_FIELD_P ? s->p_r : s->rhs_r, f == BLZ_FIELD_P ? s->p_b : s->rhs_b, s->st);
+        CKL(s);
+        s->launches++;
+    } else {
+        CK(s, cudaMemcpyAsync(front_of(s, f), src, n * sizeof(float), kind, s->st));
+    }
+    CK(s, cudaStreamSynchronize(s->st));
+    return BLZ_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,223 @@
+"""Scene settings, particle records and the seeded synthetic scenes.
+
+``SceneSettings`` keeps the solver fields of the reference's POD
+(src/SceneSettings.h:32-71) under the same names; ``to_params`` maps it to the
+C ABI's ``blz_params``.  Particle records are the reference's ``.part``
+format (src/Parser.h:196-209): little-endian float32 records of 8 values,
+pos.xyz (world), vel.xyz, pscale, temperature.
+
+The synthetic scenes stand in for the reference's demo caches (which are not
+distributed with it): every particle position and attribute comes from a
+PCG32 stream (O'Neill's published permuted congruential generator) seeded by
+the caller, so the same bytes feed the CUDA path, the oracle and the
+reference build.
+"""
+from dataclasses import dataclass, field
+import math
+
+import numpy as np
+
+from . import _abi
+
+MASK64 = (1 << 64) - 1
+
+
+class PCG32:
+    """PCG-XSH-RR 64/32 (M. O'Neill, 2014)."""
+
+    MULT = 6364136223846793005
+
+    def __init__(self, seed, seq=0xDA3E39CB94B95BDB):
+        self.inc = ((seq << 1) | 1) & MASK64
+        self.state = 0
+        self.next_u32()
+        self.state = (self.state + (seed & MASK64)) & MASK64
+        self.next_u32()
+
+    def next_u32(self):
+        old = self.state
+        self.state = (old * self.MULT + self.inc) & MASK64
+        xorshifted = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
+        rot = old >> 59
+        return ((xorshifted >> rot) | (xorshifted << ((-rot) & 31))) & 0xFFFFFFFF
+
+    def uniform(self, lo=0.0, hi=1.0):
+        return lo + (hi - lo) * (self.next_u32() * (1.0 / 4294967296.0))
+
+    def integer(self, lo, hi):
+        """Uniform integer in [lo, hi]."""
+        return lo + self.next_u32() % (hi - lo + 1)
+
+
+@dataclass
+class SceneSettings:
+    """Solver subset of the reference's SceneSettings (same field names)."""
+    gridRes: tuple = (64, 64, 64)
+    dx: float = 1.0 / 64
+    dt: float = 1.0 / 24
+    domainBboxMin: tuple = (0.0, 0.0, 0.0)
+    domainBboxMax: tuple = (1.0, 1.0, 1.0)
+    closedBounds: tuple = (1, 1, 1, 1, 1, 1)     # xMin, xMax, yMin, yMax, zMin, zMax
+    maxIterSolve: int = 200
+    density: float = 0.1
+    gravity: float = -9.8
+    buoyancy: float = 0.0
+    coolingRate: float = 0.0
+    vorticityConf: float = 0.0
+    drag: float = 0.0
+    windDir: int = 0
+    windAmp: float = 0.0
+    windSpeed: float = 0.0
+    windTurbAmp: float = 0.0
+    windTurbScale: float = 1.0
+    turbulence_amp: float = 0.0
+    turbulence_scale: float = 1.0
+    turbMaskTempRamp: tuple = (1e30, 2e30)         # both masks == 1
+    turbMaskVelRamp: tuple = (-1.0, 0.0)
+    sourceMaxParticleCount: int = 1 << 16
+    # Solver controls with no reference counterpart.
+    tol: float = 0.0
+    check_every: int = 10
+    bc_mode: int = _abi.BLZ_BC_REF_COMPAT
+    gs_order: int = _abi.BLZ_GS_RB3D
+    reset_pressure: int = 0
+    temporal_block: int = 0
+    extra: dict = field(default_factory=dict)
+
+    def to_params(self):
+        p = _abi.BlzParams()
+        p.width, p.height, p.depth = (int(v) for v in self.gridRes)
+        p.dx, p.dt = self.dx, self.dt
+        p.domain_min[:] = list(self.domainBboxMin)
+        p.domain_max[:] = list(self.domainBboxMax)
+        p.closed_bounds[:] = [int(b) for b in self.closedBounds]
+        p.density, p.gravity, p.buoyancy = self.density, self.gravity, self.buoyancy
+        p.cooling_rate, p.vorticity_conf, p.drag = self.coolingRate, self.vorticityConf, self.drag
+        p.wind_dir, p.wind_amp, p.wind_speed = self.windDir, self.windAmp, self.windSpeed
+        p.wind_turb_amp, p.wind_turb_scale = self.windTurbAmp, self.windTurbScale
+        p.turbulence_amp, p.turbulence_scale = self.turbulence_amp, self.turbulence_scale
+        p.turb_mask_temp_ramp[:] = list(self.turbMaskTempRamp)
+        p.turb_mask_vel_ramp[:] = list(self.turbMaskVelRamp)
+        p.max_iter, p.tol, p.check_every = self.maxIterSolve, self.tol, self.check_every
+        p.bc_mode, p.gs_order, p.reset_pressure = self.bc_mode, self.gs_order, self.reset_pressure
+        p.max_particles, p.temporal_block = self.sourceMaxParticleCount, self.temporal_block
+        return p
+
+
+class Timer:
+    """Frame counter and simulation time (src/Timer.h:35-36)."""
+
+    def __init__(self, iter=0, time=0.0):
+        self.iter = iter
+        self.time = time
+
+
+# ---------------------------------------------------------------------------
+# .part records
+# ---------------------------------------------------------------------------
+def write_part(path, rec8):
+    np.ascontiguousarray(rec8, dtype="<f4").reshape(-1, 8).tofile(path)
+
+
+def read_part(path):
+    """Parser::sourceParticleParse: whole 32-byte records only."""
+    raw = np.fromfile(path, dtype="<f4")
+    n = raw.size // 8
+    return raw[: n * 8].reshape(n, 8).astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# Seeded synthetic scenes
+# ---------------------------------------------------------------------------
+def _cell_to_world(s, c):
+    """World position of grid-cell coordinates given with y up (world axes)."""
+    return [s.domainBboxMin[a] + c[a] * s.dx for a in range(3)]
+
+
+def sphere_particles(rng, s, centre_cells, radius_cells, count, temp=(1.0, 1.0), pscale_cells=4.0):
+    """`count` particles uniform in a ball (rejection sampling), velocity 0."""
+    cx, cy, cz = _cell_to_world(s, centre_cells)
+    r = radius_cells * s.dx
+    out = np.zeros((count, 8), np.float32)
+    n = 0
+    while n < count:
+        x, y, z = (rng.uniform(-1.0, 1.0) for _ in range(3))
+        if x * x + y * y + z * z > 1.0:
+            continue
+        out[n] = (cx + r * x, cy + r * y, cz + r * z, 0.0, 0.0, 0.0,
+                  pscale_cells * s.dx, rng.uniform(*temp))
+        n += 1
+    return out
+
+
+def disc_particles(rng, s, centre_cells, radius_cells, count, temp=(1.0, 1.0), pscale_cells=4.0,
+                   thickness_cells=2.0):
+    """`count` particles uniform in a horizontal disc (world y up)."""
+    cx, cy, cz = _cell_to_world(s, centre_cells)
+    r = radius_cells * s.dx
+    out = np.zeros((count, 8), np.float32)
+    for n in range(count):
+        a = rng.uniform(0.0, 2.0 * math.pi)
+        rr = r * math.sqrt(rng.uniform())
+        y = cy + thickness_cells * s.dx * rng.uniform()
+        out[n] = (cx + rr * math.cos(a), y, cz + rr * math.sin(a), 0.0, 0.0, 0.0,
+                  pscale_cells * s.dx, rng.uniform(*temp))
+    return out
+
+
+def plume_scene(n=64, seed=1, particles=2000):
+    """Smoke plume: n^3, dx = 1/n, dt = 1/24, one ball of radius 6 cells at
+    cells (n/2, n/8, n/2) (y up), T = 1, beta = 1, epsilon = 0.3, no noise,
+    walls except a free-surface top, 80 sweeps from p = 0."""
+    s = SceneSettings(gridRes=(n, n, n), dx=1.0 / n, dt=1.0 / 24,
+                      closedBounds=(1, 1, 1, 0, 1, 1), maxIterSolve=80, buoyancy=1.0,
+                      vorticityConf=0.3, reset_pressure=1)
+    rng = PCG32(seed)
+    parts = sphere_particles(rng, s, (n / 2, n / 8, n / 2), 6.0, particles)
+    s.sourceMaxParticleCount = max(particles, 1)
+    return s, parts
+
+
+def fire_scene(n=128, seed=2, per_disc=5000):
+    """Fire and smoke: n^3, four discs of radius 8 cells on the floor with
+    5000 particles each, T ~ U[0.5, 1.5], pseudo-curl noise amplitude 0.5 with
+    a 4-cell period, wind 0.2 cells/step along +x, epsilon = 0.5, walls except
+    the top, RBGS to relative residual 1e-4 with a cap of 400 sweeps."""
+    s = SceneSettings(gridRes=(n, n, n), dx=1.0 / n, dt=1.0 / 24,
+                      closedBounds=(1, 1, 1, 0, 1, 1), maxIterSolve=400, tol=1e-4,
+                      buoyancy=1.0, vorticityConf=0.5, turbulence_amp=0.5, turbulence_scale=4.0,
+                      windDir=0, windAmp=0.2 * (1.0 / n) / (1.0 / 24), windSpeed=0.0)
+    rng = PCG32(seed)
+    parts = []
+    for _ in range(4):
+        c = (rng.uniform(0.2 * n, 0.8 * n), 2.0, rng.uniform(0.2 * n, 0.8 * n))
+        parts.append(disc_particles(rng, s, c, 8.0, per_disc, temp=(0.5, 1.5)))
+    parts = np.concatenate(parts)
+    s.sourceMaxParticleCount = len(parts)
+    return s, parts
+
+
+def family_scene(n=256, seed=3, bc_mode=_abi.BLZ_BC_FREE_SURFACE, tol=1e-4, max_iter=4000,
+                 check_every=20):
+    """One seeded member of the plume family used for warm-start training and
+    for the 256^3 benchmark: 1-6 balls of radius 4-16 cells on the lower half
+    of the domain, wind 0-0.4 cells/step along +x, beta = 1, epsilon = 0.3,
+    walls except a free-surface top; RBGS warm-started from the previous
+    frame's pressure to relative residual `tol`."""
+    rng = PCG32(seed)
+    nsrc = rng.integer(1, 6)
+    wind = rng.uniform(0.0, 0.4)
+    s = SceneSettings(gridRes=(n, n, n), dx=1.0 / n, dt=1.0 / 24,
+                      closedBounds=(1, 1, 1, 0, 1, 1), maxIterSolve=max_iter, tol=tol,
+                      check_every=check_every, buoyancy=1.0, vorticityConf=0.3,
+                      windDir=0, windAmp=wind * (1.0 / n) / (1.0 / 24), bc_mode=bc_mode)
+    parts = []
+    for _ in range(nsrc):
+        r = rng.uniform(4.0, 16.0)
+        c = (rng.uniform(r + 2, n - r - 2), rng.uniform(r + 2, 0.5 * n), rng.uniform(r + 2, n - r - 2))
+        count = int(min(40000, max(500, round(2000 * (r / 6.0) ** 3))))
+        parts.append(sphere_particles(rng, s, c, r, count))
+    parts = np.concatenate(parts)
+    s.sourceMaxParticleCount = len(parts)
+    s.extra = {"sources": nsrc, "wind_cells_per_step": wind}
+    return s, parts

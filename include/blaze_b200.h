@@ -1,0 +1,190 @@
+/*
+ * blaze_b200.h — C ABI of the B200-native Blaze fluid step (libblaze_b200.so).
+ *
+ * Plain C: no CUDA, torch or C++ types cross this boundary; every buffer is a
+ * pointer plus sizes implied by the grid dimensions.  Each entry point returns
+ * BLZ_OK (0) or a negative BLZ_ERR_* code and never exits the process; the
+ * text of the last failure is kept per solver (blz_last_error) or per thread
+ * (blz_last_error(NULL)).
+ *
+ * Reference interface replaced (paths inside the Blaze project):
+ *   class FluidSolver            src/FluidSolver.h:38-110
+ *     FluidSolver(Timer*, SceneSettings*)   src/FluidSolver.cu:671-741  -> blz_create
+ *     ~FluidSolver()                        src/FluidSolver.cu:743-768  -> blz_destroy
+ *     addSource()                           src/FluidSolver.cu:770-821  -> blz_set_particles + blz_add_source
+ *     step()                                src/FluidSolver.cu:858-955  -> blz_step
+ *     project() (private)                   src/FluidSolver.cu:823-856  -> blz_project
+ *     getTempGrid()                         src/FluidSolver.h:108       -> blz_field_ptr(BLZ_FIELD_T)
+ *   struct SceneSettings (solver fields)    src/SceneSettings.h:32-71   -> blz_params
+ *   Timer::iter / Timer::time               src/Timer.h:35-36           -> time argument of blz_step
+ *   Parser::sourceParticleParse records     src/Parser.h:196-209        -> rec8 layout of blz_set_particles
+ *   checkCudaErrors -> exit()               src/utils/helper_cuda.h:577 -> negative return codes
+ *
+ * Grid layout (identical to the reference so fields can be exchanged as is):
+ *   FP32, x fastest: index = i + j*w + k*w*h with (w,h,d) the field's own dims.
+ *   T, p, rhs: (W, H, D)   U: (W+1, H, D)   V: (W, H+1, D)   W: (W, H, D+1).
+ *   Object space flips y (grid j = 0 is the world top, yMax).
+ */
+#ifndef BLAZE_B200_H
+#define BLAZE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BLZ_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define BLZ_OK            0
+#define BLZ_ERR_CUDA     -1   /* a CUDA runtime call failed                 */
+#define BLZ_ERR_ARG      -2   /* bad argument (dims, null pointer, field)   */
+#define BLZ_ERR_TIMEOUT  -3   /* a bounded device wait gave up              */
+#define BLZ_ERR_NAN      -4   /* non-finite value detected                  */
+#define BLZ_ERR_NOCONV   -5   /* residual target not met within max_iter    */
+#define BLZ_ERR_ALLOC    -6   /* device or host allocation failed           */
+#define BLZ_ERR_STATE    -7   /* call not valid in the current state        */
+
+/* ---- boundary-condition handling of the pressure solve ------------------ */
+/* REF_COMPAT: the reference's Neumann-everywhere solve (the stencil counts
+ *   in-domain neighbours only, FluidSolver.cu:536-561) and its boundary
+ *   velocity copy after the gradient (FluidSolver.cu:626-668).
+ * FREE_SURFACE: open faces (closed_bounds[f] == 0) carry a Dirichlet p = 0
+ *   ghost in the stencil and in the gradient, so the projected field is
+ *   discretely divergence free and the system is non-singular.             */
+#define BLZ_BC_REF_COMPAT    0
+#define BLZ_BC_FREE_SURFACE  1
+
+/* ---- Gauss-Seidel ordering ----------------------------------------------- */
+/* RB3D: colour (i+j+k)&1, all red cells then all black cells per sweep.
+ * PLANE: the reference's schedule run race free (FluidSolver.cu:517-599):
+ *   colour (i+j)&1, planes k = 0..D-1 in order, red then black per plane.  */
+#define BLZ_GS_RB3D   0
+#define BLZ_GS_PLANE  1
+
+/* ---- fields -------------------------------------------------------------- */
+#define BLZ_FIELD_T    0
+#define BLZ_FIELD_U    1
+#define BLZ_FIELD_V    2
+#define BLZ_FIELD_W    3
+#define BLZ_FIELD_P    4   /* pressure, T dims (stored colour packed inside) */
+#define BLZ_FIELD_RHS  5   /* -div/dx with the wall fixes, T dims            */
+
+/* ---- solver parameters (SceneSettings' solver subset + new switches) ---- */
+typedef struct blz_params {
+    int   width, height, depth;   /* gridRes (T dims)                        */
+    float dx, dt;
+    float domain_min[3];          /* domainBboxMin (world)                   */
+    float domain_max[3];          /* domainBboxMax (world)                   */
+    int   closed_bounds[6];       /* xMin,xMax,yMin,yMax,zMin,zMax; 1 = wall */
+
+    float density;                /* rho in the pressure scaling             */
+    float gravity;                /* negative (world down)                   */
+    float buoyancy;               /* beta (temperature)                      */
+    float cooling_rate;
+    float vorticity_conf;         /* epsilon                                 */
+    float drag;
+
+    int   wind_dir;               /* 0:+X 1:-X 2:+Z 3:-Z                     */
+    float wind_amp, wind_speed, wind_turb_amp, wind_turb_scale;
+
+    float turbulence_amp, turbulence_scale;
+    float turb_mask_temp_ramp[2];
+    float turb_mask_vel_ramp[2];
+
+    /* pressure solve controls */
+    int    max_iter;              /* maxIterSolve: sweep cap                 */
+    double tol;                   /* relative FP64 residual target; <= 0 runs
+                                     exactly max_iter sweeps (reference)     */
+    int    check_every;           /* sweeps between residual checks (>= 1)   */
+    int    bc_mode;               /* BLZ_BC_*                                */
+    int    gs_order;              /* BLZ_GS_*                                */
+    int    reset_pressure;        /* 1: p = 0 before every solve (the
+                                     reference keeps p between frames)      */
+    int    max_particles;         /* sourceMaxParticleCount                  */
+    int    temporal_block;        /* sweeps fused per HBM pass (0 = auto)    */
+} blz_params;
+
+/* ---- per-step statistics ------------------------------------------------- */
+typedef struct blz_step_stats {
+    int    iterations;            /* GS sweeps run in the last solve         */
+    int    converged;             /* 1 if tol was met (or tol <= 0)          */
+    double residual;              /* ||b - A p||_2 (FP64) after the solve    */
+    double rhs_norm;              /* ||b||_2 (FP64)                          */
+    double rel_residual;          /* residual / rhs_norm (0 when b == 0)     */
+    float  ms_source, ms_forces, ms_divergence, ms_solve, ms_gradient,
+           ms_advect, ms_total;   /* device time per stage (CUDA events)     */
+    float  ms_sweeps;             /* device time of the GS sweep launches
+                                     alone (residual checks excluded)        */
+    int    residual_checks;       /* FP64 residual evaluations in the solve  */
+} blz_step_stats;
+
+typedef struct blz_solver blz_solver;
+
+/* Fills *p with the reference's shipped-scene defaults (rho 0.1, g -9.8,
+ * closed walls, RBGS in REF_COMPAT mode, 200 sweeps, no residual target). */
+int  blz_default_params(blz_params *p);
+
+/* FluidSolver::FluidSolver (FluidSolver.cu:671-741): allocates and zeroes all
+ * fields on the current CUDA device.  dims must be >= 4; GS needs even W.   */
+int  blz_create(const blz_params *p, blz_solver **out);
+int  blz_destroy(blz_solver *s);
+
+/* Optional caller stream (a cudaStream_t passed as void*).  NULL selects the
+ * library-owned stream.  All later work of this solver is ordered on it.    */
+int  blz_set_stream(blz_solver *s, void *cuda_stream);
+
+/* Particle upload (Parser::sourceParticleParse, Parser.h:174-210): n records
+ * of 8 host floats {pos.xyz (world), vel.xyz, pscale, temperature}.         */
+int  blz_set_particles(blz_solver *s, const float *rec8, int n);
+
+/* The device half of FluidSolver::addSource (FluidSolver.cu:796-816):
+ * cubic-pulse splat of the uploaded particles, then front = splat wherever
+ * |splat| > 1e-5 on T, U, V (negated, y flip) and W.                        */
+int  blz_add_source(blz_solver *s);
+
+/* FluidSolver::step (FluidSolver.cu:858-955): forces, projection, RK3
+ * advection and buffer swap.  time = Timer::time (seconds).  stats may be
+ * NULL.                                                                     */
+int  blz_step(blz_solver *s, float time, blz_step_stats *stats);
+
+/* Stage entry points (used by the step; exposed for stage-level parity).   */
+int  blz_forces(blz_solver *s, float time);            /* cooldown..curl noise */
+int  blz_project(blz_solver *s, blz_step_stats *st);   /* div, solve, gradient */
+int  blz_divergence(blz_solver *s);
+int  blz_solve(blz_solver *s, blz_step_stats *st);
+int  blz_gradient(blz_solver *s);
+int  blz_advect(blz_solver *s);                        /* + swap               */
+
+/* FP64 ||b - A p||_2 and ||b||_2 of the current rhs and p.                  */
+int  blz_residual(blz_solver *s, double *res_norm, double *rhs_norm);
+
+/* Field access in the reference layout.  on_device != 0: dst/src is a device
+ * pointer of the field's size; otherwise host memory.                       */
+int  blz_get_field(blz_solver *s, int field, float *dst, int on_device);
+int  blz_set_field(blz_solver *s, int field, const float *src, int on_device);
+size_t blz_field_size(const blz_solver *s, int field);  /* elements, 0 if bad */
+
+/* Device pointer of a field's current front buffer (T, U, V, W).  This is the
+ * buffer the reference's getTempGrid() Grid object reads via at(i,j,k); it
+ * changes after every blz_step (front/back ping-pong).                      */
+void *blz_field_ptr(blz_solver *s, int field);
+
+/* Gradient noise of the wind and turbulence stages (the reference's
+ * cudaNoise::perlinNoise, thirdparty/cuda-noise/cuda_noise.cuh:570-615)
+ * evaluated on the current device at n host positions {x,y,z}; results go to
+ * the host array out.  Lets callers check the noise without a solver.       */
+int  blz_perlin(const float *pos3, int n, float scale, int seed, float *out);
+
+/* Number of kernels this solver launched since creation.                    */
+long long blz_kernel_launches(const blz_solver *s);
+
+/* Last error text of s (or of the calling thread when s is NULL).           */
+const char *blz_last_error(const blz_solver *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BLAZE_B200_H */

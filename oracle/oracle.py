@@ -1,0 +1,143 @@
+"""ctypes wrapper of the CPU oracle (oracle/lib/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline leg as the checker; never by the product path.
+
+All field arrays use the reference layout shaped (z, y, x); ``dtype`` is
+float64 (the FP64 oracle) or float32 (the reference's own arithmetic).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "lib", "liboracle.so")
+
+from blaze_b200 import _abi  # noqa: E402  (shares the blz_params struct)
+
+_lib = None
+
+
+def build(force=False):
+    src = os.path.join(HERE, "blaze_oracle.cpp")
+    if force or not os.path.exists(LIB) or os.path.getmtime(src) > os.path.getmtime(LIB):
+        subprocess.run(["make", "-s", "-C", HERE, "lib/liboracle.so"] + (["-B"] if force else []), check=True)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        lib = C.CDLL(LIB)
+        P = C.POINTER(_abi.BlzParams)
+        for suf, ct in (("f64", C.c_double), ("f32", C.c_float)):
+            R = C.POINTER(ct)
+            sig = {
+                "add_source": [P, C.POINTER(C.c_float), C.c_int, R, R, R, R],
+                "forces": [P, C.c_float, R, R, R, R],
+                "divergence": [P, R, R, R, R],
+                "gs_sweeps": [P, R, R, C.c_int],
+                "solve": [P, R, R, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)],
+                "residual": [P, R, R, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+                "gradient": [P, R, R, R, R],
+                "advect": [P, R, R, R, R],
+                "step": [P, C.c_float, R, R, R, R, R, R, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                         C.POINTER(C.c_double)],
+            }
+            for name, args in sig.items():
+                fn = getattr(lib, f"orc_{name}_{suf}")
+                fn.restype = None
+                fn.argtypes = args
+        lib.orc_perlin.restype = C.c_float
+        lib.orc_perlin.argtypes = [C.c_float] * 4 + [C.c_int]
+        lib.orc_num_threads.restype = C.c_int
+        _lib = lib
+    return _lib
+
+
+def _ptr(a):
+    ct = C.c_double if a.dtype == np.float64 else C.c_float
+    assert a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def _suf(dtype):
+    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+
+class State:
+    """Fields of one simulation held on the host for the oracle."""
+
+    def __init__(self, params, dtype=np.float64):
+        self.p = params
+        self.dtype = np.dtype(dtype)
+        z = lambda f: np.zeros(params.field_shape(f), self.dtype)
+        self.T, self.U, self.V, self.W = z("T"), z("U"), z("V"), z("W")
+        self.P, self.RHS = z("P"), z("RHS")
+        self.iterations, self.residual, self.rhs_norm = 0, 0.0, 0.0
+
+    def fields(self):
+        return {"T": self.T, "U": self.U, "V": self.V, "W": self.W, "P": self.P, "RHS": self.RHS}
+
+    def load(self, **arrays):
+        for k, v in arrays.items():
+            getattr(self, k)[...] = v
+
+    def _fn(self, name):
+        return getattr(load(), f"orc_{name}_{_suf(self.dtype)}")
+
+    def add_source(self, rec8):
+        a = np.ascontiguousarray(rec8, np.float32).reshape(-1, 8)
+        self._fn("add_source")(C.byref(self.p), a.ctypes.data_as(C.POINTER(C.c_float)), len(a),
+                               _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W))
+
+    def forces(self, time):
+        self._fn("forces")(C.byref(self.p), time, _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W))
+
+    def divergence(self):
+        self._fn("divergence")(C.byref(self.p), _ptr(self.U), _ptr(self.V), _ptr(self.W), _ptr(self.RHS))
+
+    def gs_sweeps(self, n):
+        self._fn("gs_sweeps")(C.byref(self.p), _ptr(self.RHS), _ptr(self.P), n)
+
+    def solve(self):
+        it, r, b = C.c_int(), C.c_double(), C.c_double()
+        self._fn("solve")(C.byref(self.p), _ptr(self.RHS), _ptr(self.P), C.byref(it), C.byref(r), C.byref(b))
+        self.iterations, self.residual, self.rhs_norm = it.value, r.value, b.value
+        return it.value, r.value, b.value
+
+    def residual_norms(self):
+        r, b = C.c_double(), C.c_double()
+        self._fn("residual")(C.byref(self.p), _ptr(self.RHS), _ptr(self.P), C.byref(r), C.byref(b))
+        return r.value, b.value
+
+    def gradient(self):
+        self._fn("gradient")(C.byref(self.p), _ptr(self.P), _ptr(self.U), _ptr(self.V), _ptr(self.W))
+
+    def advect(self):
+        self._fn("advect")(C.byref(self.p), _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W))
+
+    def project(self):
+        self.divergence()
+        out = self.solve()
+        self.gradient()
+        return out
+
+    def step(self, time):
+        it, r, b = C.c_int(), C.c_double(), C.c_double()
+        self._fn("step")(C.byref(self.p), time, _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W),
+                         _ptr(self.P), _ptr(self.RHS), C.byref(it), C.byref(r), C.byref(b))
+        self.iterations, self.residual, self.rhs_norm = it.value, r.value, b.value
+        return it.value, r.value, b.value
+
+
+def perlin(x, y, z, scale, seed):
+    return load().orc_perlin(x, y, z, scale, seed)
+
+
+def num_threads():
+    return load().orc_num_threads()

@@ -1,0 +1,243 @@
+// ref_harness.cu — drives the Blaze reference's own CUDA build.
+//
+// TEST INFRASTRUCTURE ONLY.  Built by `make -C oracle ref` into
+// oracle/_ref/libblaze_ref.so, which compiles the reference's
+// src/FluidSolver.cu where it lies (unmodified; included below) with the
+// reference's documented flags.  It serves as (a) a parity pin: the tests run
+// the reference's kernels on seeded inputs and compare the oracle with them,
+// and (b) the reference timing arm of bench.py.  Nothing in the product links
+// it.
+//
+// The harness reaches FluidSolver's private device buffers by compiling the
+// reference with `private` defined as `public` (standard and third-party
+// headers are included first, so only the reference's own classes see it).
+#include <cassert>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <streambuf>
+#include <string>
+#include <vector>
+#include <strings.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include "../thirdparty/rapidjson/document.h"
+#include "../thirdparty/rapidjson/writer.h"
+#include "../thirdparty/rapidjson/stringbuffer.h"
+
+#include "../include/blaze_b200.h"
+
+#define private public
+#include "FluidSolver.cu"
+#undef private
+
+namespace {
+
+struct RefSim {
+    SceneSettings scn;
+    Timer tmr;
+    FluidSolver *fs = nullptr;
+    std::string dir;
+    int max_particles = 0;
+};
+
+__global__ void front_ptr_kernel(Grid **g, float **out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *out = (*g)->mFrontBuffer;
+}
+
+__global__ void ref_perlin_kernel(const float *pos, int n, float scale, int seed, float *out) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) out[t] = cudaNoise::perlinNoise(make_float3(pos[3 * t], pos[3 * t + 1], pos[3 * t + 2]), scale, seed);
+}
+
+float *front_of(RefSim *r, int f) {
+    Grid **g = f == 0 ? r->fs->d_mT : f == 1 ? r->fs->d_mU : f == 2 ? r->fs->d_mV : r->fs->d_mW;
+    float **slot = nullptr;
+    cudaMalloc(&slot, sizeof(float *));
+    front_ptr_kernel<<<1, 1>>>(g, slot);
+    float *p = nullptr;
+    cudaMemcpy(&p, slot, sizeof p, cudaMemcpyDeviceToHost);
+    cudaFree(slot);
+    return p;
+}
+
+size_t n_of(const RefSim *r, int f) {
+    const size_t W = r->scn.gridRes.x, H = r->scn.gridRes.y, D = r->scn.gridRes.z;
+    switch (f) {
+    case 0: case 4: case 5: return W * H * D;
+    case 1: return (W + 1) * H * D;
+    case 2: return W * (H + 1) * D;
+    case 3: return W * H * (D + 1);
+    }
+    return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+void *ref_create(const blz_params *p) {
+    RefSim *r = new RefSim();
+    std::memset(&r->scn, 0, sizeof r->scn);
+    SceneSettings &s = r->scn;
+    char tmpl[] = "/tmp/blaze_ref_XXXXXX";
+    if (!mkdtemp(tmpl)) { delete r; return nullptr; }
+    r->dir = tmpl;
+    std::snprintf(s.sceneDir, sizeof s.sceneDir, "%s", tmpl);
+    std::snprintf(s.sceneName, sizeof s.sceneName, "harness");
+    std::snprintf(s.particleFile, sizeof s.particleFile, "src_0000.part");
+    s.sourceAnimated = true;                       // re-read the file every frame
+    s.sourceRange = make_int2(-1000000000, 1000000000);
+    s.sourceMaxParticleCount = r->max_particles = p->max_particles > 0 ? p->max_particles : 1;
+    s.domainBboxMin = make_float3(p->domain_min[0], p->domain_min[1], p->domain_min[2]);
+    s.domainBboxMax = make_float3(p->domain_max[0], p->domain_max[1], p->domain_max[2]);
+    for (int i = 0; i < 6; ++i) s.closedBounds[i] = p->closed_bounds[i] != 0;
+    s.maxIterSolve = p->max_iter;
+    s.dx = p->dx;
+    s.dt = p->dt;
+    s.gridRes = make_int3(p->width, p->height, p->depth);
+    s.density = p->density;
+    s.gravity = p->gravity;
+    s.buoyancy = p->buoyancy;
+    s.coolingRate = p->cooling_rate;
+    s.vorticityConf = p->vorticity_conf;
+    s.drag = p->drag;
+    s.windDir = p->wind_dir;
+    s.windAmp = p->wind_amp;
+    s.windSpeed = p->wind_speed;
+    s.windTurbAmp = p->wind_turb_amp;
+    s.windTurbScale = p->wind_turb_scale;
+    s.turbulence_amp = p->turbulence_amp;
+    s.turbulence_scale = p->turbulence_scale;
+    s.turbMaskTempRamp = make_float2(p->turb_mask_temp_ramp[0], p->turb_mask_temp_ramp[1]);
+    s.turbMaskVelRamp = make_float2(p->turb_mask_vel_ramp[0], p->turb_mask_vel_ramp[1]);
+    r->tmr.iter = 0;
+    r->tmr.time = 0.0f;
+    r->fs = new FluidSolver(&r->tmr, &r->scn);
+    return r;
+}
+
+void ref_destroy(void *h) {
+    RefSim *r = (RefSim *)h;
+    if (!r) return;
+    delete r->fs;
+    char path[512];
+    std::snprintf(path, sizeof path, "rm -rf '%s'", r->dir.c_str());
+    if (system(path) != 0) { /* best effort cleanup */ }
+    delete r;
+}
+
+void ref_set_time(void *h, int iter, float time) {
+    RefSim *r = (RefSim *)h;
+    r->tmr.iter = iter;
+    r->tmr.time = time;
+}
+
+// Writes the particles as the .part file the reference parses for the
+// current frame (Parser.h:181-188).
+int ref_set_particles(void *h, const float *rec8, int n) {
+    RefSim *r = (RefSim *)h;
+    if (n < 0 || n > r->max_particles) return -2;
+    char path[600];
+    std::snprintf(path, sizeof path, "%s/src_%04d.part", r->scn.sceneDir, r->tmr.iter);
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return -1;
+    const size_t w = std::fwrite(rec8, sizeof(float) * 8, (size_t)n, f);
+    std::fclose(f);
+    return w == (size_t)n ? 0 : -1;
+}
+
+int ref_add_source(void *h) { ((RefSim *)h)->fs->addSource(); return cudaGetLastError() == cudaSuccess ? 0 : -1; }
+int ref_step(void *h) { ((RefSim *)h)->fs->step(); return cudaGetLastError() == cudaSuccess ? 0 : -1; }
+int ref_project(void *h) { ((RefSim *)h)->fs->project(); return cudaGetLastError() == cudaSuccess ? 0 : -1; }
+
+// Individual stages with the launch shapes of FluidSolver::step
+// (FluidSolver.cu:858-955) and FluidSolver::project (823-856).
+int ref_stage(void *h, int stage) {
+    RefSim *r = (RefSim *)h;
+    FluidSolver *fs = r->fs;
+    const int W = fs->mWidth, H = fs->mHeight, D = fs->mDepth;
+    const dim3 block(8, 8, 8);
+    const dim3 gridT(W / block.x, H / block.y, D / block.z);
+    const dim3 gridU((W + 1) / block.x + 1, H / block.y, D / block.z);
+    const dim3 gridV(W / block.x, (H + 1) / block.y + 1, D / block.z);
+    const dim3 gridW(W / block.x, H / block.y, (D + 1) / block.z + 1);
+    const dim3 gridUVW(W + 1 / block.x + 1, (H + 1) / block.y + 1, (D + 1) / block.z + 1);
+    const dim3 gridP((W + 1) / block.x + 1, (H + 1) / block.y + 1, (D + 1) / block.z + 1);
+    switch (stage) {
+    case 0: temperature_cooldown_kernel<<<gridT, block>>>(fs->d_mT, fs->mCoolingRate, fs->mDt); break;
+    case 1: apply_drag_kernel<<<gridUVW, block>>>(fs->d_mU, fs->d_mV, fs->d_mW, fs->mDrag, fs->mDt); break;
+    case 2:
+        copy_velocity_to_back_buffer_kernel<<<gridUVW, block>>>(fs->d_mU, fs->d_mV, fs->d_mW);
+        vorticity_confinement_kernel<<<gridT, block>>>(fs->d_mT, fs->d_mU, fs->d_mV, fs->d_mW, fs->mVorticeConf, fs->mDx, fs->mDt);
+        swap_vel_grids_kernel<<<1, 1>>>(fs->d_mU, fs->d_mV, fs->d_mW);
+        break;
+    case 3: add_buoyancy_kernel<<<gridV, block>>>(fs->d_mT, fs->d_mV, fs->mBuoyancy, fs->mGravity, fs->mDt); break;
+    case 4:
+        add_wind_kernel<<<gridUVW, block>>>(fs->d_mU, fs->d_mV, fs->d_mW, r->scn.windDir, r->scn.windAmp, r->scn.windSpeed,
+                                           r->scn.windTurbAmp, r->scn.windTurbScale, fs->mDt, r->tmr.time);
+        break;
+    case 5:
+        compute_turbulence_kernel<<<gridUVW, block>>>(fs->d_mT, fs->d_mU, fs->d_mV, fs->d_mW, fs->mTurbulenceAmp,
+                                                     fs->mTurbulenceScale, fs->mTurbMaskTempRamp, fs->mTurbMaskVelRamp,
+                                                     fs->mDt, r->tmr.time);
+        add_curl_noise_kernel<<<gridT, block>>>(fs->d_mU, fs->d_mV, fs->d_mW, fs->mDx, fs->mDt);
+        break;
+    case 6:
+        compute_divergence_kernel<<<gridT, block>>>(fs->d_mRhs, fs->d_mU, fs->d_mV, fs->d_mW, W, H, D, fs->mDensity, fs->mDx);
+        break;
+    case 7:
+        gs_solve_kernel<<<dim3(W / 16, H / 16, 1), dim3(16, 16, 1)>>>(fs->d_mRhs, fs->d_mP, fs->mDensity, fs->mDx, fs->mDt,
+                                                                      W, H, D, fs->mMaxIter);
+        break;
+    case 8:
+        pressure_gradient_update_kernel<<<gridP, block>>>(fs->d_mP, fs->d_mU, fs->d_mV, fs->d_mW, W, H, D, fs->mDensity,
+                                                          fs->mDx, fs->mDt);
+        break;
+    case 9:
+        advect_RK3_kernel<<<gridT, block>>>(fs->d_mT, fs->d_mU, fs->d_mV, fs->d_mW, fs->mDt, true);
+        advect_RK3_kernel<<<gridU, block>>>(fs->d_mU, fs->d_mU, fs->d_mV, fs->d_mW, fs->mDt, false);
+        advect_RK3_kernel<<<gridV, block>>>(fs->d_mV, fs->d_mU, fs->d_mV, fs->d_mW, fs->mDt, false);
+        advect_RK3_kernel<<<gridW, block>>>(fs->d_mW, fs->d_mU, fs->d_mV, fs->d_mW, fs->mDt, false);
+        swap_grids_kernel<<<1, 1>>>(fs->d_mT, fs->d_mU, fs->d_mV, fs->d_mW);
+        break;
+    default: return -2;
+    }
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1;
+}
+
+int ref_get_field(void *h, int f, float *dst) {
+    RefSim *r = (RefSim *)h;
+    const size_t n = n_of(r, f);
+    if (!n) return -2;
+    const float *src = f == 4 ? r->fs->d_mP : f == 5 ? r->fs->d_mRhs : front_of(r, f);
+    return cudaMemcpy(dst, src, n * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : -1;
+}
+
+int ref_set_field(void *h, int f, const float *src) {
+    RefSim *r = (RefSim *)h;
+    const size_t n = n_of(r, f);
+    if (!n) return -2;
+    float *dst = f == 4 ? r->fs->d_mP : f == 5 ? r->fs->d_mRhs : front_of(r, f);
+    return cudaMemcpy(dst, src, n * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess ? 0 : -1;
+}
+
+int ref_perlin(const float *pos3, int n, float scale, int seed, float *out) {
+    if (n <= 0) return 0;
+    float *d = nullptr;
+    if (cudaMalloc(&d, sizeof(float) * 4 * (size_t)n) != cudaSuccess) return -1;
+    cudaMemcpy(d, pos3, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice);
+    ref_perlin_kernel<<<(n + 255) / 256, 256>>>(d, n, scale, seed, d + 3 * (size_t)n);
+    const cudaError_t e = cudaMemcpy(out, d + 3 * (size_t)n, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? 0 : -1;
+}
+
+} // extern "C"

@@ -1,0 +1,87 @@
+"""The C-ABI library loads and exports every symbol include/blaze_b200.h
+declares; the ctypes structs match the C layout; argument checks work without
+a GPU.  CPU only (no compute calls)."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from blaze_b200 import _abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", h) for h in sorted(os.listdir(os.path.join(ROOT, "include"))) if h.endswith(".h")]
+
+
+def declared():
+    names = set()
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        names |= set(re.findall(r"\b(blz_\w+)\s*\(", text))
+    return names
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from blaze_b200 import build
+    path = build.build()
+    return C.CDLL(path)
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared()
+    assert "blz_step" in names and "blz_create" in names
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_ctypes_table_covers_header():
+    assert declared() == set(_abi.EXPORTS)
+
+
+def test_struct_layout_matches_c(tmp_path):
+    src = tmp_path / "layout.c"
+    fields = [f for f, _ in _abi.BlzParams._fields_]
+    sfields = [f for f, _ in _abi.BlzStepStats._fields_]
+    body = "".join(f'printf("p {f} %zu\\n", offsetof(blz_params, {f}));' for f in fields)
+    body += "".join(f'printf("s {f} %zu\\n", offsetof(blz_step_stats, {f}));' for f in sfields)
+    src.write_text(f'#include <stdio.h>\n#include <stddef.h>\n#include "blaze_b200.h"\nint main(void){{'
+                   f'printf("P %zu\\nS %zu\\n", sizeof(blz_params), sizeof(blz_step_stats));{body} return 0;}}\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        parts = line.split()
+        if len(parts) == 2:
+            got[parts[0]] = int(parts[1])
+        elif len(parts) == 3:
+            got[(parts[0], parts[1])] = int(parts[2])
+    assert got["P"] == C.sizeof(_abi.BlzParams)
+    assert got["S"] == C.sizeof(_abi.BlzStepStats)
+    for f in fields:
+        assert got[("p", f)] == getattr(_abi.BlzParams, f).offset, f
+    for f in sfields:
+        assert got[("s", f)] == getattr(_abi.BlzStepStats, f).offset, f
+
+
+def test_argument_checks_need_no_gpu(lib):
+    _abi.bind(lib)
+    p = _abi.BlzParams()
+    assert lib.blz_default_params(C.byref(p)) == 0
+    assert p.density == pytest.approx(0.1) and p.max_iter == 200
+    h = C.c_void_p()
+    for bad in (dict(width=3), dict(width=15), dict(dx=0.0), dict(bc_mode=7), dict(max_iter=-1)):
+        q = p.copy()
+        for k, v in bad.items():
+            setattr(q, k, v)
+        assert lib.blz_create(C.byref(q), C.byref(h)) == _abi.BLZ_ERR_ARG
+        assert lib.blz_last_error(None)
+    assert lib.blz_create(None, C.byref(h)) == _abi.BLZ_ERR_ARG
+    assert lib.blz_set_particles(None, None, 0) == _abi.BLZ_ERR_ARG
+
+
+def test_oracle_library_loads(oracle_mod):
+    assert oracle_mod.num_threads() >= 1

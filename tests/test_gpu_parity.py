@@ -1,0 +1,240 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 oracle on seeded
+inputs, stage by stage and over whole steps.
+
+Tolerance (FP32 kernels against the FP64 restatement): relative L2 error
+<= 5e-6 and max-abs error <= 5e-5 * max(1, max|oracle|) per field for one
+stage; looser where stated (many GS sweeps, ten chaotic steps).
+"""
+import numpy as np
+import pytest
+
+from blaze_b200 import (BLZ_BC_FREE_SURFACE, BLZ_BC_REF_COMPAT, BLZ_GS_PLANE, BLZ_GS_RB3D,
+                        SceneSettings, Timer, plume_scene)
+from conftest import max_abs, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+STAGE_REL, STAGE_ABS = 5e-6, 5e-5
+
+
+def scene(dims=(24, 19, 13), **kw):
+    W, H, D = dims
+    s = SceneSettings(gridRes=dims, dx=1.0 / 20, dt=1.0 / 24, domainBboxMin=(-0.3, 0.1, 0.2),
+                      domainBboxMax=(-0.3 + W / 20, 0.1 + H / 20, 0.2 + D / 20),
+                      closedBounds=(1, 0, 1, 0, 1, 1), maxIterSolve=30)
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def random_state(p, seed):
+    rng = np.random.default_rng(seed)
+    return {
+        "T": rng.uniform(0.0, 2.0, p.field_shape("T")),
+        "U": 0.5 * rng.standard_normal(p.field_shape("U")),
+        "V": 0.5 * rng.standard_normal(p.field_shape("V")),
+        "W": 0.5 * rng.standard_normal(p.field_shape("W")),
+        "P": rng.standard_normal(p.field_shape("P")),
+        "RHS": rng.standard_normal(p.field_shape("RHS")),
+    }
+
+
+def pair(scn, seed, fields=("T", "U", "V", "W", "P", "RHS")):
+    """A GPU solver and an FP64 oracle state loaded with the same inputs."""
+    from blaze_b200 import FluidSolver
+    from oracle import oracle
+    p = scn.to_params()
+    st = random_state(p, seed)
+    gpu = FluidSolver(Timer(), scn)
+    ref = oracle.State(p, np.float64)
+    for f in fields:
+        x = st[f].astype(np.float32)
+        gpu.set(f, x)
+        getattr(ref, f)[...] = x
+    return gpu, ref
+
+
+def assert_close(gpu, ref, fields, rel=STAGE_REL, absol=STAGE_ABS):
+    for f in fields:
+        g = gpu.get(f)
+        r = getattr(ref, f)
+        scale = max(1.0, float(np.max(np.abs(r))))
+        e_rel, e_abs = rel_l2(g, r), max_abs(g, r) / scale
+        assert e_rel <= rel and e_abs <= absol, f"{f}: rel_l2 {e_rel:.3e} scaled max {e_abs:.3e}"
+
+
+def test_perlin_bit_exact():
+    """Gradient noise on the GPU equals the oracle's FP32 value bit for bit,
+    including the float-rounded lattice hash (cuda_noise.cuh:120-124)."""
+    import ctypes as C
+    from blaze_b200 import _lib
+    from oracle import oracle
+    rng = np.random.default_rng(5)
+    pos = np.concatenate([rng.uniform(-20, 300, (3000, 3)), rng.uniform(0, 25000, (1000, 3)),
+                          np.floor(rng.uniform(0, 64, (200, 3)))]).astype(np.float32)
+    for scale, seed in ((0.25, 123), (1.6, 456), (0.125, 789), (1.0, 123)):
+        out = np.empty(len(pos), np.float32)
+        lib = _lib.load()
+        _lib.check(lib.blz_perlin(pos.ctypes.data_as(C.POINTER(C.c_float)), len(pos), scale, seed,
+                                  out.ctypes.data_as(C.POINTER(C.c_float))))
+        want = np.array([oracle.perlin(*p, scale, seed) for p in pos], np.float32)
+        np.testing.assert_array_equal(out, want)
+
+
+def test_source_splat():
+    scn = scene()
+    from blaze_b200 import FluidSolver
+    from oracle import oracle
+    rng = np.random.default_rng(11)
+    p = scn.to_params()
+    n = 400
+    lo = np.array(scn.domainBboxMin) - 0.05
+    hi = np.array(scn.domainBboxMax) + 0.05
+    rec = np.zeros((n, 8), np.float32)
+    rec[:, :3] = rng.uniform(lo, hi, (n, 3))
+    rec[:, 3:6] = rng.standard_normal((n, 3)) * (rng.uniform(size=(n, 1)) < 0.7)
+    rec[:, 6] = rng.uniform(0.0, 5.0, n) * p.dx          # some below the dx/2 cut
+    rec[:, 7] = rng.uniform(-0.5, 2.0, n)
+    base = random_state(p, 12)
+    gpu = FluidSolver(Timer(), scn)
+    ref = oracle.State(p, np.float64)
+    for f in ("T", "U", "V", "W"):
+        gpu.set(f, base[f].astype(np.float32))
+        getattr(ref, f)[...] = base[f].astype(np.float32)
+    gpu.setParticles(rec)
+    gpu.addSource()
+    ref.add_source(rec)
+    # atomics reorder the float sums: 1e-5 relative is the bar here
+    assert_close(gpu, ref, ("T", "U", "V", "W"), rel=1e-5, absol=1e-4)
+    # second frame: accumulators were re-zeroed
+    gpu.addSource()
+    ref.add_source(rec)
+    assert_close(gpu, ref, ("T", "U", "V", "W"), rel=1e-5, absol=1e-4)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(vorticityConf=0.4),
+    dict(buoyancy=1.7),
+    dict(windAmp=0.3, windDir=0, windSpeed=0.7, windTurbAmp=0.5, windTurbScale=0.3),
+    dict(windAmp=0.2, windDir=3, windSpeed=0.2, windTurbAmp=0.8, windTurbScale=0.5),
+    dict(turbulence_amp=0.5, turbulence_scale=4.0),
+    dict(turbulence_amp=0.8, turbulence_scale=2.5, turbMaskTempRamp=(0.2, 1.5), turbMaskVelRamp=(0.1, 0.9)),
+    dict(coolingRate=0.35, drag=0.2),
+    dict(vorticityConf=0.5, buoyancy=1.0, windAmp=0.2, windTurbAmp=0.3, windTurbScale=0.4,
+         turbulence_amp=0.5, turbulence_scale=4.0, coolingRate=0.1),
+], ids=["vorticity", "buoyancy", "wind_x", "wind_z", "turbulence", "turbulence_ramps", "cool_drag", "all"])
+def test_forces(kw):
+    gpu, ref = pair(scene(**kw), 21)
+    gpu.forces(1.37)
+    ref.forces(1.37)
+    assert_close(gpu, ref, ("T", "U", "V", "W"))
+
+
+@pytest.mark.parametrize("bounds", [(1, 1, 1, 1, 1, 1), (1, 0, 1, 0, 1, 1), (0, 0, 0, 0, 0, 0), (0, 1, 1, 0, 0, 1)])
+def test_divergence(bounds):
+    gpu, ref = pair(scene(closedBounds=bounds), 31)
+    gpu.divergence()
+    ref.divergence()
+    assert_close(gpu, ref, ("RHS",))
+
+
+@pytest.mark.parametrize("order", [BLZ_GS_RB3D, BLZ_GS_PLANE])
+@pytest.mark.parametrize("bc", [BLZ_BC_REF_COMPAT, BLZ_BC_FREE_SURFACE])
+def test_gs_sweeps(order, bc):
+    gpu, ref = pair(scene(gs_order=order, bc_mode=bc, maxIterSolve=30), 41)
+    gpu.solve()
+    ref.gs_sweeps(30)
+    assert_close(gpu, ref, ("P",), rel=2e-5, absol=2e-4)
+
+
+def test_residual_fp64():
+    gpu, ref = pair(scene(bc_mode=BLZ_BC_FREE_SURFACE), 51)
+    r, b = gpu.residual()
+    rr, bb = ref.residual_norms()
+    assert r == pytest.approx(rr, rel=1e-6) and b == pytest.approx(bb, rel=1e-6)
+
+
+def test_solve_to_tolerance_matches_oracle_schedule():
+    scn = scene(dims=(32, 24, 20), bc_mode=BLZ_BC_FREE_SURFACE, tol=1e-4, maxIterSolve=3000, check_every=10)
+    gpu, ref = pair(scn, 61)
+    st = gpu.solve()
+    it, r, b = ref.solve()
+    assert st["converged"] and st["rel_residual"] <= 1e-4
+    assert abs(st["iterations"] - it) <= 10
+    assert_close(gpu, ref, ("P",), rel=2e-4, absol=2e-3)
+
+
+@pytest.mark.parametrize("bc", [BLZ_BC_REF_COMPAT, BLZ_BC_FREE_SURFACE])
+@pytest.mark.parametrize("bounds", [(1, 1, 1, 1, 1, 1), (1, 0, 1, 0, 1, 1), (0, 0, 0, 0, 0, 0)])
+def test_gradient(bc, bounds):
+    gpu, ref = pair(scene(closedBounds=bounds, bc_mode=bc), 71)
+    gpu.gradient()
+    ref.gradient()
+    assert_close(gpu, ref, ("U", "V", "W"))
+
+
+def test_advect():
+    gpu, ref = pair(scene(), 81)
+    gpu.advect()
+    ref.advect()
+    assert_close(gpu, ref, ("T", "U", "V", "W"))
+
+
+@pytest.mark.parametrize("bc", [BLZ_BC_REF_COMPAT, BLZ_BC_FREE_SURFACE])
+def test_full_steps_against_oracle(bc):
+    """Whole frames (sourcing + step) of a 32^3 plume with every force on,
+    after 1 and after 10 steps."""
+    from blaze_b200 import FluidSolver
+    from oracle import oracle
+    scn, parts = plume_scene(n=32, seed=9, particles=800)
+    scn.bc_mode = bc
+    scn.windAmp, scn.windTurbAmp, scn.windTurbScale, scn.windSpeed = 0.1, 0.3, 0.5, 0.3
+    scn.turbulence_amp, scn.turbulence_scale = 0.3, 4.0
+    scn.maxIterSolve = 40
+    p = scn.to_params()
+    tmr = Timer()
+    gpu = FluidSolver(tmr, scn, particles=parts)
+    ref = oracle.State(p, np.float64)
+    for n in range(10):
+        gpu.addSource()
+        gpu.step(tmr.time)
+        ref.add_source(parts)
+        ref.step(tmr.time)
+        tmr.iter += 1
+        tmr.time += scn.dt
+        if n == 0:
+            assert_close(gpu, ref, ("T", "U", "V", "W", "P"), rel=2e-5, absol=2e-4)
+    assert_close(gpu, ref, ("T", "U", "V", "W", "P"), rel=2e-3, absol=2e-2)
+
+
+def test_step_is_deterministic():
+    from blaze_b200 import FluidSolver
+    scn, parts = plume_scene(n=32, seed=3, particles=600)
+    out = []
+    for _ in range(2):
+        tmr = Timer()
+        s = FluidSolver(tmr, scn, particles=parts)
+        for _ in range(3):
+            s.addSource()
+            s.step()
+            tmr.time += scn.dt
+        out.append({f: s.get(f) for f in ("T", "U", "V", "W", "P")})
+        s.close()
+    for f in out[0]:
+        np.testing.assert_array_equal(out[0][f], out[1][f])
+
+
+def test_error_codes_on_gpu():
+    from blaze_b200 import FluidSolver, BlazeError
+    scn = scene()
+    s = FluidSolver(Timer(), scn)
+    bad = np.zeros((1, 8), np.float32)
+    bad[0, 0] = np.nan
+    with pytest.raises(BlazeError) as e:
+        s.setParticles(bad)
+    assert e.value.code == -4
+    with pytest.raises(BlazeError) as e:
+        s.setParticles(np.zeros((scn.sourceMaxParticleCount + 1, 8), np.float32))
+    assert e.value.code == -2
+    with pytest.raises(BlazeError):
+        s.set("T", np.zeros((3, 3, 3), np.float32))
