@@ -50,5 +50,31 @@ def build(force=False, verbose=False, ptxas_info=False):
     return LIB
 
 
+SHIM_SRC = os.path.join(PKG, "shim", "FluidSolver_blaze.cu")
+SHIM_LIB = os.path.join(LIBDIR, "libblaze_fluidsolver.so")
+
+
+def build_shim(ref_src, force=False, verbose=False):
+    """Builds the drop-in FluidSolver (shim/FluidSolver_blaze.cu) against the
+    reference's own headers in `ref_src` (its src/ directory), linked to
+    libblaze_b200.so.  Returns None when those headers are absent."""
+    if not os.path.exists(os.path.join(ref_src, "FluidSolver.h")):
+        return None
+    build(verbose=verbose)
+    if not force and not _stale(SHIM_LIB, [SHIM_SRC, LIB]):
+        return SHIM_LIB
+    cmd = [_nvcc(), "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"] + ARCH + [
+        "-I", ref_src, "-I", os.path.join(os.path.dirname(PKG), "include"),
+        "-diag-suppress", "177,550,3012,20012,20013,20014,20015",
+        "-Xcompiler", "-Wno-format-overflow", "-o", SHIM_LIB, SHIM_SRC,
+        "-L", LIBDIR, "-lblaze_b200", "-Xlinker", "-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc (shim) failed:\n" + res.stdout + res.stderr)
+    return SHIM_LIB
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True, ptxas_info="--ptxas" in sys.argv)

@@ -58,6 +58,22 @@ void launch_divergence(const Geom &g, const float *U, const float *V, const floa
     k_divergence<<<gr, b, 0, st>>>(g, U, V, W, o, rhs_r, rhs_b);
 }
 
+// Quotient num/den for the neighbour count den in {1..6} on the FMA pipe:
+// q0 = num*RN(1/den), then one remainder correction e = num - q0*den (exact
+// with an FMA) and q = q0 + e*RN(1/den) (Markstein's correction step).  An
+// IEEE division would put a reciprocal and an int-to-float conversion per
+// cell on the XU pipe, which bounds the sweep well below HBM speed.
+__device__ __forceinline__ float inv_count(float den) {
+    return den == 6.0f ? 1.0f / 6.0f : den == 5.0f ? 0.2f : den == 4.0f ? 0.25f
+         : den == 3.0f ? 1.0f / 3.0f : den == 2.0f ? 0.5f : 1.0f;
+}
+__device__ __forceinline__ float div_count(float num, float den) {
+    const float inv = inv_count(den);
+    const float q0 = num * inv;
+    const float e = fmaf(-q0, den, num);
+    return fmaf(e, inv, q0);
+}
+
 // One Gauss-Seidel update p = (scale*rhs + sum p_nb)/n_nb (FluidSolver.cu:
 // 532-561), summed in the reference's neighbour order.  n_nb counts the
 // in-domain neighbours, plus a p = 0 ghost per open face when dirichlet.
@@ -65,16 +81,16 @@ __device__ __forceinline__ float gs_update(const Geom &g, const SolveParams &sp,
                                            const float *__restrict__ po, size_t q, int i, int j,
                                            int k, int s, int Wh) {
     float num = sp.scale * rhs;
-    int den = 0;
+    float den = 0.0f;
     const bool dir = sp.dirichlet;
-    if (i > 0) { num += __ldg(po + q - (s ? 0 : 1)); ++den; } else if (dir && sp.open.xlo) ++den;
-    if (i < g.W - 1) { num += __ldg(po + q + (s ? 1 : 0)); ++den; } else if (dir && sp.open.xhi) ++den;
-    if (j > 0) { num += __ldg(po + q - Wh); ++den; } else if (dir && sp.open.ylo) ++den;
-    if (j < g.H - 1) { num += __ldg(po + q + Wh); ++den; } else if (dir && sp.open.yhi) ++den;
+    if (i > 0) { num += __ldg(po + q - (s ? 0 : 1)); den += 1.0f; } else if (dir && sp.open.xlo) den += 1.0f;
+    if (i < g.W - 1) { num += __ldg(po + q + (s ? 1 : 0)); den += 1.0f; } else if (dir && sp.open.xhi) den += 1.0f;
+    if (j > 0) { num += __ldg(po + q - Wh); den += 1.0f; } else if (dir && sp.open.ylo) den += 1.0f;
+    if (j < g.H - 1) { num += __ldg(po + q + Wh); den += 1.0f; } else if (dir && sp.open.yhi) den += 1.0f;
     const size_t pl = (size_t)Wh * g.H;
-    if (k > 0) { num += __ldg(po + q - pl); ++den; } else if (dir && sp.open.zlo) ++den;
-    if (k < g.D - 1) { num += __ldg(po + q + pl); ++den; } else if (dir && sp.open.zhi) ++den;
-    return num / (float)den;
+    if (k > 0) { num += __ldg(po + q - pl); den += 1.0f; } else if (dir && sp.open.zlo) den += 1.0f;
+    if (k < g.D - 1) { num += __ldg(po + q + pl); den += 1.0f; } else if (dir && sp.open.zhi) den += 1.0f;
+    return div_count(num, den);
 }
 
 // Half sweep of colour `colour` over the whole grid (3-D red-black order).
@@ -91,14 +107,93 @@ __global__ void k_rbgs_half(Geom g, SolveParams sp, const float *__restrict__ rh
     p_c[q] = gs_update(g, sp, __ldg(rhs_c + q), p_o, q, i, j, k, s, Wh);
 }
 
+// Half sweep with four consecutive packed cells per thread (W % 8 == 0):
+// 128-bit loads of the rhs row segment, of the other colour's segments in
+// rows j-1, j, j+1 and planes k-1, k+1, plus one scalar for the x neighbour
+// that falls outside the segment; 128-bit store.
+__device__ __forceinline__ float gs_den(const SolveParams &sp, bool has_xm, bool has_xp, bool has_ym,
+                                        bool has_yp, bool has_zm, bool has_zp, bool dir) {
+    float d = 0.0f;
+    d += has_xm ? 1.0f : (dir && sp.open.xlo ? 1.0f : 0.0f);
+    d += has_xp ? 1.0f : (dir && sp.open.xhi ? 1.0f : 0.0f);
+    d += has_ym ? 1.0f : (dir && sp.open.ylo ? 1.0f : 0.0f);
+    d += has_yp ? 1.0f : (dir && sp.open.yhi ? 1.0f : 0.0f);
+    d += has_zm ? 1.0f : (dir && sp.open.zlo ? 1.0f : 0.0f);
+    d += has_zp ? 1.0f : (dir && sp.open.zhi ? 1.0f : 0.0f);
+    return d;
+}
+
+__global__ void __launch_bounds__(256)
+k_rbgs_half4(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float *__restrict__ p_o,
+             float *__restrict__ p_c, int colour) {
+    const int Wh = g.W >> 1, Wq = Wh >> 2;
+    const int mq = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (mq >= Wq || j >= g.H) return;
+    const int s = (j + k + colour) & 1;               // cell m is at i = 2m + s
+    const int m0 = mq * 4;
+    const size_t q = (size_t)m0 + (size_t)Wh * ((size_t)j + (size_t)g.H * (size_t)k);
+    const size_t pl = (size_t)Wh * g.H;
+    const float4 r = __ldg(reinterpret_cast<const float4 *>(rhs_c + q));
+    const float4 o = __ldg(reinterpret_cast<const float4 *>(p_o + q));
+    const bool has_ym = j > 0, has_yp = j < g.H - 1, has_zm = k > 0, has_zp = k < g.D - 1;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 ym = has_ym ? __ldg(reinterpret_cast<const float4 *>(p_o + q - Wh)) : zero4;
+    const float4 yp = has_yp ? __ldg(reinterpret_cast<const float4 *>(p_o + q + Wh)) : zero4;
+    const float4 zm = has_zm ? __ldg(reinterpret_cast<const float4 *>(p_o + q - pl)) : zero4;
+    const float4 zp = has_zp ? __ldg(reinterpret_cast<const float4 *>(p_o + q + pl)) : zero4;
+    // x neighbours: s = 0 -> (m-1, m); s = 1 -> (m, m+1) in the other colour.
+    const bool first = m0 == 0, last = m0 + 4 == Wh;
+    float xl[4], xr[4];
+    if (s == 0) {
+        xl[0] = first ? 0.0f : __ldg(p_o + q - 1);
+        xl[1] = o.x; xl[2] = o.y; xl[3] = o.z;
+        xr[0] = o.x; xr[1] = o.y; xr[2] = o.z; xr[3] = o.w;
+    } else {
+        xl[0] = o.x; xl[1] = o.y; xl[2] = o.z; xl[3] = o.w;
+        xr[0] = o.y; xr[1] = o.z; xr[2] = o.w;
+        xr[3] = last ? 0.0f : __ldg(p_o + q + 4);
+    }
+    const bool dir = sp.dirichlet;
+    const float ra[4] = {r.x, r.y, r.z, r.w};
+    const float yma[4] = {ym.x, ym.y, ym.z, ym.w}, ypa[4] = {yp.x, yp.y, yp.z, yp.w};
+    const float zma[4] = {zm.x, zm.y, zm.z, zm.w}, zpa[4] = {zp.x, zp.y, zp.z, zp.w};
+    float out[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const bool has_xm = !(s == 0 && first && t == 0);
+        const bool has_xp = !(s == 1 && last && t == 3);
+        float num = sp.scale * ra[t];
+        if (has_xm) num += xl[t];
+        if (has_xp) num += xr[t];
+        if (has_ym) num += yma[t];
+        if (has_yp) num += ypa[t];
+        if (has_zm) num += zma[t];
+        if (has_zp) num += zpa[t];
+        out[t] = div_count(num, gs_den(sp, has_xm, has_xp, has_ym, has_yp, has_zm, has_zp, dir));
+    }
+    *reinterpret_cast<float4 *>(p_c + q) = make_float4(out[0], out[1], out[2], out[3]);
+}
+
 void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                         const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
                         long long *launches) {
-    const dim3 b(32, 8, 1);
-    const dim3 gr(((g.W >> 1) + b.x - 1) / b.x, (g.H + b.y - 1) / b.y, g.D);
-    for (int it = 0; it < sweeps; ++it) {
-        k_rbgs_half<<<gr, b, 0, st>>>(g, sp, rhs_r, p_b, p_r, 0);
-        k_rbgs_half<<<gr, b, 0, st>>>(g, sp, rhs_b, p_r, p_b, 1);
+    if ((g.W & 7) == 0) {
+        const int Wq = g.W >> 3;
+        const dim3 b(std::min(32, Wq), std::max(1, 256 / std::min(32, Wq)), 1);
+        const dim3 gr((Wq + b.x - 1) / b.x, (g.H + b.y - 1) / b.y, g.D);
+        for (int it = 0; it < sweeps; ++it) {
+            k_rbgs_half4<<<gr, b, 0, st>>>(g, sp, rhs_r, p_b, p_r, 0);
+            k_rbgs_half4<<<gr, b, 0, st>>>(g, sp, rhs_b, p_r, p_b, 1);
+        }
+    } else {
+        const dim3 b(32, 8, 1);
+        const dim3 gr(((g.W >> 1) + b.x - 1) / b.x, (g.H + b.y - 1) / b.y, g.D);
+        for (int it = 0; it < sweeps; ++it) {
+            k_rbgs_half<<<gr, b, 0, st>>>(g, sp, rhs_r, p_b, p_r, 0);
+            k_rbgs_half<<<gr, b, 0, st>>>(g, sp, rhs_b, p_r, p_b, 1);
+        }
     }
     *launches += 2LL * sweeps;
 }

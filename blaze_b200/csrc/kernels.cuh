@@ -31,10 +31,11 @@ dim3 face_block();
 dim3 face_grid(const Geom &g);
 
 // -- sourcing ---------------------------------------------------------------
-void launch_splat(const Geom &g, const float *rec8, int n, float *accT, float *accU, float *accV,
-                  float *accW, cudaStream_t st);
-void launch_source_apply(const Geom &g, const int box[3][2], float *front, float *acc, int field,
-                         cudaStream_t st);
+// Cells per bin edge of the sourcing gather (one CTA of kSplatBin^3 threads).
+constexpr int kSplatBin = 8;
+void launch_splat_gather(const Geom &g, const float *rec8, const int *boxes, const int *bin_start,
+                         const int *bin_list, const int *active, int n_active, int nbx, int nby,
+                         float *T, float *U, float *V, float *W, cudaStream_t st);
 
 // -- forces -------------------------------------------------------------------
 void launch_scale(float *a, size_t n, float s, cudaStream_t st);

@@ -27,10 +27,12 @@ struct blz_solver {
     int cur = 0;                                // front = [cur]
     float *p_r = nullptr, *p_b = nullptr, *rhs_r = nullptr, *rhs_b = nullptr;
     float *scratch = nullptr;                   // 6 T-sized arrays (vorticity)
-    float *acc[4]{};                            // splat accumulators, kept zero
+    // sourcing: compacted particle records, per-field index boxes and the
+    // 8^3-cell bins (CSR) built on the host by blz_set_particles
     float *parts = nullptr;
-    int n_parts = 0, cap_parts = 0;
-    int box[4][3][2]{};                         // per-field apply box [lo, hi)
+    int *boxes = nullptr, *bin_start = nullptr, *bin_list = nullptr, *active = nullptr;
+    int n_parts = 0, cap_parts = 0, cap_list = 0, n_active = 0;
+    int nbx = 0, nby = 0, nbz = 0;
     double *partials = nullptr;
     int n_partials = 0;
     double *d_norm2 = nullptr, *h_norm2 = nullptr;
@@ -129,8 +131,8 @@ static void release(blz_solver *s) {
     for (int b = 0; b < 2; ++b) { cudaFree(s->T[b]); cudaFree(s->U[b]); cudaFree(s->V[b]); cudaFree(s->W[b]); }
     cudaFree(s->p_r); cudaFree(s->p_b); cudaFree(s->rhs_r); cudaFree(s->rhs_b);
     cudaFree(s->scratch);
-    for (auto *a : s->acc) cudaFree(a);
-    cudaFree(s->parts); cudaFree(s->partials); cudaFree(s->d_norm2);
+    cudaFree(s->parts); cudaFree(s->boxes); cudaFree(s->bin_start); cudaFree(s->bin_list); cudaFree(s->active);
+    cudaFree(s->partials); cudaFree(s->d_norm2);
     if (s->h_norm2) cudaFreeHost(s->h_norm2);
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
     if (s->own_stream && s->st) cudaStreamDestroy(s->st);
@@ -176,9 +178,16 @@ int blz_create(const blz_params *p, blz_solver **out) {
         ok = alloc(&s->T[b], nT) && alloc(&s->U[b], nU) && alloc(&s->V[b], nV) && alloc(&s->W[b], nW);
     ok = ok && alloc(&s->p_r, nT / 2) && alloc(&s->p_b, nT / 2) && alloc(&s->rhs_r, nT / 2) && alloc(&s->rhs_b, nT / 2);
     ok = ok && alloc(&s->scratch, 6 * nT);
-    ok = ok && alloc(&s->acc[0], nT) && alloc(&s->acc[1], nU) && alloc(&s->acc[2], nV) && alloc(&s->acc[3], nW);
+    (void)nU; (void)nV; (void)nW;
     s->cap_parts = std::max(p->max_particles, 1);
+    s->nbx = (g.W + kSplatBin) / kSplatBin;          // covers face index W
+    s->nby = (g.H + kSplatBin) / kSplatBin;
+    s->nbz = (g.D + kSplatBin) / kSplatBin;
+    const size_t nbins = (size_t)s->nbx * s->nby * s->nbz;
     ok = ok && alloc(&s->parts, 8 * (size_t)s->cap_parts);
+    ok = ok && cudaMalloc(&s->boxes, sizeof(int) * 24 * (size_t)s->cap_parts) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->bin_start, sizeof(int) * (nbins + 1)) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->active, sizeof(int) * nbins) == cudaSuccess;
     s->n_partials = residual_blocks(g);
     ok = ok && cudaMalloc(&s->partials, 2 * sizeof(double) * s->n_partials) == cudaSuccess;
     ok = ok && cudaMalloc(&s->d_norm2, 2 * sizeof(double)) == cudaSuccess;
@@ -216,22 +225,26 @@ int blz_set_stream(blz_solver *s, void *stream) {
     return BLZ_OK;
 }
 
-// The index box a particle can touch in one field, with the splat kernel's
-// formulas (Grid.h:319-324), widened by one cell.
-static void particle_box(const blz_params &P, const float *r, int f, int out[3][2]) {
+// The cells of one field a particle's splat visits: the reference's box
+// (Grid.h:319-324) in the same float operations, so host and device agree.
+static inline int trunc_box(float v) { return (int)std::fmin(std::fmax(v, -1.0e9f), 1.0e9f); }
+
+static void particle_boxes(const blz_params &P, const float *r, int out[24]) {
     const float ox[4] = {0.5f, 0.0f, 0.5f, 0.5f}, oy[4] = {0.5f, 0.5f, 0.0f, 0.5f}, oz[4] = {0.5f, 0.5f, 0.5f, 0.0f};
-    const int w = P.width + (f == 1), h = P.height + (f == 2), d = P.depth + (f == 3);
-    const double rad = r[6] / 2.0, dx = P.dx;
-    const double dsy = (double)P.domain_max[1] - P.domain_min[1];
-    double lo[3] = {(r[0] - rad - P.domain_min[0]) / dx - ox[f], (dsy - (r[1] + rad - P.domain_min[1])) / dx - oy[f],
-                    (r[2] - rad - P.domain_min[2]) / dx - oz[f]};
-    double hi[3] = {(r[0] + rad - P.domain_min[0]) / dx - ox[f], (dsy - (r[1] - rad - P.domain_min[1])) / dx - oy[f],
-                    (r[2] + rad - P.domain_min[2]) / dx - oz[f]};
-    const int n[3] = {w, h, d};
-    for (int a = 0; a < 3; ++a) {
-        const double l = std::fmax(std::fmin(lo[a], 1e9), -1e9), u = std::fmax(std::fmin(hi[a], 1e9), -1e9);
-        out[a][0] = std::max((int)std::floor(l) - 1, 0);
-        out[a][1] = std::min((int)std::floor(u) + 2, n[a]);
+    const float dsy = P.domain_max[1] - P.domain_min[1];
+    const float radius = r[6] / 2.0f, dx = P.dx;
+    for (int f = 0; f < 4; ++f) {
+        int *b = out + 6 * f;
+        const float value = f == 0 ? r[7] : r[2 + f];
+        if (!(std::fabs(value) > 1e-5f)) { for (int a = 0; a < 6; ++a) b[a] = 0; continue; }
+        const int w = P.width + (f == 1), h = P.height + (f == 2), d = P.depth + (f == 3);
+        b[0] = std::max(trunc_box(((r[0] - radius) - P.domain_min[0]) / dx - ox[f]), 0);
+        b[1] = std::min(trunc_box(((r[0] + radius) - P.domain_min[0]) / dx - ox[f]) + 1, w);
+        b[2] = std::max(trunc_box((dsy - ((r[1] + radius) - P.domain_min[1])) / dx - oy[f]), 0);
+        b[3] = std::min(trunc_box((dsy - ((r[1] - radius) - P.domain_min[1])) / dx - oy[f]) + 1, h);
+        b[4] = std::max(trunc_box(((r[2] - radius) - P.domain_min[2]) / dx - oz[f]), 0);
+        b[5] = std::min(trunc_box(((r[2] + radius) - P.domain_min[2]) / dx - oz[f]) + 1, d);
+        if (b[1] <= b[0] || b[3] <= b[2] || b[5] <= b[4]) for (int a = 0; a < 6; ++a) b[a] = 0;
     }
 }
 
@@ -239,43 +252,94 @@ int blz_set_particles(blz_solver *s, const float *rec8, int n) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     if (n < 0 || (n > 0 && !rec8)) return fail(s, BLZ_ERR_ARG, "bad particle array (n=%d)", n);
     if (n > s->cap_parts) return fail(s, BLZ_ERR_ARG, "%d particles exceed max_particles=%d", n, s->cap_parts);
-    for (int f = 0; f < 4; ++f)
-        for (int a = 0; a < 3; ++a) { s->box[f][a][0] = 1 << 30; s->box[f][a][1] = -1; }
     const float half_dx = s->P.dx / 2.0f;
+    // Keep the particles whose pscale passes the reference's cut
+    // (FluidSolver.cu:83), in order, with their per-field boxes.
+    std::vector<float> keep;
+    std::vector<int> boxes;
+    keep.reserve(8 * (size_t)n);
+    boxes.reserve(24 * (size_t)n);
     for (int p = 0; p < n; ++p) {
         const float *r = rec8 + 8 * (size_t)p;
         for (int c = 0; c < 8; ++c)
             if (!std::isfinite(r[c])) return fail(s, BLZ_ERR_NAN, "particle %d has a non-finite value", p);
         if (!(r[6] > half_dx)) continue;
+        int b[24];
+        particle_boxes(s->P, r, b);
+        keep.insert(keep.end(), r, r + 8);
+        boxes.insert(boxes.end(), b, b + 24);
+    }
+    const int m = (int)(keep.size() / 8);
+    // Bin every kept particle into each 8^3 block its boxes overlap (CSR,
+    // particle order inside each bin).
+    const int nbx = s->nbx, nby = s->nby, nbz = s->nbz;
+    const size_t nbins = (size_t)nbx * nby * nbz;
+    std::vector<int> count(nbins + 1, 0);
+    auto bin_range = [&](const int *b, int lo[3], int hi[3]) {
+        lo[0] = lo[1] = lo[2] = 1 << 30; hi[0] = hi[1] = hi[2] = -1;
+        bool any = false;
         for (int f = 0; f < 4; ++f) {
-            int b[3][2];
-            particle_box(s->P, r, f, b);
+            const int *bb = b + 6 * f;
+            if (bb[1] <= bb[0]) continue;
+            any = true;
             for (int a = 0; a < 3; ++a) {
-                s->box[f][a][0] = std::min(s->box[f][a][0], b[a][0]);
-                s->box[f][a][1] = std::max(s->box[f][a][1], b[a][1]);
+                lo[a] = std::min(lo[a], bb[2 * a] / kSplatBin);
+                hi[a] = std::max(hi[a], (bb[2 * a + 1] - 1) / kSplatBin);
             }
         }
+        return any;
+    };
+    for (int p = 0; p < m; ++p) {
+        int lo[3], hi[3];
+        if (!bin_range(&boxes[24 * (size_t)p], lo, hi)) continue;
+        for (int z = lo[2]; z <= hi[2]; ++z)
+            for (int y = lo[1]; y <= hi[1]; ++y)
+                for (int x = lo[0]; x <= hi[0]; ++x) count[(size_t)x + nbx * ((size_t)y + (size_t)nby * z) + 1]++;
     }
-    if (n > 0) CK(s, cudaMemcpyAsync(s->parts, rec8, 8 * sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, s->st));
+    for (size_t b = 0; b < nbins; ++b) count[b + 1] += count[b];
+    const int total = count[nbins];
+    std::vector<int> list(std::max(total, 1)), fillpos(count.begin(), count.end() - 1), active;
+    for (int p = 0; p < m; ++p) {
+        int lo[3], hi[3];
+        if (!bin_range(&boxes[24 * (size_t)p], lo, hi)) continue;
+        for (int z = lo[2]; z <= hi[2]; ++z)
+            for (int y = lo[1]; y <= hi[1]; ++y)
+                for (int x = lo[0]; x <= hi[0]; ++x) list[fillpos[(size_t)x + nbx * ((size_t)y + (size_t)nby * z)]++] = p;
+    }
+    for (size_t b = 0; b < nbins; ++b)
+        if (count[b + 1] > count[b]) active.push_back((int)b);
+    if (total > s->cap_list) {
+        cudaFree(s->bin_list);
+        s->bin_list = nullptr;
+        s->cap_list = 0;
+        if (cudaMalloc(&s->bin_list, sizeof(int) * (size_t)total) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(s, BLZ_ERR_ALLOC, "bin list allocation failed (%d entries)", total);
+        }
+        s->cap_list = total;
+    }
+    if (m > 0) {
+        CK(s, cudaMemcpyAsync(s->parts, keep.data(), sizeof(float) * keep.size(), cudaMemcpyHostToDevice, s->st));
+        CK(s, cudaMemcpyAsync(s->boxes, boxes.data(), sizeof(int) * boxes.size(), cudaMemcpyHostToDevice, s->st));
+    }
+    CK(s, cudaMemcpyAsync(s->bin_start, count.data(), sizeof(int) * (nbins + 1), cudaMemcpyHostToDevice, s->st));
+    if (total > 0) CK(s, cudaMemcpyAsync(s->bin_list, list.data(), sizeof(int) * (size_t)total, cudaMemcpyHostToDevice, s->st));
+    if (!active.empty())
+        CK(s, cudaMemcpyAsync(s->active, active.data(), sizeof(int) * active.size(), cudaMemcpyHostToDevice, s->st));
     CK(s, cudaStreamSynchronize(s->st));
-    s->n_parts = n;
+    s->n_parts = m;
+    s->n_active = (int)active.size();
     return BLZ_OK;
 }
 
 int blz_add_source(blz_solver *s) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
-    if (s->n_parts <= 0) return BLZ_OK;
+    if (s->n_active <= 0) return BLZ_OK;
     const int c = s->cur;
-    launch_splat(s->g, s->parts, s->n_parts, s->acc[0], s->acc[1], s->acc[2], s->acc[3], s->st);
+    launch_splat_gather(s->g, s->parts, s->boxes, s->bin_start, s->bin_list, s->active, s->n_active, s->nbx,
+                        s->nby, s->T[c], s->U[c], s->V[c], s->W[c], s->st);
     CKL(s);
-    float *front[4] = {s->T[c], s->U[c], s->V[c], s->W[c]};
     s->launches += 1;
-    for (int f = 0; f < 4; ++f) {
-        if (s->box[f][0][1] <= s->box[f][0][0]) continue;
-        launch_source_apply(s->g, s->box[f], front[f], s->acc[f], f, s->st);
-        CKL(s);
-        s->launches += 1;
-    }
     return BLZ_OK;
 }
 

@@ -140,8 +140,11 @@ def test_divergence(bounds):
 
 @pytest.mark.parametrize("order", [BLZ_GS_RB3D, BLZ_GS_PLANE])
 @pytest.mark.parametrize("bc", [BLZ_BC_REF_COMPAT, BLZ_BC_FREE_SURFACE])
-def test_gs_sweeps(order, bc):
-    gpu, ref = pair(scene(gs_order=order, bc_mode=bc, maxIterSolve=30), 41)
+@pytest.mark.parametrize("dims", [(24, 19, 13), (22, 9, 11), (64, 8, 6)], ids=["w24", "w22", "w64"])
+def test_gs_sweeps(order, bc, dims):
+    """W % 8 == 0 takes the 4-cells-per-thread kernel, other even W the
+    one-cell kernel; both must equal the oracle's sweeps."""
+    gpu, ref = pair(scene(dims=dims, gs_order=order, bc_mode=bc, maxIterSolve=30), 41)
     gpu.solve()
     ref.gs_sweeps(30)
     assert_close(gpu, ref, ("P",), rel=2e-5, absol=2e-4)

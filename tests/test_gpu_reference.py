@@ -52,14 +52,24 @@ def run_ours(name):
     return out, p
 
 
-@pytest.mark.parametrize("name", list(cases.CASES))
-def test_cuda_path_matches_reference_build(name):
+@pytest.fixture(scope="module")
+def reference_outputs(tmp_path_factory):
+    """All cases run once through the reference build, in a subprocess: the
+    reference's error handling calls exit(), which must not end pytest."""
+    import subprocess
     from oracle import ref
     if not ref.available():
         pytest.skip("reference build not present")
-    sys.path.insert(0, os.path.join(HERE, "golden"))
-    import make_golden
-    want = make_golden.run_case(name)
+    out = tmp_path_factory.mktemp("refcases")
+    res = subprocess.run([sys.executable, os.path.join(HERE, "golden", "make_golden.py"), str(out)],
+                         capture_output=True, text=True, timeout=900)
+    assert res.returncode == 0, "reference build failed:\n" + res.stdout[-3000:] + res.stderr[-3000:]
+    return out
+
+
+@pytest.mark.parametrize("name", list(cases.CASES))
+def test_cuda_path_matches_reference_build(name, reference_outputs):
+    want = dict(np.load(os.path.join(str(reference_outputs), f"{name}.npz")))
     got, p = run_ours(name)
     tol_rel, tol_abs = (1e-5, 1e-4) if cases.CASES[name][1] != "step" else (1e-4, 1e-3)
     for f, g in want.items():
