@@ -39,6 +39,7 @@ class BlzParams(C.Structure):
         ("max_iter", C.c_int), ("tol", C.c_double), ("check_every", C.c_int),
         ("bc_mode", C.c_int), ("gs_order", C.c_int), ("reset_pressure", C.c_int),
         ("max_particles", C.c_int), ("temporal_block", C.c_int),
+        ("device_loop", C.c_int), ("sweep_variant", C.c_int),
     ]
 
     def dims(self):
@@ -72,6 +73,7 @@ class BlzStepStats(C.Structure):
         ("ms_source", C.c_float), ("ms_forces", C.c_float), ("ms_divergence", C.c_float),
         ("ms_solve", C.c_float), ("ms_gradient", C.c_float), ("ms_advect", C.c_float),
         ("ms_total", C.c_float), ("ms_sweeps", C.c_float), ("residual_checks", C.c_int),
+        ("sweep_variant", C.c_int), ("device_loop", C.c_int),
     ]
 
     def as_dict(self):
@@ -94,6 +96,7 @@ EXPORTS = {
     "blz_solve": (C.c_int, [C.c_void_p, _P(BlzStepStats)]),
     "blz_gradient": (C.c_int, [C.c_void_p]),
     "blz_advect": (C.c_int, [C.c_void_p]),
+    "blz_sweeps": (C.c_int, [C.c_void_p, C.c_int]),
     "blz_residual": (C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double)]),
     "blz_get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "blz_set_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),

@@ -116,10 +116,12 @@ __device__ __forceinline__ uint32_t lattice_hash(uint32_t s) {
     return s;
 }
 
+// The reference build forms the lattice sum as fma(z, 149812, fma(x, 1723,
+// y*93241)) + 3824 + seed; past 2^24 the fused roundings pick different
+// lattice gradients, so the same sequence is written out explicitly here.
 __device__ __forceinline__ uint32_t lattice_seed(float x, float y, float z, float seed) {
-    float acc = __fmul_rn(x, 1723.0f);
-    acc = __fadd_rn(acc, __fmul_rn(y, 93241.0f));
-    acc = __fadd_rn(acc, __fmul_rn(z, 149812.0f));
+    float acc = __fmaf_rn(x, 1723.0f, __fmul_rn(y, 93241.0f));
+    acc = __fmaf_rn(z, 149812.0f, acc);
     acc = __fadd_rn(acc, 3824.0f);
     acc = __fadd_rn(acc, seed);
     return lattice_hash(__float2uint_rz(acc));

@@ -234,10 +234,15 @@ __device__ __forceinline__ float3 pseudo_curl(const Geom &g, const float *__rest
     const float u0 = __ldg(nU + lin(i, j, k, g.W + 1, g.H)), u1 = __ldg(nU + lin(i + 1, j, k, g.W + 1, g.H));
     const float v0 = __ldg(nV + lin(i, j, k, g.W, g.H + 1)), v1 = __ldg(nV + lin(i, j + 1, k, g.W, g.H + 1));
     const float w0 = __ldg(nW + lin(i, j, k, g.W, g.H)), w1 = __ldg(nW + lin(i, j, k + 1, g.W, g.H));
-    const float dudx = (u1 - v0) * g.inv_dx;
-    const float dvdy = (v1 - v0) * g.inv_dx;
-    const float dwdz = (w1 - v0) * g.inv_dx;
-    float cx = dvdy - dwdz, cy = dwdz - dudx, cz = dudx - dvdy;
+    // Explicit roundings: where the differences are equal (e.g. masked-out
+    // noise on three faces) the curl must be exactly zero.  A contracted
+    // fma(a, s, -b*s) leaves a rounding residue instead, which the
+    // normalisation below inflates to the full noise speed in an arbitrary
+    // direction.
+    const float dudx = __fmul_rn(__fsub_rn(u1, v0), g.inv_dx);
+    const float dvdy = __fmul_rn(__fsub_rn(v1, v0), g.inv_dx);
+    const float dwdz = __fmul_rn(__fsub_rn(w1, v0), g.inv_dx);
+    float cx = __fsub_rn(dvdy, dwdz), cy = __fsub_rn(dwdz, dudx), cz = __fsub_rn(dudx, dvdy);
     const float avg = len3((u0 + u1) / 2.0f, (v0 + v1) / 2.0f, (w0 + w1) / 2.0f);
     const float den = len3(cx, cy, cz) + tiny;
     const float h = 0.5f * g.dt;

@@ -123,37 +123,22 @@ __device__ __forceinline__ float gs_den(const SolveParams &sp, bool has_xm, bool
     return d;
 }
 
-__global__ void __launch_bounds__(256)
-k_rbgs_half4(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float *__restrict__ p_o,
-             float *__restrict__ p_c, int colour) {
-    const int Wh = g.W >> 1, Wq = Wh >> 2;
-    const int mq = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
-    if (mq >= Wq || j >= g.H) return;
-    const int s = (j + k + colour) & 1;               // cell m is at i = 2m + s
-    const int m0 = mq * 4;
-    const size_t q = (size_t)m0 + (size_t)Wh * ((size_t)j + (size_t)g.H * (size_t)k);
-    const size_t pl = (size_t)Wh * g.H;
-    const float4 r = __ldg(reinterpret_cast<const float4 *>(rhs_c + q));
-    const float4 o = __ldg(reinterpret_cast<const float4 *>(p_o + q));
-    const bool has_ym = j > 0, has_yp = j < g.H - 1, has_zm = k > 0, has_zp = k < g.D - 1;
-    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 ym = has_ym ? __ldg(reinterpret_cast<const float4 *>(p_o + q - Wh)) : zero4;
-    const float4 yp = has_yp ? __ldg(reinterpret_cast<const float4 *>(p_o + q + Wh)) : zero4;
-    const float4 zm = has_zm ? __ldg(reinterpret_cast<const float4 *>(p_o + q - pl)) : zero4;
-    const float4 zp = has_zp ? __ldg(reinterpret_cast<const float4 *>(p_o + q + pl)) : zero4;
-    // x neighbours: s = 0 -> (m-1, m); s = 1 -> (m, m+1) in the other colour.
-    const bool first = m0 == 0, last = m0 + 4 == Wh;
+__device__ __forceinline__ float4 ld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+
+// Updates four consecutive packed cells m0..m0+3 of one row: o is the other
+// colour at the same packed indices, xe its value just outside the segment
+// (m0-1 when the row's cells sit at even i, m0+4 when odd), ym/yp/zm/zp the
+// other colour in rows j-1, j+1 and planes k-1, k+1.
+__device__ __forceinline__ float4 gs_segment(const SolveParams &sp, int s, bool first, bool last, float4 r,
+                                             float4 o, float xe, float4 ym, float4 yp, float4 zm, float4 zp,
+                                             bool has_ym, bool has_yp, bool has_zm, bool has_zp) {
     float xl[4], xr[4];
     if (s == 0) {
-        xl[0] = first ? 0.0f : __ldg(p_o + q - 1);
-        xl[1] = o.x; xl[2] = o.y; xl[3] = o.z;
+        xl[0] = xe; xl[1] = o.x; xl[2] = o.y; xl[3] = o.z;
         xr[0] = o.x; xr[1] = o.y; xr[2] = o.z; xr[3] = o.w;
     } else {
         xl[0] = o.x; xl[1] = o.y; xl[2] = o.z; xl[3] = o.w;
-        xr[0] = o.y; xr[1] = o.z; xr[2] = o.w;
-        xr[3] = last ? 0.0f : __ldg(p_o + q + 4);
+        xr[0] = o.y; xr[1] = o.z; xr[2] = o.w; xr[3] = xe;
     }
     const bool dir = sp.dirichlet;
     const float ra[4] = {r.x, r.y, r.z, r.w};
@@ -173,19 +158,77 @@ k_rbgs_half4(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const floa
         if (has_zp) num += zpa[t];
         out[t] = div_count(num, gs_den(sp, has_xm, has_xp, has_ym, has_yp, has_zm, has_zp, dir));
     }
-    *reinterpret_cast<float4 *>(p_c + q) = make_float4(out[0], out[1], out[2], out[3]);
+    return make_float4(out[0], out[1], out[2], out[3]);
 }
+
+// Half sweep, four packed cells per thread along x (W % 8 == 0), KZ
+// consecutive planes per thread: the thread marches in z carrying the other
+// colour's segments of planes k-1 and k in registers, so each plane adds one
+// 128-bit load of plane k+1 instead of two.  Every variant performs the same
+// operations per cell, so all give bitwise identical results.
+template <int KZ>
+__global__ void __launch_bounds__(256)
+k_rbgs_seg(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float *__restrict__ p_o,
+           float *__restrict__ p_c, int colour) {
+    const int Wh = g.W >> 1, Wq = Wh >> 2;
+    const int mq = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k0 = blockIdx.z * KZ;
+    if (mq >= Wq || j >= g.H || k0 >= g.D) return;
+    const int m0 = mq * 4;
+    const size_t pl = (size_t)Wh * g.H;
+    const size_t row = (size_t)m0 + (size_t)Wh * (size_t)j;
+    const bool has_ym = j > 0, has_yp = j < g.H - 1;
+    const bool first = m0 == 0, last = m0 + 4 == Wh;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 zm = k0 > 0 ? ld4(p_o + row + (size_t)(k0 - 1) * pl) : zero4;
+    float4 cur = ld4(p_o + row + (size_t)k0 * pl);
+#pragma unroll
+    for (int kk = 0; kk < KZ; ++kk) {
+        const int k = k0 + kk;
+        if (k >= g.D) break;
+        const size_t q = row + (size_t)k * pl;
+        const bool has_zm = k > 0, has_zp = k < g.D - 1;
+        const float4 zp = has_zp ? ld4(p_o + q + pl) : zero4;
+        const float4 r = ld4(rhs_c + q);
+        const float4 ym = has_ym ? ld4(p_o + q - Wh) : zero4;
+        const float4 yp = has_yp ? ld4(p_o + q + Wh) : zero4;
+        const int s = (j + k + colour) & 1;
+        const float xe = s == 0 ? (first ? 0.0f : __ldg(p_o + q - 1)) : (last ? 0.0f : __ldg(p_o + q + 4));
+        *reinterpret_cast<float4 *>(p_c + q) =
+            gs_segment(sp, s, first, last, r, cur, xe, ym, yp, zm, zp, has_ym, has_yp, has_zm, has_zp);
+        zm = cur;
+        cur = zp;
+    }
+}
+
+// (planes per thread, rows per block) of each segment-kernel variant.
+static const int kVariantKZ[kSweepVariants] = {1, 2, 4, 8, 2, 4};
+static const int kVariantBY[kSweepVariants] = {8, 8, 4, 4, 4, 8};
+
+int sweep_variant_count(const Geom &g) { return (g.W & 7) == 0 ? kSweepVariants : 0; }
 
 void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                         const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
-                        long long *launches) {
+                        long long *launches, int variant) {
     if ((g.W & 7) == 0) {
-        const int Wq = g.W >> 3;
-        const dim3 b(std::min(32, Wq), std::max(1, 256 / std::min(32, Wq)), 1);
-        const dim3 gr((Wq + b.x - 1) / b.x, (g.H + b.y - 1) / b.y, g.D);
+        const int v = (variant >= 0 && variant < kSweepVariants) ? variant : 0;
+        const int Wq = g.W >> 3, kz = kVariantKZ[v], by = kVariantBY[v];
+        const int bx = std::min(32, Wq);
+        const dim3 b(bx, std::max(1, std::min(by * (32 / bx), 256 / bx)), 1);
+        const dim3 gr((Wq + b.x - 1) / b.x, (g.H + b.y - 1) / b.y, (g.D + kz - 1) / kz);
         for (int it = 0; it < sweeps; ++it) {
-            k_rbgs_half4<<<gr, b, 0, st>>>(g, sp, rhs_r, p_b, p_r, 0);
-            k_rbgs_half4<<<gr, b, 0, st>>>(g, sp, rhs_b, p_r, p_b, 1);
+            for (int c = 0; c < 2; ++c) {
+                const float *rc = c ? rhs_b : rhs_r;
+                const float *po = c ? p_r : p_b;
+                float *pc = c ? p_b : p_r;
+                switch (kz) {
+                case 1: k_rbgs_seg<1><<<gr, b, 0, st>>>(g, sp, rc, po, pc, c); break;
+                case 2: k_rbgs_seg<2><<<gr, b, 0, st>>>(g, sp, rc, po, pc, c); break;
+                case 4: k_rbgs_seg<4><<<gr, b, 0, st>>>(g, sp, rc, po, pc, c); break;
+                default: k_rbgs_seg<8><<<gr, b, 0, st>>>(g, sp, rc, po, pc, c); break;
+                }
+            }
         }
     } else {
         const dim3 b(32, 8, 1);
@@ -232,14 +275,17 @@ void launch_plane_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_
 
 // ---------------------------------------------------------------------------
 // FP64 residual ||b - A p||_2 and ||b||_2, b = scale*rhs.  Grid-stride over
-// packed pairs with a fixed launch shape, warp-shuffle then shared-memory
+// row segments with a fixed launch shape, warp-shuffle then shared-memory
 // reduction per block, then one block sums the per-block partials in order:
-// the result is bit-reproducible.
+// the result is bit-reproducible.  Per cell, A p is formed in deviation form
+// sum_nb (p_c - p_nb) (+ p_c per Dirichlet ghost): differences of a smooth
+// pressure are exact in FP32, so the stencil loses nothing to the magnitude
+// of p; b and r are then FP64 and the squares accumulate in FP64.
 // ---------------------------------------------------------------------------
 constexpr int kResThreads = 256;
 
 int residual_blocks(const Geom &g) {
-    const long long items = (long long)(g.W >> 1) * g.H * g.D;
+    const long long items = (long long)(g.W >> 1) * g.H * g.D / ((g.W & 7) == 0 ? 4 : 1);
     return (int)std::min<long long>((items + kResThreads - 1) / kResThreads, 148 * 8);
 }
 
@@ -249,35 +295,123 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+__device__ __forceinline__ float ghost_terms(const SolveParams &sp, bool has_xm, bool has_xp, bool has_ym,
+                                             bool has_yp, bool has_zm, bool has_zp) {
+    if (!sp.dirichlet) return 0.0f;
+    const OpenFaces &o = sp.open;
+    return (float)((!has_xm && o.xlo) + (!has_xp && o.xhi) + (!has_ym && o.ylo) + (!has_yp && o.yhi) +
+                   (!has_zm && o.zlo) + (!has_zp && o.zhi));
+}
+
+// Residual contributions of four packed cells of one colour (layout as in
+// gs_segment; own = this colour's values).
+__device__ __forceinline__ void residual_segment(const SolveParams &sp, double scale, int s, bool first,
+                                                 bool last, float4 rhs, float4 own, float4 o, float xe,
+                                                 float4 ym, float4 yp, float4 zm, float4 zp, bool has_ym,
+                                                 bool has_yp, bool has_zm, bool has_zp, double &r2,
+                                                 double &b2) {
+    float xl[4], xr[4];
+    if (s == 0) {
+        xl[0] = xe; xl[1] = o.x; xl[2] = o.y; xl[3] = o.z;
+        xr[0] = o.x; xr[1] = o.y; xr[2] = o.z; xr[3] = o.w;
+    } else {
+        xl[0] = o.x; xl[1] = o.y; xl[2] = o.z; xl[3] = o.w;
+        xr[0] = o.y; xr[1] = o.z; xr[2] = o.w; xr[3] = xe;
+    }
+    const float ra[4] = {rhs.x, rhs.y, rhs.z, rhs.w}, pa[4] = {own.x, own.y, own.z, own.w};
+    const float yma[4] = {ym.x, ym.y, ym.z, ym.w}, ypa[4] = {yp.x, yp.y, yp.z, yp.w};
+    const float zma[4] = {zm.x, zm.y, zm.z, zm.w}, zpa[4] = {zp.x, zp.y, zp.z, zp.w};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const bool has_xm = !(s == 0 && first && t == 0);
+        const bool has_xp = !(s == 1 && last && t == 3);
+        const float pc = pa[t];
+        float d = ghost_terms(sp, has_xm, has_xp, has_ym, has_yp, has_zm, has_zp) * pc;
+        if (has_xm) d += pc - xl[t];
+        if (has_xp) d += pc - xr[t];
+        if (has_ym) d += pc - yma[t];
+        if (has_yp) d += pc - ypa[t];
+        if (has_zm) d += pc - zma[t];
+        if (has_zp) d += pc - zpa[t];
+        const double b = scale * (double)ra[t];
+        const double r = b - (double)d;
+        r2 += r * r;
+        b2 += b * b;
+    }
+}
+
+__global__ void __launch_bounds__(kResThreads)
+k_residual_seg(Geom g, SolveParams sp, double scale, const float *__restrict__ rr,
+               const float *__restrict__ rb, const float *__restrict__ pr, const float *__restrict__ pb,
+               double *__restrict__ partials) {
+    const int Wh = g.W >> 1, Wq = Wh >> 2;
+    const int items = Wq * g.H * g.D;
+    const int pl = Wh * g.H;
+    double r2 = 0.0, b2 = 0.0;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < items; t += gridDim.x * blockDim.x) {
+        const int mq = t % Wq, jk = t / Wq;
+        const int j = jk % g.H, k = jk / g.H;
+        const int m0 = 4 * mq;
+        const int q = m0 + Wh * j + pl * k;
+        const bool has_ym = j > 0, has_yp = j < g.H - 1, has_zm = k > 0, has_zp = k < g.D - 1;
+        const bool first = m0 == 0, last = m0 + 4 == Wh;
+        const float4 pr4 = ld4(pr + q), pb4 = ld4(pb + q);
+        const int sr = (j + k) & 1, sb = sr ^ 1;        // red / black row offsets
+        // red cells: the other colour is black
+        residual_segment(sp, scale, sr, first, last, ld4(rr + q), pr4, pb4,
+                         sr == 0 ? (first ? 0.f : __ldg(pb + q - 1)) : (last ? 0.f : __ldg(pb + q + 4)),
+                         has_ym ? ld4(pb + q - Wh) : zero4, has_yp ? ld4(pb + q + Wh) : zero4,
+                         has_zm ? ld4(pb + q - pl) : zero4, has_zp ? ld4(pb + q + pl) : zero4,
+                         has_ym, has_yp, has_zm, has_zp, r2, b2);
+        residual_segment(sp, scale, sb, first, last, ld4(rb + q), pb4, pr4,
+                         sb == 0 ? (first ? 0.f : __ldg(pr + q - 1)) : (last ? 0.f : __ldg(pr + q + 4)),
+                         has_ym ? ld4(pr + q - Wh) : zero4, has_yp ? ld4(pr + q + Wh) : zero4,
+                         has_zm ? ld4(pr + q - pl) : zero4, has_zp ? ld4(pr + q + pl) : zero4,
+                         has_ym, has_yp, has_zm, has_zp, r2, b2);
+    }
+    __shared__ double s_r[kResThreads / 32], s_b[kResThreads / 32];
+    r2 = warp_sum(r2);
+    b2 = warp_sum(b2);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { s_r[wid] = r2; s_b[wid] = b2; }
+    __syncthreads();
+    if (wid == 0) {
+        r2 = lane < kResThreads / 32 ? s_r[lane] : 0.0;
+        b2 = lane < kResThreads / 32 ? s_b[lane] : 0.0;
+        r2 = warp_sum(r2);
+        b2 = warp_sum(b2);
+        if (lane == 0) { partials[2 * blockIdx.x] = r2; partials[2 * blockIdx.x + 1] = b2; }
+    }
+}
+
+// One packed pair per item (any even W).
 __global__ void __launch_bounds__(kResThreads)
 k_residual(Geom g, SolveParams sp, double scale, const float *__restrict__ rr,
            const float *__restrict__ rb, const float *__restrict__ pr, const float *__restrict__ pb,
            double *__restrict__ partials) {
     const int Wh = g.W >> 1;
-    const long long items = (long long)Wh * g.H * g.D;
+    const int items = Wh * g.H * g.D;
     double r2 = 0.0, b2 = 0.0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < items;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int m = (int)(t % Wh);
-        const long long jk = t / Wh;
-        const int j = (int)(jk % g.H), k = (int)(jk / g.H);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < items; t += gridDim.x * blockDim.x) {
+        const int m = t % Wh, jk = t / Wh;
+        const int j = jk % g.H, k = jk / g.H;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int i = 2 * m + h;
             const bool black = (i + j + k) & 1;
-            const size_t q = (size_t)t;
-            const double b = scale * (double)__ldg((black ? rb : rr) + q);
-            double nb = 0.0, n = 0.0;
-            const OpenFaces &o = sp.open;
-            const bool dir = sp.dirichlet;
-            if (i > 0) { nb += pval(pr, pb, i - 1, j, k, Wh, g.H); n += 1.0; } else if (dir && o.xlo) n += 1.0;
-            if (i < g.W - 1) { nb += pval(pr, pb, i + 1, j, k, Wh, g.H); n += 1.0; } else if (dir && o.xhi) n += 1.0;
-            if (j > 0) { nb += pval(pr, pb, i, j - 1, k, Wh, g.H); n += 1.0; } else if (dir && o.ylo) n += 1.0;
-            if (j < g.H - 1) { nb += pval(pr, pb, i, j + 1, k, Wh, g.H); n += 1.0; } else if (dir && o.yhi) n += 1.0;
-            if (k > 0) { nb += pval(pr, pb, i, j, k - 1, Wh, g.H); n += 1.0; } else if (dir && o.zlo) n += 1.0;
-            if (k < g.D - 1) { nb += pval(pr, pb, i, j, k + 1, Wh, g.H); n += 1.0; } else if (dir && o.zhi) n += 1.0;
-            const double p = (double)__ldg((black ? pb : pr) + q);
-            const double r = b - (n * p - nb);
+            const double b = scale * (double)__ldg((black ? rb : rr) + t);
+            const float pc = __ldg((black ? pb : pr) + t);
+            const bool has_xm = i > 0, has_xp = i < g.W - 1, has_ym = j > 0, has_yp = j < g.H - 1;
+            const bool has_zm = k > 0, has_zp = k < g.D - 1;
+            float d = ghost_terms(sp, has_xm, has_xp, has_ym, has_yp, has_zm, has_zp) * pc;
+            if (has_xm) d += pc - pval(pr, pb, i - 1, j, k, Wh, g.H);
+            if (has_xp) d += pc - pval(pr, pb, i + 1, j, k, Wh, g.H);
+            if (has_ym) d += pc - pval(pr, pb, i, j - 1, k, Wh, g.H);
+            if (has_yp) d += pc - pval(pr, pb, i, j + 1, k, Wh, g.H);
+            if (has_zm) d += pc - pval(pr, pb, i, j, k - 1, Wh, g.H);
+            if (has_zp) d += pc - pval(pr, pb, i, j, k + 1, Wh, g.H);
+            const double r = b - (double)d;
             r2 += r * r;
             b2 += b * b;
         }
@@ -322,7 +456,10 @@ int launch_residual(const Geom &g, const SolveParams &sp, const float *rhs_r, co
                     double *out2, cudaStream_t st) {
     const int blocks = std::min(residual_blocks(g), max_partials);
     const double scale = (double)sp.scale_d;
-    k_residual<<<blocks, kResThreads, 0, st>>>(g, sp, scale, rhs_r, rhs_b, p_r, p_b, partials);
+    if ((g.W & 7) == 0)
+        k_residual_seg<<<blocks, kResThreads, 0, st>>>(g, sp, scale, rhs_r, rhs_b, p_r, p_b, partials);
+    else
+        k_residual<<<blocks, kResThreads, 0, st>>>(g, sp, scale, rhs_r, rhs_b, p_r, p_b, partials);
     k_reduce_pairs<<<1, 1024, 0, st>>>(partials, blocks, out2);
     return 2;
 }

@@ -56,9 +56,15 @@ void launch_turb_apply(const Geom &g, float *U, float *V, float *W, const float 
 // -- projection ---------------------------------------------------------------
 void launch_divergence(const Geom &g, const float *U, const float *V, const float *W,
                        const OpenFaces &o, float *rhs_r, float *rhs_b, cudaStream_t st);
+// Red-black sweeps.  For W % 8 == 0, `variant` picks one of
+// kSweepVariants launch shapes of the segment kernel (planes per thread and
+// rows per block; all give identical results); other W use the one-cell
+// kernel.
+constexpr int kSweepVariants = 6;
+int  sweep_variant_count(const Geom &g);
 void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                         const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
-                        long long *launches);
+                        long long *launches, int variant = 0);
 void launch_plane_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                          const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
                          long long *launches);
@@ -76,6 +82,20 @@ void launch_unpack(const Geom &g, const float *red, const float *black, float *n
                    cudaStream_t st);
 
 void launch_perlin(const float *pos3, int n, float scale, int seed, float *out, cudaStream_t st);
+
+// Device-side state of a graph-run solve (see graph_solve.cu).
+struct SolveCtl {
+    int iters, checks, converged, pad;
+    double r2, b2;                      // last ||r||^2, ||b||^2
+    unsigned long long sweep_ns, t0;    // global-timer time inside sweep batches
+};
+cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
+                              float *p_r, float *p_b, double *partials, int n_partials, double *norm2,
+                              SolveCtl *ctl, int chunk, int max_iter, double tol, int variant, cudaStream_t st,
+                              cudaGraphExec_t *exec_out, int *body_kernels, int *prologue_kernels);
+
+// Sets the calling thread's error text (what blz_last_error(NULL) returns).
+void set_thread_error(const char *msg);
 
 // -- advection ------------------------------------------------------------------
 void launch_advect(const Geom &g, const float *T, const float *U, const float *V, const float *W,

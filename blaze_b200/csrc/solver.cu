@@ -9,8 +9,12 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "kernels.cuh"
@@ -38,6 +42,11 @@ struct blz_solver {
     double *d_norm2 = nullptr, *h_norm2 = nullptr;
     cudaEvent_t ev[8]{};
     long long launches = 0;
+    int variant = -2;                           // sweep launch shape (-2: not chosen yet)
+    // device-loop solve: instantiated graph and its control block
+    cudaGraphExec_t solve_exec = nullptr;
+    SolveCtl *ctl = nullptr, *h_ctl = nullptr;
+    int graph_body = 0, graph_prologue = 0;
     std::string err;
 };
 
@@ -53,6 +62,10 @@ static int fail(blz_solver *s, int code, const char *fmt, ...) {
     g_thread_err = buf;
     return code;
 }
+
+namespace blz {
+void set_thread_error(const char *msg) { g_thread_err = msg; }
+} // namespace blz
 
 #define CK(s, x)                                                                            \
     do {                                                                                    \
@@ -117,6 +130,8 @@ int blz_default_params(blz_params *p) {
     p->gs_order = BLZ_GS_RB3D;
     p->reset_pressure = 0;
     p->max_particles = 1 << 16;
+    p->device_loop = 1;
+    p->sweep_variant = -1;
     return BLZ_OK;
 }
 
@@ -134,6 +149,9 @@ static void release(blz_solver *s) {
     cudaFree(s->parts); cudaFree(s->boxes); cudaFree(s->bin_start); cudaFree(s->bin_list); cudaFree(s->active);
     cudaFree(s->partials); cudaFree(s->d_norm2);
     if (s->h_norm2) cudaFreeHost(s->h_norm2);
+    if (s->solve_exec) cudaGraphExecDestroy(s->solve_exec);
+    cudaFree(s->ctl);
+    if (s->h_ctl) cudaFreeHost(s->h_ctl);
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
     if (s->own_stream && s->st) cudaStreamDestroy(s->st);
 }
@@ -192,6 +210,8 @@ int blz_create(const blz_params *p, blz_solver **out) {
     ok = ok && cudaMalloc(&s->partials, 2 * sizeof(double) * s->n_partials) == cudaSuccess;
     ok = ok && cudaMalloc(&s->d_norm2, 2 * sizeof(double)) == cudaSuccess;
     ok = ok && cudaMallocHost(&s->h_norm2, 2 * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->ctl, sizeof(SolveCtl)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&s->h_ctl, sizeof(SolveCtl)) == cudaSuccess;
     if (!ok) { cudaGetLastError(); int r = fail(s, BLZ_ERR_ALLOC, "device allocation failed for %dx%dx%d", g.W, g.H, g.D); return bail(r); }
     for (auto &ev : s->ev)
         if (cudaEventCreate(&ev) != cudaSuccess) { int r = fail(s, BLZ_ERR_CUDA, "cudaEventCreate failed"); return bail(r); }
@@ -427,13 +447,98 @@ static int residual_sync(blz_solver *s, double *r, double *b) {
     return BLZ_OK;
 }
 
+// Sweep launch-shape autotuner: each variant of the segment kernel runs a few
+// sweeps on scratch copies of p (the solver's state is untouched; rhs is only
+// read), timed with CUDA events; the fastest is kept per (device, grid dims)
+// for the life of the process.  BLZ_SWEEP_VARIANT or params.sweep_variant
+// forces a choice.
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
+
+static int choose_variant(blz_solver *s) {
+    if (s->variant != -2) return BLZ_OK;
+    const int nv = sweep_variant_count(s->g);
+    if (nv == 0) { s->variant = -1; return BLZ_OK; }
+    if (s->P.sweep_variant >= 0) { s->variant = std::min(s->P.sweep_variant, nv - 1); return BLZ_OK; }
+    if (const char *env = std::getenv("BLZ_SWEEP_VARIANT")) {
+        s->variant = std::max(0, std::min(std::atoi(env), nv - 1));
+        return BLZ_OK;
+    }
+    const auto key = std::make_tuple(s->device, s->g.W, s->g.H, s->g.D);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) { s->variant = it->second; return BLZ_OK; }
+    }
+    const size_t half = n_of(s->P, 0) / 2;
+    float *tr = s->scratch, *tb = s->scratch + half;
+    CK(s, cudaMemcpyAsync(tr, s->p_r, half * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
+    CK(s, cudaMemcpyAsync(tb, s->p_b, half * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
+    const SolveParams sp = solve_params(s->P);
+    int best = 0;
+    float best_ms = 1e30f;
+    long long dummy = 0;
+    for (int v = 0; v < nv; ++v) {
+        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 1, s->st, &dummy, v);
+        CK(s, cudaEventRecord(s->ev[6], s->st));
+        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 3, s->st, &dummy, v);
+        CK(s, cudaEventRecord(s->ev[7], s->st));
+        CKL(s);
+        CK(s, cudaEventSynchronize(s->ev[7]));
+        float ms = 0.0f;
+        CK(s, cudaEventElapsedTime(&ms, s->ev[6], s->ev[7]));
+        if (ms < best_ms) { best_ms = ms; best = v; }
+    }
+    s->launches += 8LL * nv;
+    s->variant = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+    return BLZ_OK;
+}
+
 static int sweeps(blz_solver *s, int n) {
     const SolveParams sp = solve_params(s->P);
-    if (s->P.gs_order == BLZ_GS_PLANE)
+    if (s->P.gs_order == BLZ_GS_PLANE) {
         launch_plane_sweeps(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, s->st, &s->launches);
-    else
-        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, s->st, &s->launches);
+    } else {
+        int rc = choose_variant(s);
+        if (rc != BLZ_OK) return rc;
+        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, s->st, &s->launches, s->variant);
+    }
     CKL(s);
+    return BLZ_OK;
+}
+
+// The residual-controlled solve as one graph launch (graph_solve.cu).
+static int solve_device_loop(blz_solver *s, blz_step_stats *st) {
+    const blz_params &P = s->P;
+    int rc = choose_variant(s);
+    if (rc != BLZ_OK) return rc;
+    if (!s->solve_exec) {
+        cudaError_t e = build_solve_graph(s->g, solve_params(P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->partials,
+                                          s->n_partials, s->d_norm2, s->ctl, std::max(1, P.check_every), P.max_iter,
+                                          P.tol, s->variant, s->st, &s->solve_exec, &s->graph_body,
+                                          &s->graph_prologue);
+        if (e != cudaSuccess) return fail(s, BLZ_ERR_CUDA, "building the solve graph failed: %s", cudaGetErrorString(e));
+    }
+    CK(s, cudaGraphLaunch(s->solve_exec, s->st));
+    CK(s, cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s->st));
+    CK(s, cudaStreamSynchronize(s->st));
+    const SolveCtl &c = *s->h_ctl;
+    s->launches += s->graph_prologue + (long long)(c.checks - 1) * s->graph_body;
+    if (st) {
+        const double r = std::sqrt(c.r2), b = std::sqrt(c.b2);
+        st->iterations = c.iters;
+        st->residual = r;
+        st->rhs_norm = b;
+        st->rel_residual = b > 0.0 ? r / b : 0.0;
+        st->converged = c.converged;
+        st->ms_sweeps = (float)(c.sweep_ns * 1e-6);
+        st->residual_checks = c.checks;
+        st->sweep_variant = s->variant;
+        st->device_loop = 1;
+        if (!std::isfinite(r)) return fail(s, BLZ_ERR_NAN, "non-finite residual after %d sweeps", c.iters);
+    }
     return BLZ_OK;
 }
 
@@ -445,6 +550,9 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
         CK(s, cudaMemsetAsync(s->p_r, 0, half * sizeof(float), s->st));
         CK(s, cudaMemsetAsync(s->p_b, 0, half * sizeof(float), s->st));
     }
+    const int chunk_sz = std::max(1, P.check_every);
+    if (P.device_loop && P.tol > 0.0 && P.gs_order == BLZ_GS_RB3D && P.max_iter % chunk_sz == 0)
+        return solve_device_loop(s, st);
     int done = 0, rc, checks = 0;
     double r = 0.0, b = 0.0;
     bool have = false;
@@ -492,9 +600,17 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
         st->converged = P.tol <= 0.0 || b == 0.0 || r / b <= P.tol;
         st->ms_sweeps = ms_sweeps;
         st->residual_checks = checks;
+        st->sweep_variant = s->variant;
+        st->device_loop = 0;
         if (!std::isfinite(r)) return fail(s, BLZ_ERR_NAN, "non-finite residual after %d sweeps", done);
     }
     return BLZ_OK;
+}
+
+int blz_sweeps(blz_solver *s, int n) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    if (n < 0) return fail(s, BLZ_ERR_ARG, "negative sweep count %d", n);
+    return n > 0 ? sweeps(s, n) : BLZ_OK;
 }
 
 int blz_gradient(blz_solver *s) {

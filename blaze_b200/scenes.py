@@ -82,6 +82,8 @@ class SceneSettings:
     gs_order: int = _abi.BLZ_GS_RB3D
     reset_pressure: int = 0
     temporal_block: int = 0
+    device_loop: int = 1
+    sweep_variant: int = -1
     extra: dict = field(default_factory=dict)
 
     def to_params(self):
@@ -101,6 +103,7 @@ class SceneSettings:
         p.max_iter, p.tol, p.check_every = self.maxIterSolve, self.tol, self.check_every
         p.bc_mode, p.gs_order, p.reset_pressure = self.bc_mode, self.gs_order, self.reset_pressure
         p.max_particles, p.temporal_block = self.sourceMaxParticleCount, self.temporal_block
+        p.device_loop, p.sweep_variant = self.device_loop, self.sweep_variant
         return p
 
 

@@ -82,6 +82,9 @@ class FluidSolver:
         check(self._lib.blz_solve(self._h, C.byref(self.last_stats)), self._h)
         return self.last_stats.as_dict()
 
+    def sweeps(self, n):
+        check(self._lib.blz_sweeps(self._h, int(n)), self._h)
+
     def gradient(self):
         check(self._lib.blz_gradient(self._h), self._h)
 

@@ -105,6 +105,13 @@ typedef struct blz_params {
                                      reference keeps p between frames)      */
     int    max_particles;         /* sourceMaxParticleCount                  */
     int    temporal_block;        /* sweeps fused per HBM pass (0 = auto)    */
+    int    device_loop;           /* 1: a residual-controlled solve runs as one
+                                     CUDA graph whose conditional WHILE node
+                                     decides on the device (no host round
+                                     trip per check); needs max_iter to be a
+                                     multiple of check_every                 */
+    int    sweep_variant;         /* -1: autotune the sweep launch shape per
+                                     grid size (first solve); >= 0: force one */
 } blz_params;
 
 /* ---- per-step statistics ------------------------------------------------- */
@@ -119,6 +126,8 @@ typedef struct blz_step_stats {
     float  ms_sweeps;             /* device time of the GS sweep launches
                                      alone (residual checks excluded)        */
     int    residual_checks;       /* FP64 residual evaluations in the solve  */
+    int    sweep_variant;         /* sweep launch shape used (-1: one-cell)   */
+    int    device_loop;           /* 1 if the solve ran as a device loop      */
 } blz_step_stats;
 
 typedef struct blz_solver blz_solver;
@@ -157,6 +166,11 @@ int  blz_divergence(blz_solver *s);
 int  blz_solve(blz_solver *s, blz_step_stats *st);
 int  blz_gradient(blz_solver *s);
 int  blz_advect(blz_solver *s);                        /* + swap               */
+
+/* Exactly n Gauss-Seidel sweeps (params' order and boundary handling) on the
+ * current rhs and p, with no residual checks (the inner loop of
+ * gs_solve_kernel, FluidSolver.cu:526-597, run n times).                    */
+int  blz_sweeps(blz_solver *s, int n);
 
 /* FP64 ||b - A p||_2 and ||b||_2 of the current rhs and p.                  */
 int  blz_residual(blz_solver *s, double *res_norm, double *rhs_norm);

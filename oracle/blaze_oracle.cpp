@@ -57,13 +57,15 @@ static inline uint32_t f2u_sat(float x) {
     return (uint32_t)x;
 }
 
-// Lattice seed, cuda_noise.cuh:120-124; the sum is formed left to right in
-// float (every product of an integer-valued corner and the constants is exact
-// below 2^24, so fused multiply-adds give the same value).
+// Lattice seed, cuda_noise.cuh:120-124: x*1723 + y*93241 + z*149812 + 3824 +
+// seed in float.  The reference's CUDA build contracts the sum into
+// fma(z, 149812, fma(x, 1723, y*93241)), then adds 3824 and seed; once a
+// product exceeds 2^24 the contraction changes the rounded value and with it
+// the hashed lattice gradient, so the oracle forms it the same way.  Pinned
+// bit for bit against the reference build's own noise (tests/golden/perlin.npz).
 static inline uint32_t lattice_seed(float x, float y, float z, float seed) {
-    float acc = x * 1723.0f;
-    acc = acc + y * 93241.0f;
-    acc = acc + z * 149812.0f;
+    float acc = std::fma(x, 1723.0f, y * 93241.0f);
+    acc = std::fma(z, 149812.0f, acc);
     acc = acc + 3824.0f;
     acc = acc + seed;
     return lattice_hash(f2u_sat(acc));

@@ -241,3 +241,51 @@ def test_error_codes_on_gpu():
     assert e.value.code == -2
     with pytest.raises(BlazeError):
         s.set("T", np.zeros((3, 3, 3), np.float32))
+
+
+def test_device_loop_matches_host_loop():
+    """The graph-run solve (conditional WHILE node deciding on the device)
+    follows the host loop's schedule exactly: same sweep count, same checks,
+    bitwise the same pressure."""
+    from blaze_b200 import FluidSolver
+    out = []
+    for dl in (0, 1):
+        scn = scene(dims=(32, 24, 20), bc_mode=BLZ_BC_FREE_SURFACE, tol=1e-4, maxIterSolve=3000,
+                    check_every=10, device_loop=dl)
+        gpu, _ = pair(scn, 63)
+        st = gpu.solve()
+        assert st["device_loop"] == dl
+        out.append((st["iterations"], st["residual_checks"], st["converged"], gpu.get("P")))
+        gpu.close()
+    assert out[0][:3] == out[1][:3]
+    np.testing.assert_array_equal(out[0][3], out[1][3])
+
+
+def test_device_loop_hits_the_cap():
+    from blaze_b200 import FluidSolver
+    scn = scene(dims=(32, 24, 20), bc_mode=BLZ_BC_FREE_SURFACE, tol=1e-12, maxIterSolve=40, check_every=10)
+    gpu, _ = pair(scn, 64)
+    st = gpu.solve()
+    assert st["device_loop"] == 1 and st["iterations"] == 40 and not st["converged"]
+    assert st["residual_checks"] == 5
+
+
+def test_sweep_variants_are_bitwise_identical():
+    """Every launch shape of the segment sweep kernel gives the same bits."""
+    ref = None
+    for v in range(6):
+        gpu, _ = pair(scene(dims=(64, 20, 18), bc_mode=BLZ_BC_FREE_SURFACE, sweep_variant=v), 65)
+        gpu.sweeps(7)
+        p = gpu.get("P")
+        gpu.close()
+        if ref is None:
+            ref = p
+        else:
+            np.testing.assert_array_equal(p, ref, err_msg=f"variant {v}")
+
+
+def test_fixed_sweeps_match_oracle():
+    gpu, ref = pair(scene(dims=(40, 16, 12), bc_mode=BLZ_BC_FREE_SURFACE), 66)
+    gpu.sweeps(12)
+    ref.gs_sweeps(12)
+    assert_close(gpu, ref, ("P",), rel=2e-5, absol=2e-4)
