@@ -143,7 +143,11 @@ def run_ours(args, ws, rank, local):
     torch.cuda.set_device(local)
     scn, parts = family_scene(n=args.grid, seed=SEED + rank, tol=TOL, max_iter=args.max_iter, check_every=CHECK_EVERY)
     W, H, D = scn.gridRes
-    stream = torch.cuda.current_stream()
+    # A dedicated stream shared by the solver and the timing events (the
+    # legacy default stream has handle 0, which the library reads as "use
+    # your own stream").
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     tmr = Timer()
     solver = FluidSolver(tmr, scn, particles=parts, stream=stream.cuda_stream)
 
@@ -269,7 +273,8 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "stage_ms": {k: float(np.mean([s[k] for s in stats])) for k in
-                     ("ms_forces", "ms_divergence", "ms_solve", "ms_gradient", "ms_advect", "ms_sweeps")},
+                     ("ms_forces", "ms_divergence", "ms_solve", "ms_gradient", "ms_advect", "ms_sweeps",
+                      "ms_checks")},
     }
     if not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(scn, parts, float(sweeps.mean()))

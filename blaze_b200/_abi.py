@@ -18,6 +18,9 @@ BLZ_BC_REF_COMPAT = 0
 BLZ_BC_FREE_SURFACE = 1
 BLZ_GS_RB3D = 0
 BLZ_GS_PLANE = 1
+BLZ_ADVECT_RK3 = 0
+BLZ_ADVECT_EULER = 1
+BLZ_ADVECT_RK2 = 2
 
 FIELD_T, FIELD_U, FIELD_V, FIELD_W, FIELD_P, FIELD_RHS = range(6)
 FIELD_NAMES = {"T": FIELD_T, "U": FIELD_U, "V": FIELD_V, "W": FIELD_W, "P": FIELD_P, "RHS": FIELD_RHS}
@@ -39,7 +42,7 @@ class BlzParams(C.Structure):
         ("max_iter", C.c_int), ("tol", C.c_double), ("check_every", C.c_int),
         ("bc_mode", C.c_int), ("gs_order", C.c_int), ("reset_pressure", C.c_int),
         ("max_particles", C.c_int), ("temporal_block", C.c_int),
-        ("device_loop", C.c_int), ("sweep_variant", C.c_int),
+        ("device_loop", C.c_int), ("sweep_variant", C.c_int), ("advect_scheme", C.c_int),
     ]
 
     def dims(self):
@@ -73,11 +76,19 @@ class BlzStepStats(C.Structure):
         ("ms_source", C.c_float), ("ms_forces", C.c_float), ("ms_divergence", C.c_float),
         ("ms_solve", C.c_float), ("ms_gradient", C.c_float), ("ms_advect", C.c_float),
         ("ms_total", C.c_float), ("ms_sweeps", C.c_float), ("residual_checks", C.c_int),
-        ("sweep_variant", C.c_int), ("device_loop", C.c_int),
+        ("sweep_variant", C.c_int), ("device_loop", C.c_int), ("ms_checks", C.c_float),
     ]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+BLZ_CONV_SLACK = 256
+
+
+class BlzConvDesc(C.Structure):
+    _fields_ = [("W", C.c_int), ("H", C.c_int), ("D", C.c_int), ("cin", C.c_int), ("cout", C.c_int),
+                ("relu", C.c_int), ("out_f32", C.c_int)]
 
 
 # Every entry point declared in include/blaze_b200.h, with its ctypes signature.
@@ -103,6 +114,7 @@ EXPORTS = {
     "blz_field_size": (C.c_size_t, [C.c_void_p, C.c_int]),
     "blz_field_ptr": (C.c_void_p, [C.c_void_p, C.c_int]),
     "blz_perlin": (C.c_int, [_P(C.c_float), C.c_int, C.c_float, C.c_int, _P(C.c_float)]),
+    "blz_conv3d": (C.c_int, [_P(BlzConvDesc), C.c_void_p, C.c_void_p, _P(C.c_float), C.c_void_p, C.c_void_p]),
     "blz_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "blz_last_error": (C.c_char_p, [C.c_void_p]),
 }

@@ -25,18 +25,24 @@ __global__ void k_ctl_begin(SolveCtl *c) {
     c->checks = 0;
     c->converged = 0;
     c->sweep_ns = 0;
+    c->check_ns = 0;
 }
 
+// Ends the sweep interval (stop != 0) and starts the check interval, or
+// starts a sweep interval.
 __global__ void k_ctl_mark(SolveCtl *c, int stop) {
     const unsigned long long t = global_ns();
-    if (stop) c->sweep_ns += t - c->t0;
+    if (stop) { c->sweep_ns += t - c->t0; c->t1 = t; }
     else c->t0 = t;
 }
 
 // Reads {||r||^2, ||b||^2}, records them, and sets whether the loop goes on.
 __global__ void k_ctl_check(SolveCtl *c, const double *__restrict__ norm2, cudaGraphConditionalHandle h,
                             int after_sweeps, int chunk, int max_iter, double tol) {
-    if (after_sweeps) c->iters += chunk;
+    if (after_sweeps) {
+        c->iters += chunk;
+        c->check_ns += global_ns() - c->t1;
+    }
     c->checks += 1;
     const double r2 = norm2[0], b2 = norm2[1];
     c->r2 = r2;

@@ -17,26 +17,40 @@ __device__ __forceinline__ void vel_at(const FieldRef &u, const FieldRef &v, con
     vz = trilinear(w, r, px, py, pz);
 }
 
-// Backtrace from the sample point of src at (i,j,k): RK3 with stages at
-// 0.5 dt and 0.75 dt and weights 2/9, 3/9, 4/9; trilinear velocity.
-template <bool CLAMP>
+// Backtrace from the sample point of src at (i,j,k) with trilinear velocity:
+// RK3 (stages at 0.5 dt and 0.75 dt, weights 2/9, 3/9, 4/9;
+// FluidSolver.cu:431-456), forward Euler (392-407) or midpoint RK2
+// (409-429); then the tricubic sample at the departure point.
+template <bool CLAMP, int SCHEME>
 __device__ __forceinline__ float advect_one(const Geom &g, const FieldRef &src, const FieldRef &u,
                                             const FieldRef &v, const FieldRef &w, int i, int j,
                                             int k) {
     const float r = g.inv_dx, dt = g.dt;
     const float px = ((float)i + src.ox) * g.dx, py = ((float)j + src.oy) * g.dx, pz = ((float)k + src.oz) * g.dx;
-    float k1x, k1y, k1z, k2x, k2y, k2z, k3x, k3y, k3z;
+    float k1x, k1y, k1z;
     vel_at(u, v, w, r, px, py, pz, k1x, k1y, k1z);
-    const float h1 = 0.5f * dt, h2 = 0.75f * dt;
-    vel_at(u, v, w, r, px - h1 * k1x, py - h1 * k1y, pz - h1 * k1z, k2x, k2y, k2z);
-    vel_at(u, v, w, r, px - h2 * k2x, py - h2 * k2y, pz - h2 * k2z, k3x, k3y, k3z);
-    const float a = 2.0f / 9.0f, b = 3.0f / 9.0f, c = 4.0f / 9.0f;
-    const float qx = px - dt * (a * k1x + b * k2x + c * k3x);
-    const float qy = py - dt * (a * k1y + b * k2y + c * k3y);
-    const float qz = pz - dt * (a * k1z + b * k2z + c * k3z);
+    float qx, qy, qz;
+    if (SCHEME == BLZ_ADVECT_EULER) {
+        qx = px - dt * k1x; qy = py - dt * k1y; qz = pz - dt * k1z;
+    } else if (SCHEME == BLZ_ADVECT_RK2) {
+        const float h1 = 0.5f * dt;
+        float mx, my, mz;
+        vel_at(u, v, w, r, px - h1 * k1x, py - h1 * k1y, pz - h1 * k1z, mx, my, mz);
+        qx = px - dt * mx; qy = py - dt * my; qz = pz - dt * mz;
+    } else {
+        float k2x, k2y, k2z, k3x, k3y, k3z;
+        const float h1 = 0.5f * dt, h2 = 0.75f * dt;
+        vel_at(u, v, w, r, px - h1 * k1x, py - h1 * k1y, pz - h1 * k1z, k2x, k2y, k2z);
+        vel_at(u, v, w, r, px - h2 * k2x, py - h2 * k2y, pz - h2 * k2z, k3x, k3y, k3z);
+        const float a = 2.0f / 9.0f, b = 3.0f / 9.0f, c = 4.0f / 9.0f;
+        qx = px - dt * (a * k1x + b * k2x + c * k3x);
+        qy = py - dt * (a * k1y + b * k2y + c * k3y);
+        qz = pz - dt * (a * k1z + b * k2z + c * k3z);
+    }
     return tricubic<CLAMP>(src, r, qx, qy, qz);
 }
 
+template <int SCHEME>
 __global__ void __launch_bounds__(256)
 k_advect(Geom g, const float *__restrict__ T, const float *__restrict__ U,
          const float *__restrict__ V, const float *__restrict__ W, float *__restrict__ Tn,
@@ -47,18 +61,23 @@ k_advect(Geom g, const float *__restrict__ T, const float *__restrict__ U,
     if (i > g.W || j > g.H || k > g.D) return;
     const FieldRef u = fU(U, g), v = fV(V, g), w = fW(W, g);
     if (i < g.W && j < g.H && k < g.D)
-        Tn[lin(i, j, k, g.W, g.H)] = advect_one<true>(g, fT(T, g), u, v, w, i, j, k);
+        Tn[lin(i, j, k, g.W, g.H)] = advect_one<true, SCHEME>(g, fT(T, g), u, v, w, i, j, k);
     if (j < g.H && k < g.D)
-        Un[lin(i, j, k, g.W + 1, g.H)] = advect_one<false>(g, u, u, v, w, i, j, k);
+        Un[lin(i, j, k, g.W + 1, g.H)] = advect_one<false, SCHEME>(g, u, u, v, w, i, j, k);
     if (i < g.W && k < g.D)
-        Vn[lin(i, j, k, g.W, g.H + 1)] = advect_one<false>(g, v, u, v, w, i, j, k);
+        Vn[lin(i, j, k, g.W, g.H + 1)] = advect_one<false, SCHEME>(g, v, u, v, w, i, j, k);
     if (i < g.W && j < g.H)
-        Wn[lin(i, j, k, g.W, g.H)] = advect_one<false>(g, w, u, v, w, i, j, k);
+        Wn[lin(i, j, k, g.W, g.H)] = advect_one<false, SCHEME>(g, w, u, v, w, i, j, k);
 }
 
 void launch_advect(const Geom &g, const float *T, const float *U, const float *V, const float *W,
-                   float *Tn, float *Un, float *Vn, float *Wn, cudaStream_t st) {
-    k_advect<<<face_grid(g), face_block(), 0, st>>>(g, T, U, V, W, Tn, Un, Vn, Wn);
+                   float *Tn, float *Un, float *Vn, float *Wn, cudaStream_t st, int scheme) {
+    if (scheme == BLZ_ADVECT_EULER)
+        k_advect<BLZ_ADVECT_EULER><<<face_grid(g), face_block(), 0, st>>>(g, T, U, V, W, Tn, Un, Vn, Wn);
+    else if (scheme == BLZ_ADVECT_RK2)
+        k_advect<BLZ_ADVECT_RK2><<<face_grid(g), face_block(), 0, st>>>(g, T, U, V, W, Tn, Un, Vn, Wn);
+    else
+        k_advect<BLZ_ADVECT_RK3><<<face_grid(g), face_block(), 0, st>>>(g, T, U, V, W, Tn, Un, Vn, Wn);
 }
 
 } // namespace blz

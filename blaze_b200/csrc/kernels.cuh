@@ -88,17 +88,31 @@ struct SolveCtl {
     int iters, checks, converged, pad;
     double r2, b2;                      // last ||r||^2, ||b||^2
     unsigned long long sweep_ns, t0;    // global-timer time inside sweep batches
+    unsigned long long check_ns, t1;    // ... and inside the residual checks
 };
 cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
                               float *p_r, float *p_b, double *partials, int n_partials, double *norm2,
                               SolveCtl *ctl, int chunk, int max_iter, double tol, int variant, cudaStream_t st,
                               cudaGraphExec_t *exec_out, int *body_kernels, int *prologue_kernels);
 
+// -- learned warm start: tensor-core convolution (unet_conv.cu) -------------
+struct ConvDesc {
+    int W, H, D;        // interior voxels (tensors carry a 1-voxel zero halo)
+    int cin, cout;      // cin % 16 == 0; cout in {16, 32, 64, 128}
+    int relu, out_f32;
+};
+int conv3d_smem_bytes(int cout);
+}  // namespace blz
+#include <cuda_bf16.h>
+namespace blz {
+cudaError_t launch_conv3d(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
+                          void *y, int *err, cudaStream_t st);
+
 // Sets the calling thread's error text (what blz_last_error(NULL) returns).
 void set_thread_error(const char *msg);
 
 // -- advection ------------------------------------------------------------------
 void launch_advect(const Geom &g, const float *T, const float *U, const float *V, const float *W,
-                   float *Tn, float *Un, float *Vn, float *Wn, cudaStream_t st);
+                   float *Tn, float *Un, float *Vn, float *Wn, cudaStream_t st, int scheme);
 
 } // namespace blz

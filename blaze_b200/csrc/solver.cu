@@ -173,6 +173,8 @@ int blz_create(const blz_params *p, blz_solver **out) {
         return fail(nullptr, BLZ_ERR_ARG, "bad bc_mode %d", p->bc_mode);
     if (p->gs_order != BLZ_GS_RB3D && p->gs_order != BLZ_GS_PLANE)
         return fail(nullptr, BLZ_ERR_ARG, "bad gs_order %d", p->gs_order);
+    if (p->advect_scheme < BLZ_ADVECT_RK3 || p->advect_scheme > BLZ_ADVECT_RK2)
+        return fail(nullptr, BLZ_ERR_ARG, "bad advect_scheme %d", p->advect_scheme);
 
     blz_solver *s = new blz_solver();
     s->P = *p;
@@ -534,6 +536,7 @@ static int solve_device_loop(blz_solver *s, blz_step_stats *st) {
         st->rel_residual = b > 0.0 ? r / b : 0.0;
         st->converged = c.converged;
         st->ms_sweeps = (float)(c.sweep_ns * 1e-6);
+        st->ms_checks = (float)(c.check_ns * 1e-6);
         st->residual_checks = c.checks;
         st->sweep_variant = s->variant;
         st->device_loop = 1;
@@ -602,6 +605,7 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
         st->residual_checks = checks;
         st->sweep_variant = s->variant;
         st->device_loop = 0;
+        st->ms_checks = 0.0f;
         if (!std::isfinite(r)) return fail(s, BLZ_ERR_NAN, "non-finite residual after %d sweeps", done);
     }
     return BLZ_OK;
@@ -633,7 +637,8 @@ int blz_project(blz_solver *s, blz_step_stats *st) {
 int blz_advect(blz_solver *s) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     const int c = s->cur, b = c ^ 1;
-    launch_advect(s->g, s->T[c], s->U[c], s->V[c], s->W[c], s->T[b], s->U[b], s->V[b], s->W[b], s->st);
+    launch_advect(s->g, s->T[c], s->U[c], s->V[c], s->W[c], s->T[b], s->U[b], s->V[b], s->W[b], s->st,
+                  s->P.advect_scheme);
     CKL(s);
     s->launches++;
     s->cur = b;                                                                 // swap_grids_kernel

@@ -1,0 +1,257 @@
+// unet_conv.cu — 3x3x3 convolution as an implicit GEMM on the tcgen05
+// tensor cores (BF16 operands, FP32 accumulation in tensor memory).
+//
+// Activations are channels-last with a one-voxel zero halo on every side:
+// element (x, y, z, c) of a W x H x D x C tensor sits at
+// ((z+1)*Hp + (y+1))*Wp + (x+1)) * C + c with Wp = W+2, Hp = H+2, plus
+// kSlack zero voxels before and after the tensor.  Weights are [27][Cout][Cin]
+// (tap = (dz+1)*9 + (dy+1)*3 + (dx+1)), bias FP32 [Cout].
+//
+// One CTA computes M = 128 consecutive voxels of the padded plane z (its
+// interior rows) for all N = Cout outputs.  For each 16-channel chunk of the
+// input it stages the 9 input rows (dy, dz) of 130 voxels once, in the
+// canonical K-major layout of the UMMA operand descriptor (8-voxel core
+// matrices of 16 B rows, 128 B apart; the two 8-channel halves 2080 B
+// apart).  Because a voxel's row is exactly 16 B at a linear position, the
+// A operand of tap (dx, dy, dz) is the same block seen 16*(dx+1) B further
+// on: 27 MMAs of M=128 x N x K=16 read one staged block.  The halo makes
+// the zero padding of the convolution a plain memory read.
+#include <cuda_bf16.h>
+
+#include "kernels.cuh"
+
+namespace blz {
+
+namespace {
+
+constexpr int kConvM = 128;
+constexpr int kRowVox = kConvM + 2;                 // 130 voxels per staged row
+constexpr int kKgBytes = kRowVox * 16;              // one 8-channel half of a row
+constexpr int kRowBytes = 2 * kKgBytes;             // 4160 B per staged row (16 ch)
+constexpr int kABytes = 9 * kRowBytes;              // 37440 B
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// UMMA shared-memory descriptor: K-major, no swizzle (canonical layout
+// ((8,m),2):((1,SBO),LBO) in 16-byte units), descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;                          // version
+    return d;                                        // base offset 0, layout SWIZZLE_NONE
+}
+
+// Instruction descriptor, kind::f16: D FP32, A and B BF16, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, int *err) {
+    // Bounded: gives up after ~2^26 polls, records the timeout and returns.
+    for (int it = 0; it < (1 << 26); ++it) {
+        uint32_t done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    if (err) atomicExch(err, 1);
+    return false;
+}
+
+} // namespace
+
+template <int N, bool RELU, bool OUT_F32>
+__global__ void __launch_bounds__(128)
+k_conv3d_tc(int W, int H, int D, int cin, int cout_stride, const __nv_bfloat16 *__restrict__ x,
+            const __nv_bfloat16 *__restrict__ w, const float *__restrict__ bias, void *__restrict__ y,
+            int *err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char *sA = smem;
+    unsigned char *sB = smem + kABytes;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    constexpr int kCols = N < 32 ? 32 : N;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Wp = W + 2, Hp = H + 2;
+    const long long plane = (long long)Wp * Hp;
+    const int z = blockIdx.y;
+    const long long P0 = (long long)Wp + (long long)kConvM * blockIdx.x;   // first voxel of the tile
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base)), "r"(kCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const uint32_t aS = smem_u32(sA), bS = smem_u32(sB), mb = smem_u32(&mbar);
+    constexpr uint32_t idesc = umma_idesc_bf16(kConvM, N);
+    const int chunks = cin / 16;
+    bool ok = true;
+    for (int c = 0; c < chunks && ok; ++c) {
+        // Stage the 9 input rows of this 16-channel chunk ...
+        for (int e = tid; e < 9 * kRowVox * 2; e += 128) {
+            const int r = e / (kRowVox * 2), rem = e % (kRowVox * 2);
+            const int v = rem >> 1, kg = rem & 1;
+            const int dz = r / 3 - 1, dy = r % 3 - 1;
+            const long long g = (long long)(z + 1 + dz) * plane + P0 - 1 + (long long)dy * Wp + v;
+            cp_async16(aS + r * kRowBytes + kg * kKgBytes + v * 16, x + g * cin + c * 16 + kg * 8);
+        }
+        // ... and the 27 taps' weights of the chunk (B: N x 16, K-major).
+        for (int e = tid; e < 27 * N * 2; e += 128) {
+            const int t = e / (N * 2), rem = e % (N * 2);
+            const int n = rem >> 1, kg = rem & 1;
+            cp_async16(bS + t * N * 32 + kg * N * 16 + n * 16, w + ((size_t)t * N + n) * cin + c * 16 + kg * 8);
+        }
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+            for (int t = 0; t < 27; ++t) {
+                const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+                const int r = (dz + 1) * 3 + (dy + 1);
+                const uint64_t ad = umma_desc(aS + r * kRowBytes + (dx + 1) * 16, kKgBytes, 128);
+                const uint64_t bd = umma_desc(bS + t * N * 32, N * 16, 128);
+                const uint32_t acc = (c > 0 || t > 0) ? 1u : 0u;
+                asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                             ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(mb) : "memory");
+        }
+        // The staged block is reused by the next chunk only once the MMAs
+        // that read it have completed.
+        // (CTA-uniform outcome, so the .sync.aligned TMEM loads below never
+        // run in a divergent warp.)
+        ok = __syncthreads_and(mbar_wait(mb, (uint32_t)(c & 1), err)) != 0;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+        // Epilogue: warp w owns TMEM lanes 32w..32w+31 = voxels of the tile.
+        const long long P = P0 + 32 * warp + lane;
+        const int xp = (int)(P % Wp), yp = (int)(P / Wp);
+        const bool inside = xp >= 1 && xp <= W && yp >= 1 && yp <= H;
+        const long long outv = (long long)(z + 1) * plane + P;
+#pragma unroll
+        for (int n0 = 0; n0 < N; n0 += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)n0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+                           "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                         : "r"(taddr) : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (inside) {
+                float v[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    v[q] = __uint_as_float(r[q]) + __ldg(bias + n0 + q);
+                    if (RELU) v[q] = fmaxf(v[q], 0.0f);
+                }
+                if (OUT_F32) {
+                    float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(y) + outv * cout_stride + n0);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                } else {
+                    __nv_bfloat162 h[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                    uint4 *dst = reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(y) + outv * cout_stride + n0);
+                    dst[0] = *reinterpret_cast<uint4 *>(&h[0]);
+                    dst[1] = *reinterpret_cast<uint4 *>(&h[4]);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+}
+
+int conv3d_smem_bytes(int cout) { return kABytes + 27 * cout * 32; }
+
+template <int N, bool RELU, bool F32>
+static cudaError_t launch_n(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
+                            void *y, int *err, cudaStream_t st) {
+    const int smem = conv3d_smem_bytes(N);
+    cudaError_t e = cudaFuncSetAttribute(k_conv3d_tc<N, RELU, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const long long interior = (long long)(cd.W + 2) * cd.H;
+    const dim3 grid((unsigned)((interior + kConvM - 1) / kConvM), (unsigned)cd.D);
+    k_conv3d_tc<N, RELU, F32><<<grid, 128, smem, st>>>(cd.W, cd.H, cd.D, cd.cin, cd.cout, x, w, bias, y, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_conv3d(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
+                          void *y, int *err, cudaStream_t st) {
+    if (cd.cin % 16 || cd.cin <= 0) return cudaErrorInvalidValue;
+#define BLZ_CONV_CASE(NN)                                                                  \
+    if (cd.cout == NN) {                                                                   \
+        if (cd.out_f32) return cd.relu ? launch_n<NN, true, true>(cd, x, w, bias, y, err, st) \
+                                       : launch_n<NN, false, true>(cd, x, w, bias, y, err, st); \
+        return cd.relu ? launch_n<NN, true, false>(cd, x, w, bias, y, err, st)            \
+                       : launch_n<NN, false, false>(cd, x, w, bias, y, err, st);          \
+    }
+    BLZ_CONV_CASE(16)
+    BLZ_CONV_CASE(32)
+    BLZ_CONV_CASE(64)
+    BLZ_CONV_CASE(128)
+#undef BLZ_CONV_CASE
+    return cudaErrorInvalidValue;
+}
+
+} // namespace blz
+
+namespace {
+__device__ int g_conv_timeout;          // set by a convolution whose MMA wait gave up
+}
+
+extern "C" int blz_conv3d(const blz_conv_desc *d, const void *x, const void *w, const float *bias, void *y,
+                          void *cuda_stream) {
+    using namespace blz;
+    if (!d || !x || !w || !bias || !y) return BLZ_ERR_ARG;
+    if (d->W < 1 || d->H < 1 || d->D < 1 || d->cin <= 0 || d->cin % 16 ||
+        (d->cout != 16 && d->cout != 32 && d->cout != 64 && d->cout != 128)) {
+        set_thread_error("blz_conv3d: need cin % 16 == 0 and cout in {16, 32, 64, 128}");
+        return BLZ_ERR_ARG;
+    }
+    int *flag = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void **)&flag, g_conv_timeout);
+    if (e == cudaSuccess) e = cudaMemsetAsync(flag, 0, sizeof(int), (cudaStream_t)cuda_stream);
+    const ConvDesc cd{d->W, d->H, d->D, d->cin, d->cout, d->relu, d->out_f32};
+    if (e == cudaSuccess)
+        e = launch_conv3d(cd, static_cast<const __nv_bfloat16 *>(x), static_cast<const __nv_bfloat16 *>(w), bias, y,
+                          flag, (cudaStream_t)cuda_stream);
+    int timeout = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&timeout, flag, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)cuda_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)cuda_stream);
+    if (e != cudaSuccess) {
+        set_thread_error(cudaGetErrorString(e));
+        return BLZ_ERR_CUDA;
+    }
+    if (timeout) {
+        set_thread_error("blz_conv3d: tensor-core completion wait timed out");
+        return BLZ_ERR_TIMEOUT;
+    }
+    return BLZ_OK;
+}

@@ -84,6 +84,7 @@ class SceneSettings:
     temporal_block: int = 0
     device_loop: int = 1
     sweep_variant: int = -1
+    advect_scheme: int = _abi.BLZ_ADVECT_RK3
     extra: dict = field(default_factory=dict)
 
     def to_params(self):
@@ -104,6 +105,7 @@ class SceneSettings:
         p.bc_mode, p.gs_order, p.reset_pressure = self.bc_mode, self.gs_order, self.reset_pressure
         p.max_particles, p.temporal_block = self.sourceMaxParticleCount, self.temporal_block
         p.device_loop, p.sweep_variant = self.device_loop, self.sweep_variant
+        p.advect_scheme = self.advect_scheme
         return p
 
 

@@ -112,7 +112,14 @@ typedef struct blz_params {
                                      multiple of check_every                 */
     int    sweep_variant;         /* -1: autotune the sweep launch shape per
                                      grid size (first solve); >= 0: force one */
+    int    advect_scheme;         /* BLZ_ADVECT_*: backtrace integrator       */
 } blz_params;
+
+/* Backtrace integrators (FluidSolver.cu:392-456; the reference's step uses
+ * RK3, the other two kernels exist there but are never launched).          */
+#define BLZ_ADVECT_RK3    0
+#define BLZ_ADVECT_EULER  1
+#define BLZ_ADVECT_RK2    2
 
 /* ---- per-step statistics ------------------------------------------------- */
 typedef struct blz_step_stats {
@@ -128,6 +135,8 @@ typedef struct blz_step_stats {
     int    residual_checks;       /* FP64 residual evaluations in the solve  */
     int    sweep_variant;         /* sweep launch shape used (-1: one-cell)   */
     int    device_loop;           /* 1 if the solve ran as a device loop      */
+    float  ms_checks;             /* device-loop solve: time inside the FP64
+                                     residual checks (device global timer)   */
 } blz_step_stats;
 
 typedef struct blz_solver blz_solver;

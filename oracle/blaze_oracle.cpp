@@ -747,11 +747,19 @@ static void advect_field(const Geo<R> &g, const Field<R> &U, const Field<R> &V, 
                 const R px = (R(i) + src.ox) * dx, py = (R(j) + src.oy) * dx, pz = (R(k) + src.oz) * dx;
                 const V3<R> k1 = vel_at(g, U, V, W, px, py, pz);
                 const R h1 = R(0.5) * dt, h2 = R(0.75) * dt;
-                const V3<R> k2 = vel_at(g, U, V, W, px - h1 * k1.x, py - h1 * k1.y, pz - h1 * k1.z);
-                const V3<R> k3 = vel_at(g, U, V, W, px - h2 * k2.x, py - h2 * k2.y, pz - h2 * k2.z);
-                const R qx = px - dt * (a * k1.x + b * k2.x + c * k3.x);
-                const R qy = py - dt * (a * k1.y + b * k2.y + c * k3.y);
-                const R qz = pz - dt * (a * k1.z + b * k2.z + c * k3.z);
+                R qx, qy, qz;
+                if (g.P->advect_scheme == BLZ_ADVECT_EULER) {       // FluidSolver.cu:392-407
+                    qx = px - dt * k1.x; qy = py - dt * k1.y; qz = pz - dt * k1.z;
+                } else if (g.P->advect_scheme == BLZ_ADVECT_RK2) {  // FluidSolver.cu:409-429
+                    const V3<R> m = vel_at(g, U, V, W, px - h1 * k1.x, py - h1 * k1.y, pz - h1 * k1.z);
+                    qx = px - dt * m.x; qy = py - dt * m.y; qz = pz - dt * m.z;
+                } else {                                            // FluidSolver.cu:431-456
+                    const V3<R> k2 = vel_at(g, U, V, W, px - h1 * k1.x, py - h1 * k1.y, pz - h1 * k1.z);
+                    const V3<R> k3 = vel_at(g, U, V, W, px - h2 * k2.x, py - h2 * k2.y, pz - h2 * k2.z);
+                    qx = px - dt * (a * k1.x + b * k2.x + c * k3.x);
+                    qy = py - dt * (a * k1.y + b * k2.y + c * k3.y);
+                    qz = pz - dt * (a * k1.z + b * k2.z + c * k3.z);
+                }
                 dst[(size_t)i + (size_t)src.w * ((size_t)j + (size_t)src.h * k)] =
                     tricubic(src, dx, qx, qy, qz, clamp);
             }

@@ -176,8 +176,9 @@ def test_gradient(bc, bounds):
     assert_close(gpu, ref, ("U", "V", "W"))
 
 
-def test_advect():
-    gpu, ref = pair(scene(), 81)
+@pytest.mark.parametrize("scheme", [0, 1, 2], ids=["rk3", "euler", "rk2"])
+def test_advect(scheme):
+    gpu, ref = pair(scene(advect_scheme=scheme), 81)
     gpu.advect()
     ref.advect()
     assert_close(gpu, ref, ("T", "U", "V", "W"))
@@ -289,3 +290,18 @@ def test_fixed_sweeps_match_oracle():
     gpu.sweeps(12)
     ref.gs_sweeps(12)
     assert_close(gpu, ref, ("P",), rel=2e-5, absol=2e-4)
+
+
+def test_sweep_variants_identical_full_width_rows():
+    """W = 256: a warp spans a whole packed row (32 segments of 4)."""
+    ref = None
+    for v in range(6):
+        gpu, _ = pair(scene(dims=(256, 6, 8), bc_mode=BLZ_BC_FREE_SURFACE, sweep_variant=v), 67)
+        gpu.sweeps(5)
+        p = gpu.get("P")
+        gpu.close()
+        assert np.isfinite(p).all()
+        if ref is None:
+            ref = p
+        else:
+            np.testing.assert_array_equal(p, ref, err_msg=f"variant {v}")

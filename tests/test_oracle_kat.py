@@ -68,12 +68,14 @@ def test_divergence_of_linear_field(oracle_mod):
     np.testing.assert_allclose(st2.RHS[1:-1, 1:-1, 0], want, rtol=1e-12)
 
 
-def test_advection_uniform_flow_shifts_cubic_exactly(oracle_mod):
-    """RK3 in a uniform field backtraces by exactly dt*u, and the Lagrange
-    tricubic reproduces a cubic polynomial: T(x) -> T(x - dt*u) in the
-    interior (Grid.h:148-222, FluidSolver.cu:431-456)."""
+@pytest.mark.parametrize("scheme", [0, 1, 2], ids=["rk3", "euler", "rk2"])
+def test_advection_uniform_flow_shifts_cubic_exactly(oracle_mod, scheme):
+    """RK3, forward Euler and RK2 in a uniform field all backtrace by exactly
+    dt*u, and the Lagrange tricubic reproduces a cubic polynomial:
+    T(x) -> T(x - dt*u) in the interior (Grid.h:148-222,
+    FluidSolver.cu:392-456)."""
     n = (24, 20, 18)
-    p = params(n)
+    p = params(n, advect_scheme=scheme)
     st = oracle_mod.State(p)
     W, H, D = n
     u0, v0, w0 = 0.9, -0.6, 0.4                     # cells moved: dt*u/dx < 1
