@@ -134,12 +134,22 @@ def read_part(path):
 # ---------------------------------------------------------------------------
 # Seeded synthetic scenes
 # ---------------------------------------------------------------------------
+# Particle pscale in cells.  The reference sums overlapping cubic pulses of
+# radius pscale/2 (Grid.h:309-335), so the splatted temperature of a ball of
+# particles is roughly (particles per cell) x (pulse volume) x (mean pulse
+# weight 0.2).  At the configs' density (2000 particles in a ball of radius 6
+# cells, 2.2 per cell) 1.5 cells gives a splatted temperature of about 1, the
+# configured source value; 4 cells would give about 25 and a far stronger
+# buoyancy than the scene describes.
+PSCALE_CELLS = 1.5
+
+
 def _cell_to_world(s, c):
     """World position of grid-cell coordinates given with y up (world axes)."""
     return [s.domainBboxMin[a] + c[a] * s.dx for a in range(3)]
 
 
-def sphere_particles(rng, s, centre_cells, radius_cells, count, temp=(1.0, 1.0), pscale_cells=4.0):
+def sphere_particles(rng, s, centre_cells, radius_cells, count, temp=(1.0, 1.0), pscale_cells=PSCALE_CELLS):
     """`count` particles uniform in a ball (rejection sampling), velocity 0."""
     cx, cy, cz = _cell_to_world(s, centre_cells)
     r = radius_cells * s.dx
@@ -155,7 +165,7 @@ def sphere_particles(rng, s, centre_cells, radius_cells, count, temp=(1.0, 1.0),
     return out
 
 
-def disc_particles(rng, s, centre_cells, radius_cells, count, temp=(1.0, 1.0), pscale_cells=4.0,
+def disc_particles(rng, s, centre_cells, radius_cells, count, temp=(1.0, 1.0), pscale_cells=PSCALE_CELLS,
                    thickness_cells=2.0):
     """`count` particles uniform in a horizontal disc (world y up)."""
     cx, cy, cz = _cell_to_world(s, centre_cells)
