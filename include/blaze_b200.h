@@ -201,6 +201,28 @@ void *blz_field_ptr(blz_solver *s, int field);
  * the host array out.  Lets callers check the noise without a solver.       */
 int  blz_perlin(const float *pos3, int n, float scale, int seed, float *out);
 
+/* ---- learned warm start: building blocks --------------------------------- */
+/* Activation tensors of the warm-start network are BF16, channels last, with a
+ * one-voxel zero halo: element (x,y,z,c) of a W x H x D x C tensor is at
+ * ((((z+1)*(H+2) + (y+1))*(W+2) + (x+1))*C + c), and BLZ_CONV_SLACK zero
+ * voxels precede and follow the (W+2)(H+2)(D+2) voxels.  No counterpart in
+ * the reference (it has no learned components).                             */
+#define BLZ_CONV_SLACK 256
+typedef struct blz_conv_desc {
+    int W, H, D;          /* interior voxels                                  */
+    int cin, cout;        /* cin % 16 == 0; cout in {16, 32, 64, 128}         */
+    int relu;             /* apply max(0, .) after the bias                   */
+    int out_f32;          /* output FP32 instead of BF16 (same layout)        */
+} blz_conv_desc;
+
+/* y = conv3x3x3(x, w) + bias on the tcgen05 tensor cores (BF16 operands, FP32
+ * accumulation in tensor memory).  x, y: device tensors in the layout above
+ * (pointers to the first voxel, after the slack); w: device BF16
+ * [27][cout][cin] with tap = (dz+1)*9 + (dy+1)*3 + (dx+1); bias: device FP32
+ * [cout].  Only interior voxels of y are written.  cuda_stream may be NULL.  */
+int  blz_conv3d(const blz_conv_desc *d, const void *x, const void *w, const float *bias, void *y,
+                void *cuda_stream);
+
 /* Number of kernels this solver launched since creation.                    */
 long long blz_kernel_launches(const blz_solver *s);
 
