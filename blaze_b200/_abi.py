@@ -114,6 +114,7 @@ EXPORTS = {
     "blz_field_size": (C.c_size_t, [C.c_void_p, C.c_int]),
     "blz_field_ptr": (C.c_void_p, [C.c_void_p, C.c_int]),
     "blz_perlin": (C.c_int, [_P(C.c_float), C.c_int, C.c_float, C.c_int, _P(C.c_float)]),
+    "blz_residual_noalloc": (C.c_int, [_P(BlzParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "blz_conv3d": (C.c_int, [_P(BlzConvDesc), C.c_void_p, C.c_void_p, _P(C.c_float), C.c_void_p, C.c_void_p]),
     "blz_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "blz_last_error": (C.c_char_p, [C.c_void_p]),

@@ -201,6 +201,23 @@ void *blz_field_ptr(blz_solver *s, int field);
  * the host array out.  Lets callers check the noise without a solver.       */
 int  blz_perlin(const float *pos3, int n, float scale, int seed, float *out);
 
+/* FP64 residual norms without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc (a host
+ * application or plugin host that owns all device memory through its own
+ * pool, or code that must not let an allocation synchronise the device).
+ * Inputs are the caller's device arrays rhs and p in the reference layout
+ * (T dims, as blz_get_field returns them); out2_dev receives {||b - A p||_2,
+ * ||b||_2} (2 device doubles, b = rho dx^2/dt * rhs, A and the boundary
+ * handling as in blz_params), on cuda_stream (NULL: the legacy default
+ * stream).  Its scratch is a static 64 KiB device array (one FP64 pair per
+ * z-plane), so depth must be <= 4096; larger grids return BLZ_ERR_ARG.
+ * The first call on each device looks up that array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU (other streams or
+ * threads) race and must be serialised by the caller.                      */
+int  blz_residual_noalloc(const blz_params *p, const float *rhs_dev, const float *p_dev,
+                          double *out2_dev, void *cuda_stream);
+
 /* ---- learned warm start: building blocks --------------------------------- */
 /* Activation tensors of the warm-start network are BF16, channels last, with a
  * one-voxel zero halo: element (x,y,z,c) of a W x H x D x C tensor is at
