@@ -31,7 +31,7 @@ METRIC = "256³ steps/s: learned warm-start vs plain RBGS at equal residual; HBM
 GRID = 256
 SEED = 3
 TOL = 1e-4
-MAX_ITER = 12000
+MAX_ITER = 40000
 CHECK_EVERY = 20
 # Sweeps per frame the reference arm runs (maxIterSolve): the mean the plain
 # RBGS step needs on this scene and frame window, measured on a B200.
@@ -142,6 +142,8 @@ def run_ours(args, ws, rank, local):
 
     torch.cuda.set_device(local)
     scn, parts = family_scene(n=args.grid, seed=SEED + rank, tol=TOL, max_iter=args.max_iter, check_every=CHECK_EVERY)
+    if args.host_loop:
+        scn.device_loop = 0
     W, H, D = scn.gridRes
     # A dedicated stream shared by the solver and the timing events (the
     # legacy default stream has handle 0, which the library reads as "use
@@ -343,6 +345,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) pass")
     ap.add_argument("--max-iter", type=int, default=MAX_ITER, help="GS sweep cap per frame (profiling runs)")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="drive the convergence loop from the host (every kernel a separate launch, for launch lists)")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":

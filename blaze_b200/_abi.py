@@ -77,6 +77,7 @@ class BlzStepStats(C.Structure):
         ("ms_solve", C.c_float), ("ms_gradient", C.c_float), ("ms_advect", C.c_float),
         ("ms_total", C.c_float), ("ms_sweeps", C.c_float), ("residual_checks", C.c_int),
         ("sweep_variant", C.c_int), ("device_loop", C.c_int), ("ms_checks", C.c_float),
+        ("ms_warm_start", C.c_float), ("warm_started", C.c_int),
     ]
 
     def as_dict(self):
@@ -116,6 +117,21 @@ EXPORTS = {
     "blz_perlin": (C.c_int, [_P(C.c_float), C.c_int, C.c_float, C.c_int, _P(C.c_float)]),
     "blz_residual_noalloc": (C.c_int, [_P(BlzParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "blz_conv3d": (C.c_int, [_P(BlzConvDesc), C.c_void_p, C.c_void_p, _P(C.c_float), C.c_void_p, C.c_void_p]),
+    "blz_unet_layer_info": (C.c_int, [C.c_int, _P(C.c_longlong)]),
+    "blz_unet_create": (C.c_int, [C.c_int, C.c_int, C.c_int, _P(C.c_void_p)]),
+    "blz_unet_destroy": (C.c_int, [C.c_void_p]),
+    "blz_unet_num_params": (C.c_longlong, [C.c_void_p]),
+    "blz_unet_kernel_launches": (C.c_longlong, [C.c_void_p]),
+    "blz_unet_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "blz_unet_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "blz_unet_get_grads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "blz_unet_set_kappa": (C.c_int, [C.c_void_p, C.c_float]),
+    "blz_unet_forward": (C.c_int, [C.c_void_p, _P(BlzParams), _P(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]),
+    "blz_unet_loss_grad": (C.c_int, [C.c_void_p, _P(BlzParams), _P(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p,
+                                     _P(C.c_double), C.c_void_p]),
+    "blz_unet_adam": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]),
+    "blz_set_warm_start": (C.c_int, [C.c_void_p, C.c_void_p]),
     "blz_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "blz_last_error": (C.c_char_p, [C.c_void_p]),
 }

@@ -100,16 +100,31 @@ struct ConvDesc {
     int W, H, D;        // interior voxels (tensors carry a 1-voxel zero halo)
     int cin, cout;      // cin % 16 == 0; cout in {16, 32, 64, 128}
     int relu, out_f32;
+    int out_stride;     // channels per output voxel (>= cout; 0: cout)
+    int out_offset;     // first output channel written (multiple of 8)
 };
 int conv3d_smem_bytes(int cout);
 }  // namespace blz
 #include <cuda_bf16.h>
 namespace blz {
+// bias may be null; aux (BF16, same layout as y) masks the output to the
+// voxels and channels where aux > 0 (the backward pass of a ReLU).
 cudaError_t launch_conv3d(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
-                          void *y, int *err, cudaStream_t st);
+                          void *y, int *err, cudaStream_t st, const __nv_bfloat16 *aux = nullptr);
 
 // Sets the calling thread's error text (what blz_last_error(NULL) returns).
 void set_thread_error(const char *msg);
+
+// Solve parameters (scale, open faces, Dirichlet ghosts) of a parameter block.
+SolveParams solve_params_of(const blz_params &P);
+
+// Learned warm start (unet.cu): p := p + kappa rms(r) net(b, mask, p, r) on the
+// colour-packed pressure, ordered on st; adds its launches to *launches.
+int unet_warm_start(blz_unet *u, const blz_params &P, const float *rhs_r, const float *rhs_b, float *p_r,
+                    float *p_b, cudaStream_t st, long long *launches);
+// BLZ_ERR_TIMEOUT if a tensor-core completion wait of the last warm start
+// gave up (synchronises st).
+int unet_timeout_flag(blz_unet *u, cudaStream_t st);
 
 // -- advection ------------------------------------------------------------------
 void launch_advect(const Geom &g, const float *T, const float *U, const float *V, const float *W,

@@ -40,8 +40,9 @@ struct blz_solver {
     double *partials = nullptr;
     int n_partials = 0;
     double *d_norm2 = nullptr, *h_norm2 = nullptr;
-    cudaEvent_t ev[8]{};
+    cudaEvent_t ev[10]{};
     long long launches = 0;
+    blz_unet *warm = nullptr;                   // learned warm start (caller owned)
     int variant = -2;                           // sweep launch shape (-2: not chosen yet)
     // device-loop solve: instantiated graph and its control block
     cudaGraphExec_t solve_exec = nullptr;
@@ -106,6 +107,10 @@ static SolveParams solve_params(const blz_params &P) {
     sp.dirichlet = P.bc_mode == BLZ_BC_FREE_SURFACE;
     return sp;
 }
+
+namespace blz {
+SolveParams solve_params_of(const blz_params &P) { return solve_params(P); }
+} // namespace blz
 
 extern "C" {
 
@@ -545,6 +550,8 @@ static int solve_device_loop(blz_solver *s, blz_step_stats *st) {
     return BLZ_OK;
 }
 
+static int solve_body(blz_solver *s, blz_step_stats *st);
+
 int blz_solve(blz_solver *s, blz_step_stats *st) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     const blz_params &P = s->P;
@@ -553,6 +560,42 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
         CK(s, cudaMemsetAsync(s->p_r, 0, half * sizeof(float), s->st));
         CK(s, cudaMemsetAsync(s->p_b, 0, half * sizeof(float), s->st));
     }
+    if (s->warm) {
+        CK(s, cudaEventRecord(s->ev[8], s->st));
+        const int rc = unet_warm_start(s->warm, P, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->st, &s->launches);
+        if (rc != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
+        CK(s, cudaEventRecord(s->ev[9], s->st));
+    }
+    int rc = solve_body(s, st);
+    if (rc != BLZ_OK) return rc;
+    if (s->warm) {
+        if ((rc = unet_timeout_flag(s->warm, s->st)) != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
+        if (st) {
+            float t = 0.0f;
+            CK(s, cudaEventElapsedTime(&t, s->ev[8], s->ev[9]));
+            st->ms_warm_start = t;
+            st->warm_started = 1;
+        }
+    } else if (st) {
+        st->ms_warm_start = 0.0f;
+        st->warm_started = 0;
+    }
+    return BLZ_OK;
+}
+
+int blz_set_warm_start(blz_solver *s, blz_unet *u) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    if (u) {
+        if (blz_unet_num_params(u) <= 0) return fail(s, BLZ_ERR_ARG, "bad network");
+        if (s->P.width % 8 || s->P.height % 8 || s->P.depth % 8)
+            return fail(s, BLZ_ERR_ARG, "the warm start needs grid dims that are multiples of 8");
+    }
+    s->warm = u;
+    return BLZ_OK;
+}
+
+static int solve_body(blz_solver *s, blz_step_stats *st) {
+    const blz_params &P = s->P;
     const int chunk_sz = std::max(1, P.check_every);
     if (P.device_loop && P.tol > 0.0 && P.gs_order == BLZ_GS_RB3D && P.max_iter % chunk_sz == 0)
         return solve_device_loop(s, st);

@@ -71,9 +71,9 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, int *e
 
 template <int N, bool RELU, bool OUT_F32>
 __global__ void __launch_bounds__(128)
-k_conv3d_tc(int W, int H, int D, int cin, int cout_stride, const __nv_bfloat16 *__restrict__ x,
+k_conv3d_tc(int W, int H, int D, int cin, int out_stride, int out_offset, const __nv_bfloat16 *__restrict__ x,
             const __nv_bfloat16 *__restrict__ w, const float *__restrict__ bias, void *__restrict__ y,
-            int *err) {
+            const __nv_bfloat16 *__restrict__ aux, int *err) {
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *sA = smem;
     unsigned char *sB = smem + kABytes;
@@ -164,18 +164,32 @@ k_conv3d_tc(int W, int H, int D, int cin, int cout_stride, const __nv_bfloat16 *
                 float v[16];
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
-                    v[q] = __uint_as_float(r[q]) + __ldg(bias + n0 + q);
+                    v[q] = __uint_as_float(r[q]) + (bias ? __ldg(bias + n0 + q) : 0.0f);
                     if (RELU) v[q] = fmaxf(v[q], 0.0f);
                 }
+                const long long o = outv * out_stride + out_offset + n0;
+                if (aux) {
+                    // Backward through a ReLU: keep the gradient where the
+                    // forward activation was positive.
+                    const uint4 a0 = __ldg(reinterpret_cast<const uint4 *>(aux + o));
+                    const uint4 a1 = __ldg(reinterpret_cast<const uint4 *>(aux + o) + 1);
+                    const __nv_bfloat16 *ah0 = reinterpret_cast<const __nv_bfloat16 *>(&a0);
+                    const __nv_bfloat16 *ah1 = reinterpret_cast<const __nv_bfloat16 *>(&a1);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        if (!(__bfloat162float(ah0[q]) > 0.0f)) v[q] = 0.0f;
+                        if (!(__bfloat162float(ah1[q]) > 0.0f)) v[8 + q] = 0.0f;
+                    }
+                }
                 if (OUT_F32) {
-                    float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(y) + outv * cout_stride + n0);
+                    float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(y) + o);
 #pragma unroll
                     for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
                 } else {
                     __nv_bfloat162 h[8];
 #pragma unroll
                     for (int q = 0; q < 8; ++q) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
-                    uint4 *dst = reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(y) + outv * cout_stride + n0);
+                    uint4 *dst = reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(y) + o);
                     dst[0] = *reinterpret_cast<uint4 *>(&h[0]);
                     dst[1] = *reinterpret_cast<uint4 *>(&h[4]);
                 }
@@ -192,25 +206,29 @@ int conv3d_smem_bytes(int cout) { return kABytes + 27 * cout * 32; }
 
 template <int N, bool RELU, bool F32>
 static cudaError_t launch_n(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
-                            void *y, int *err, cudaStream_t st) {
+                            void *y, const __nv_bfloat16 *aux, int *err, cudaStream_t st) {
     const int smem = conv3d_smem_bytes(N);
     cudaError_t e = cudaFuncSetAttribute(k_conv3d_tc<N, RELU, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const long long interior = (long long)(cd.W + 2) * cd.H;
     const dim3 grid((unsigned)((interior + kConvM - 1) / kConvM), (unsigned)cd.D);
-    k_conv3d_tc<N, RELU, F32><<<grid, 128, smem, st>>>(cd.W, cd.H, cd.D, cd.cin, cd.cout, x, w, bias, y, err);
+    const int os = cd.out_stride > 0 ? cd.out_stride : cd.cout;
+    k_conv3d_tc<N, RELU, F32><<<grid, 128, smem, st>>>(cd.W, cd.H, cd.D, cd.cin, os, cd.out_offset, x, w, bias, y,
+                                                        aux, err);
     return cudaGetLastError();
 }
 
 cudaError_t launch_conv3d(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
-                          void *y, int *err, cudaStream_t st) {
-    if (cd.cin % 16 || cd.cin <= 0) return cudaErrorInvalidValue;
-#define BLZ_CONV_CASE(NN)                                                                  \
-    if (cd.cout == NN) {                                                                   \
-        if (cd.out_f32) return cd.relu ? launch_n<NN, true, true>(cd, x, w, bias, y, err, st) \
-                                       : launch_n<NN, false, true>(cd, x, w, bias, y, err, st); \
-        return cd.relu ? launch_n<NN, true, false>(cd, x, w, bias, y, err, st)            \
-                       : launch_n<NN, false, false>(cd, x, w, bias, y, err, st);          \
+                          void *y, int *err, cudaStream_t st, const __nv_bfloat16 *aux) {
+    if (cd.cin % 16 || cd.cin <= 0 || cd.out_offset % 8 || (cd.out_stride > 0 && cd.out_stride % 8) ||
+        (aux && cd.out_f32))
+        return cudaErrorInvalidValue;
+#define BLZ_CONV_CASE(NN)                                                                        \
+    if (cd.cout == NN) {                                                                         \
+        if (cd.out_f32) return cd.relu ? launch_n<NN, true, true>(cd, x, w, bias, y, aux, err, st) \
+                                       : launch_n<NN, false, true>(cd, x, w, bias, y, aux, err, st); \
+        return cd.relu ? launch_n<NN, true, false>(cd, x, w, bias, y, aux, err, st)             \
+                       : launch_n<NN, false, false>(cd, x, w, bias, y, aux, err, st);          \
     }
     BLZ_CONV_CASE(16)
     BLZ_CONV_CASE(32)
@@ -238,7 +256,7 @@ extern "C" int blz_conv3d(const blz_conv_desc *d, const void *x, const void *w, 
     int *flag = nullptr;
     cudaError_t e = cudaGetSymbolAddress((void **)&flag, g_conv_timeout);
     if (e == cudaSuccess) e = cudaMemsetAsync(flag, 0, sizeof(int), (cudaStream_t)cuda_stream);
-    const ConvDesc cd{d->W, d->H, d->D, d->cin, d->cout, d->relu, d->out_f32};
+    const ConvDesc cd{d->W, d->H, d->D, d->cin, d->cout, d->relu, d->out_f32, d->cout, 0};
     if (e == cudaSuccess)
         e = launch_conv3d(cd, static_cast<const __nv_bfloat16 *>(x), static_cast<const __nv_bfloat16 *>(w), bias, y,
                           flag, (cudaStream_t)cuda_stream);

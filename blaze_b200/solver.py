@@ -132,3 +132,10 @@ class FluidSolver:
 
     def kernel_launches(self):
         return self._lib.blz_kernel_launches(self._h)
+
+    # -- learned warm start ---------------------------------------------------------------
+    def set_warm_start(self, net):
+        """Attach a WarmStartUNet (dims equal to the grid's) or detach with
+        None; the solver keeps a reference so the network outlives it."""
+        check(self._lib.blz_set_warm_start(self._h, net.handle if net is not None else None), self._h)
+        self._warm = net

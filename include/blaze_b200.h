@@ -137,6 +137,9 @@ typedef struct blz_step_stats {
     int    device_loop;           /* 1 if the solve ran as a device loop      */
     float  ms_checks;             /* device-loop solve: time inside the FP64
                                      residual checks (device global timer)   */
+    float  ms_warm_start;         /* device time of the learned warm start
+                                     (inside ms_solve; 0 without a network)  */
+    int    warm_started;          /* 1 if a network set the initial pressure  */
 } blz_step_stats;
 
 typedef struct blz_solver blz_solver;
@@ -239,6 +242,53 @@ typedef struct blz_conv_desc {
  * [cout].  Only interior voxels of y are written.  cuda_stream may be NULL.  */
 int  blz_conv3d(const blz_conv_desc *d, const void *x, const void *w, const float *bias, void *y,
                 void *cuda_stream);
+
+/* ---- learned warm start: the network -------------------------------------- */
+/* A 4-level 3-D U-Net (channels 16/32/64/128; per level two 3x3x3 convolutions
+ * with ReLU; 2x2x2 average pooling; 2x2x2 stride-2 transposed convolutions;
+ * skip concatenation [upsampled, skip]; a 1x1x1 head), BF16 activations, FP32
+ * accumulation.  It maps, per cell, b = rho dx^2/dt * rhs, a Neumann-ghost
+ * indicator, the previous pressure p and the residual r = b - A p (each over
+ * its FP64 rms on the whole grid) to delta, and the warm start is
+ * p + kappa * rms(r) * delta.  Parameters are one FP32 array; layer l's
+ * weights start at info[4] and its bias at info[5] (blz_unet_layer_info).
+ * Weights of a 3x3x3 layer are [27][cout][cin] (tap as in blz_conv3d), of a
+ * transposed convolution [8][cout][cin] (parity a + 2b + 4c for the fine
+ * voxel (2x+a, 2y+b, 2z+c)), of the head [1][1][16].  Layer order: encoder
+ * e0a e0b e1a e1b e2a e2b e3a e3b, decoder d2a d2b d1a d1b d0a d0b, transposed
+ * u2 u1 u0, head.                                                            */
+typedef struct blz_unet blz_unet;
+
+/* info = {kind (0: 3x3x3, 1: transposed 2x2x2, 2: head), cin, cout, taps,
+ * weight offset, bias offset}; BLZ_ERR_ARG past the last layer.             */
+int  blz_unet_layer_info(int layer, long long info[6]);
+/* Network for a width x height x depth crop (each a positive multiple of 8),
+ * with all activations allocated on the current device; parameters zero.   */
+int  blz_unet_create(int width, int height, int depth, blz_unet **out);
+int  blz_unet_destroy(blz_unet *u);
+long long blz_unet_num_params(const blz_unet *u);
+long long blz_unet_kernel_launches(const blz_unet *u);
+int  blz_unet_set_params(blz_unet *u, const float *params, int on_device);   /* resets Adam */
+int  blz_unet_get_params(const blz_unet *u, float *params, int on_device);
+int  blz_unet_get_grads(const blz_unet *u, float *grads, int on_device);
+int  blz_unet_set_kappa(blz_unet *u, float kappa);
+/* Raw network output delta over the crop [origin, origin + dims) of the grid
+ * that grid describes (dims and boundary handling), from device arrays rhs
+ * and p in the reference layout; out: device FP32, crop dims, x fastest.    */
+int  blz_unet_forward(blz_unet *u, const blz_params *grid, const int origin[3], const float *rhs,
+                      const float *p, float *out, void *cuda_stream);
+/* Loss and gradients of one training sample: L = mean over the crop of
+ * (delta - (p_target - p) / (kappa rms(r)))^2.  Fills the parameter
+ * gradients and loss[0] = L, loss[1] = mean target^2; synchronises.        */
+int  blz_unet_loss_grad(blz_unet *u, const blz_params *grid, const int origin[3], const float *rhs,
+                        const float *p, const float *p_target, double loss[2], void *cuda_stream);
+/* One Adam step (bias-corrected) with the gradients of the last loss_grad.  */
+int  blz_unet_adam(blz_unet *u, float lr, float beta1, float beta2, float eps, void *cuda_stream);
+/* Attach (or, with NULL, detach) a network whose dims equal the grid's: every
+ * later solve of s starts from the network's warm start of the current
+ * pressure and then sweeps to the same residual target.  The network stays
+ * owned by the caller and must outlive the attachment.                     */
+int  blz_set_warm_start(blz_solver *s, blz_unet *u);
 
 /* Number of kernels this solver launched since creation.                    */
 long long blz_kernel_launches(const blz_solver *s);

@@ -65,3 +65,152 @@ def test_conv3d_tensor_cores(shape, cin, cout, relu, out_f32):
     assert err <= tol[0] and mx <= tol[1], (float(err), float(mx))
     # the halo stays zero
     assert float(yv[0].abs().max()) == 0.0 and float(yv[:, :, 0].abs().max()) == 0.0
+
+
+# ---------------------------------------------------------------------------
+# The warm-start network against the FP64 oracle with BF16 rounding emulated
+# at the GPU's storage points (oracle/unet_oracle.py).  What remains is FP32
+# (tensor memory) versus FP64 accumulation, plus the rare BF16 rounding that
+# flips because of it: tolerances below are relative L2 per tensor.
+# ---------------------------------------------------------------------------
+def _grid(W, H, D, bc=1):
+    from blaze_b200.scenes import SceneSettings
+    return SceneSettings(gridRes=(W, H, D), dx=1.0 / W, closedBounds=(1, 1, 1, 0, 1, 1), bc_mode=bc).to_params()
+
+
+def _net_params(seed):
+    from oracle import unet_oracle as uo
+    rng = np.random.default_rng(seed)
+    lay, n = uo.layout()
+    p = np.zeros(n, np.float32)
+    for name, (kind, cin, cout, taps, wo, bo) in lay.items():
+        fan = taps * cin if kind != uo.UP else cin
+        p[wo:bo] = rng.standard_normal(bo - wo) * np.sqrt(2.0 / fan)
+        p[bo:bo + cout] = 0.05 * rng.standard_normal(cout)
+    return p
+
+
+def _fields(W, H, D, seed):
+    rng = np.random.default_rng(seed)
+    rhs = rng.standard_normal((D, H, W)).astype(np.float32)
+    p = (0.5 * rng.standard_normal((D, H, W))).astype(np.float32)
+    pt = p + (0.2 * rng.standard_normal((D, H, W))).astype(np.float32)
+    return rhs, p, pt
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("grid_dims,crop,origin,bc", [
+    ((16, 16, 16), (16, 16, 16), (0, 0, 0), 1),
+    ((24, 16, 16), (16, 8, 16), (8, 4, 0), 1),
+    ((16, 16, 24), (16, 16, 16), (0, 0, 8), 0)])
+def test_unet_forward_matches_oracle(grid_dims, crop, origin, bc):
+    import torch
+    from oracle import unet_oracle as uo
+    from blaze_b200.unet import WarmStartUNet
+    W, H, D = grid_dims
+    g = _grid(W, H, D, bc)
+    rhs, p, _ = _fields(W, H, D, 1)
+    params = _net_params(2)
+    net = WarmStartUNet(crop, params, kappa=0.8)
+    got = net.forward(g, torch.from_numpy(rhs).cuda(), torch.from_numpy(p).cuda(), origin).cpu().numpy()
+    want = uo.forward(params, g, rhs, p, origin, crop, 0.8)
+    assert _rel(got, want) <= 2e-3, _rel(got, want)
+    net.close()
+
+
+def test_unet_gradients_match_oracle():
+    import torch
+    from oracle import unet_oracle as uo
+    from blaze_b200.unet import WarmStartUNet
+    W, H, D = 16, 16, 16
+    g = _grid(W, H, D)
+    rhs, p, pt = _fields(W, H, D, 3)
+    params = _net_params(4)
+    net = WarmStartUNet((W, H, D), params, kappa=0.5)
+    dev = lambda a: torch.from_numpy(a).cuda()
+    loss, t2 = net.loss_grad(g, dev(rhs), dev(p), dev(pt))
+    got = net.get_grads()
+    wl, wt2, want, _ = uo.loss_and_grads(params, g, rhs, p, pt, (0, 0, 0), (W, H, D), 0.5)
+    assert abs(loss - wl) <= 1e-3 * wl and abs(t2 - wt2) <= 1e-5 * wt2, (loss, wl, t2, wt2)
+    lay, _ = uo.layout()
+    errs = {}
+    for name, (kind, cin, cout, taps, wo, bo) in lay.items():
+        errs[name] = (_rel(got[wo:bo], want[wo:bo]), _rel(got[bo:bo + cout], want[bo:bo + cout]))
+    bad = {k: v for k, v in errs.items() if v[0] > 1e-2 or v[1] > 1e-2}
+    assert not bad, bad
+    # Adam against the same update in FP64
+    net.adam(1e-3)
+    new = net.get_params()
+    z = np.zeros_like(want)
+    ref, _, _ = uo.adam(params.astype(np.float64), got.astype(np.float64), z, z, 1, 1e-3)
+    assert np.abs(new - ref).max() <= 1e-6, np.abs(new - ref).max()
+    net.close()
+
+
+def test_unet_training_lowers_the_loss():
+    import torch
+    from blaze_b200.unet import WarmStartUNet, init_params
+    W, H, D = 16, 16, 16
+    g = _grid(W, H, D)
+    rhs, p, pt = _fields(W, H, D, 5)
+    net = WarmStartUNet((W, H, D), init_params(0))
+    dev = lambda a: torch.from_numpy(a).cuda()
+    r, pp, tt = dev(rhs), dev(p), dev(pt)
+    first = net.loss_grad(g, r, pp, tt)[0]
+    for _ in range(40):
+        net.adam(2e-3)
+        last = net.loss_grad(g, r, pp, tt)[0]
+    assert last < 0.5 * first, (first, last)
+    net.close()
+
+
+def test_warm_start_through_the_solver():
+    """blz_solve with a network attached starts from p + kappa rms(r) delta."""
+    import torch
+    from oracle import unet_oracle as uo
+    from blaze_b200 import FluidSolver, Timer
+    from blaze_b200.scenes import SceneSettings
+    from blaze_b200.unet import WarmStartUNet
+    W, H, D = 16, 16, 16
+    scn = SceneSettings(gridRes=(W, H, D), dx=1.0 / W, closedBounds=(1, 1, 1, 0, 1, 1), bc_mode=1,
+                        maxIterSolve=0, tol=0.0, device_loop=0)
+    rhs, p, _ = _fields(W, H, D, 7)
+    params = _net_params(8)
+    net = WarmStartUNet((W, H, D), params, kappa=0.6)
+    g = scn.to_params()
+    delta = net.forward(g, torch.from_numpy(rhs).cuda(), torch.from_numpy(p).cuda()).cpu().numpy()
+    so = uo.scales(g, rhs, p, 0.6)[3]
+    solver = FluidSolver(Timer(), scn)
+    solver.set("RHS", rhs)
+    solver.set("P", p)
+    solver.set_warm_start(net)
+    st = solver.solve()
+    assert st["warm_started"] == 1 and st["ms_warm_start"] > 0.0
+    got = solver.get("P")
+    want = p.astype(np.float64) + float(so) * delta
+    assert np.abs(got - want).max() <= 1e-5 * np.abs(want - p).max() + 1e-6
+    solver.set_warm_start(None)
+    solver.set("P", p)
+    st = solver.solve()
+    assert st["warm_started"] == 0 and np.array_equal(solver.get("P"), p)
+    solver.close()
+    net.close()
+
+
+def test_unet_rejects_bad_arguments():
+    import ctypes as C
+    from blaze_b200 import _lib
+    lib = _lib.load()
+    h = C.c_void_p()
+    assert lib.blz_unet_create(12, 16, 16, C.byref(h)) == -2
+    assert lib.blz_unet_create(16, 16, 16, C.byref(h)) == 0
+    g = _grid(16, 16, 16)
+    org = (C.c_int * 3)(8, 0, 0)
+    buf = C.c_void_p(1)
+    assert lib.blz_unet_forward(h, C.byref(g), org, buf, buf, buf, None) == -2     # crop leaves the grid
+    assert lib.blz_unet_get_grads(h, buf, 1) == -7                                 # no gradients yet
+    lib.blz_unet_destroy(h)
