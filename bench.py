@@ -1,11 +1,16 @@
 """Benchmark of the per-frame fluid step at 256^3 (plume-family scene).
 
 A step is one frame: particle sourcing + FluidSolver::step (forces,
-divergence, red-black Gauss-Seidel to relative FP64 residual 1e-4 warm-started
-from the previous frame's pressure, gradient, RK3 advection).  Prints one
-JSON line (rank 0).
+divergence, red-black Gauss-Seidel to relative FP64 residual 1e-4, gradient,
+RK3 advection).  After W warm-up frames the state is snapshotted and the same
+K frames are timed twice from it: plain (RBGS warm-started from the previous
+frame's pressure) and learned (the U-Net warm start of
+blaze_b200/weights/plume<N>.npz, then RBGS to the same residual).  `value`
+is the learned pass when those weights exist; both passes are in the line.
+Prints one JSON line (rank 0).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--plain-only] [--weights PATH]
 
 --impl reference times the reference's own CUDA build (oracle/_ref) on the
 same scene and particles through its FluidSolver API, with maxIterSolve equal
@@ -136,6 +141,18 @@ def cpu_baseline(scn, parts, mean_sweeps):
                       f"({per_sweep * 1e3:.1f} ms/sweep, {per_step:.1f} s/step)"}
 
 
+def _load_net(args, W, H, D):
+    """The trained warm-start network for this grid, or (None, reason)."""
+    from blaze_b200.unet import WarmStartUNet, weights_path
+    if args.plain_only:
+        return None, "disabled (--plain-only)"
+    path = args.weights or weights_path(f"plume{W}.npz")
+    if not os.path.exists(path):
+        return None, f"no trained weights for {W}^3 ({os.path.relpath(path, ROOT)})"
+    net = WarmStartUNet((W, H, D)).load(path)
+    return net, os.path.relpath(path, ROOT)
+
+
 def run_ours(args, ws, rank, local):
     import torch
     from blaze_b200 import FluidSolver, Timer, family_scene
@@ -152,6 +169,7 @@ def run_ours(args, ws, rank, local):
     torch.cuda.set_stream(stream)
     tmr = Timer()
     solver = FluidSolver(tmr, scn, particles=parts, stream=stream.cuda_stream)
+    net, net_src = _load_net(args, W, H, D)
 
     def frame():
         solver.addSource()
@@ -163,14 +181,24 @@ def run_ours(args, ws, rank, local):
     for _ in range(args.warmup):
         frame()
     torch.cuda.synchronize()
-    # State after warm-up, so that the end-to-end pass replays the same frames.
+    # State after warm-up: every timed pass below replays the same frames from it.
     snap = {f: solver.get(f) for f in ("T", "U", "V", "W", "P")}
     clock0 = (tmr.iter, tmr.time)
-    if ws > 1:
-        torch.distributed.barrier()
-    launches0 = solver.kernel_launches()
-    stats = []
-    with ClockSampler(local) as clk:
+
+    def restore():
+        for f, a in snap.items():
+            solver.set(f, a)
+        tmr.iter, tmr.time = clock0
+        torch.cuda.synchronize()
+
+    def timed_pass(learned):
+        """K frames from the snapshot; device time (max over ranks), stats, launches."""
+        restore()
+        solver.set_warm_start(net if learned else None)
+        if ws > 1:
+            torch.distributed.barrier()
+        l0 = solver.kernel_launches()
+        stats = []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
@@ -180,21 +208,23 @@ def run_ours(args, ws, rank, local):
         torch.cuda.synchronize()
         if ws > 1:
             torch.distributed.barrier()
-    ms = e0.elapsed_time(e1)
-    launches = solver.kernel_launches() - launches0
-    if ws > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    sweeps = np.array([s["iterations"] for s in stats], float)
-    checks = np.array([s["residual_checks"] for s in stats], float)
-    rel = np.array([s["rel_residual"] for s in stats], float)
-    ms_sweeps = float(sum(s["ms_sweeps"] for s in stats))
-    conv = all(s["converged"] for s in stats)
-    variant = stats[-1]["sweep_variant"]
-    device_loop = stats[-1]["device_loop"]
-    # The dominant kernel timed with CUDA events on this stream, on the state
-    # the timed region left (the e2e pass below restarts from the snapshot).
+        ms = e0.elapsed_time(e1)
+        if ws > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, stats, solver.kernel_launches() - l0
+
+    with ClockSampler(local) as clk:
+        ms_plain, st_plain, launches_plain = timed_pass(False)
+        if net is not None:
+            ms_learn, st_learn, launches_learn = timed_pass(True)
+    head_learned = net is not None
+    ms, stats, launches = (ms_learn, st_learn, launches_learn) if head_learned else (ms_plain, st_plain, launches_plain)
+
+    # The dominant kernel (half sweep) timed with CUDA events on this stream,
+    # on the state the timed passes left.
+    solver.set_warm_start(None)
     n_meas = 20
     m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     solver.sweeps(2)
@@ -209,9 +239,8 @@ def run_ours(args, ws, rank, local):
     # records go host->device (the reference re-reads an animated source every
     # frame) and the advanced temperature field comes back device->host.
     if not args.no_e2e:
-        for f, a in snap.items():
-            solver.set(f, a)
-        tmr.iter, tmr.time = clock0
+        restore()
+        solver.set_warm_start(net if head_learned else None)
         pinned_parts = torch.empty((len(parts), 8), dtype=torch.float32, pin_memory=True)
         pinned_parts.numpy()[...] = parts
         t_host = torch.empty(scn.to_params().field_shape("T"), dtype=torch.float32, pin_memory=True)
@@ -226,15 +255,36 @@ def run_ours(args, ws, rank, local):
             tmr.time += scn.dt
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - w0
-    if ws > 1 and e2e_s is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        if ws > 1:
+            t = torch.tensor([e2e_s], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = float(t.item())
+    solver.set_warm_start(None)
 
     if rank != 0:
+        solver.close()
         return None
     peak, peak_kind = load_peaks()
     n_cells = W * H * D
+
+    def summary(ms_, st_):
+        sw = np.array([s["iterations"] for s in st_], float)
+        ck = np.array([s["residual_checks"] for s in st_], float)
+        rel = np.array([s["rel_residual"] for s in st_], float)
+        out = {"steps_per_s": ws * args.steps / (ms_ * 1e-3), "ms_per_step": ms_ / args.steps,
+               "mean_sweeps": float(sw.mean()), "sweeps_per_frame": [int(x) for x in sw],
+               "max_rel_residual": float(rel.max()), "all_converged": all(s["converged"] for s in st_),
+               "hbm_gbs_step": float(np.mean([step_bytes(W, H, D, a, c) for a, c in zip(sw, ck)]))
+               / (ms_ / args.steps * 1e-3) / 1e9,
+               "stage_ms": {k: float(np.mean([s[k] for s in st_])) for k in
+                            ("ms_forces", "ms_divergence", "ms_solve", "ms_gradient", "ms_advect", "ms_sweeps",
+                             "ms_checks", "ms_warm_start")}}
+        return out
+
+    plain = summary(ms_plain, st_plain)
+    learned = summary(ms_learn, st_learn) if head_learned else None
+    sweeps = np.array([s["iterations"] for s in st_plain], float)
+    ms_sweeps = float(sum(s["ms_sweeps"] for s in st_plain))
     half_launches = 2.0 * sweeps.sum()
     avg_half_ms_region = ms_sweeps / half_launches if half_launches else float("nan")
     alg_half = 6.0 * n_cells                      # rhs_c + p_other read, p_c written (4 B each, half the cells)
@@ -247,40 +297,53 @@ def run_ours(args, ws, rank, local):
         except Exception:
             traffic = None
     value = ws * args.steps / (ms * 1e-3)
-    alg_bytes = float(np.mean([step_bytes(W, H, D, s, c) for s, c in zip(sweeps, checks)]))
+    head = learned if head_learned else plain
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"plume-family {W}^3 scene (seed {SEED}, {scn.extra['sources']} sources, "
-                               f"wind {scn.extra['wind_cells_per_step']:.2f} cells/step), plain RBGS with "
-                               f"free-surface top, warm-started, to FP64 relative residual {TOL:g}",
+                               f"wind {scn.extra['wind_cells_per_step']:.2f} cells/step), "
+                               f"{'learned warm start + ' if head_learned else 'plain '}RBGS with free-surface "
+                               f"top to FP64 relative residual {TOL:g} per frame",
                    "grid": [W, H, D], "particles": int(len(parts)), "tol": TOL, "check_every": CHECK_EVERY,
-                   "mean_sweeps": float(sweeps.mean()), "sweeps_per_frame": [int(x) for x in sweeps],
-                   "max_rel_residual": float(rel.max()),
-                   "all_converged": conv, "l2": "inputs larger than L2 (0.9 GB of fields per replica)",
-                   "parallelism": f"replicas x{ws}", "device_loop": bool(device_loop),
-                   "learned_warm_start": "not built"},
-        "hbm_gbs_step": alg_bytes / (ms / args.steps * 1e-3) / 1e9,
+                   "max_iter": args.max_iter, "mean_sweeps": head["mean_sweeps"],
+                   "sweeps_per_frame": head["sweeps_per_frame"], "max_rel_residual": head["max_rel_residual"],
+                   "all_converged": head["all_converged"],
+                   "l2": "inputs larger than L2 (0.9 GB of fields per replica)",
+                   "parallelism": f"replicas x{ws}", "device_loop": bool(st_plain[-1]["device_loop"]),
+                   "learned_warm_start": net_src if head_learned else f"off: {net_src}",
+                   "timed_passes": "plain and learned each replay the same K frames from one post-warm-up "
+                                   "snapshot; value is the learned pass when a network is loaded"},
+        "plain": plain,
+        "learned": learned,
+        "learned_speedup": (learned["steps_per_s"] / plain["steps_per_s"]) if head_learned else None,
+        "hbm_gbs_step": head["hbm_gbs_step"],
         "roofline": {"bound": "hbm", "kernel": "k_rbgs_seg (half sweep)", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "alg_bytes_per_launch": alg_half, "avg_launch_ms": half_ms_events,
                      "avg_launch_ms_in_timed_region": avg_half_ms_region,
-                     "timing": f"CUDA events around {n_meas} sweeps on the bench stream after the timed region; "
+                     "timing": f"CUDA events around {n_meas} sweeps on the bench stream after the timed passes; "
                                "in-region figure from the device global timer around each sweep batch",
-                     "sweep_variant": variant},
+                     "sweep_variant": st_plain[-1]["sweep_variant"]},
         "e2e": None if e2e_s is None else
                {"value": ws * args.steps / e2e_s, "unit": "steps/s",
                 "h2d_bytes_per_step": int(parts.nbytes), "d2h_bytes_per_step": int(n_cells * 4)},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
-        "stage_ms": {k: float(np.mean([s[k] for s in stats])) for k in
-                     ("ms_forces", "ms_divergence", "ms_solve", "ms_gradient", "ms_advect", "ms_sweeps",
-                      "ms_checks")},
+        "stage_ms": head["stage_ms"],
     }
+    if head_learned:
+        keep = ("plain_seeds", "policy_seeds", "train_seeds", "frames", "iters", "crop", "kappa", "target_tol",
+                "eval_seeds", "sweep_ratio", "time_ratio")
+        line["config"]["network"] = {k: net.meta[k] for k in keep if k in net.meta}
+        if "rounds" in net.meta:
+            line["config"]["network"]["rounds"] = [(r["kind"], r["pairs"]) for r in net.meta["rounds"]]
     if not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(scn, parts, float(sweeps.mean()))
     solver.close()
+    if net is not None:
+        net.close()
     return line
 
 
@@ -345,6 +408,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) pass")
     ap.add_argument("--max-iter", type=int, default=MAX_ITER, help="GS sweep cap per frame (profiling runs)")
+    ap.add_argument("--plain-only", action="store_true", help="skip the learned warm-start pass")
+    ap.add_argument("--weights", default=None, help="warm-start network weights (npz)")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the convergence loop from the host (every kernel a separate launch, for launch lists)")
     args = ap.parse_args()

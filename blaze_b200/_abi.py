@@ -130,8 +130,18 @@ EXPORTS = {
                                    C.c_void_p]),
     "blz_unet_loss_grad": (C.c_int, [C.c_void_p, _P(BlzParams), _P(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p,
                                      _P(C.c_double), C.c_void_p]),
+    "blz_unet_tensor_shape": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_int)]),
+    "blz_unet_get_tensor": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_float), C.c_longlong]),
     "blz_unet_adam": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]),
     "blz_set_warm_start": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "blz_batch_create": (C.c_int, [_P(C.c_void_p), C.c_int, _P(C.c_void_p)]),
+    "blz_batch_destroy": (C.c_int, [C.c_void_p]),
+    "blz_batch_stream": (C.c_void_p, [C.c_void_p]),
+    "blz_batch_add_source": (C.c_int, [C.c_void_p]),
+    "blz_batch_step": (C.c_int, [C.c_void_p, _P(C.c_float), _P(BlzStepStats)]),
+    "blz_batch_solve": (C.c_int, [C.c_void_p, _P(BlzStepStats)]),
+    "blz_batch_kernel_launches": (C.c_longlong, [C.c_void_p]),
+    "blz_batch_last_ms": (C.c_float, [C.c_void_p]),
     "blz_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "blz_last_error": (C.c_char_p, [C.c_void_p]),
 }

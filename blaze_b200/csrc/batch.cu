@@ -1,0 +1,438 @@
+// batch.cu — many independent simulations of uneven grid sizes stepped
+// together.  No counterpart in the reference, which runs one FluidSolver.
+//
+// The pressure solve is the frame's dominant cost and, for grids of 48^3..128^3
+// cells, a single grid's half sweep is a few microseconds of HBM traffic, less
+// than a kernel launch.  The batch therefore runs every grid's solve in the
+// same launches: each half sweep is one persistent grid-stride launch over the
+// segment work items of all grids (k_batch_sweep), the FP64 residual is one
+// launch over every grid's residual blocks plus one block per grid deciding
+// continue/stop, and a CUDA graph with a conditional WHILE node repeats
+// {check_every sweeps, residual, decision} until no grid is left running.
+// Each grid stops exactly where its own device-loop solve stops, with the
+// same pressure bit for bit.  The launch shape (planes per thread and block
+// size) is autotuned per batch on scratch copies of the pressures.
+//
+// When no grid's forces depend on time (no curl noise, no moving wind
+// noise), a whole frame — every grid's forces and divergence, the batched
+// solve, every grid's gradient and advection — is one graph launch (one graph
+// per front/back parity of the grids' fields).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+using namespace blz;
+
+namespace {
+
+__global__ void k_batch_begin(BatchCtl *ctl, int n) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) ctl[s] = BatchCtl{0, 0, 0, 1, 0.0, 0.0};
+}
+
+__global__ void k_batch_cond(const BatchCtl *__restrict__ ctl, int n, cudaGraphConditionalHandle h) {
+    int any = 0;
+    for (int s = threadIdx.x; s < n; s += blockDim.x) any |= ctl[s].active;
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+constexpr int kKZ[4] = {1, 2, 4, 8};
+constexpr int kBlocks[2] = {128, 256};
+
+} // namespace
+
+struct blz_batch {
+    std::vector<blz_solver *> sims;
+    std::vector<const blz_params *> params;
+    int n = 0, chunk = 1;
+    cudaStream_t st = nullptr;
+    BatchSim *d_sims = nullptr;
+    BatchCtl *d_ctl = nullptr, *h_ctl = nullptr;
+    long long *d_item0 = nullptr;             // 4 tables (kz = 1, 2, 4, 8) of n + 1 offsets
+    int *d_blk0 = nullptr;
+    int total_blocks = 0;
+    double *partials = nullptr;
+    int kz = -1, block = 256, grid = 0;       // chosen launch shape (kz < 0: not tuned yet)
+    bool time_free = false;                   // frame graphs allowed
+    cudaGraphExec_t solve_exec = nullptr;
+    cudaGraphExec_t frame_exec[2] = {nullptr, nullptr};
+    long long frame_stage_launches[2] = {0, 0};
+    int parity = 0;                           // front/back parity of the grids (all equal)
+    long long launches = 0;
+    int prologue = 0, body = 0;               // kernels per graph part
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.0f;
+};
+
+static thread_local std::string g_batch_err;
+
+static int bfail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    set_thread_error(buf);
+    return code;
+}
+
+#define BCK(x)                                                                                  \
+    do {                                                                                        \
+        cudaError_t e_ = (x);                                                                   \
+        if (e_ != cudaSuccess) return bfail(BLZ_ERR_CUDA, "%s failed: %s", #x, cudaGetErrorString(e_)); \
+    } while (0)
+
+static const long long *item0_of(const blz_batch *b, int kz) {
+    const int t = kz == 1 ? 0 : kz == 2 ? 1 : kz == 4 ? 2 : 3;
+    return b->d_item0 + (size_t)t * (b->n + 1);
+}
+
+// Body of the batched solve, appended to the capture in progress on b->st:
+// check_every sweeps over the active grids, their residual and decision.
+static void capture_body(blz_batch *b, cudaGraphConditionalHandle h) {
+    launch_batch_sweeps(b->d_sims, item0_of(b, b->kz), b->n, b->chunk, b->kz, b->grid, b->block, b->d_ctl, b->st);
+    launch_batch_check(b->d_sims, b->d_blk0, b->n, b->total_blocks, b->d_ctl, b->partials, 1, b->chunk, b->st);
+    k_batch_cond<<<1, 256, 0, b->st>>>(b->d_ctl, b->n, h);
+}
+
+// Builds [stages before the solve] + solve loop + [stages after] as one graph.
+// with_stages: every grid's forces + divergence before and gradient + advect
+// after the loop (their launches are counted into *stage_launches).
+static int build_graph(blz_batch *b, bool with_stages, cudaGraphExec_t *out, long long *stage_launches) {
+    cudaGraph_t graph = nullptr, body = nullptr;
+    cudaGraphConditionalHandle h;
+    cudaGraphNode_t cond;
+    int rc = BLZ_OK;
+    long long l0 = 0, l1 = 0;
+    auto launches_now = [&]() {
+        long long t = 0;
+        for (auto *s : b->sims) t += blz_kernel_launches(s);
+        return t;
+    };
+    cudaError_t e = cudaGraphCreate(&graph, 0);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, graph, 0, 0);
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(b->st, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) goto done;
+    l0 = launches_now();
+    if (with_stages)
+        for (auto *s : b->sims) {
+            if ((rc = blz_forces(s, 0.0f)) != BLZ_OK || (rc = blz_divergence(s)) != BLZ_OK) break;
+        }
+    if (rc == BLZ_OK) {
+        k_batch_begin<<<(b->n + 255) / 256, 256, 0, b->st>>>(b->d_ctl, b->n);
+        launch_batch_check(b->d_sims, b->d_blk0, b->n, b->total_blocks, b->d_ctl, b->partials, 0, b->chunk, b->st);
+        k_batch_cond<<<1, 256, 0, b->st>>>(b->d_ctl, b->n, h);
+        cudaStreamCaptureStatus status;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        e = cudaStreamGetCaptureInfo(b->st, &status, nullptr, nullptr, &deps, &ndeps);
+        if (e == cudaSuccess) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            e = cudaGraphAddNode(&cond, graph, deps, ndeps, &cp);
+            if (e == cudaSuccess) {
+                body = cp.conditional.phGraph_out[0];
+                e = cudaStreamUpdateCaptureDependencies(b->st, &cond, 1, cudaStreamSetCaptureDependencies);
+            }
+        }
+    }
+    {
+        cudaGraph_t g2 = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(b->st, &g2);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (e != cudaSuccess || rc != BLZ_OK) goto done;
+    e = cudaStreamBeginCaptureToGraph(b->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) goto done;
+    capture_body(b, h);
+    {
+        cudaGraph_t g2 = nullptr;
+        e = cudaStreamEndCapture(b->st, &g2);
+    }
+    if (e != cudaSuccess) goto done;
+    if (with_stages) {
+        e = cudaStreamBeginCaptureToGraph(b->st, graph, &cond, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) goto done;
+        for (auto *s : b->sims) {
+            if ((rc = blz_gradient(s)) != BLZ_OK || (rc = blz_advect(s)) != BLZ_OK) break;
+        }
+        cudaGraph_t g2 = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(b->st, &g2);
+        if (e == cudaSuccess) e = e2;
+        if (e != cudaSuccess || rc != BLZ_OK) goto done;
+    }
+    l1 = launches_now();
+    if (stage_launches) *stage_launches = l1 - l0;
+    e = cudaGraphInstantiate(out, graph, 0);
+done:
+    if (e != cudaSuccess) {
+        cudaStreamCaptureStatus status;
+        if (cudaStreamIsCapturing(b->st, &status) == cudaSuccess && status != cudaStreamCaptureStatusNone) {
+            cudaGraph_t junk = nullptr;
+            cudaStreamEndCapture(b->st, &junk);
+        }
+        cudaGetLastError();
+        if (rc == BLZ_OK) rc = bfail(BLZ_ERR_CUDA, "building the batch graph failed: %s", cudaGetErrorString(e));
+    }
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+}
+
+// Autotuner: planes per thread x block size, two sweeps of the whole batch on
+// scratch copies of every pressure (all shapes give identical results).
+static int tune(blz_batch *b) {
+    if (b->kz >= 0) return BLZ_OK;
+    std::vector<BatchSim> h(b->n), hs(b->n);
+    BCK(cudaMemcpy(h.data(), b->d_sims, sizeof(BatchSim) * b->n, cudaMemcpyDeviceToHost));
+    size_t total = 0;
+    for (auto &s : h) total += (size_t)s.g.W * s.g.H * s.g.D;
+    float *scratch = nullptr;
+    BatchSim *d_scr = nullptr;
+    BCK(cudaMalloc(&scratch, total * sizeof(float)));
+    cudaError_t e = cudaMalloc(&d_scr, sizeof(BatchSim) * b->n);
+    size_t off = 0;
+    for (int i = 0; i < b->n && e == cudaSuccess; ++i) {
+        const size_t half = (size_t)h[i].g.W * h[i].g.H * h[i].g.D / 2;
+        hs[i] = h[i];
+        hs[i].p_r = scratch + off;
+        hs[i].p_b = scratch + off + half;
+        e = cudaMemcpyAsync(hs[i].p_r, h[i].p_r, half * sizeof(float), cudaMemcpyDeviceToDevice, b->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hs[i].p_b, h[i].p_b, half * sizeof(float), cudaMemcpyDeviceToDevice, b->st);
+        off += 2 * half;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_scr, hs.data(), sizeof(BatchSim) * b->n, cudaMemcpyHostToDevice, b->st);
+    if (e == cudaSuccess) {
+        k_batch_begin<<<(b->n + 255) / 256, 256, 0, b->st>>>(b->d_ctl, b->n);
+        e = cudaGetLastError();
+    }
+    float best = 1e30f;
+    for (int ki = 0; ki < 4 && e == cudaSuccess; ++ki)
+        for (int bi = 0; bi < 2 && e == cudaSuccess; ++bi) {
+            const int kz = kKZ[ki], blk = kBlocks[bi], grid = batch_sweep_grid(kz, blk);
+            launch_batch_sweeps(d_scr, item0_of(b, kz), b->n, 1, kz, grid, blk, b->d_ctl, b->st);
+            e = cudaEventRecord(b->ev0, b->st);
+            launch_batch_sweeps(d_scr, item0_of(b, kz), b->n, 2, kz, grid, blk, b->d_ctl, b->st);
+            if (e == cudaSuccess) e = cudaEventRecord(b->ev1, b->st);
+            if (e == cudaSuccess) e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaEventSynchronize(b->ev1);
+            float ms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+            b->launches += 6;
+            if (e == cudaSuccess && ms < best) { best = ms; b->kz = kz; b->block = blk; b->grid = grid; }
+        }
+    cudaStreamSynchronize(b->st);
+    cudaFree(scratch);
+    cudaFree(d_scr);
+    if (e != cudaSuccess) {
+        b->kz = -1;
+        return bfail(BLZ_ERR_CUDA, "batch autotune failed: %s", cudaGetErrorString(e));
+    }
+    return BLZ_OK;
+}
+
+static void release(blz_batch *b) {
+    if (b->solve_exec) cudaGraphExecDestroy(b->solve_exec);
+    for (auto &x : b->frame_exec) if (x) cudaGraphExecDestroy(x);
+    cudaFree(b->d_sims); cudaFree(b->d_ctl); cudaFree(b->d_item0); cudaFree(b->d_blk0); cudaFree(b->partials);
+    if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->st) cudaStreamDestroy(b->st);
+}
+
+static int read_stats(blz_batch *b, blz_step_stats *stats, int loop_ran) {
+    BCK(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BatchCtl) * b->n, cudaMemcpyDeviceToHost, b->st));
+    BCK(cudaStreamSynchronize(b->st));
+    int max_checks = 0;
+    for (int i = 0; i < b->n; ++i) max_checks = std::max(max_checks, b->h_ctl[i].checks);
+    if (loop_ran) b->launches += b->prologue + (long long)std::max(0, max_checks - 1) * b->body;
+    BCK(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+    for (int i = 0; i < b->n; ++i) {
+        const BatchCtl &c = b->h_ctl[i];
+        const double r = std::sqrt(c.r2), bn = std::sqrt(c.b2);
+        if (!std::isfinite(r)) return bfail(BLZ_ERR_NAN, "simulation %d: non-finite residual after %d sweeps", i, c.iters);
+        if (!stats) continue;
+        blz_step_stats &st = stats[i];
+        st = blz_step_stats{};
+        st.iterations = c.iters;
+        st.converged = c.converged;
+        st.residual = r;
+        st.rhs_norm = bn;
+        st.rel_residual = bn > 0.0 ? r / bn : 0.0;
+        st.residual_checks = c.checks;
+        st.sweep_variant = b->kz;
+        st.device_loop = 1;
+    }
+    return BLZ_OK;
+}
+
+extern "C" {
+
+int blz_batch_create(blz_solver *const *sims, int n, blz_batch **out) {
+    if (!out || !sims || n < 1) return bfail(BLZ_ERR_ARG, "need at least one solver");
+    *out = nullptr;
+    blz_batch *b = new blz_batch();
+    b->n = n;
+    std::vector<BatchSim> h(n);
+    std::vector<long long> item0(4 * (size_t)(n + 1));
+    std::vector<int> blk0(n + 1);
+    for (int i = 0; i < n; ++i) {
+        if (!sims[i]) { delete b; return bfail(BLZ_ERR_ARG, "solver %d is null", i); }
+        const blz_params *P = nullptr;
+        solver_batch_view(sims[i], &h[i], &P);
+        if (P->width % 8 || P->gs_order != BLZ_GS_RB3D || !(P->tol > 0.0) || P->check_every < 1 ||
+            P->max_iter % P->check_every) {
+            delete b;
+            return bfail(BLZ_ERR_ARG, "solver %d: the batch needs width %% 8 == 0, 3-D red-black order, tol > 0 "
+                                      "and max_iter a multiple of check_every >= 1", i);
+        }
+        if (i > 0 && P->check_every != b->params[0]->check_every) {
+            delete b;
+            return bfail(BLZ_ERR_ARG, "solver %d: all solvers of a batch need the same check_every", i);
+        }
+        b->sims.push_back(sims[i]);
+        b->params.push_back(P);
+    }
+    b->chunk = b->params[0]->check_every;
+    b->time_free = true;
+    for (const blz_params *P : b->params)
+        if (std::fabs(P->turbulence_amp) > 0.0f || (P->wind_amp > 0.0f && P->wind_speed != 0.0f && P->wind_turb_amp != 0.0f))
+            b->time_free = false;
+    for (int t = 0; t < 4; ++t) {
+        long long acc = 0;
+        for (int i = 0; i < n; ++i) {
+            item0[(size_t)t * (n + 1) + i] = acc;
+            acc += batch_sweep_items(h[i].g, kKZ[t]);
+        }
+        item0[(size_t)t * (n + 1) + n] = acc;
+    }
+    int acc = 0;
+    for (int i = 0; i < n; ++i) { blk0[i] = acc; acc += residual_blocks(h[i].g); }
+    blk0[n] = acc;
+    b->total_blocks = acc;
+    int rc = BLZ_OK;
+    auto ck = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && rc == BLZ_OK) rc = bfail(BLZ_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    };
+    ck(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaMalloc(&b->d_sims, sizeof(BatchSim) * n), "cudaMalloc");
+    ck(cudaMalloc(&b->d_ctl, sizeof(BatchCtl) * n), "cudaMalloc");
+    ck(cudaMallocHost(&b->h_ctl, sizeof(BatchCtl) * n), "cudaMallocHost");
+    ck(cudaMalloc(&b->d_item0, sizeof(long long) * item0.size()), "cudaMalloc");
+    ck(cudaMalloc(&b->d_blk0, sizeof(int) * (n + 1)), "cudaMalloc");
+    ck(cudaMalloc(&b->partials, sizeof(double) * 2 * (size_t)acc), "cudaMalloc");
+    ck(cudaEventCreate(&b->ev0), "cudaEventCreate");
+    ck(cudaEventCreate(&b->ev1), "cudaEventCreate");
+    if (rc == BLZ_OK) ck(cudaMemcpy(b->d_sims, h.data(), sizeof(BatchSim) * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+    if (rc == BLZ_OK) ck(cudaMemcpy(b->d_item0, item0.data(), sizeof(long long) * item0.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+    if (rc == BLZ_OK) ck(cudaMemcpy(b->d_blk0, blk0.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice), "cudaMemcpy");
+    for (int i = 0; i < n && rc == BLZ_OK; ++i) rc = blz_set_stream(sims[i], b->st);
+    b->prologue = 1 + 2 + 1;
+    if (rc != BLZ_OK) {
+        release(b);
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return BLZ_OK;
+}
+
+int blz_batch_destroy(blz_batch *b) {
+    if (!b) return BLZ_OK;
+    cudaStreamSynchronize(b->st);
+    // The solvers fall back to their own streams.
+    for (auto *s : b->sims) blz_set_stream(s, nullptr);
+    release(b);
+    delete b;
+    return BLZ_OK;
+}
+
+void *blz_batch_stream(blz_batch *b) { return b ? (void *)b->st : nullptr; }
+
+long long blz_batch_kernel_launches(const blz_batch *b) { return b ? b->launches : 0; }
+
+float blz_batch_last_ms(const blz_batch *b) { return b ? b->last_ms : 0.0f; }
+
+int blz_batch_add_source(blz_batch *b) {
+    if (!b) return bfail(BLZ_ERR_ARG, "null batch");
+    for (auto *s : b->sims) {
+        const long long l0 = blz_kernel_launches(s);
+        const int rc = blz_add_source(s);
+        if (rc != BLZ_OK) return rc;
+        b->launches += blz_kernel_launches(s) - l0;
+    }
+    return BLZ_OK;
+}
+
+// The batched solve alone (after every solver's divergence).
+int blz_batch_solve(blz_batch *b, blz_step_stats *stats) {
+    if (!b) return bfail(BLZ_ERR_ARG, "null batch");
+    int rc = tune(b);
+    if (rc != BLZ_OK) return rc;
+    b->body = 2 * b->chunk + 2 + 1;
+    if (!b->solve_exec && (rc = build_graph(b, false, &b->solve_exec, nullptr)) != BLZ_OK) return rc;
+    BCK(cudaEventRecord(b->ev0, b->st));
+    BCK(cudaGraphLaunch(b->solve_exec, b->st));
+    BCK(cudaEventRecord(b->ev1, b->st));
+    return read_stats(b, stats, 1);
+}
+
+// One frame of every simulation: forces (at times[i]), divergence, the
+// batched solve, gradient and advection (sourcing is blz_batch_add_source).
+int blz_batch_step(blz_batch *b, const float *times, blz_step_stats *stats) {
+    if (!b) return bfail(BLZ_ERR_ARG, "null batch");
+    int rc = tune(b);
+    if (rc != BLZ_OK) return rc;
+    b->body = 2 * b->chunk + 2 + 1;
+    if (b->time_free) {
+        const int par = b->parity;
+        if (!b->frame_exec[par]) {
+            // Capturing runs no kernel but flips every solver's front index
+            // (blz_advect) and counts launches that did not happen: undo both.
+            std::vector<long long> before(b->n);
+            for (int i = 0; i < b->n; ++i) before[i] = blz_kernel_launches(b->sims[i]);
+            rc = build_graph(b, true, &b->frame_exec[par], &b->frame_stage_launches[par]);
+            for (int i = 0; i < b->n; ++i) {
+                solver_flip_front(b->sims[i]);
+                solver_add_launches(b->sims[i], before[i] - blz_kernel_launches(b->sims[i]));
+            }
+            if (rc != BLZ_OK) return rc;
+        }
+        BCK(cudaEventRecord(b->ev0, b->st));
+        BCK(cudaGraphLaunch(b->frame_exec[par], b->st));
+        BCK(cudaEventRecord(b->ev1, b->st));
+        for (auto *s : b->sims) solver_flip_front(s);
+        b->parity ^= 1;
+        b->launches += b->frame_stage_launches[par];
+        return read_stats(b, stats, 1);
+    }
+    if (!b->solve_exec && (rc = build_graph(b, false, &b->solve_exec, nullptr)) != BLZ_OK) return rc;
+    BCK(cudaEventRecord(b->ev0, b->st));
+    long long l0 = 0, l1 = 0;
+    for (auto *s : b->sims) l0 += blz_kernel_launches(s);
+    for (int i = 0; i < b->n; ++i) {
+        if ((rc = blz_forces(b->sims[i], times ? times[i] : 0.0f)) != BLZ_OK) return rc;
+        if ((rc = blz_divergence(b->sims[i])) != BLZ_OK) return rc;
+    }
+    BCK(cudaGraphLaunch(b->solve_exec, b->st));
+    for (auto *s : b->sims) {
+        if ((rc = blz_gradient(s)) != BLZ_OK) return rc;
+        if ((rc = blz_advect(s)) != BLZ_OK) return rc;
+    }
+    BCK(cudaEventRecord(b->ev1, b->st));
+    for (auto *s : b->sims) l1 += blz_kernel_launches(s);
+    b->launches += l1 - l0;
+    b->parity ^= 1;
+    return read_stats(b, stats, 1);
+}
+
+} // extern "C"

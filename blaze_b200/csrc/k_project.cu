@@ -167,14 +167,10 @@ __device__ __forceinline__ float4 gs_segment(const SolveParams &sp, int s, bool 
 // 128-bit load of plane k+1 instead of two.  Every variant performs the same
 // operations per cell, so all give bitwise identical results.
 template <int KZ>
-__global__ void __launch_bounds__(256)
-k_rbgs_seg(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float *__restrict__ p_o,
-           float *__restrict__ p_c, int colour) {
-    const int Wh = g.W >> 1, Wq = Wh >> 2;
-    const int mq = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k0 = blockIdx.z * KZ;
-    if (mq >= Wq || j >= g.H || k0 >= g.D) return;
+__device__ __forceinline__ void seg_sweep(const Geom &g, const SolveParams &sp, const float *__restrict__ rhs_c,
+                                          const float *__restrict__ p_o, float *__restrict__ p_c, int colour,
+                                          int mq, int j, int k0) {
+    const int Wh = g.W >> 1;
     const int m0 = mq * 4;
     const size_t pl = (size_t)Wh * g.H;
     const size_t row = (size_t)m0 + (size_t)Wh * (size_t)j;
@@ -200,6 +196,18 @@ k_rbgs_seg(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float 
         zm = cur;
         cur = zp;
     }
+}
+
+template <int KZ>
+__global__ void __launch_bounds__(256)
+k_rbgs_seg(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float *__restrict__ p_o,
+           float *__restrict__ p_c, int colour) {
+    const int Wq = g.W >> 3;
+    const int mq = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k0 = blockIdx.z * KZ;
+    if (mq >= Wq || j >= g.H || k0 >= g.D) return;
+    seg_sweep<KZ>(g, sp, rhs_c, p_o, p_c, colour, mq, j, k0);
 }
 
 // (planes per thread, rows per block) of each segment-kernel variant.
@@ -340,16 +348,18 @@ __device__ __forceinline__ void residual_segment(const SolveParams &sp, double s
     }
 }
 
-__global__ void __launch_bounds__(kResThreads)
-k_residual_seg(Geom g, SolveParams sp, double scale, const float *__restrict__ rr,
-               const float *__restrict__ rb, const float *__restrict__ pr, const float *__restrict__ pb,
-               double *__restrict__ partials) {
+// Block `blk` of `nblk` of the segment residual: grid-stride over the row
+// segments, then the block's FP64 sums go to partials[2*blk], [2*blk + 1].
+__device__ __forceinline__ void residual_seg_block(const Geom &g, const SolveParams &sp, double scale,
+                                                   const float *__restrict__ rr, const float *__restrict__ rb,
+                                                   const float *__restrict__ pr, const float *__restrict__ pb,
+                                                   int blk, int nblk, double *__restrict__ partials) {
     const int Wh = g.W >> 1, Wq = Wh >> 2;
     const int items = Wq * g.H * g.D;
     const int pl = Wh * g.H;
     double r2 = 0.0, b2 = 0.0;
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < items; t += gridDim.x * blockDim.x) {
+    for (int t = blk * kResThreads + threadIdx.x; t < items; t += nblk * kResThreads) {
         const int mq = t % Wq, jk = t / Wq;
         const int j = jk % g.H, k = jk / g.H;
         const int m0 = 4 * mq;
@@ -381,8 +391,15 @@ k_residual_seg(Geom g, SolveParams sp, double scale, const float *__restrict__ r
         b2 = lane < kResThreads / 32 ? s_b[lane] : 0.0;
         r2 = warp_sum(r2);
         b2 = warp_sum(b2);
-        if (lane == 0) { partials[2 * blockIdx.x] = r2; partials[2 * blockIdx.x + 1] = b2; }
+        if (lane == 0) { partials[2 * blk] = r2; partials[2 * blk + 1] = b2; }
     }
+}
+
+__global__ void __launch_bounds__(kResThreads)
+k_residual_seg(Geom g, SolveParams sp, double scale, const float *__restrict__ rr,
+               const float *__restrict__ rb, const float *__restrict__ pr, const float *__restrict__ pb,
+               double *__restrict__ partials) {
+    residual_seg_block(g, sp, scale, rr, rb, pr, pb, blockIdx.x, gridDim.x, partials);
 }
 
 // One packed pair per item (any even W).
@@ -431,8 +448,9 @@ k_residual(Geom g, SolveParams sp, double scale, const float *__restrict__ rr,
     }
 }
 
-__global__ void __launch_bounds__(1024) k_reduce_pairs(const double *__restrict__ partials, int n,
-                                                       double *__restrict__ out2) {
+// Sums n {r2, b2} pairs in a fixed order with one 1024-thread block; lane 0
+// of warp 0 writes the totals to out2 (global or shared memory).
+__device__ __forceinline__ void reduce_pairs_block(const double *__restrict__ partials, int n, double *out2) {
     __shared__ double s_r[32], s_b[32];
     double r2 = 0.0, b2 = 0.0;
     for (int t = threadIdx.x; t < n; t += blockDim.x) { r2 += partials[2 * t]; b2 += partials[2 * t + 1]; }
@@ -449,6 +467,11 @@ __global__ void __launch_bounds__(1024) k_reduce_pairs(const double *__restrict_
         b2 = warp_sum(b2);
         if (lane == 0) { out2[0] = r2; out2[1] = b2; }
     }
+}
+
+__global__ void __launch_bounds__(1024) k_reduce_pairs(const double *__restrict__ partials, int n,
+                                                       double *__restrict__ out2) {
+    reduce_pairs_block(partials, n, out2);
 }
 
 int launch_residual(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
@@ -573,6 +596,125 @@ void launch_unpack(const Geom &g, const float *red, const float *black, float *n
     const dim3 b(32, 8, 1);
     const dim3 gr(((g.W >> 1) + b.x - 1) / b.x, (g.H + b.y - 1) / b.y, g.D);
     k_unpack<<<gr, b, 0, st>>>(g, red, black, nat);
+}
+
+// ---------------------------------------------------------------------------
+// Batched solve over many independent grids (the graph is built in batch.cu).
+// Work items are the single-grid segment kernel's threads of every grid, in
+// grid order; a persistent grid-stride launch covers them all, so each half
+// sweep of the whole batch is one launch.  Items of a grid whose solve has
+// finished are skipped.  Per grid, every item does exactly what the
+// single-grid kernel's thread does, and the residual blocks and their
+// reduction are the single-grid residual's, so a grid's sweeps, residuals
+// and stopping point equal those of its own solve bit for bit.
+// ---------------------------------------------------------------------------
+long long batch_sweep_items(const Geom &g, int kz) {
+    return (long long)(g.W >> 3) * g.H * ((g.D + kz - 1) / kz);
+}
+
+template <int KZ>
+__global__ void __launch_bounds__(256)
+k_batch_sweep(const BatchSim *__restrict__ sims, const long long *__restrict__ item0, int nsims,
+              const BatchCtl *__restrict__ ctl, int colour) {
+    extern __shared__ long long s_item0[];
+    for (int i = threadIdx.x; i <= nsims; i += blockDim.x) s_item0[i] = item0[i];
+    __syncthreads();
+    const long long total = s_item0[nsims];
+    for (long long it = blockIdx.x * (long long)blockDim.x + threadIdx.x; it < total;
+         it += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nsims - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_item0[mid] <= it) lo = mid; else hi = mid - 1;
+        }
+        if (!ctl[lo].active) continue;
+        const BatchSim &S = sims[lo];
+        const long long local = it - s_item0[lo];
+        const int Wq = S.g.W >> 3;
+        const int mq = (int)(local % Wq);
+        const long long rest = local / Wq;
+        const int j = (int)(rest % S.g.H), k0 = (int)(rest / S.g.H) * KZ;
+        seg_sweep<KZ>(S.g, S.sp, colour ? S.rhs_b : S.rhs_r, colour ? S.p_r : S.p_b, colour ? S.p_b : S.p_r,
+                      colour, mq, j, k0);
+    }
+}
+
+int batch_sweep_grid(int kz, int block) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    switch (kz) {
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_sweep<1>, block, 0); break;
+    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_sweep<2>, block, 0); break;
+    case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_sweep<4>, block, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_sweep<8>, block, 0); break;
+    }
+    return sms * std::max(1, per);
+}
+
+void launch_batch_sweeps(const BatchSim *sims, const long long *item0, int nsims, int sweeps, int kz, int grid,
+                         int block, const BatchCtl *ctl, cudaStream_t st) {
+    const size_t smem = sizeof(long long) * (size_t)(nsims + 1);
+    for (int it = 0; it < sweeps; ++it)
+        for (int c = 0; c < 2; ++c) {
+            switch (kz) {
+            case 1: k_batch_sweep<1><<<grid, block, smem, st>>>(sims, item0, nsims, ctl, c); break;
+            case 2: k_batch_sweep<2><<<grid, block, smem, st>>>(sims, item0, nsims, ctl, c); break;
+            case 4: k_batch_sweep<4><<<grid, block, smem, st>>>(sims, item0, nsims, ctl, c); break;
+            default: k_batch_sweep<8><<<grid, block, smem, st>>>(sims, item0, nsims, ctl, c); break;
+            }
+        }
+}
+
+__device__ __forceinline__ int find_sim(const int *__restrict__ start, int nsims, int b) {
+    int lo = 0, hi = nsims - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(start + mid) <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Residual blocks of every active grid: grid s owns blocks [blk0[s], blk0[s+1]),
+// as many as its own residual launch has.
+__global__ void __launch_bounds__(kResThreads)
+k_batch_residual(const BatchSim *__restrict__ sims, const int *__restrict__ blk0, int nsims,
+                 const BatchCtl *__restrict__ ctl, double *__restrict__ partials) {
+    const int s = find_sim(blk0, nsims, blockIdx.x);
+    if (!ctl[s].active) return;
+    const BatchSim &S = sims[s];
+    const int b0 = __ldg(blk0 + s);
+    residual_seg_block(S.g, S.sp, S.sp.scale_d, S.rhs_r, S.rhs_b, S.p_r, S.p_b, blockIdx.x - b0,
+                       __ldg(blk0 + s + 1) - b0, partials + 2 * (size_t)b0);
+}
+
+// One block per grid: its residual totals and the single-grid loop's decision.
+__global__ void __launch_bounds__(1024)
+k_batch_check(const BatchSim *__restrict__ sims, const int *__restrict__ blk0, const double *__restrict__ partials,
+              BatchCtl *__restrict__ ctl, int after_sweeps, int chunk) {
+    const int s = blockIdx.x;
+    if (!ctl[s].active) return;
+    __shared__ double out2[2];
+    const int b0 = blk0[s];
+    reduce_pairs_block(partials + 2 * (size_t)b0, blk0[s + 1] - b0, out2);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        BatchCtl c = ctl[s];
+        if (after_sweeps) c.iters += chunk;
+        c.checks += 1;
+        c.r2 = out2[0];
+        c.b2 = out2[1];
+        const bool conv = c.b2 == 0.0 || sqrt(c.r2) / sqrt(c.b2) <= sims[s].tol;
+        c.converged = conv;
+        c.active = (!conv && c.iters < sims[s].max_iter) ? 1 : 0;
+        ctl[s] = c;
+    }
+}
+
+void launch_batch_check(const BatchSim *sims, const int *blk0, int nsims, int total_blocks, BatchCtl *ctl,
+                        double *partials, int after_sweeps, int chunk, cudaStream_t st) {
+    k_batch_residual<<<total_blocks, kResThreads, 0, st>>>(sims, blk0, nsims, ctl, partials);
+    k_batch_check<<<nsims, 1024, 0, st>>>(sims, blk0, partials, ctl, after_sweeps, chunk);
 }
 
 } // namespace blz

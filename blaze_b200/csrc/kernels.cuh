@@ -95,6 +95,38 @@ cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float 
                               SolveCtl *ctl, int chunk, int max_iter, double tol, int variant, cudaStream_t st,
                               cudaGraphExec_t *exec_out, int *body_kernels, int *prologue_kernels);
 
+// -- batched solve over many grids (k_project.cu kernels, batch.cu graph) ---
+struct BatchSim {
+    Geom g;
+    SolveParams sp;
+    const float *rhs_r, *rhs_b;
+    float *p_r, *p_b;
+    int max_iter;
+    double tol;
+};
+struct BatchCtl {
+    int iters, checks, converged, active;
+    double r2, b2;
+};
+// Segment-kernel threads of one grid for KZ planes per thread (W % 8 == 0).
+long long batch_sweep_items(const Geom &g, int kz);
+// Persistent grid size (SMs x resident blocks) of the batched sweep.
+int  batch_sweep_grid(int kz, int block);
+// `sweeps` red+black sweeps over every active grid; item0: nsims + 1
+// prefix offsets of the grids' items for this kz.
+void launch_batch_sweeps(const BatchSim *sims, const long long *item0, int nsims, int sweeps, int kz, int grid,
+                         int block, const BatchCtl *ctl, cudaStream_t st);
+// FP64 residual of every active grid (grid s owns partial blocks
+// [blk0[s], blk0[s+1]), residual_blocks(g_s) of them) and the per-grid
+// continue/stop decision.  2 launches.
+void launch_batch_check(const BatchSim *sims, const int *blk0, int nsims, int total_blocks, BatchCtl *ctl,
+                        double *partials, int after_sweeps, int chunk, cudaStream_t st);
+
+// Solver internals the batch uses (solver.cu).
+void solver_batch_view(blz_solver *s, BatchSim *out, const blz_params **P);
+void solver_flip_front(blz_solver *s);
+void solver_add_launches(blz_solver *s, long long n);
+
 // -- learned warm start: tensor-core convolution (unet_conv.cu) -------------
 struct ConvDesc {
     int W, H, D;        // interior voxels (tensors carry a 1-voxel zero halo)

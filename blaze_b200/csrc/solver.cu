@@ -787,3 +787,21 @@ int blz_set_field(blz_solver *s, int f, const float *src, int on_device) {
 }
 
 } // extern "C"
+
+namespace blz {
+// What the batch (batch.cu) needs of a solver: its solve arrays and
+// parameters, and the front/back flip a replayed frame graph implies.
+void solver_batch_view(blz_solver *s, BatchSim *out, const blz_params **P) {
+    out->g = s->g;
+    out->sp = solve_params(s->P);
+    out->rhs_r = s->rhs_r;
+    out->rhs_b = s->rhs_b;
+    out->p_r = s->p_r;
+    out->p_b = s->p_b;
+    out->max_iter = s->P.max_iter;
+    out->tol = s->P.tol;
+    if (P) *P = &s->P;
+}
+void solver_flip_front(blz_solver *s) { s->cur ^= 1; }
+void solver_add_launches(blz_solver *s, long long n) { s->launches += n; }
+} // namespace blz

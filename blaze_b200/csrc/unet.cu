@@ -1087,6 +1087,47 @@ int blz_unet_loss_grad(blz_unet *u, const blz_params *grid, const int origin[3],
     return BLZ_OK;
 }
 
+static const Ten *tensor_by_id(const blz_unet *u, int id) {
+    const Ten *t[] = {&u->X0,    &u->e0a,   &u->cat0,  &u->d0a,   &u->d0b,   &u->p1,    &u->e1a,   &u->cat1,
+                      &u->d1a,   &u->d1b,   &u->p2,    &u->e2a,   &u->cat2,  &u->d2a,   &u->d2b,   &u->p3,
+                      &u->e3a,   &u->e3b,   &u->g_d0b, &u->g_d0a, &u->g_cat0, &u->g_e0b, &u->g_e0a, &u->g_p1,
+                      &u->g_d1b, &u->g_d1a, &u->g_cat1, &u->g_e1b, &u->g_e1a, &u->g_p2, &u->g_d2b, &u->g_d2a,
+                      &u->g_cat2, &u->g_e2b, &u->g_e2a, &u->g_p3, &u->g_e3b, &u->g_e3a};
+    if (id < 0 || id >= (int)(sizeof t / sizeof t[0])) return nullptr;
+    return t[id];
+}
+
+// Padded shape (D+2, H+2, W+2, C) of tensor `id`: the 18 activations in
+// forward order (X0 e0a cat0 d0a d0b p1 e1a cat1 d1a d1b p2 e2a cat2 d2a d2b
+// p3 e3a e3b), then the 20 activation gradients (g_d0b g_d0a g_cat0 g_e0b
+// g_e0a g_p1 g_d1b g_d1a g_cat1 g_e1b g_e1a g_p2 g_d2b g_d2a g_cat2 g_e2b
+// g_e2a g_p3 g_e3b g_e3a), which exist after the first training call.
+int blz_unet_tensor_shape(const blz_unet *u, int id, int shape[4]) {
+    const Ten *t = u ? tensor_by_id(u, id) : nullptr;
+    if (!t || !shape) return ufail(BLZ_ERR_ARG, "no tensor %d", id);
+    if (!t->buf) return ufail(BLZ_ERR_STATE, "tensor %d not allocated (gradients need a training call)", id);
+    const LDims &d = u->L[t->level];
+    shape[0] = d.D + 2; shape[1] = d.H + 2; shape[2] = d.W + 2; shape[3] = t->C;
+    return BLZ_OK;
+}
+
+int blz_unet_get_tensor(const blz_unet *u, int id, float *out, long long capacity) {
+    const Ten *t = u ? tensor_by_id(u, id) : nullptr;
+    if (!t || !out) return ufail(BLZ_ERR_ARG, "no tensor %d", id);
+    if (!t->buf) return ufail(BLZ_ERR_STATE, "tensor %d not allocated (gradients need a training call)", id);
+    const LDims &d = u->L[t->level];
+    const size_t n = (size_t)(d.W + 2) * (d.H + 2) * (d.D + 2) * t->C;
+    if ((long long)n > capacity) return ufail(BLZ_ERR_ARG, "capacity %lld < %zu", capacity, n);
+    std::vector<uint16_t> h(n);
+    UCK(cudaDeviceSynchronize());
+    UCK(cudaMemcpy(h.data(), t->base(), n * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) {
+        const uint32_t bits = (uint32_t)h[i] << 16;
+        std::memcpy(out + i, &bits, sizeof bits);
+    }
+    return BLZ_OK;
+}
+
 int blz_unet_adam(blz_unet *u, float lr, float beta1, float beta2, float eps, void *stream) {
     if (!u) return ufail(BLZ_ERR_ARG, "null network");
     if (!u->have_grads) return ufail(BLZ_ERR_STATE, "no gradients: call blz_unet_loss_grad first");

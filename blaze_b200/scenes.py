@@ -236,3 +236,32 @@ def family_scene(n=256, seed=3, bc_mode=_abi.BLZ_BC_FREE_SURFACE, tol=1e-4, max_
     s.sourceMaxParticleCount = len(parts)
     s.extra = {"sources": nsrc, "wind_cells_per_step": wind}
     return s, parts
+
+
+BATCH_DIMS = [(48, 48, 48), (64, 64, 64), (96, 96, 96), (128, 64, 64), (64, 128, 64)]
+
+
+def batch_scenes(count=64, seed=4, tol=1e-4, max_iter=20000, check_every=20, dims=None):
+    """`count` independent plume scenes for batched runs: grid dims drawn
+    uniformly from `dims` (default 48^3, 64^3, 96^3, 128x64x64, 64x128x64),
+    1-3 balls of radius 3-8 cells in the lower half, epsilon ~ U[0.1, 0.6],
+    beta = 1, walls except a free-surface top, RBGS warm-started to relative
+    residual `tol`.  dx = 1/W.  Returns [(SceneSettings, particles)]."""
+    rng = PCG32(seed)
+    dims = dims or BATCH_DIMS
+    out = []
+    for _ in range(count):
+        W, H, D = dims[rng.integer(0, len(dims) - 1)]
+        s = SceneSettings(gridRes=(W, H, D), dx=1.0 / W, dt=1.0 / 24, closedBounds=(1, 1, 1, 0, 1, 1),
+                          maxIterSolve=max_iter, tol=tol, check_every=check_every, buoyancy=1.0,
+                          vorticityConf=rng.uniform(0.1, 0.6), bc_mode=_abi.BLZ_BC_FREE_SURFACE)
+        parts = []
+        for _ in range(rng.integer(1, 3)):
+            r = rng.uniform(3.0, min(8.0, min(W, H, D) / 4.0))
+            c = (rng.uniform(r + 1, W - r - 1), rng.uniform(r + 1, 0.5 * H), rng.uniform(r + 1, D - r - 1))
+            count_p = int(min(8000, max(200, round(2000 * (r / 6.0) ** 3))))
+            parts.append(sphere_particles(rng, s, c, r, count_p))
+        parts = np.concatenate(parts)
+        s.sourceMaxParticleCount = len(parts)
+        out.append((s, parts))
+    return out

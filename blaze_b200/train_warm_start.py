@@ -1,22 +1,29 @@
 """Harvest, training and evaluation of the learned warm start.
 
-    python -m blaze_b200.train_warm_start --grid 256 --train-seeds 100-111 \
-        --frames 10 --iters 2000 --out blaze_b200/weights/plume256.npz
+    python -m blaze_b200.train_warm_start --grid 256 --plain-seeds 100-107 \
+        --policy-seeds 108-115 --rounds 2 --out blaze_b200/weights/plume256.npz
 
-1. Harvest: plume-family scenes (blaze_b200.scenes.family_scene) run with the
-   plain solver exactly as deployed (warm-started RBGS to relative residual
-   `--tol`).  For each harvested frame the pair is (rhs, p_prev) -> p*, where
-   p* continues the frame's own solve with more sweeps to `--target-tol`; the
-   simulation then goes on from the `--tol` solution, so the next p_prev has
-   the error a deployed solve leaves.  Pairs stay on the GPU (FP32).
+1. Harvest: plume-family scenes (blaze_b200.scenes.family_scene) run as
+   deployed: RBGS to relative residual `--tol` every frame, either plain
+   (warm-started from the previous frame's pressure) or with the current
+   network's warm start ("on policy").  For each harvested frame the pair is
+   (rhs, p_prev) -> p*, where p* continues the frame's own solve with more
+   sweeps towards `--target-tol`; the simulation then goes on from the
+   `--tol` solution, so the next p_prev carries exactly the error a
+   deployed solve leaves.  On-policy rounds (as in DAgger) add pairs from
+   trajectories the network itself shaped, so it learns to correct its own
+   accumulated error.  Pairs stay on the GPU (FP32).
 2. Training: Adam on single samples, each a random pair, a random crop whose
    origin is a multiple of 8 (the pooling grid of the full-grid inference)
    and a random mirror in x and/or z (the pressure system is symmetric under
-   both).  Loss and gradients come from the library's own forward and
-   backward kernels (blz_unet_loss_grad); kappa is the pairs' mean
+   both); half the samples add a smooth random perturbation to p_prev (the
+   target stays p*).  Loss and gradients come from the library's own forward
+   and backward kernels (blz_unet_loss_grad); kappa is the pairs' mean
    rms(p* - p_prev) / rms(b - A p_prev).
-3. Evaluation: held-out seeds, each frame solved twice from the same state,
-   plain and warm-started, both to `--tol`; reports sweeps and solve time.
+3. Evaluation: held-out seeds, each run twice from the same start, a plain
+   trajectory and a learned one (each frame warm-started by the network,
+   then RBGS to the same residual, continuing from its own solutions);
+   reports sweeps and solve time per frame.
 """
 import argparse
 import json
@@ -63,9 +70,12 @@ def _tighten(solver, target, cap, chunk=500):
     return done, (r / b if b > 0 else 0.0)
 
 
-def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, log=print):
+def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, log=print, policy=None,
+            extra_cap=60000):
     """List of dicts {rhs, p_prev, p_star} (device FP32, (D, H, W)) and the
-    kappa statistic."""
+    rms(p* - p_prev) / rms(r) ratios.  With `policy` (a full-grid
+    WarmStartUNet) the frames after the warm-up are solved warm-started by
+    it, as deployed."""
     pairs, ratios = [], []
     for seed in seeds:
         solver, scn, tmr = _solver(n, seed, tol, max_iter, check_every)
@@ -79,10 +89,13 @@ def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, lo
                 rhs = _field(solver, "RHS", shape)
                 p_prev = _field(solver, "P", shape)
                 r0, b0 = solver.residual()
+                if policy is not None:
+                    solver.set_warm_start(policy)
             st = solver.solve()
+            solver.set_warm_start(None)
             if f >= warmup:
                 p_tol = _field(solver, "P", shape)
-                extra, rel = _tighten(solver, target_tol, 100000)
+                extra, rel = _tighten(solver, target_tol, extra_cap)
                 p_star = _field(solver, "P", shape)
                 solver.set_device("P", p_tol.data_ptr())
                 d = (p_star - p_prev).double()
@@ -96,16 +109,28 @@ def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, lo
             solver.advect()
             tmr.iter += 1
             tmr.time += scn.dt
-        log(f"harvest seed {seed}: {frames} pairs in {time.time() - t0:.1f}s, "
-            f"sweeps {[p['sweeps'] for p in pairs[-frames:]]}, extra {[p['extra'] for p in pairs[-frames:]]}")
+        log(f"harvest seed {seed} ({'on policy' if policy is not None else 'plain'}): {frames} pairs in "
+            f"{time.time() - t0:.1f}s, sweeps {[p['sweeps'] for p in pairs[-frames:]]}, "
+            f"target rel {[float('%.2g' % p['rel']) for p in pairs[-frames:]]}")
         solver.close()
-    kappa = float(np.mean(ratios)) if ratios else 1.0
-    return pairs, kappa
+    return pairs, ratios
 
 
-def train(net, params_blz, pairs, iters, crop, lr=1e-3, lr_end=2e-5, seed=0, log=print, log_every=100):
+def _smooth_noise(shape, gen):
+    """Unit-rms random field varying on scales of 8-32 cells."""
+    import torch
+    D, H, W = shape
+    f = 8 * (1 << int(torch.randint(0, 3, (1,), generator=gen)))
+    c = torch.randn((1, 1, max(1, D // f), max(1, H // f), max(1, W // f)), generator=gen).cuda()
+    n = torch.nn.functional.interpolate(c, size=(D, H, W), mode="trilinear", align_corners=False)[0, 0]
+    return n / n.pow(2).mean().sqrt().clamp_min(1e-20)
+
+
+def train(net, params_blz, pairs, iters, crop, lr=1e-3, lr_end=2e-5, seed=0, log=print, log_every=100,
+          perturb=0.5):
     import torch
     rng = np.random.default_rng(seed)
+    gen = torch.Generator().manual_seed(seed)
     W, H, D = params_blz.width, params_blz.height, params_blz.depth
     cw, ch, cd = crop
     hist = []
@@ -117,6 +142,9 @@ def train(net, params_blz, pairs, iters, crop, lr=1e-3, lr_end=2e-5, seed=0, log
         rhs, pp, ps = pr["rhs"], pr["p_prev"], pr["p_star"]
         if dims:
             rhs, pp, ps = (torch.flip(a, dims).contiguous() for a in (rhs, pp, ps))
+        if rng.random() < perturb:
+            amp = float(rng.uniform(0.1, 0.6)) * float((ps - pp).pow(2).mean().sqrt())
+            pp = pp + amp * _smooth_noise(pp.shape, gen)
         org = (8 * int(rng.integers((W - cw) // 8 + 1)), 8 * int(rng.integers((H - ch) // 8 + 1)),
                8 * int(rng.integers((D - cd) // 8 + 1)))
         loss, t2 = net.loss_grad(params_blz, rhs, pp, ps, org)
@@ -134,59 +162,60 @@ def train(net, params_blz, pairs, iters, crop, lr=1e-3, lr_end=2e-5, seed=0, log
 
 
 def evaluate(net, n, seeds, frames, warmup, tol, max_iter, check_every, log=print):
-    """Per frame: sweeps and solve ms, plain and warm-started, from the same state."""
-    import torch
+    """Per seed, a plain and a learned trajectory from the same start (the
+    first `warmup` frames plain in both); per frame: sweeps and solve ms."""
     rows = []
     for seed in seeds:
-        solver, scn, tmr = _solver(n, seed, tol, max_iter, check_every)
-        shape = scn.to_params().field_shape("P")
-        for f in range(warmup + frames):
-            solver.addSource()
-            solver.forces(tmr.time)
-            solver.divergence()
-            if f >= warmup:
-                p_prev = _field(solver, "P", shape)
-                torch.cuda.synchronize()
-                sp = solver.solve()
-                p_plain = _field(solver, "P", shape)
-                solver.set_device("P", p_prev.data_ptr())
-                solver.set_warm_start(net)
-                sl = solver.solve()
-                solver.set_warm_start(None)
-                solver.set_device("P", p_plain.data_ptr())
-                rows.append({"seed": seed, "frame": f, "plain_sweeps": sp["iterations"],
-                             "learned_sweeps": sl["iterations"], "plain_ms": sp["ms_sweeps"] + sp["ms_checks"],
-                             "learned_ms": sl["ms_sweeps"] + sl["ms_checks"] + sl["ms_warm_start"],
-                             "warm_ms": sl["ms_warm_start"], "plain_rel": sp["rel_residual"],
-                             "learned_rel": sl["rel_residual"],
-                             "converged": bool(sp["converged"] and sl["converged"])})
-                log(f"eval seed {seed} frame {f}: plain {sp['iterations']} sweeps, learned {sl['iterations']} "
-                    f"(+{sl['ms_warm_start']:.2f} ms network)")
-            else:
-                solver.solve()
-            solver.gradient()
-            solver.advect()
-            tmr.iter += 1
-            tmr.time += scn.dt
-        solver.close()
+        for learned in (False, True):
+            solver, scn, tmr = _solver(n, seed, tol, max_iter, check_every)
+            for f in range(warmup + frames):
+                solver.addSource()
+                solver.forces(tmr.time)
+                solver.divergence()
+                solver.set_warm_start(net if (learned and f >= warmup) else None)
+                st = solver.solve()
+                if f >= warmup:
+                    rows.append({"seed": seed, "frame": f, "learned": learned, "sweeps": st["iterations"],
+                                 "ms": st["ms_sweeps"] + st["ms_checks"] + st["ms_warm_start"],
+                                 "warm_ms": st["ms_warm_start"], "rel": st["rel_residual"],
+                                 "converged": bool(st["converged"])})
+                solver.gradient()
+                solver.advect()
+                tmr.iter += 1
+                tmr.time += scn.dt
+            sw = [r["sweeps"] for r in rows if r["seed"] == seed and r["learned"] == learned]
+            log(f"eval seed {seed} {'learned' if learned else 'plain'}: sweeps {sw}")
+            solver.close()
     return rows
+
+
+def _ratios(rows):
+    plain = [r for r in rows if not r["learned"]]
+    learned = [r for r in rows if r["learned"]]
+    return (sum(r["sweeps"] for r in plain) / max(1, sum(r["sweeps"] for r in learned)),
+            sum(r["ms"] for r in plain) / max(1e-9, sum(r["ms"] for r in learned)),
+            all(r["converged"] for r in rows))
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--grid", type=int, default=256)
-    ap.add_argument("--train-seeds", default="100-111")
+    ap.add_argument("--plain-seeds", default="100-107", help="seeds harvested with plain solves ('' for none)")
+    ap.add_argument("--policy-seeds", default="108-115", help="seeds harvested on policy in each round")
+    ap.add_argument("--rounds", type=int, default=1, help="on-policy harvest + training rounds")
     ap.add_argument("--eval-seeds", default="900-901")
-    ap.add_argument("--frames", type=int, default=10)
+    ap.add_argument("--frames", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=4)
-    ap.add_argument("--eval-frames", type=int, default=4)
+    ap.add_argument("--eval-frames", type=int, default=8)
     ap.add_argument("--tol", type=float, default=1e-4)
     ap.add_argument("--target-tol", type=float, default=1e-5)
+    ap.add_argument("--extra-cap", type=int, default=60000, help="sweeps spent tightening each target")
     ap.add_argument("--max-iter", type=int, default=40000)
     ap.add_argument("--check-every", type=int, default=20)
-    ap.add_argument("--iters", type=int, default=2000)
+    ap.add_argument("--iters", type=int, default=1500, help="Adam steps per training round")
     ap.add_argument("--crop", type=int, default=128)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--perturb", type=float, default=0.5)
     ap.add_argument("--init", default=None, help="start from these weights (npz)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", required=True)
@@ -202,40 +231,59 @@ def main(argv=None):
 
     torch.cuda.set_device(0)
     n = args.grid
-    t0 = time.time()
-    pairs, kappa = harvest(n, _seed_list(args.train_seeds), args.frames, args.warmup, args.tol, args.target_tol,
-                           args.max_iter, args.check_every, log)
-    t_harvest = time.time() - t0
-    log(f"harvested {len(pairs)} pairs in {t_harvest:.1f}s, kappa {kappa:.4f}")
     crop = (min(args.crop, n),) * 3
-    net = WarmStartUNet(crop, init_params(args.seed), kappa=kappa)
+    grid = family_scene(n=n, seed=0)[0].to_params()
+    params = init_params(args.seed)
+    kappa = 1.0
     if args.init:
-        net.load(args.init)
-        net.set_kappa(kappa)
-    grid = family_scene(n=n, seed=_seed_list(args.train_seeds)[0])[0].to_params()
-    hist, t_train = train(net, grid, pairs, args.iters, crop, lr=args.lr, seed=args.seed, log=log)
-    params = net.get_params()
-    net.close()
+        with np.load(args.init, allow_pickle=False) as z:
+            params, kappa = z["params"], float(z["kappa"])
+    pairs, ratios, hist_all = [], [], []
+    t_harvest = t_train = 0.0
+    full = WarmStartUNet((n, n, n), params, kappa=kappa)
+    rounds = []
+    plain_seeds = _seed_list(args.plain_seeds)
+    policy_seeds = _seed_list(args.policy_seeds)
+    schedule = ([("plain", plain_seeds)] if plain_seeds else []) + [("policy", policy_seeds)] * args.rounds
+    for r, (kind, seeds) in enumerate(schedule):
+        if kind == "policy" and not args.init and r == 0:
+            raise SystemExit("on-policy rounds need a network: give --plain-seeds or --init")
+        t0 = time.time()
+        new, rat = harvest(n, seeds, args.frames, args.warmup, args.tol, args.target_tol, args.max_iter,
+                           args.check_every, log, policy=full if kind == "policy" else None,
+                           extra_cap=args.extra_cap)
+        t_harvest += time.time() - t0
+        pairs += new
+        ratios += rat
+        kappa = float(np.mean(ratios)) if ratios else 1.0
+        log(f"round {r} ({kind}): {len(new)} new pairs, {len(pairs)} in all, kappa {kappa:.4f}")
+        net = WarmStartUNet(crop, full.get_params(), kappa=kappa)
+        lr = args.lr if (r == 0 and not args.init) else 0.3 * args.lr
+        hist, t = train(net, grid, pairs, args.iters, crop, lr=lr, seed=args.seed + r, log=log,
+                        perturb=args.perturb)
+        t_train += t
+        hist_all += hist
+        full.set_params(net.get_params())
+        full.set_kappa(kappa)
+        net.close()
+        rounds.append({"kind": kind, "seeds": seeds, "pairs": len(pairs),
+                       "final_loss": float(np.mean([h[0] for h in hist[-100:]])),
+                       "final_target2": float(np.mean([h[1] for h in hist[-100:]]))})
     del pairs
     torch.cuda.empty_cache()
-    full = WarmStartUNet((n, n, n), params, kappa=kappa)
     rows = evaluate(full, n, _seed_list(args.eval_seeds), args.eval_frames, args.warmup, args.tol, args.max_iter,
                     args.check_every, log)
-    plain = sum(r["plain_sweeps"] for r in rows)
-    learned = sum(r["learned_sweeps"] for r in rows)
+    sweep_ratio, time_ratio, conv = _ratios(rows)
     summary = {
-        "grid": n, "train_seeds": args.train_seeds, "eval_seeds": args.eval_seeds, "frames": args.frames,
-        "warmup": args.warmup, "pairs": len(hist) and len(_seed_list(args.train_seeds)) * args.frames,
-        "tol": args.tol, "target_tol": args.target_tol, "iters": args.iters, "crop": crop[0], "kappa": kappa,
-        "harvest_s": t_harvest, "train_s": t_train,
-        "final_loss": float(np.mean([h[0] for h in hist[-100:]])),
-        "final_target2": float(np.mean([h[1] for h in hist[-100:]])),
-        "eval": rows, "sweep_ratio": plain / max(learned, 1),
-        "time_ratio": sum(r["plain_ms"] for r in rows) / max(sum(r["learned_ms"] for r in rows), 1e-9)}
+        "grid": n, "plain_seeds": args.plain_seeds, "policy_seeds": args.policy_seeds, "rounds": rounds,
+        "eval_seeds": args.eval_seeds, "frames": args.frames, "warmup": args.warmup, "tol": args.tol,
+        "target_tol": args.target_tol, "extra_cap": args.extra_cap, "iters": args.iters, "crop": crop[0],
+        "perturb": args.perturb, "init": args.init, "kappa": kappa, "harvest_s": t_harvest, "train_s": t_train,
+        "eval": rows, "sweep_ratio": sweep_ratio, "time_ratio": time_ratio, "eval_all_converged": conv}
     full.meta = {k: v for k, v in summary.items() if k != "eval"}
     full.save(args.out)
     full.close()
-    log(json.dumps({k: v for k, v in summary.items() if k != "eval"}))
+    log(json.dumps({k: v for k, v in summary.items() if k not in ("eval", "rounds")}))
     if args.report:
         with open(args.report, "w") as f:
             json.dump(summary, f, indent=1)

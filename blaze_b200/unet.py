@@ -22,6 +22,10 @@ from ._lib import check, load
 KIND_CONV3, KIND_UP, KIND_HEAD = 0, 1, 2
 LAYER_NAMES = ["e0a", "e0b", "e1a", "e1b", "e2a", "e2b", "e3a", "e3b",
                "d2a", "d2b", "d1a", "d1b", "d0a", "d0b", "u2", "u1", "u0", "head"]
+TENSOR_NAMES = ["X0", "e0a", "cat0", "d0a", "d0b", "p1", "e1a", "cat1", "d1a", "d1b", "p2", "e2a", "cat2", "d2a",
+                "d2b", "p3", "e3a", "e3b", "g_d0b", "g_d0a", "g_cat0", "g_e0b", "g_e0a", "g_p1", "g_d1b", "g_d1a",
+                "g_cat1", "g_e1b", "g_e1a", "g_p2", "g_d2b", "g_d2a", "g_cat2", "g_e2b", "g_e2a", "g_p3", "g_e3b",
+                "g_e3a"]
 WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
 
 
@@ -129,6 +133,15 @@ class WarmStartUNet:
 
     def kernel_launches(self):
         return int(self._lib.blz_unet_kernel_launches(self._h))
+
+    def tensor(self, name):
+        """FP32 host copy of an internal tensor, padded (D+2, H+2, W+2, C)."""
+        i = TENSOR_NAMES.index(name)
+        shape = (C.c_int * 4)()
+        check(self._lib.blz_unet_tensor_shape(self._h, i, shape))
+        out = np.empty(tuple(shape), np.float32)
+        check(self._lib.blz_unet_get_tensor(self._h, i, out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
+        return out
 
     # -- weight files ---------------------------------------------------------------
     def save(self, path, **meta):

@@ -282,6 +282,16 @@ int  blz_unet_forward(blz_unet *u, const blz_params *grid, const int origin[3], 
  * gradients and loss[0] = L, loss[1] = mean target^2; synchronises.        */
 int  blz_unet_loss_grad(blz_unet *u, const blz_params *grid, const int origin[3], const float *rhs,
                         const float *p, const float *p_target, double loss[2], void *cuda_stream);
+/* Introspection for parity tests: padded shape {D+2, H+2, W+2, C} and FP32
+ * host copy (halo included, no slack) of internal tensor `id`: activations
+ * 0..17 in forward order (X0 e0a cat0 d0a d0b p1 e1a cat1 d1a d1b p2 e2a
+ * cat2 d2a d2b p3 e3a e3b; a concat tensor holds [upsampled, skip]), then
+ * the activation gradients 18..37 (g_d0b g_d0a g_cat0 g_e0b g_e0a g_p1 g_d1b
+ * g_d1a g_cat1 g_e1b g_e1a g_p2 g_d2b g_d2a g_cat2 g_e2b g_e2a g_p3 g_e3b
+ * g_e3a; g_x is dL/dx, masked by x's ReLU where x is an activation), which
+ * exist after the first blz_unet_loss_grad.  Synchronises the device.      */
+int  blz_unet_tensor_shape(const blz_unet *u, int id, int shape[4]);
+int  blz_unet_get_tensor(const blz_unet *u, int id, float *out, long long capacity);
 /* One Adam step (bias-corrected) with the gradients of the last loss_grad.  */
 int  blz_unet_adam(blz_unet *u, float lr, float beta1, float beta2, float eps, void *cuda_stream);
 /* Attach (or, with NULL, detach) a network whose dims equal the grid's: every
@@ -289,6 +299,36 @@ int  blz_unet_adam(blz_unet *u, float lr, float beta1, float beta2, float eps, v
  * pressure and then sweeps to the same residual target.  The network stays
  * owned by the caller and must outlive the attachment.                     */
 int  blz_set_warm_start(blz_solver *s, blz_unet *u);
+
+/* ---- batched simulations ---------------------------------------------------- */
+/* Many independent solvers (uneven grid sizes) stepped together.  No
+ * counterpart in the reference, which runs one FluidSolver per process.  The
+ * pressure solves of all grids share launches: each half sweep is one
+ * persistent launch over every grid's work items, the FP64 residual one
+ * launch over every grid's blocks plus one block per grid that decides,
+ * exactly as that grid's own device-loop solve would, whether it goes on; a
+ * CUDA graph with a conditional WHILE node loops until no grid goes on.  Each
+ * grid's pressure, sweep count and residual equal those of its own solve bit
+ * for bit.  The sweep launch shape is autotuned per batch.  When no grid's
+ * forces depend on time (no curl noise, no moving wind noise), every frame
+ * is one graph launch.  Every solver needs width % 8 == 0, 3-D red-black
+ * order, tol > 0, the same check_every, and max_iter a multiple of it.  The
+ * batch puts all solvers on its own stream; while batched, step them only
+ * through the batch (the solvers stay owned by the caller and must outlive
+ * the batch, which returns them to their own streams when destroyed).      */
+typedef struct blz_batch blz_batch;
+int  blz_batch_create(blz_solver *const *solvers, int n, blz_batch **out);
+int  blz_batch_destroy(blz_batch *b);
+void *blz_batch_stream(blz_batch *b);                      /* the batch's cudaStream_t */
+int  blz_batch_add_source(blz_batch *b);                   /* blz_add_source of every solver */
+/* One frame of every solver: forces at times[i] (NULL: 0), divergence, the
+ * batched solve, gradient, advection; stats[i] (may be NULL) gets solver i's
+ * solve statistics.  Synchronises.                                          */
+int  blz_batch_step(blz_batch *b, const float *times, blz_step_stats *stats);
+/* The batched solve alone, after every solver's divergence.                 */
+int  blz_batch_solve(blz_batch *b, blz_step_stats *stats);
+long long blz_batch_kernel_launches(const blz_batch *b);
+float blz_batch_last_ms(const blz_batch *b);             /* device ms of the last step/solve */
 
 /* Number of kernels this solver launched since creation.                    */
 long long blz_kernel_launches(const blz_solver *s);

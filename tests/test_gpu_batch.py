@@ -1,0 +1,88 @@
+"""Batched simulations against the same simulations stepped one by one: every
+field of every grid, and every solve's sweep count and residual, must be
+identical bit for bit (the batch runs the single-grid kernels' per-cell code
+and stopping rule)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("T", "U", "V", "W", "P")
+
+
+def _make(scenes):
+    from blaze_b200 import FluidSolver, Timer
+    return [FluidSolver(Timer(), s, particles=p) for s, p in scenes]
+
+
+def _scenes(turbulence=False):
+    from blaze_b200.scenes import batch_scenes
+    dims = [(16, 16, 16), (24, 16, 16), (32, 24, 16), (16, 32, 24), (40, 16, 24)]
+    sc = batch_scenes(5, seed=11, tol=1e-4, max_iter=4000, check_every=10, dims=dims)
+    if turbulence:
+        sc[1][0].turbulence_amp, sc[1][0].turbulence_scale = 0.3, 4.0
+    return sc
+
+
+@pytest.mark.parametrize("turbulence", [False, True], ids=["frame-graph", "direct"])
+def test_batch_equals_single(turbulence):
+    from blaze_b200.batch import Batch
+    frames = 4
+    single = _make(_scenes(turbulence))
+    single_stats = [[] for _ in single]
+    for f in range(frames):
+        for i, s in enumerate(single):
+            s.addSource()
+            single_stats[i].append(s.step(f / 24.0))
+    batched = _make(_scenes(turbulence))
+    batch = Batch(batched)
+    batch_stats = []
+    for f in range(frames):
+        batch.add_source()
+        batch_stats.append(batch.step([f / 24.0] * len(batched)))
+    assert batch.kernel_launches() > 0
+    batch.close()
+    for i in range(len(single)):
+        for f in range(frames):
+            a, b = single_stats[i][f], batch_stats[f][i]
+            assert a["iterations"] == b["iterations"] and a["residual_checks"] == b["residual_checks"], (i, f, a, b)
+            assert a["residual"] == b["residual"] and a["converged"] == b["converged"]
+        for name in FIELDS:
+            assert np.array_equal(single[i].get(name), batched[i].get(name)), (i, name)
+    for s in single + batched:
+        s.close()
+
+
+def test_batch_solve_only():
+    from blaze_b200.batch import Batch
+    sims = _make(_scenes())
+    for s in sims:
+        s.addSource()
+        s.forces(0.0)
+        s.divergence()
+    batch = Batch(sims)
+    stats = batch.solve()
+    assert all(st["converged"] for st in stats)
+    for s, st in zip(sims, stats):
+        r, b = s.residual()
+        assert r / b <= 1e-4 and abs(r - st["residual"]) <= 1e-12 * max(r, 1e-30)
+    batch.close()
+
+
+def test_batch_rejects_mismatched_solvers():
+    import ctypes as C
+    from blaze_b200 import FluidSolver, Timer, _lib
+    from blaze_b200.scenes import batch_scenes
+    lib = _lib.load()
+    sc = batch_scenes(2, seed=3, tol=1e-4, max_iter=400, dims=[(16, 16, 16)])
+    sc[1][0].check_every = 10
+    sims = [FluidSolver(Timer(), s) for s, _ in sc]
+    arr = (C.c_void_p * 2)(*[s._h.value for s in sims])
+    h = C.c_void_p()
+    assert lib.blz_batch_create(arr, 2, C.byref(h)) == -2
+    sc2 = batch_scenes(1, seed=3, tol=1e-4, max_iter=400, dims=[(20, 16, 16)])
+    s2 = FluidSolver(Timer(), sc2[0][0])
+    arr2 = (C.c_void_p * 1)(s2._h.value)
+    assert lib.blz_batch_create(arr2, 1, C.byref(h)) == -2          # width % 8 != 0
+    for s in sims + [s2]:
+        s.close()
