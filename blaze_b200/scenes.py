@@ -252,7 +252,9 @@ def batch_scenes(count=64, seed=4, tol=1e-4, max_iter=20000, check_every=20, dim
     out = []
     for _ in range(count):
         W, H, D = dims[rng.integer(0, len(dims) - 1)]
-        s = SceneSettings(gridRes=(W, H, D), dx=1.0 / W, dt=1.0 / 24, closedBounds=(1, 1, 1, 0, 1, 1),
+        dx = 1.0 / W
+        s = SceneSettings(gridRes=(W, H, D), dx=dx, dt=1.0 / 24, closedBounds=(1, 1, 1, 0, 1, 1),
+                          domainBboxMax=(W * dx, H * dx, D * dx),
                           maxIterSolve=max_iter, tol=tol, check_every=check_every, buoyancy=1.0,
                           vorticityConf=rng.uniform(0.1, 0.6), bc_mode=_abi.BLZ_BC_FREE_SURFACE)
         parts = []

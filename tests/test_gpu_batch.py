@@ -43,6 +43,7 @@ def test_batch_equals_single(turbulence):
     assert batch.kernel_launches() > 0
     batch.close()
     for i in range(len(single)):
+        assert all(st["iterations"] > 0 and st["rhs_norm"] > 0 for st in single_stats[i]), i
         for f in range(frames):
             a, b = single_stats[i][f], batch_stats[f][i]
             assert a["iterations"] == b["iterations"] and a["residual_checks"] == b["residual_checks"], (i, f, a, b)
@@ -65,6 +66,7 @@ def test_batch_solve_only():
     assert all(st["converged"] for st in stats)
     for s, st in zip(sims, stats):
         r, b = s.residual()
+        assert b > 0 and st["iterations"] > 0
         assert r / b <= 1e-4 and abs(r - st["residual"]) <= 1e-12 * max(r, 1e-30)
     batch.close()
 
