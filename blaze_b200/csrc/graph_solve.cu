@@ -61,7 +61,8 @@ __global__ void k_ctl_check(SolveCtl *c, const double *__restrict__ norm2, cudaG
 cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
                               float *p_r, float *p_b, double *partials, int n_partials, double *norm2,
                               SolveCtl *ctl, int chunk, int max_iter, double tol, int variant, cudaStream_t st,
-                              cudaGraphExec_t *exec_out, int *body_kernels, int *prologue_kernels) {
+                              cudaGraphExec_t *exec_out, int *body_kernels, int *prologue_kernels, float *q_r,
+                              float *q_b) {
     cudaError_t err = cudaSuccess;
     cudaGraph_t graph = nullptr, body = nullptr;
     cudaGraphConditionalHandle handle;
@@ -93,9 +94,9 @@ cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float 
     // Body: chunk sweeps (timed with the global timer), residual, decision.
     CKG(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     k_ctl_mark<<<1, 1, 0, st>>>(ctl, 0);
-    launch_rbgs_sweeps(g, sp, rhs_r, rhs_b, p_r, p_b, chunk, st, &dummy, variant);
+    launch_rbgs_sweeps(g, sp, rhs_r, rhs_b, p_r, p_b, chunk, st, &dummy, variant, q_r, q_b);
     k_ctl_mark<<<1, 1, 0, st>>>(ctl, 1);
-    *body_kernels = 2 + 2 * chunk + launch_residual(g, sp, rhs_r, rhs_b, p_r, p_b, partials, n_partials, norm2, st) + 1;
+    *body_kernels = 2 + (int)dummy + launch_residual(g, sp, rhs_r, rhs_b, p_r, p_b, partials, n_partials, norm2, st) + 1;
     k_ctl_check<<<1, 1, 0, st>>>(ctl, norm2, handle, 1, chunk, max_iter, tol);
     CKG(cudaStreamEndCapture(st, &body));
     CKG(cudaGraphInstantiate(exec_out, graph, 0));

@@ -210,17 +210,152 @@ k_rbgs_seg(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float 
     seg_sweep<KZ>(g, sp, rhs_c, p_o, p_c, colour, mq, j, k0);
 }
 
-// (planes per thread, rows per block) of each segment-kernel variant.
-static const int kVariantKZ[kSweepVariants] = {1, 2, 4, 8, 2, 4};
-static const int kVariantBY[kSweepVariants] = {8, 8, 4, 4, 4, 8};
+// ---------------------------------------------------------------------------
+// Temporal blocking: two red-black sweeps per pass over HBM, out of place
+// (reads rhs and the black half of p_in, writes both halves of p_out; a
+// red update never reads the old red values, so p_in's red half is not
+// needed).  A CTA owns TY full-width rows and ZC planes of the output and
+// carries a 4-row / 4-plane halo; it marches a wavefront along z: at step t
+// level 0 updates red on plane t, level 1 black on t-1, level 2 red on t-2,
+// level 3 black on t-3, each level over a region one row and one plane
+// narrower than the one before, so every update reads exactly the values
+// the in-place sweeps would (the z neighbours from the thread's own
+// registers, the in-plane neighbours from shared memory, four plane slots
+// per colour).  Per cell the arithmetic is gs_segment's, so a pass equals
+// two sweeps of the segment kernel bit for bit.  HBM traffic per pass is
+// about 10 B/cell instead of 24 B/cell for two unblocked sweeps; the price is
+// recomputing the halo.
+// ---------------------------------------------------------------------------
+constexpr int kTbThreads = 768;
 
-int sweep_variant_count(const Geom &g) { return (g.W & 7) == 0 ? kSweepVariants : 0; }
+__host__ __device__ inline int tb_rows_tile(int Wq, int H) {
+    const int ty = kTbThreads / Wq - 8;
+    return ty < H ? ty : H;
+}
+
+__global__ void __launch_bounds__(kTbThreads, 1)
+k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float *__restrict__ rhs_b,
+           const float *__restrict__ pin_b, float *__restrict__ pout_r, float *__restrict__ pout_b, int TY, int ZC) {
+    extern __shared__ float4 sm4[];
+    const int Wh = g.W >> 1, Wq = Wh >> 2;
+    const int rows = TY + 8;
+    const int mq = threadIdx.x, r = threadIdx.y;
+    const int j0 = blockIdx.x * TY, z0 = blockIdx.y * ZC;
+    const int z1 = z0 + ZC < g.D ? z0 + ZC : g.D;
+    const int j = j0 - 4 + r;
+    const bool row_ok = j >= 0 && j < g.H;
+    const int m0 = 4 * mq;
+    const size_t pl = (size_t)Wh * g.H;
+    const size_t rowoff = (size_t)m0 + (size_t)Wh * (size_t)(row_ok ? j : 0);
+    const bool first = m0 == 0, last = m0 + 4 == Wh;
+    const bool has_ym = j > 0, has_yp = j < g.H - 1;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    // slot (colour, plane & 3), row, quad
+    auto S = [&](int colour, int plane, int row) -> float4 * {
+        return sm4 + ((size_t)((colour * 4 + (plane & 3)) * rows + row)) * Wq;
+    };
+    auto load_black = [&](int k) -> float4 {
+        return (row_ok && k >= 0 && k < g.D) ? ld4(pin_b + rowoff + (size_t)k * pl) : zero4;
+    };
+    // One level: the colour `c` cells of this thread's quad on plane k.
+    auto update = [&](int c, int k, float4 o, float4 zm, float4 zp) -> float4 {
+        const int oc = c ^ 1;
+        const float4 *so = S(oc, k, r);
+        const float4 ym = has_ym ? S(oc, k, r - 1)[mq] : zero4;
+        const float4 yp = has_yp ? S(oc, k, r + 1)[mq] : zero4;
+        const int s = (j + k + c) & 1;
+        const float *sf = reinterpret_cast<const float *>(so);
+        const float xe = s == 0 ? (first ? 0.0f : sf[m0 - 1]) : (last ? 0.0f : sf[m0 + 4]);
+        const bool has_zm = k > 0, has_zp = k < g.D - 1;
+        const float4 rv = ld4((c ? rhs_b : rhs_r) + rowoff + (size_t)k * pl);
+        return gs_segment(sp, s, first, last, rv, o, xe, ym, yp, has_zm ? zm : zero4, has_zp ? zp : zero4,
+                          has_ym, has_yp, has_zm, has_zp);
+    };
+    auto active = [&](int h, int k) {
+        return row_ok && r >= 1 + h && r < rows - 1 - h && k >= z0 - 3 + h && k < z1 + 3 - h && k >= 0 &&
+               k < g.D;
+    };
+    // register windows: black planes t-3..t+1, red planes t-4..t
+    float4 bm3 = zero4, bm2 = zero4, bm1 = load_black(z0 - 4), b0 = load_black(z0 - 3), bp1;
+    float4 rm4 = zero4, rm3 = zero4, rm2 = zero4, rm1 = zero4, r0 = zero4;
+    S(1, z0 - 4, r)[mq] = bm1;
+    S(1, z0 - 3, r)[mq] = b0;
+    for (int t = z0 - 3; t < z1 + 3; ++t) {
+        bp1 = load_black(t + 1);
+        S(1, t + 1, r)[mq] = bp1;
+        __syncthreads();
+        if (active(0, t)) { r0 = update(0, t, b0, bm1, bp1); S(0, t, r)[mq] = r0; }
+        __syncthreads();
+        if (active(1, t - 1)) { bm1 = update(1, t - 1, rm1, rm2, r0); S(1, t - 1, r)[mq] = bm1; }
+        __syncthreads();
+        if (active(2, t - 2)) { rm2 = update(0, t - 2, bm2, bm3, bm1); S(0, t - 2, r)[mq] = rm2; }
+        __syncthreads();
+        const int k3 = t - 3;
+        if (active(3, k3)) {
+            bm3 = update(1, k3, rm3, rm4, rm2);
+            if (k3 >= z0 && r >= 4 && r < 4 + TY) {
+                *reinterpret_cast<float4 *>(pout_r + rowoff + (size_t)k3 * pl) = rm3;
+                *reinterpret_cast<float4 *>(pout_b + rowoff + (size_t)k3 * pl) = bm3;
+            }
+        }
+        rm4 = rm3; rm3 = rm2; rm2 = rm1; rm1 = r0;
+        bm3 = bm2; bm2 = bm1; bm1 = b0; b0 = bp1;
+    }
+}
+
+static bool tb_supported(const Geom &g) {
+    if ((g.W & 7) != 0) return false;
+    const int Wq = g.W >> 3;
+    return Wq <= 48 && tb_rows_tile(Wq, g.H) >= 1;
+}
+
+static size_t tb_smem(const Geom &g, int TY) { return sizeof(float4) * 8 * (size_t)(TY + 8) * (g.W >> 3); }
+
+// One pass = two sweeps from (p_in) into (p_out).
+static void launch_tb_pass(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
+                           const float *pin_b, float *pout_r, float *pout_b, int ZC, cudaStream_t st) {
+    const int Wq = g.W >> 3, TY = tb_rows_tile(Wq, g.H);
+    const size_t smem = tb_smem(g, TY);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_rbgs_tb2, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr_set = true;
+    }
+    const dim3 b(Wq, TY + 8, 1);
+    const dim3 gr((g.H + TY - 1) / TY, (g.D + ZC - 1) / ZC, 1);
+    k_rbgs_tb2<<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC);
+}
+
+// (planes per thread, rows per block) of each segment-kernel variant; the
+// variants after them are the temporal-blocking pass with ZC planes per CTA.
+static const int kVariantKZ[kSegVariants] = {1, 2, 4, 8, 2, 4};
+static const int kVariantBY[kSegVariants] = {8, 8, 4, 4, 4, 8};
+static const int kVariantZC[kSweepVariants - kSegVariants] = {16, 32};
+
+int sweep_variant_count(const Geom &g) {
+    if ((g.W & 7) != 0) return 0;
+    return tb_supported(g) ? kSweepVariants : kSegVariants;
+}
 
 void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                         const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
-                        long long *launches, int variant) {
+                        long long *launches, int variant, float *q_r, float *q_b) {
+    if (variant >= kSegVariants && variant < kSweepVariants && q_r && q_b && tb_supported(g)) {
+        // Passes alternate p -> q -> p, an even number of them, so the
+        // result lands in p; the remaining sweeps run unblocked.
+        const int passes = (sweeps / 4) * 2;
+        const int zc = kVariantZC[variant - kSegVariants];
+        for (int i = 0; i < passes; ++i) {
+            if ((i & 1) == 0) launch_tb_pass(g, sp, rhs_r, rhs_b, p_b, q_r, q_b, zc, st);
+            else launch_tb_pass(g, sp, rhs_r, rhs_b, q_b, p_r, p_b, zc, st);
+        }
+        *launches += passes;
+        sweeps -= 2 * passes;
+        variant = 2;
+    }
+    if (sweeps <= 0) return;
     if ((g.W & 7) == 0) {
-        const int v = (variant >= 0 && variant < kSweepVariants) ? variant : 0;
+        const int v = (variant >= 0 && variant < kSegVariants) ? variant : 0;
         const int Wq = g.W >> 3, kz = kVariantKZ[v], by = kVariantBY[v];
         const int bx = std::min(32, Wq);
         const dim3 b(bx, std::max(1, std::min(by * (32 / bx), 256 / bx)), 1);

@@ -57,14 +57,17 @@ void launch_turb_apply(const Geom &g, float *U, float *V, float *W, const float 
 void launch_divergence(const Geom &g, const float *U, const float *V, const float *W,
                        const OpenFaces &o, float *rhs_r, float *rhs_b, cudaStream_t st);
 // Red-black sweeps.  For W % 8 == 0, `variant` picks one of
-// kSweepVariants launch shapes of the segment kernel (planes per thread and
-// rows per block; all give identical results); other W use the one-cell
-// kernel.
-constexpr int kSweepVariants = 6;
+// kSegVariants launch shapes of the segment kernel (planes per thread and
+// rows per block), or (variants kSegVariants.. kSweepVariants-1, with a
+// scratch pressure q of the grid's size) the temporal-blocking kernel, two
+// sweeps per pass; all give identical results.  Other W use the one-cell
+// kernel.  sweep_variant_count: variants available for this grid (0: W % 8).
+constexpr int kSegVariants = 6;
+constexpr int kSweepVariants = 8;
 int  sweep_variant_count(const Geom &g);
 void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                         const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
-                        long long *launches, int variant = 0);
+                        long long *launches, int variant = 0, float *q_r = nullptr, float *q_b = nullptr);
 void launch_plane_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                          const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
                          long long *launches);
@@ -93,7 +96,8 @@ struct SolveCtl {
 cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
                               float *p_r, float *p_b, double *partials, int n_partials, double *norm2,
                               SolveCtl *ctl, int chunk, int max_iter, double tol, int variant, cudaStream_t st,
-                              cudaGraphExec_t *exec_out, int *body_kernels, int *prologue_kernels);
+                              cudaGraphExec_t *exec_out, int *body_kernels, int *prologue_kernels,
+                              float *q_r = nullptr, float *q_b = nullptr);
 
 // -- batched solve over many grids (k_project.cu kernels, batch.cu graph) ---
 struct BatchSim {

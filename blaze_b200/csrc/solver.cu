@@ -459,6 +459,11 @@ static int residual_sync(blz_solver *s, double *r, double *b) {
 // read), timed with CUDA events; the fastest is kept per (device, grid dims)
 // for the life of the process.  BLZ_SWEEP_VARIANT or params.sweep_variant
 // forces a choice.
+// Scratch pressure of the temporal-blocking sweeps (slot 4 of the six
+// T-sized scratch arrays; the autotuner's copy of p uses slots 0-1).
+static float *q_r(blz_solver *s) { return s->scratch + 4 * n_of(s->P, 0); }
+static float *q_b(blz_solver *s) { return s->scratch + 4 * n_of(s->P, 0) + n_of(s->P, 0) / 2; }
+
 static std::mutex g_tune_mu;
 static std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
 
@@ -486,9 +491,10 @@ static int choose_variant(blz_solver *s) {
     float best_ms = 1e30f;
     long long dummy = 0;
     for (int v = 0; v < nv; ++v) {
-        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 1, s->st, &dummy, v);
+        // 4 + 8 sweeps: whole passes for the temporal-blocking variants
+        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 4, s->st, &dummy, v, q_r(s), q_b(s));
         CK(s, cudaEventRecord(s->ev[6], s->st));
-        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 3, s->st, &dummy, v);
+        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 8, s->st, &dummy, v, q_r(s), q_b(s));
         CK(s, cudaEventRecord(s->ev[7], s->st));
         CKL(s);
         CK(s, cudaEventSynchronize(s->ev[7]));
@@ -496,7 +502,7 @@ static int choose_variant(blz_solver *s) {
         CK(s, cudaEventElapsedTime(&ms, s->ev[6], s->ev[7]));
         if (ms < best_ms) { best_ms = ms; best = v; }
     }
-    s->launches += 8LL * nv;
+    s->launches += dummy;
     s->variant = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[key] = best;
@@ -510,7 +516,8 @@ static int sweeps(blz_solver *s, int n) {
     } else {
         int rc = choose_variant(s);
         if (rc != BLZ_OK) return rc;
-        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, s->st, &s->launches, s->variant);
+        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, s->st, &s->launches, s->variant,
+                           q_r(s), q_b(s));
     }
     CKL(s);
     return BLZ_OK;
@@ -525,7 +532,7 @@ static int solve_device_loop(blz_solver *s, blz_step_stats *st) {
         cudaError_t e = build_solve_graph(s->g, solve_params(P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->partials,
                                           s->n_partials, s->d_norm2, s->ctl, std::max(1, P.check_every), P.max_iter,
                                           P.tol, s->variant, s->st, &s->solve_exec, &s->graph_body,
-                                          &s->graph_prologue);
+                                          &s->graph_prologue, q_r(s), q_b(s));
         if (e != cudaSuccess) return fail(s, BLZ_ERR_CUDA, "building the solve graph failed: %s", cudaGetErrorString(e));
     }
     CK(s, cudaGraphLaunch(s->solve_exec, s->st));

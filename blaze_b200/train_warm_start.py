@@ -71,7 +71,7 @@ def _tighten(solver, target, cap, chunk=500):
 
 
 def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, log=print, policy=None,
-            extra_cap=60000):
+            extra_cap=60000, stride=1):
     """List of dicts {rhs, p_prev, p_star} (device FP32, (D, H, W)) and the
     rms(p* - p_prev) / rms(r) ratios.  With `policy` (a full-grid
     WarmStartUNet) the frames after the warm-up are solved warm-started by
@@ -85,15 +85,16 @@ def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, lo
             solver.addSource()
             solver.forces(tmr.time)
             solver.divergence()
-            if f >= warmup:
+            keep = f >= warmup and (f - warmup) % stride == 0
+            if keep:
                 rhs = _field(solver, "RHS", shape)
                 p_prev = _field(solver, "P", shape)
                 r0, b0 = solver.residual()
-                if policy is not None:
-                    solver.set_warm_start(policy)
+            if f >= warmup and policy is not None:
+                solver.set_warm_start(policy)
             st = solver.solve()
             solver.set_warm_start(None)
-            if f >= warmup:
+            if keep:
                 p_tol = _field(solver, "P", shape)
                 extra, rel = _tighten(solver, target_tol, extra_cap)
                 p_star = _field(solver, "P", shape)
@@ -109,9 +110,10 @@ def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, lo
             solver.advect()
             tmr.iter += 1
             tmr.time += scn.dt
-        log(f"harvest seed {seed} ({'on policy' if policy is not None else 'plain'}): {frames} pairs in "
-            f"{time.time() - t0:.1f}s, sweeps {[p['sweeps'] for p in pairs[-frames:]]}, "
-            f"target rel {[float('%.2g' % p['rel']) for p in pairs[-frames:]]}")
+        kept = [p for p in pairs if p["seed"] == seed]
+        log(f"harvest seed {seed} ({'on policy' if policy is not None else 'plain'}): {len(kept)} pairs in "
+            f"{time.time() - t0:.1f}s, sweeps {[p['sweeps'] for p in kept]}, "
+            f"target rel {[float('%.2g' % p['rel']) for p in kept]}")
         solver.close()
     return pairs, ratios
 
@@ -204,7 +206,8 @@ def main(argv=None):
     ap.add_argument("--policy-seeds", default="108-115", help="seeds harvested on policy in each round")
     ap.add_argument("--rounds", type=int, default=1, help="on-policy harvest + training rounds")
     ap.add_argument("--eval-seeds", default="900-901")
-    ap.add_argument("--frames", type=int, default=8)
+    ap.add_argument("--frames", type=int, default=8, help="frames after the warm-up per harvested seed")
+    ap.add_argument("--stride", type=int, default=1, help="harvest every stride-th of those frames")
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--eval-frames", type=int, default=8)
     ap.add_argument("--tol", type=float, default=1e-4)
@@ -251,7 +254,7 @@ def main(argv=None):
         t0 = time.time()
         new, rat = harvest(n, seeds, args.frames, args.warmup, args.tol, args.target_tol, args.max_iter,
                            args.check_every, log, policy=full if kind == "policy" else None,
-                           extra_cap=args.extra_cap)
+                           extra_cap=args.extra_cap, stride=args.stride)
         t_harvest += time.time() - t0
         pairs += new
         ratios += rat
@@ -276,7 +279,8 @@ def main(argv=None):
     sweep_ratio, time_ratio, conv = _ratios(rows)
     summary = {
         "grid": n, "plain_seeds": args.plain_seeds, "policy_seeds": args.policy_seeds, "rounds": rounds,
-        "eval_seeds": args.eval_seeds, "frames": args.frames, "warmup": args.warmup, "tol": args.tol,
+        "eval_seeds": args.eval_seeds, "frames": args.frames, "stride": args.stride, "warmup": args.warmup,
+        "tol": args.tol,
         "target_tol": args.target_tol, "extra_cap": args.extra_cap, "iters": args.iters, "crop": crop[0],
         "perturb": args.perturb, "init": args.init, "kappa": kappa, "harvest_s": t_harvest, "train_s": t_train,
         "eval": rows, "sweep_ratio": sweep_ratio, "time_ratio": time_ratio, "eval_all_converged": conv}

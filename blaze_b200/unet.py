@@ -186,3 +186,38 @@ class WarmStartUNet:
 
 def weights_path(name):
     return os.path.join(WEIGHTS_DIR, name)
+
+
+def _main(argv=None):
+    """Times the network's forward pass on a random n^3 grid:
+    python -m blaze_b200.unet --forward 256 --reps 5"""
+    import argparse
+    import time
+    import torch
+    from .scenes import SceneSettings
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--forward", type=int, default=128, help="grid edge (multiple of 8)")
+    ap.add_argument("--reps", type=int, default=5)
+    args = ap.parse_args(argv)
+    n = args.forward
+    g = SceneSettings(gridRes=(n, n, n), dx=1.0 / n, closedBounds=(1, 1, 1, 0, 1, 1), bc_mode=1).to_params()
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    rhs = torch.randn((n, n, n), device="cuda", generator=gen)
+    p = 0.1 * torch.randn((n, n, n), device="cuda", generator=gen)
+    net = WarmStartUNet((n, n, n), init_params(0))
+    out = torch.empty((n, n, n), device="cuda")
+    net.forward(g, rhs, p, out=out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.reps):
+        net.forward(g, rhs, p, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.reps
+    print(json.dumps({"grid": n, "forward_ms": ms, "launches_per_forward": net.kernel_launches() // (args.reps + 1)}))
+    net.close()
+
+
+if __name__ == "__main__":
+    _main()
