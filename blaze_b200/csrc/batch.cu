@@ -5,7 +5,8 @@
 // cells, a single grid's half sweep is a few microseconds of HBM traffic, less
 // than a kernel launch.  The batch therefore runs every grid's solve in the
 // same launches: each half sweep is one persistent grid-stride launch over the
-// segment work items of all grids (k_batch_sweep), the FP64 residual is one
+// segment work items of the grids still running (k_batch_sweep; the list is
+// rebuilt after every check, so a grid that finished costs nothing), the FP64 residual is one
 // launch over every grid's residual blocks plus one block per grid deciding
 // continue/stop, and a CUDA graph with a conditional WHILE node repeats
 // {check_every sweeps, residual, decision} until no grid is left running.
@@ -35,11 +36,26 @@ __global__ void k_batch_begin(BatchCtl *ctl, int n) {
     if (s < n) ctl[s] = BatchCtl{0, 0, 0, 1, 0.0, 0.0};
 }
 
-__global__ void k_batch_cond(const BatchCtl *__restrict__ ctl, int n, cudaGraphConditionalHandle h) {
-    int any = 0;
-    for (int s = threadIdx.x; s < n; s += blockDim.x) any |= ctl[s].active;
-    any = __syncthreads_or(any);
-    if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+// Lists the grids still running with their item offsets (for the next
+// sweeps) and, inside the solve graph, sets whether the loop goes on.
+__global__ void k_batch_active(const BatchCtl *__restrict__ ctl, int n, const long long *__restrict__ item0,
+                               BatchActive *act, int *act_sim, long long *act_item0, int set_cond,
+                               cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0) return;
+    int na = 0;
+    long long acc = 0;
+    for (int s = 0; s < n; ++s) {
+        if (!ctl[s].active) continue;
+        act_sim[na] = s;
+        act_item0[na] = acc;
+        acc += item0[s + 1] - item0[s];
+        ++na;
+    }
+    act_item0[na] = acc;
+    act->n = na;
+    act->sim = act_sim;
+    act->item0 = act_item0;
+    if (set_cond) cudaGraphSetConditional(h, na > 0 ? 1u : 0u);
 }
 
 constexpr int kKZ[4] = {1, 2, 4, 8};
@@ -55,6 +71,9 @@ struct blz_batch {
     BatchSim *d_sims = nullptr;
     BatchCtl *d_ctl = nullptr, *h_ctl = nullptr;
     long long *d_item0 = nullptr;             // 4 tables (kz = 1, 2, 4, 8) of n + 1 offsets
+    BatchActive *d_act = nullptr;             // grids still running, rebuilt after each check
+    int *d_act_sim = nullptr;
+    long long *d_act_item0 = nullptr;
     int *d_blk0 = nullptr;
     int total_blocks = 0;
     double *partials = nullptr;
@@ -93,12 +112,17 @@ static const long long *item0_of(const blz_batch *b, int kz) {
     return b->d_item0 + (size_t)t * (b->n + 1);
 }
 
+static void active_list(blz_batch *b, int kz, int set_cond, cudaGraphConditionalHandle h) {
+    k_batch_active<<<1, 32, 0, b->st>>>(b->d_ctl, b->n, item0_of(b, kz), b->d_act, b->d_act_sim, b->d_act_item0,
+                                        set_cond, h);
+}
+
 // Body of the batched solve, appended to the capture in progress on b->st:
-// check_every sweeps over the active grids, their residual and decision.
+// check_every sweeps over the grids still running, their residual and decision.
 static void capture_body(blz_batch *b, cudaGraphConditionalHandle h) {
-    launch_batch_sweeps(b->d_sims, item0_of(b, b->kz), b->n, b->chunk, b->kz, b->grid, b->block, b->d_ctl, b->st);
+    launch_batch_sweeps(b->d_sims, b->d_act, b->n, b->chunk, b->kz, b->grid, b->block, b->st);
     launch_batch_check(b->d_sims, b->d_blk0, b->n, b->total_blocks, b->d_ctl, b->partials, 1, b->chunk, b->st);
-    k_batch_cond<<<1, 256, 0, b->st>>>(b->d_ctl, b->n, h);
+    active_list(b, b->kz, 1, h);
 }
 
 // Builds [stages before the solve] + solve loop + [stages after] as one graph.
@@ -127,7 +151,7 @@ static int build_graph(blz_batch *b, bool with_stages, cudaGraphExec_t *out, lon
     if (rc == BLZ_OK) {
         k_batch_begin<<<(b->n + 255) / 256, 256, 0, b->st>>>(b->d_ctl, b->n);
         launch_batch_check(b->d_sims, b->d_blk0, b->n, b->total_blocks, b->d_ctl, b->partials, 0, b->chunk, b->st);
-        k_batch_cond<<<1, 256, 0, b->st>>>(b->d_ctl, b->n, h);
+        active_list(b, b->kz, 1, h);
         cudaStreamCaptureStatus status;
         const cudaGraphNode_t *deps = nullptr;
         size_t ndeps = 0;
@@ -218,15 +242,16 @@ static int tune(blz_batch *b) {
     for (int ki = 0; ki < 4 && e == cudaSuccess; ++ki)
         for (int bi = 0; bi < 2 && e == cudaSuccess; ++bi) {
             const int kz = kKZ[ki], blk = kBlocks[bi], grid = batch_sweep_grid(kz, blk);
-            launch_batch_sweeps(d_scr, item0_of(b, kz), b->n, 1, kz, grid, blk, b->d_ctl, b->st);
+            active_list(b, kz, 0, 0);
+            launch_batch_sweeps(d_scr, b->d_act, b->n, 1, kz, grid, blk, b->st);
             e = cudaEventRecord(b->ev0, b->st);
-            launch_batch_sweeps(d_scr, item0_of(b, kz), b->n, 2, kz, grid, blk, b->d_ctl, b->st);
+            launch_batch_sweeps(d_scr, b->d_act, b->n, 2, kz, grid, blk, b->st);
             if (e == cudaSuccess) e = cudaEventRecord(b->ev1, b->st);
             if (e == cudaSuccess) e = cudaGetLastError();
             if (e == cudaSuccess) e = cudaEventSynchronize(b->ev1);
             float ms = 0.0f;
             if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-            b->launches += 6;
+            b->launches += 7;
             if (e == cudaSuccess && ms < best) { best = ms; b->kz = kz; b->block = blk; b->grid = grid; }
         }
     cudaStreamSynchronize(b->st);
@@ -243,6 +268,7 @@ static void release(blz_batch *b) {
     if (b->solve_exec) cudaGraphExecDestroy(b->solve_exec);
     for (auto &x : b->frame_exec) if (x) cudaGraphExecDestroy(x);
     cudaFree(b->d_sims); cudaFree(b->d_ctl); cudaFree(b->d_item0); cudaFree(b->d_blk0); cudaFree(b->partials);
+    cudaFree(b->d_act); cudaFree(b->d_act_sim); cudaFree(b->d_act_item0);
     if (b->h_ctl) cudaFreeHost(b->h_ctl);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -329,6 +355,9 @@ int blz_batch_create(blz_solver *const *sims, int n, blz_batch **out) {
     ck(cudaMallocHost(&b->h_ctl, sizeof(BatchCtl) * n), "cudaMallocHost");
     ck(cudaMalloc(&b->d_item0, sizeof(long long) * item0.size()), "cudaMalloc");
     ck(cudaMalloc(&b->d_blk0, sizeof(int) * (n + 1)), "cudaMalloc");
+    ck(cudaMalloc(&b->d_act, sizeof(BatchActive)), "cudaMalloc");
+    ck(cudaMalloc(&b->d_act_sim, sizeof(int) * n), "cudaMalloc");
+    ck(cudaMalloc(&b->d_act_item0, sizeof(long long) * (n + 1)), "cudaMalloc");
     ck(cudaMalloc(&b->partials, sizeof(double) * 2 * (size_t)acc), "cudaMalloc");
     ck(cudaEventCreate(&b->ev0), "cudaEventCreate");
     ck(cudaEventCreate(&b->ev1), "cudaEventCreate");
@@ -336,7 +365,7 @@ int blz_batch_create(blz_solver *const *sims, int n, blz_batch **out) {
     if (rc == BLZ_OK) ck(cudaMemcpy(b->d_item0, item0.data(), sizeof(long long) * item0.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
     if (rc == BLZ_OK) ck(cudaMemcpy(b->d_blk0, blk0.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice), "cudaMemcpy");
     for (int i = 0; i < n && rc == BLZ_OK; ++i) rc = blz_set_stream(sims[i], b->st);
-    b->prologue = 1 + 2 + 1;
+    b->prologue = 1 + 2 + 1;                 // begin, residual + decision, active list
     if (rc != BLZ_OK) {
         release(b);
         delete b;

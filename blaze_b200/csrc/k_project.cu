@@ -747,23 +747,28 @@ long long batch_sweep_items(const Geom &g, int kz) {
     return (long long)(g.W >> 3) * g.H * ((g.D + kz - 1) / kz);
 }
 
+// Items of the grids still running: act->n grids, grid act->sim[i] owning
+// items [act->item0[i], act->item0[i+1]) (rebuilt after every check).
 template <int KZ>
 __global__ void __launch_bounds__(256)
-k_batch_sweep(const BatchSim *__restrict__ sims, const long long *__restrict__ item0, int nsims,
-              const BatchCtl *__restrict__ ctl, int colour) {
+k_batch_sweep(const BatchSim *__restrict__ sims, const BatchActive *__restrict__ act, int colour) {
     extern __shared__ long long s_item0[];
-    for (int i = threadIdx.x; i <= nsims; i += blockDim.x) s_item0[i] = item0[i];
+    const int na = act->n;
+    int *s_sim = reinterpret_cast<int *>(s_item0 + na + 1);
+    for (int i = threadIdx.x; i <= na; i += blockDim.x) {
+        s_item0[i] = act->item0[i];
+        if (i < na) s_sim[i] = act->sim[i];
+    }
     __syncthreads();
-    const long long total = s_item0[nsims];
+    const long long total = s_item0[na];
     for (long long it = blockIdx.x * (long long)blockDim.x + threadIdx.x; it < total;
          it += (long long)gridDim.x * blockDim.x) {
-        int lo = 0, hi = nsims - 1;
+        int lo = 0, hi = na - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (s_item0[mid] <= it) lo = mid; else hi = mid - 1;
         }
-        if (!ctl[lo].active) continue;
-        const BatchSim &S = sims[lo];
+        const BatchSim &S = sims[s_sim[lo]];
         const long long local = it - s_item0[lo];
         const int Wq = S.g.W >> 3;
         const int mq = (int)(local % Wq);
@@ -787,16 +792,16 @@ int batch_sweep_grid(int kz, int block) {
     return sms * std::max(1, per);
 }
 
-void launch_batch_sweeps(const BatchSim *sims, const long long *item0, int nsims, int sweeps, int kz, int grid,
-                         int block, const BatchCtl *ctl, cudaStream_t st) {
-    const size_t smem = sizeof(long long) * (size_t)(nsims + 1);
+void launch_batch_sweeps(const BatchSim *sims, const BatchActive *act, int nsims, int sweeps, int kz, int grid,
+                         int block, cudaStream_t st) {
+    const size_t smem = sizeof(long long) * (size_t)(nsims + 1) + sizeof(int) * (size_t)nsims;
     for (int it = 0; it < sweeps; ++it)
         for (int c = 0; c < 2; ++c) {
             switch (kz) {
-            case 1: k_batch_sweep<1><<<grid, block, smem, st>>>(sims, item0, nsims, ctl, c); break;
-            case 2: k_batch_sweep<2><<<grid, block, smem, st>>>(sims, item0, nsims, ctl, c); break;
-            case 4: k_batch_sweep<4><<<grid, block, smem, st>>>(sims, item0, nsims, ctl, c); break;
-            default: k_batch_sweep<8><<<grid, block, smem, st>>>(sims, item0, nsims, ctl, c); break;
+            case 1: k_batch_sweep<1><<<grid, block, smem, st>>>(sims, act, c); break;
+            case 2: k_batch_sweep<2><<<grid, block, smem, st>>>(sims, act, c); break;
+            case 4: k_batch_sweep<4><<<grid, block, smem, st>>>(sims, act, c); break;
+            default: k_batch_sweep<8><<<grid, block, smem, st>>>(sims, act, c); break;
             }
         }
 }

@@ -112,14 +112,21 @@ struct BatchCtl {
     int iters, checks, converged, active;
     double r2, b2;
 };
+// The grids still running and their work-item offsets (device memory,
+// capacity n grids).
+struct BatchActive {
+    int n;
+    int *sim;
+    long long *item0;
+};
 // Segment-kernel threads of one grid for KZ planes per thread (W % 8 == 0).
 long long batch_sweep_items(const Geom &g, int kz);
 // Persistent grid size (SMs x resident blocks) of the batched sweep.
 int  batch_sweep_grid(int kz, int block);
-// `sweeps` red+black sweeps over every active grid; item0: nsims + 1
-// prefix offsets of the grids' items for this kz.
-void launch_batch_sweeps(const BatchSim *sims, const long long *item0, int nsims, int sweeps, int kz, int grid,
-                         int block, const BatchCtl *ctl, cudaStream_t st);
+// `sweeps` red+black sweeps over the grids listed in *act (built for this
+// kz); nsims bounds its size.
+void launch_batch_sweeps(const BatchSim *sims, const BatchActive *act, int nsims, int sweeps, int kz, int grid,
+                         int block, cudaStream_t st);
 // FP64 residual of every active grid (grid s owns partial blocks
 // [blk0[s], blk0[s+1]), residual_blocks(g_s) of them) and the per-grid
 // continue/stop decision.  2 launches.

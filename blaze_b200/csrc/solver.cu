@@ -469,14 +469,15 @@ static std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
 
 static int choose_variant(blz_solver *s) {
     if (s->variant != -2) return BLZ_OK;
-    const int nv = sweep_variant_count(s->g);
+    const int nv = s->P.temporal_block == 1 ? std::min(sweep_variant_count(s->g), kSegVariants)
+                                            : sweep_variant_count(s->g);
     if (nv == 0) { s->variant = -1; return BLZ_OK; }
     if (s->P.sweep_variant >= 0) { s->variant = std::min(s->P.sweep_variant, nv - 1); return BLZ_OK; }
     if (const char *env = std::getenv("BLZ_SWEEP_VARIANT")) {
         s->variant = std::max(0, std::min(std::atoi(env), nv - 1));
         return BLZ_OK;
     }
-    const auto key = std::make_tuple(s->device, s->g.W, s->g.H, s->g.D);
+    const auto key = std::make_tuple(s->device, s->g.W, s->g.H, s->g.D * 2 + (nv > kSegVariants ? 1 : 0));
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(key);

@@ -11,9 +11,13 @@
 //                                face when the solve has no Dirichlet ghost)
 //   2  p_prev / rms(p_prev)
 //   3  r / rms(r)                r = b - A p_prev, A the solver's 7-point operator
-// Output: delta = head(features); the warm start is p = p_prev + kappa*rms(r)*delta,
-// added in FP32.  rms() runs over the whole grid in FP64; kappa is a constant of
-// the trained weights (the training set's mean rms(p* - p_prev) / rms(r)).
+// Output: delta = head(features) and the correction d = kappa*rms(r)*delta;
+// the warm start is p = p_prev + alpha*d, added in FP32, with alpha =
+// <r, d> / <d, A d> the step along d that minimises the energy norm of the
+// error (so the warm start is never worse than p_prev in that norm; a perfect
+// d gives alpha = 1).  rms() and the inner products run over the whole grid
+// in FP64; kappa is a constant of the trained weights (the training set's
+// mean rms(p* - p_prev) / rms(r)).
 //
 // The 3x3x3 convolutions (forward and data gradient) run on the tcgen05 tensor
 // cores (unet_conv.cu).  Pooling, the transposed convolutions, weight gradients,
@@ -261,8 +265,53 @@ __global__ void k_skip_grad(const bf16 *__restrict__ dcat, const bf16 *__restric
 
 // 2x2x2 stride-2 transposed convolution: fine voxel (2x+a, 2y+b, 2z+c)
 // = bias + W[a + 2b + 4c] . x[x, y, z].  W: FP32 [8][cout][cin].  Output into
-// channels [0, cout) of a tensor with channel stride ys.  One thread per
-// coarse voxel, one parity (blockIdx.y) and 8 output channels (blockIdx.z).
+// channels [0, cout) of a tensor with channel stride ys.  A block covers 128
+// coarse voxels and one parity (blockIdx.y), whose COUT x CIN weights sit in
+// shared memory and are read as uniform broadcasts; each thread computes all
+// COUT outputs of its fine voxel from its coarse voxel's CIN inputs, 32 at a
+// time in registers.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128)
+k_upconv_t(const bf16 *__restrict__ x, LDims dc, const float *__restrict__ w, const float *__restrict__ bias,
+           bf16 *__restrict__ y, int ys) {
+    __shared__ __align__(16) float sw[COUT * CIN];
+    const int par = blockIdx.y;
+    for (int e = threadIdx.x; e < COUT * CIN; e += blockDim.x) sw[e] = __ldg(w + (size_t)par * COUT * CIN + e);
+    __syncthreads();
+    const long long n = (long long)dc.W * dc.H * dc.D;
+    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const int cx = (int)(v % dc.W), cy = (int)((v / dc.W) % dc.H), cz = (int)(v / ((long long)dc.W * dc.H));
+    const LDims df{dc.W * 2, dc.H * 2, dc.D * 2};
+    float acc[COUT];
+#pragma unroll
+    for (int o = 0; o < COUT; ++o) acc[o] = __ldg(bias + o);
+    const bf16 *xp = x + pvox(dc, cx, cy, cz) * CIN;
+#pragma unroll 1
+    for (int c0 = 0; c0 < CIN; c0 += 32) {
+        float xv[32];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) unpack8(ld8(xp + c0 + 8 * q), xv + 8 * q);
+#pragma unroll
+        for (int o = 0; o < COUT; ++o) {
+            const float4 *wr = reinterpret_cast<const float4 *>(sw + o * CIN + c0);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float4 ww = wr[q];
+                acc[o] = fmaf(ww.x, xv[4 * q], acc[o]);
+                acc[o] = fmaf(ww.y, xv[4 * q + 1], acc[o]);
+                acc[o] = fmaf(ww.z, xv[4 * q + 2], acc[o]);
+                acc[o] = fmaf(ww.w, xv[4 * q + 3], acc[o]);
+            }
+        }
+    }
+    const long long f = pvox(df, 2 * cx + (par & 1), 2 * cy + ((par >> 1) & 1), 2 * cz + (par >> 2));
+#pragma unroll
+    for (int o = 0; o < COUT; o += 8) st8(y + f * ys + o, acc + o);
+}
+
+// Generic transposed convolution (any cin, cout multiple of 8): one thread
+// per coarse voxel, parity (blockIdx.y) and 8 output channels (blockIdx.z).
 __global__ void __launch_bounds__(128)
 k_upconv(const bf16 *__restrict__ x, LDims dc, int cin, int cout, const float *__restrict__ w,
          const float *__restrict__ bias, bf16 *__restrict__ y, int ys) {
@@ -440,18 +489,91 @@ __device__ __forceinline__ float head_out(const bf16 *d0b, long long P, const fl
     return o;
 }
 
-// Warm start: p += scales[3] * out over the whole grid (colour packed p).
-__global__ void k_unet_apply(const bf16 *__restrict__ d0b, LDims d, const float *__restrict__ head,
-                             const float *__restrict__ scales, float *__restrict__ pr, float *__restrict__ pb) {
+// Warm start, step 1: the correction d = kappa rms(r) * out over the grid
+// (natural layout, FP32).
+__global__ void k_unet_delta(const bf16 *__restrict__ d0b, LDims d, const float *__restrict__ head,
+                             const float *__restrict__ scales, float *__restrict__ delta) {
     const long long n = (long long)d.W * d.H * d.D;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int i = (int)(t % d.W), j = (int)((t / d.W) % d.H), k = (int)(t / ((long long)d.W * d.H));
     float f[16];
-    const float o = head_out(d0b, pvox(d, i, j, k), head, f);
+    delta[t] = __ldg(scales + 3) * head_out(d0b, pvox(d, i, j, k), head, f);
+}
+
+// (A x) at one cell, A the solve's operator (as in cell_brp).
+__device__ __forceinline__ float apply_A(const GridInfo &g, const float *__restrict__ x, int i, int j, int k) {
+    const float xc = __ldg(x + lin(i, j, k, g.W, g.H));
+    float ax = 0.0f;
+    const bool d = g.dirichlet;
+    if (i > 0) ax += xc - __ldg(x + lin(i - 1, j, k, g.W, g.H)); else if (d && g.open.xlo) ax += xc;
+    if (i < g.W - 1) ax += xc - __ldg(x + lin(i + 1, j, k, g.W, g.H)); else if (d && g.open.xhi) ax += xc;
+    if (j > 0) ax += xc - __ldg(x + lin(i, j - 1, k, g.W, g.H)); else if (d && g.open.ylo) ax += xc;
+    if (j < g.H - 1) ax += xc - __ldg(x + lin(i, j + 1, k, g.W, g.H)); else if (d && g.open.yhi) ax += xc;
+    if (k > 0) ax += xc - __ldg(x + lin(i, j, k - 1, g.W, g.H)); else if (d && g.open.zlo) ax += xc;
+    if (k < g.D - 1) ax += xc - __ldg(x + lin(i, j, k + 1, g.W, g.H)); else if (d && g.open.zhi) ax += xc;
+    return ax;
+}
+
+// Step 2: <r, d> and <d, A d> (FP64) with r = b - A p, one pair per block.
+__global__ void __launch_bounds__(kNormThreads)
+k_unet_energy(GridInfo g, CellArr rhs, CellArr p, const float *__restrict__ delta, double *partials) {
+    const long long n = (long long)g.W * g.H * g.D;
+    double rd = 0.0, dad = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % g.W);
+        const long long jk = t / g.W;
+        const int j = (int)(jk % g.H), k = (int)(jk / g.H);
+        float b, pc, r;
+        cell_brp(g, rhs, p, i, j, k, b, pc, r);
+        const double dc = (double)__ldg(delta + t);
+        rd += (double)r * dc;
+        dad += dc * (double)apply_A(g, delta, i, j, k);
+    }
+    __shared__ double s[2][kNormThreads / 32];
+    rd = warp_sum_d(rd);
+    dad = warp_sum_d(dad);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) { s[0][w] = rd; s[1][w] = dad; }
+    __syncthreads();
+    if (w == 0) {
+        rd = lane < kNormThreads / 32 ? s[0][lane] : 0.0;
+        dad = lane < kNormThreads / 32 ? s[1][lane] : 0.0;
+        rd = warp_sum_d(rd);
+        dad = warp_sum_d(dad);
+        if (lane == 0) { partials[2 * blockIdx.x] = rd; partials[2 * blockIdx.x + 1] = dad; }
+    }
+}
+
+// Step 3: alpha = <r, d> / <d, A d>, the step along d that minimises the
+// energy norm of the error, ||p* - p - alpha d||_A (0 when d is 0).
+__global__ void k_unet_alpha(const double *partials, int nblk, float *alpha) {
+    __shared__ double s[2][32];
+    double a[2] = {0.0, 0.0};
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) { a[0] += partials[2 * b]; a[1] += partials[2 * b + 1]; }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int q = 0; q < 2; ++q) {
+        a[q] = warp_sum_d(a[q]);
+        if (lane == 0) s[q][w] = a[q];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double rd = 0.0, dad = 0.0;
+        for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i) { rd += s[0][i]; dad += s[1][i]; }
+        *alpha = dad > 0.0 ? (float)(rd / dad) : 0.0f;
+    }
+}
+
+// Step 4: p += alpha d (colour packed p).
+__global__ void k_unet_update(LDims d, const float *__restrict__ delta, const float *__restrict__ alpha,
+                              float *__restrict__ pr, float *__restrict__ pb) {
+    const long long n = (long long)d.W * d.H * d.D;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = (int)(t % d.W), j = (int)((t / d.W) % d.H), k = (int)(t / ((long long)d.W * d.H));
     float *a = ((i + j + k) & 1) ? pb : pr;
     const size_t q = pidx(i, j, k, d.W >> 1, d.H);
-    a[q] = fmaf(__ldg(scales + 3), o, a[q]);
+    a[q] = fmaf(__ldg(alpha), __ldg(delta + t), a[q]);
 }
 
 // Raw network output over the crop, natural layout.
@@ -598,6 +720,7 @@ struct blz_unet {
         g_e2b, g_e2a, g_p3, g_e3b, g_e3a;
     double *partials = nullptr, *sums = nullptr, *h_sums = nullptr;
     float *scales = nullptr;
+    float *delta = nullptr, *alpha = nullptr;   // warm start: correction field and its step
     int *err = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;
@@ -644,6 +767,7 @@ void release(blz_unet *u) {
     cudaFree(u->params); cudaFree(u->grads); cudaFree(u->adam_m); cudaFree(u->adam_v);
     cudaFree(u->wf); cudaFree(u->wd);
     cudaFree(u->partials); cudaFree(u->sums); cudaFree(u->scales); cudaFree(u->err);
+    cudaFree(u->delta); cudaFree(u->alpha);
     if (u->h_sums) cudaFreeHost(u->h_sums);
     if (u->ev0) cudaEventDestroy(u->ev0);
     if (u->ev1) cudaEventDestroy(u->ev1);
@@ -723,9 +847,15 @@ int up_fwd(blz_unet *u, int l, const Ten &x, const Ten &y, cudaStream_t st) {
     const LayerDef &L = kLayers[l];
     const LDims &dc = u->L[L.level + 1];
     const long long n = (long long)dc.W * dc.H * dc.D;
-    const dim3 grid(nblk(n, 128), 8, L.cout / 8);
-    k_upconv<<<grid, 128, 0, st>>>(x.base(), dc, L.cin, L.cout, u->params + u->w_off[l], u->params + u->b_off[l],
-                                   y.base(), y.C);
+    const float *w = u->params + u->w_off[l], *b = u->params + u->b_off[l];
+    const dim3 g2(nblk(n, 128), 8);
+    if (L.cin == 32 && L.cout == 16) k_upconv_t<32, 16><<<g2, 128, 0, st>>>(x.base(), dc, w, b, y.base(), y.C);
+    else if (L.cin == 64 && L.cout == 32) k_upconv_t<64, 32><<<g2, 128, 0, st>>>(x.base(), dc, w, b, y.base(), y.C);
+    else if (L.cin == 128 && L.cout == 64) k_upconv_t<128, 64><<<g2, 128, 0, st>>>(x.base(), dc, w, b, y.base(), y.C);
+    else {
+        const dim3 grid(nblk(n, 128), 8, L.cout / 8);
+        k_upconv<<<grid, 128, 0, st>>>(x.base(), dc, L.cin, L.cout, w, b, y.base(), y.C);
+    }
     ++u->launches;
     UCKL();
     return BLZ_OK;
@@ -910,9 +1040,14 @@ int unet_warm_start(blz_unet *u, const blz_params &P, const float *rhs_r, const 
     if ((rc = prepare_input(u, g, CellArr{rhs_r, rhs_b}, CellArr{p_r, p_b}, org, st)) != BLZ_OK) return rc;
     if ((rc = forward_core(u, st)) != BLZ_OK) return rc;
     const LDims &d = u->L[0];
-    k_unet_apply<<<nblk((long long)d.W * d.H * d.D, 256), 256, 0, st>>>(u->d0b.base(), d, u->params + u->w_off[HEAD],
-                                                                        u->scales, p_r, p_b);
-    ++u->launches;
+    const long long n = (long long)d.W * d.H * d.D;
+    if (!u->delta) UCK(cudaMalloc(&u->delta, sizeof(float) * n));
+    k_unet_delta<<<nblk(n, 256), 256, 0, st>>>(u->d0b.base(), d, u->params + u->w_off[HEAD], u->scales, u->delta);
+    k_unet_energy<<<kNormBlocks, kNormThreads, 0, st>>>(g, CellArr{rhs_r, rhs_b}, CellArr{p_r, p_b}, u->delta,
+                                                        u->partials);
+    k_unet_alpha<<<1, 256, 0, st>>>(u->partials, kNormBlocks, u->alpha);
+    k_unet_update<<<nblk(n, 256), 256, 0, st>>>(d, u->delta, u->alpha, p_r, p_b);
+    u->launches += 4;
     UCKL();
     if (launches) *launches += u->launches - l0;
     return BLZ_OK;
@@ -969,6 +1104,8 @@ int blz_unet_create(int width, int height, int depth, blz_unet **out) {
     ck(cudaMalloc(&u->sums, 2 * sizeof(double)), "cudaMalloc sums");
     ck(cudaMallocHost(&u->h_sums, 2 * sizeof(double)), "cudaMallocHost");
     ck(cudaMalloc(&u->scales, 4 * sizeof(float)), "cudaMalloc scales");
+    ck(cudaMalloc(&u->alpha, sizeof(float)), "cudaMalloc alpha");
+    if (rc == BLZ_OK) ck(cudaMemset(u->alpha, 0, sizeof(float)), "cudaMemset alpha");
     ck(cudaMalloc(&u->err, sizeof(int)), "cudaMalloc err");
     if (rc == BLZ_OK) ck(cudaMemset(u->err, 0, sizeof(int)), "cudaMemset err");
     if (rc == BLZ_OK) ck(cudaMemset(u->scales, 0, 4 * sizeof(float)), "cudaMemset scales");
@@ -1001,6 +1138,12 @@ int blz_unet_destroy(blz_unet *u) {
 long long blz_unet_num_params(const blz_unet *u) { return u ? (long long)u->n_params : 0; }
 
 long long blz_unet_kernel_launches(const blz_unet *u) { return u ? u->launches : 0; }
+
+float blz_unet_last_alpha(const blz_unet *u) {
+    float a = 0.0f;
+    if (u && u->alpha) cudaMemcpy(&a, u->alpha, sizeof(float), cudaMemcpyDeviceToHost);
+    return a;
+}
 
 int blz_unet_set_params(blz_unet *u, const float *params, int on_device) {
     if (!u || !params) return ufail(BLZ_ERR_ARG, "null argument");

@@ -204,6 +204,221 @@ k_conv3d_tc(int W, int H, int D, int cin, int out_stride, int out_offset, const 
 
 int conv3d_smem_bytes(int cout) { return kABytes + 27 * cout * 32; }
 
+// ---------------------------------------------------------------------------
+// z-marching variant for layers with cin, cout in {16, 32} (the full- and
+// half-resolution layers, which carry most of the network's voxels).  A CTA
+// keeps the layer's weights resident in shared memory and walks one 128-voxel
+// tile through `zs` consecutive planes.  Output plane z needs input planes
+// z-1, z, z+1 (padded planes z, z+1, z+2), 3 rows each; a ring of 5 plane
+// slots is filled by cp.async one plane ahead, so each plane's rows are
+// staged once per tile instead of three times, and the TMEM accumulator is
+// double buffered: the MMAs of plane z run while the epilogue of plane z-1
+// drains the other buffer and the rows of plane z+3 arrive.
+//   iteration z: issue loads of padded plane z+3 (slot (z+3)%5, whose last
+//   reader, plane z-2's MMAs, completed in iteration z-1) | wait for planes
+//   <= z+2 | one thread issues 27 x cin/16 MMAs into buffer z&1 and commits to
+//   mbarrier z&1 | all threads wait for plane z-1's commit and store it.
+// ---------------------------------------------------------------------------
+constexpr int kZmSlots = 5;
+
+template <int CIN> __host__ __device__ constexpr int zm_slot_bytes() { return (CIN / 16) * 3 * kRowBytes; }
+template <int N, int CIN> __host__ __device__ constexpr int zm_w_bytes() { return 27 * (CIN / 16) * N * 32; }
+template <int N, int CIN> __host__ __device__ constexpr int zm_smem_bytes() { return zm_w_bytes<N, CIN>() + kZmSlots * zm_slot_bytes<CIN>(); }
+
+template <int N, int CIN, bool RELU>
+__global__ void __launch_bounds__(128)
+k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const __nv_bfloat16 *__restrict__ x,
+            const __nv_bfloat16 *__restrict__ w, const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y,
+            const __nv_bfloat16 *__restrict__ aux, int *err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int CH = CIN / 16;
+    constexpr int kSlot = zm_slot_bytes<CIN>();
+    constexpr int kCols = 2 * N < 32 ? 32 : 2 * N;
+    unsigned char *sB = smem;
+    unsigned char *sA = smem + zm_w_bytes<N, CIN>();
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Wp = W + 2, Hp = H + 2;
+    const long long plane = (long long)Wp * Hp;
+    const long long P0 = (long long)Wp + (long long)kConvM * blockIdx.x;
+    const int z0 = blockIdx.y * zs;
+    const int nz = (z0 + zs < D ? z0 + zs : D) - z0;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base)), "r"(kCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const uint32_t aS = smem_u32(sA), bS = smem_u32(sB);
+
+    // Weights of every 16-channel chunk: block (ch, tap) = N rows x 32 B, K-major.
+    for (int e = tid; e < 27 * CH * N * 2; e += 128) {
+        const int kg = e & 1, n = (e >> 1) % N, ct = (e >> 1) / N;          // ct = ch * 27 + tap
+        const int ch = ct / 27, t = ct % 27;
+        cp_async16(bS + ct * N * 32 + kg * N * 16 + n * 16, w + ((size_t)t * N + n) * CIN + ch * 16 + kg * 8);
+    }
+    // Rows dy = -1, 0, 1 of padded plane pz (130 voxels each, the tile's row
+    // segment and one voxel either side), per chunk and 8-channel half.
+    auto load_plane = [&](int pz) {
+        const uint32_t dst = aS + (uint32_t)((pz % kZmSlots) * kSlot);
+        for (int e = tid; e < CH * 3 * kRowVox * 2; e += 128) {
+            const int kg = e & 1;
+            int rest = e >> 1;
+            const int v = rest % kRowVox;
+            rest /= kRowVox;
+            const int dy = rest % 3, ch = rest / 3;
+            const long long g = (long long)pz * plane + P0 - 1 + (long long)(dy - 1) * Wp + v;
+            cp_async16(dst + ch * 3 * kRowBytes + dy * kRowBytes + kg * kKgBytes + v * 16,
+                       x + g * CIN + ch * 16 + kg * 8);
+        }
+    };
+    if (nz > 0) {
+        load_plane(z0);
+        load_plane(z0 + 1);
+        load_plane(z0 + 2);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    constexpr uint32_t idesc = umma_idesc_bf16(kConvM, N);
+
+    auto epilogue = [&](int it) -> bool {
+        const bool done = mbar_wait(smem_u32(&mbar[it & 1]), (uint32_t)((it >> 1) & 1), err);
+        const bool ok = __syncthreads_and(done) != 0;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (!ok) return false;
+        const long long P = P0 + 32 * warp + lane;
+        const int xp = (int)(P % Wp), yp = (int)(P / Wp);
+        const bool inside = xp >= 1 && xp <= W && yp >= 1 && yp <= H;
+        const long long outv = (long long)(z0 + it + 1) * plane + P;
+#pragma unroll
+        for (int n0 = 0; n0 < N; n0 += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)((it & 1) * N + n0);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+                           "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                         : "r"(taddr) : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (inside) {
+                float v[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    v[q] = __uint_as_float(r[q]) + (bias ? __ldg(bias + n0 + q) : 0.0f);
+                    if (RELU) v[q] = fmaxf(v[q], 0.0f);
+                }
+                const long long o = outv * out_stride + out_offset + n0;
+                if (aux) {
+                    const uint4 a0 = __ldg(reinterpret_cast<const uint4 *>(aux + o));
+                    const uint4 a1 = __ldg(reinterpret_cast<const uint4 *>(aux + o) + 1);
+                    const __nv_bfloat16 *ah0 = reinterpret_cast<const __nv_bfloat16 *>(&a0);
+                    const __nv_bfloat16 *ah1 = reinterpret_cast<const __nv_bfloat16 *>(&a1);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        if (!(__bfloat162float(ah0[q]) > 0.0f)) v[q] = 0.0f;
+                        if (!(__bfloat162float(ah1[q]) > 0.0f)) v[8 + q] = 0.0f;
+                    }
+                }
+                __nv_bfloat162 h[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                uint4 *dst = reinterpret_cast<uint4 *>(y + o);
+                dst[0] = *reinterpret_cast<uint4 *>(&h[0]);
+                dst[1] = *reinterpret_cast<uint4 *>(&h[4]);
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        return true;
+    };
+
+    bool ok = true;
+    int issued = 0;                                     // MMA groups committed
+    for (int it = 0; it < nz && ok; ++it) {
+        const int z = z0 + it;
+        if (it + 1 < nz) load_plane(z + 3);
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 1;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t acc = tmem + (uint32_t)((it & 1) * N);
+#pragma unroll 1
+            for (int ch = 0; ch < CH; ++ch) {
+#pragma unroll 1
+                for (int t = 0; t < 27; ++t) {
+                    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+                    const uint32_t slot = aS + (uint32_t)(((z + 1 + dz) % kZmSlots) * kSlot);
+                    const uint64_t ad = umma_desc(slot + ch * 3 * kRowBytes + (dy + 1) * kRowBytes + (dx + 1) * 16,
+                                                  kKgBytes, 128);
+                    const uint64_t bd = umma_desc(bS + (ch * 27 + t) * N * 32, N * 16, 128);
+                    const uint32_t accum = (ch > 0 || t > 0) ? 1u : 0u;
+                    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                                 " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                                 ::"r"(acc), "l"(ad), "l"(bd), "r"(idesc), "r"(accum) : "memory");
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(&mbar[it & 1])) : "memory");
+        }
+        issued = it + 1;
+        if (it > 0) ok = epilogue(it - 1);
+    }
+    if (ok && nz > 0) ok = epilogue(nz - 1);
+    if (!ok && issued > 0) {
+        // A wait gave up: give the last committed MMAs one more bounded wait
+        // before the accumulator columns are released.
+        mbar_wait(smem_u32(&mbar[(issued - 1) & 1]), (uint32_t)(((issued - 1) >> 1) & 1), nullptr);
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+}
+
+constexpr int kZmPlanes = 16;
+
+template <int N, int CIN, bool RELU>
+static cudaError_t launch_zm(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
+                             void *y, const __nv_bfloat16 *aux, int *err, cudaStream_t st) {
+    constexpr int smem = zm_smem_bytes<N, CIN>();
+    cudaError_t e = cudaFuncSetAttribute(k_conv3d_zm<N, CIN, RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const long long interior = (long long)(cd.W + 2) * cd.H;
+    const dim3 grid((unsigned)((interior + kConvM - 1) / kConvM), (unsigned)((cd.D + kZmPlanes - 1) / kZmPlanes));
+    const int os = cd.out_stride > 0 ? cd.out_stride : cd.cout;
+    k_conv3d_zm<N, CIN, RELU><<<grid, 128, smem, st>>>(cd.W, cd.H, cd.D, kZmPlanes, os, cd.out_offset, x, w, bias,
+                                                       static_cast<__nv_bfloat16 *>(y), aux, err);
+    return cudaGetLastError();
+}
+
+// The z-marching kernel for cin, cout in {16, 32} and BF16 output.
+static bool zm_dispatch(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
+                        void *y, const __nv_bfloat16 *aux, int *err, cudaStream_t st, cudaError_t *res) {
+    if (cd.out_f32 || (cd.cin != 16 && cd.cin != 32) || (cd.cout != 16 && cd.cout != 32)) return false;
+#define BLZ_ZM(NN, CC)                                                                              \
+    if (cd.cout == NN && cd.cin == CC) {                                                            \
+        *res = cd.relu ? launch_zm<NN, CC, true>(cd, x, w, bias, y, aux, err, st)                   \
+                       : launch_zm<NN, CC, false>(cd, x, w, bias, y, aux, err, st);                 \
+        return true;                                                                                \
+    }
+    BLZ_ZM(16, 16)
+    BLZ_ZM(16, 32)
+    BLZ_ZM(32, 16)
+    BLZ_ZM(32, 32)
+#undef BLZ_ZM
+    return false;
+}
+
 template <int N, bool RELU, bool F32>
 static cudaError_t launch_n(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
                             void *y, const __nv_bfloat16 *aux, int *err, cudaStream_t st) {
@@ -223,6 +438,8 @@ cudaError_t launch_conv3d(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv
     if (cd.cin % 16 || cd.cin <= 0 || cd.out_offset % 8 || (cd.out_stride > 0 && cd.out_stride % 8) ||
         (aux && cd.out_f32))
         return cudaErrorInvalidValue;
+    cudaError_t res = cudaSuccess;
+    if (zm_dispatch(cd, x, w, bias, y, aux, err, st, &res)) return res;
 #define BLZ_CONV_CASE(NN)                                                                        \
     if (cd.cout == NN) {                                                                         \
         if (cd.out_f32) return cd.relu ? launch_n<NN, true, true>(cd, x, w, bias, y, aux, err, st) \

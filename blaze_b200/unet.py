@@ -134,6 +134,10 @@ class WarmStartUNet:
     def kernel_launches(self):
         return int(self._lib.blz_unet_kernel_launches(self._h))
 
+    def last_alpha(self):
+        """Step alpha of the last warm start (p + alpha d)."""
+        return float(self._lib.blz_unet_last_alpha(self._h))
+
     def tensor(self, name):
         """FP32 host copy of an internal tensor, padded (D+2, H+2, W+2, C)."""
         i = TENSOR_NAMES.index(name)

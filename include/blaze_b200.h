@@ -104,7 +104,9 @@ typedef struct blz_params {
     int    reset_pressure;        /* 1: p = 0 before every solve (the
                                      reference keeps p between frames)      */
     int    max_particles;         /* sourceMaxParticleCount                  */
-    int    temporal_block;        /* sweeps fused per HBM pass (0 = auto)    */
+    int    temporal_block;        /* 0: the autotuner may pick the two-sweeps-
+                                     per-HBM-pass kernel; 1: unblocked
+                                     sweeps only                             */
     int    device_loop;           /* 1: a residual-controlled solve runs as one
                                      CUDA graph whose conditional WHILE node
                                      decides on the device (no host round
@@ -249,8 +251,10 @@ int  blz_conv3d(const blz_conv_desc *d, const void *x, const void *w, const floa
  * skip concatenation [upsampled, skip]; a 1x1x1 head), BF16 activations, FP32
  * accumulation.  It maps, per cell, b = rho dx^2/dt * rhs, a Neumann-ghost
  * indicator, the previous pressure p and the residual r = b - A p (each over
- * its FP64 rms on the whole grid) to delta, and the warm start is
- * p + kappa * rms(r) * delta.  Parameters are one FP32 array; layer l's
+ * its FP64 rms on the whole grid) to delta; with d = kappa * rms(r) * delta
+ * the warm start is p + alpha * d, alpha = <r, d> / <d, A d> (FP64 over the
+ * grid): the step along d that minimises the energy norm of the error, so it
+ * is never worse than p in that norm.  Parameters are one FP32 array; layer l's
  * weights start at info[4] and its bias at info[5] (blz_unet_layer_info).
  * Weights of a 3x3x3 layer are [27][cout][cin] (tap as in blz_conv3d), of a
  * transposed convolution [8][cout][cin] (parity a + 2b + 4c for the fine
@@ -268,6 +272,7 @@ int  blz_unet_create(int width, int height, int depth, blz_unet **out);
 int  blz_unet_destroy(blz_unet *u);
 long long blz_unet_num_params(const blz_unet *u);
 long long blz_unet_kernel_launches(const blz_unet *u);
+float blz_unet_last_alpha(const blz_unet *u);   /* alpha of the last warm start (synchronises) */
 int  blz_unet_set_params(blz_unet *u, const float *params, int on_device);   /* resets Adam */
 int  blz_unet_get_params(const blz_unet *u, float *params, int on_device);
 int  blz_unet_get_grads(const blz_unet *u, float *grads, int on_device);

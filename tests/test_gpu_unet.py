@@ -35,7 +35,10 @@ def conv_ref(x, w, b, relu):
 
 @pytest.mark.parametrize("shape,cin,cout,relu", [
     ((20, 9, 5), 16, 16, False), ((130, 6, 4), 32, 64, True), ((8, 8, 8), 48, 32, True),
-    ((33, 17, 3), 16, 128, False), ((64, 64, 2), 64, 16, True)])
+    ((33, 17, 3), 16, 128, False), ((64, 64, 2), 64, 16, True),
+    # the z-marching kernel (cin, cout in {16, 32}, BF16 out): several z slabs, ragged tiles
+    ((37, 11, 21), 32, 32, True), ((24, 8, 17), 32, 16, False), ((19, 13, 33), 16, 32, True),
+    ((5, 3, 1), 16, 16, True)])
 @pytest.mark.parametrize("out_f32", [1, 0], ids=["f32", "bf16"])
 def test_conv3d_tensor_cores(shape, cin, cout, relu, out_f32):
     import torch
@@ -167,7 +170,8 @@ def test_unet_training_lowers_the_loss():
 
 
 def test_warm_start_through_the_solver():
-    """blz_solve with a network attached starts from p + kappa rms(r) delta."""
+    """blz_solve with a network attached starts from p + alpha d, d = kappa
+    rms(r) delta, alpha = <r, d> / <d, A d> (the energy-norm optimal step)."""
     import torch
     from oracle import unet_oracle as uo
     from blaze_b200 import FluidSolver, Timer
@@ -189,8 +193,15 @@ def test_warm_start_through_the_solver():
     st = solver.solve()
     assert st["warm_started"] == 1 and st["ms_warm_start"] > 0.0
     got = solver.get("P")
-    want = p.astype(np.float64) + float(so) * delta
+    d = float(so) * delta.astype(np.float64)
+    _, _, r = uo.residual_parts(g, rhs, p)
+    Ad = -uo.residual_parts(g, np.zeros_like(rhs), d.astype(np.float32))[2].astype(np.float64)
+    alpha = float(np.sum(r * d) / np.sum(d * Ad))
+    assert abs(net.last_alpha() - alpha) <= 1e-4 * abs(alpha), (net.last_alpha(), alpha)
+    want = p.astype(np.float64) + net.last_alpha() * d
     assert np.abs(got - want).max() <= 1e-5 * np.abs(want - p).max() + 1e-6
+    # the step never increases the energy norm of the error
+    assert np.sum(r * d) * alpha >= 0.0
     solver.set_warm_start(None)
     solver.set("P", p)
     st = solver.solve()
