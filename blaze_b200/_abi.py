@@ -123,6 +123,7 @@ EXPORTS = {
     "blz_unet_num_params": (C.c_longlong, [C.c_void_p]),
     "blz_unet_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "blz_unet_last_alpha": (C.c_float, [C.c_void_p]),
+    "blz_unet_set_smoothing": (C.c_int, [C.c_void_p, C.c_int]),
     "blz_unet_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "blz_unet_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "blz_unet_get_grads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),

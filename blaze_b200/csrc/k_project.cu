@@ -233,9 +233,21 @@ __host__ __device__ inline int tb_rows_tile(int Wq, int H) {
     return ty < H ? ty : H;
 }
 
+__device__ __forceinline__ void cp_async16_tb(float4 *dst, const float *src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
 __global__ void __launch_bounds__(kTbThreads, 1)
 k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float *__restrict__ rhs_b,
            const float *__restrict__ pin_b, float *__restrict__ pout_r, float *__restrict__ pout_b, int TY, int ZC) {
+    // Shared memory, in units of one plane slot (rows x Wq float4):
+    //   [0, 8)   p, colour c and plane k at slot c*4 + (k & 3)
+    //   [8, 12)  red rhs, plane k at 8 + (k & 3)
+    //   [12, 16) black rhs, plane k at 12 + (k & 3)
+    //   [16, 18) black p input staging, plane k at 16 + (k & 1)
+    // rhs and staged input are prefetched one step ahead with cp.async and
+    // only ever read back by the thread that loaded them.
     extern __shared__ float4 sm4[];
     const int Wh = g.W >> 1, Wq = Wh >> 2;
     const int rows = TY + 8;
@@ -250,12 +262,21 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     const bool first = m0 == 0, last = m0 + 4 == Wh;
     const bool has_ym = j > 0, has_yp = j < g.H - 1;
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    // slot (colour, plane & 3), row, quad
+    const size_t slot = (size_t)rows * Wq;
     auto S = [&](int colour, int plane, int row) -> float4 * {
-        return sm4 + ((size_t)((colour * 4 + (plane & 3)) * rows + row)) * Wq;
+        return sm4 + (size_t)(colour * 4 + (plane & 3)) * slot + (size_t)row * Wq;
     };
-    auto load_black = [&](int k) -> float4 {
-        return (row_ok && k >= 0 && k < g.D) ? ld4(pin_b + rowoff + (size_t)k * pl) : zero4;
+    float4 *own = sm4 + (size_t)r * Wq + mq;                 // this thread's element of slot 0
+    auto RR = [&](int plane) { return own + (size_t)(8 + (plane & 3)) * slot; };
+    auto RB = [&](int plane) { return own + (size_t)(12 + (plane & 3)) * slot; };
+    auto ST = [&](int plane) { return own + (size_t)(16 + (plane & 1)) * slot; };
+    auto valid = [&](int k) { return row_ok && k >= 0 && k < g.D; };
+    auto prefetch = [&](int k_red, int k_black, int k_in) {
+        // red rhs: levels 0 and 2 cover planes [z0-3, z1+3); black rhs: levels 1 and 3 cover [z0-2, z1+2)
+        if (valid(k_red) && k_red >= z0 - 3 && k_red < z1 + 3) cp_async16_tb(RR(k_red), rhs_r + rowoff + (size_t)k_red * pl);
+        if (valid(k_black) && k_black >= z0 - 2 && k_black < z1 + 2) cp_async16_tb(RB(k_black), rhs_b + rowoff + (size_t)k_black * pl);
+        if (valid(k_in) && k_in < z1 + 4) cp_async16_tb(ST(k_in), pin_b + rowoff + (size_t)k_in * pl);
+        asm volatile("cp.async.commit_group;" ::: "memory");
     };
     // One level: the colour `c` cells of this thread's quad on plane k.
     auto update = [&](int c, int k, float4 o, float4 zm, float4 zp) -> float4 {
@@ -267,7 +288,7 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
         const float *sf = reinterpret_cast<const float *>(so);
         const float xe = s == 0 ? (first ? 0.0f : sf[m0 - 1]) : (last ? 0.0f : sf[m0 + 4]);
         const bool has_zm = k > 0, has_zp = k < g.D - 1;
-        const float4 rv = ld4((c ? rhs_b : rhs_r) + rowoff + (size_t)k * pl);
+        const float4 rv = c ? *RB(k) : *RR(k);
         return gs_segment(sp, s, first, last, rv, o, xe, ym, yp, has_zm ? zm : zero4, has_zp ? zp : zero4,
                           has_ym, has_yp, has_zm, has_zp);
     };
@@ -276,12 +297,17 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
                k < g.D;
     };
     // register windows: black planes t-3..t+1, red planes t-4..t
-    float4 bm3 = zero4, bm2 = zero4, bm1 = load_black(z0 - 4), b0 = load_black(z0 - 3), bp1;
+    float4 bm3 = zero4, bm2 = zero4, bp1;
+    float4 bm1 = valid(z0 - 4) ? ld4(pin_b + rowoff + (size_t)(z0 - 4) * pl) : zero4;
+    float4 b0 = valid(z0 - 3) ? ld4(pin_b + rowoff + (size_t)(z0 - 3) * pl) : zero4;
     float4 rm4 = zero4, rm3 = zero4, rm2 = zero4, rm1 = zero4, r0 = zero4;
     S(1, z0 - 4, r)[mq] = bm1;
     S(1, z0 - 3, r)[mq] = b0;
+    prefetch(z0 - 3, z0 - 4, z0 - 2);                 // what the first step reads
     for (int t = z0 - 3; t < z1 + 3; ++t) {
-        bp1 = load_black(t + 1);
+        prefetch(t + 1, t, t + 2);                    // what the next step reads
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        bp1 = valid(t + 1) ? *ST(t + 1) : zero4;
         S(1, t + 1, r)[mq] = bp1;
         __syncthreads();
         if (active(0, t)) { r0 = update(0, t, b0, bm1, bp1); S(0, t, r)[mq] = r0; }
@@ -301,6 +327,7 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
         rm4 = rm3; rm3 = rm2; rm2 = rm1; rm1 = r0;
         bm3 = bm2; bm2 = bm1; bm1 = b0; b0 = bp1;
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 static bool tb_supported(const Geom &g) {
@@ -309,7 +336,7 @@ static bool tb_supported(const Geom &g) {
     return Wq <= 48 && tb_rows_tile(Wq, g.H) >= 1;
 }
 
-static size_t tb_smem(const Geom &g, int TY) { return sizeof(float4) * 8 * (size_t)(TY + 8) * (g.W >> 3); }
+static size_t tb_smem(const Geom &g, int TY) { return sizeof(float4) * 18 * (size_t)(TY + 8) * (g.W >> 3); }
 
 // One pass = two sweeps from (p_in) into (p_out).
 static void launch_tb_pass(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,

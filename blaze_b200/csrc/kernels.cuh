@@ -161,10 +161,16 @@ void set_thread_error(const char *msg);
 // Solve parameters (scale, open faces, Dirichlet ghosts) of a parameter block.
 SolveParams solve_params_of(const blz_params &P);
 
-// Learned warm start (unet.cu): p := p + kappa rms(r) net(b, mask, p, r) on the
-// colour-packed pressure, ordered on st; adds its launches to *launches.
-int unet_warm_start(blz_unet *u, const blz_params &P, const float *rhs_r, const float *rhs_b, float *p_r,
-                    float *p_b, cudaStream_t st, long long *launches);
+// Learned warm start (unet.cu), ordered on st, launches added to *launches:
+// unet_correction computes the packed correction d (returned with a packed
+// zero right-hand side); the caller sweeps p and d unet_smoothing(u) times;
+// unet_combine adds alpha d with alpha minimising the residual norm.
+int unet_correction(blz_unet *u, const blz_params &P, const float *rhs_r, const float *rhs_b, const float *p_r,
+                    const float *p_b, cudaStream_t st, long long *launches, float **d_r, float **d_b,
+                    const float **z_r, const float **z_b);
+int unet_combine(blz_unet *u, const blz_params &P, const float *rhs_r, const float *rhs_b, float *p_r, float *p_b,
+                 cudaStream_t st, long long *launches);
+int unet_smoothing(const blz_unet *u);
 // BLZ_ERR_TIMEOUT if a tensor-core completion wait of the last warm start
 // gave up (synchronises st).
 int unet_timeout_flag(blz_unet *u, cudaStream_t st);

@@ -568,9 +568,24 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
         CK(s, cudaMemsetAsync(s->p_r, 0, half * sizeof(float), s->st));
         CK(s, cudaMemsetAsync(s->p_b, 0, half * sizeof(float), s->st));
     }
+    int pre = 0;                                 // sweeps of p before the solve proper
     if (s->warm) {
         CK(s, cudaEventRecord(s->ev[8], s->st));
-        const int rc = unet_warm_start(s->warm, P, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->st, &s->launches);
+        float *d_r = nullptr, *d_b = nullptr;
+        const float *z_r = nullptr, *z_b = nullptr;
+        int rc = unet_correction(s->warm, P, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->st, &s->launches, &d_r, &d_b,
+                                 &z_r, &z_b);
+        if (rc != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
+        pre = unet_smoothing(s->warm);
+        if (pre > 0 && P.gs_order == BLZ_GS_RB3D) {
+            if ((rc = sweeps(s, pre)) != BLZ_OK) return rc;
+            launch_rbgs_sweeps(s->g, solve_params(P), z_r, z_b, d_r, d_b, pre, s->st, &s->launches,
+                               s->variant, q_r(s), q_b(s));
+            CKL(s);
+        } else {
+            pre = 0;
+        }
+        rc = unet_combine(s->warm, P, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->st, &s->launches);
         if (rc != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
         CK(s, cudaEventRecord(s->ev[9], s->st));
     }
@@ -583,6 +598,7 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
             CK(s, cudaEventElapsedTime(&t, s->ev[8], s->ev[9]));
             st->ms_warm_start = t;
             st->warm_started = 1;
+            st->iterations += pre;
         }
     } else if (st) {
         st->ms_warm_start = 0.0f;

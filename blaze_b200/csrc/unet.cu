@@ -11,13 +11,15 @@
 //                                face when the solve has no Dirichlet ghost)
 //   2  p_prev / rms(p_prev)
 //   3  r / rms(r)                r = b - A p_prev, A the solver's 7-point operator
-// Output: delta = head(features) and the correction d = kappa*rms(r)*delta;
-// the warm start is p = p_prev + alpha*d, added in FP32, with alpha =
-// <r, d> / <d, A d> the step along d that minimises the energy norm of the
-// error (so the warm start is never worse than p_prev in that norm; a perfect
-// d gives alpha = 1).  rms() and the inner products run over the whole grid
-// in FP64; kappa is a constant of the trained weights (the training set's
-// mean rms(p* - p_prev) / rms(r)).
+// Output: delta = head(features) and the correction d = kappa*rms(r)*delta.
+// The solver then sweeps p and d alike k times (d with a zero right-hand
+// side; Gauss-Seidel is affine, so S^k(p + alpha d) = S^k(p) + alpha M^k d
+// for every alpha) and adds alpha M^k d with alpha minimising the residual
+// norm ||b - A (S^k(p) + alpha M^k d)||: the combination chosen on what the
+// stopping rule measures, after the smoother has removed the error it removes
+// anyway; a useless d gets alpha ~ 0.  rms() and the inner products run over
+// the whole grid in FP64; kappa is a constant of the trained weights (the
+// training set's mean rms(p* - p_prev) / rms(r)).
 //
 // The 3x3x3 convolutions (forward and data gradient) run on the tcgen05 tensor
 // cores (unet_conv.cu).  Pooling, the transposed convolutions, weight gradients,
@@ -490,63 +492,50 @@ __device__ __forceinline__ float head_out(const bf16 *d0b, long long P, const fl
 }
 
 // Warm start, step 1: the correction d = kappa rms(r) * out over the grid
-// (natural layout, FP32).
+// (colour packed, FP32).
 __global__ void k_unet_delta(const bf16 *__restrict__ d0b, LDims d, const float *__restrict__ head,
-                             const float *__restrict__ scales, float *__restrict__ delta) {
+                             const float *__restrict__ scales, float *__restrict__ dr, float *__restrict__ db) {
     const long long n = (long long)d.W * d.H * d.D;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int i = (int)(t % d.W), j = (int)((t / d.W) % d.H), k = (int)(t / ((long long)d.W * d.H));
     float f[16];
-    delta[t] = __ldg(scales + 3) * head_out(d0b, pvox(d, i, j, k), head, f);
+    (((i + j + k) & 1) ? db : dr)[pidx(i, j, k, d.W >> 1, d.H)] = __ldg(scales + 3) * head_out(d0b, pvox(d, i, j, k), head, f);
 }
 
-// (A x) at one cell, A the solve's operator (as in cell_brp).
-__device__ __forceinline__ float apply_A(const GridInfo &g, const float *__restrict__ x, int i, int j, int k) {
-    const float xc = __ldg(x + lin(i, j, k, g.W, g.H));
-    float ax = 0.0f;
-    const bool d = g.dirichlet;
-    if (i > 0) ax += xc - __ldg(x + lin(i - 1, j, k, g.W, g.H)); else if (d && g.open.xlo) ax += xc;
-    if (i < g.W - 1) ax += xc - __ldg(x + lin(i + 1, j, k, g.W, g.H)); else if (d && g.open.xhi) ax += xc;
-    if (j > 0) ax += xc - __ldg(x + lin(i, j - 1, k, g.W, g.H)); else if (d && g.open.ylo) ax += xc;
-    if (j < g.H - 1) ax += xc - __ldg(x + lin(i, j + 1, k, g.W, g.H)); else if (d && g.open.yhi) ax += xc;
-    if (k > 0) ax += xc - __ldg(x + lin(i, j, k - 1, g.W, g.H)); else if (d && g.open.zlo) ax += xc;
-    if (k < g.D - 1) ax += xc - __ldg(x + lin(i, j, k + 1, g.W, g.H)); else if (d && g.open.zhi) ax += xc;
-    return ax;
-}
-
-// Step 2: <r, d> and <d, A d> (FP64) with r = b - A p, one pair per block.
+// Step 3: <r, q> and <q, q> (FP64) with r = b - A p and q = A d, one pair per block.
 __global__ void __launch_bounds__(kNormThreads)
-k_unet_energy(GridInfo g, CellArr rhs, CellArr p, const float *__restrict__ delta, double *partials) {
+k_unet_project(GridInfo g, CellArr rhs, CellArr p, CellArr dl, double *partials) {
     const long long n = (long long)g.W * g.H * g.D;
-    double rd = 0.0, dad = 0.0;
+    const GridInfo g0{g.W, g.H, g.D, g.open, g.dirichlet, 0.0f};
+    double rq = 0.0, qq = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t % g.W);
         const long long jk = t / g.W;
         const int j = (int)(jk % g.H), k = (int)(jk / g.H);
-        float b, pc, r;
+        float b, pc, r, zb, dc, mq;
         cell_brp(g, rhs, p, i, j, k, b, pc, r);
-        const double dc = (double)__ldg(delta + t);
-        rd += (double)r * dc;
-        dad += dc * (double)apply_A(g, delta, i, j, k);
+        cell_brp(g0, rhs, dl, i, j, k, zb, dc, mq);      // with b = 0: mq = -(A d)
+        rq -= (double)r * (double)mq;
+        qq += (double)mq * (double)mq;
     }
     __shared__ double s[2][kNormThreads / 32];
-    rd = warp_sum_d(rd);
-    dad = warp_sum_d(dad);
+    rq = warp_sum_d(rq);
+    qq = warp_sum_d(qq);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0) { s[0][w] = rd; s[1][w] = dad; }
+    if (lane == 0) { s[0][w] = rq; s[1][w] = qq; }
     __syncthreads();
     if (w == 0) {
-        rd = lane < kNormThreads / 32 ? s[0][lane] : 0.0;
-        dad = lane < kNormThreads / 32 ? s[1][lane] : 0.0;
-        rd = warp_sum_d(rd);
-        dad = warp_sum_d(dad);
-        if (lane == 0) { partials[2 * blockIdx.x] = rd; partials[2 * blockIdx.x + 1] = dad; }
+        rq = lane < kNormThreads / 32 ? s[0][lane] : 0.0;
+        qq = lane < kNormThreads / 32 ? s[1][lane] : 0.0;
+        rq = warp_sum_d(rq);
+        qq = warp_sum_d(qq);
+        if (lane == 0) { partials[2 * blockIdx.x] = rq; partials[2 * blockIdx.x + 1] = qq; }
     }
 }
 
-// Step 3: alpha = <r, d> / <d, A d>, the step along d that minimises the
-// energy norm of the error, ||p* - p - alpha d||_A (0 when d is 0).
+// alpha = <r, A d> / <A d, A d>: the step along d that minimises the
+// residual norm ||b - A (p + alpha d)|| (0 when A d is 0).
 __global__ void k_unet_alpha(const double *partials, int nblk, float *alpha) {
     __shared__ double s[2][32];
     double a[2] = {0.0, 0.0};
@@ -558,22 +547,20 @@ __global__ void k_unet_alpha(const double *partials, int nblk, float *alpha) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double rd = 0.0, dad = 0.0;
-        for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i) { rd += s[0][i]; dad += s[1][i]; }
-        *alpha = dad > 0.0 ? (float)(rd / dad) : 0.0f;
+        double rq = 0.0, qq = 0.0;
+        for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i) { rq += s[0][i]; qq += s[1][i]; }
+        *alpha = qq > 0.0 ? (float)(rq / qq) : 0.0f;
     }
 }
 
-// Step 4: p += alpha d (colour packed p).
-__global__ void k_unet_update(LDims d, const float *__restrict__ delta, const float *__restrict__ alpha,
-                              float *__restrict__ pr, float *__restrict__ pb) {
-    const long long n = (long long)d.W * d.H * d.D;
+// Step 4: p += alpha d (both colour packed, n/2 values each).
+__global__ void k_unet_update(long long half, const float *__restrict__ dr, const float *__restrict__ db,
+                              const float *__restrict__ alpha, float *__restrict__ pr, float *__restrict__ pb) {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int i = (int)(t % d.W), j = (int)((t / d.W) % d.H), k = (int)(t / ((long long)d.W * d.H));
-    float *a = ((i + j + k) & 1) ? pb : pr;
-    const size_t q = pidx(i, j, k, d.W >> 1, d.H);
-    a[q] = fmaf(__ldg(alpha), __ldg(delta + t), a[q]);
+    if (t >= half) return;
+    const float a = __ldg(alpha);
+    pr[t] = fmaf(a, __ldg(dr + t), pr[t]);
+    pb[t] = fmaf(a, __ldg(db + t), pb[t]);
 }
 
 // Raw network output over the crop, natural layout.
@@ -720,7 +707,8 @@ struct blz_unet {
         g_e2b, g_e2a, g_p3, g_e3b, g_e3a;
     double *partials = nullptr, *sums = nullptr, *h_sums = nullptr;
     float *scales = nullptr;
-    float *delta = nullptr, *alpha = nullptr;   // warm start: correction field and its step
+    float *dpk = nullptr, *alpha = nullptr;     // warm start: packed correction + zero rhs; its step
+    int smooth = 40;                            // sweeps of p and d before the step is chosen
     int *err = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;
@@ -767,7 +755,7 @@ void release(blz_unet *u) {
     cudaFree(u->params); cudaFree(u->grads); cudaFree(u->adam_m); cudaFree(u->adam_v);
     cudaFree(u->wf); cudaFree(u->wd);
     cudaFree(u->partials); cudaFree(u->sums); cudaFree(u->scales); cudaFree(u->err);
-    cudaFree(u->delta); cudaFree(u->alpha);
+    cudaFree(u->dpk); cudaFree(u->alpha);
     if (u->h_sums) cudaFreeHost(u->h_sums);
     if (u->ev0) cudaEventDestroy(u->ev0);
     if (u->ev1) cudaEventDestroy(u->ev1);
@@ -1026,9 +1014,15 @@ int sync_conv_flag(blz_unet *u, cudaStream_t st) {
 } // namespace
 
 namespace blz {
-// Warm start of the solver's colour-packed pressure in place (solver.cu).
-int unet_warm_start(blz_unet *u, const blz_params &P, const float *rhs_r, const float *rhs_b, float *p_r,
-                    float *p_b, cudaStream_t st, long long *launches) {
+// Learned warm start, in the order blz_solve runs it:
+// unet_correction computes d (colour packed) from rhs and the current p; the
+// solver then smooths p and d alike (unet_smoothing(u) sweeps each, d with a
+// zero right-hand side: Gauss-Seidel is affine, so this is exactly smoothing
+// p + alpha d for every alpha at once); unet_combine picks alpha minimising the
+// residual norm of p + alpha d and adds alpha d.
+int unet_correction(blz_unet *u, const blz_params &P, const float *rhs_r, const float *rhs_b, const float *p_r,
+                    const float *p_b, cudaStream_t st, long long *launches, float **d_r, float **d_b,
+                    const float **z_r, const float **z_b) {
     if (u->L[0].W != P.width || u->L[0].H != P.height || u->L[0].D != P.depth)
         return ufail(BLZ_ERR_ARG, "warm-start network built for %dx%dx%d, grid is %dx%dx%d", u->L[0].W, u->L[0].H,
                      u->L[0].D, P.width, P.height, P.depth);
@@ -1041,17 +1035,39 @@ int unet_warm_start(blz_unet *u, const blz_params &P, const float *rhs_r, const 
     if ((rc = forward_core(u, st)) != BLZ_OK) return rc;
     const LDims &d = u->L[0];
     const long long n = (long long)d.W * d.H * d.D;
-    if (!u->delta) UCK(cudaMalloc(&u->delta, sizeof(float) * n));
-    k_unet_delta<<<nblk(n, 256), 256, 0, st>>>(u->d0b.base(), d, u->params + u->w_off[HEAD], u->scales, u->delta);
-    k_unet_energy<<<kNormBlocks, kNormThreads, 0, st>>>(g, CellArr{rhs_r, rhs_b}, CellArr{p_r, p_b}, u->delta,
-                                                        u->partials);
-    k_unet_alpha<<<1, 256, 0, st>>>(u->partials, kNormBlocks, u->alpha);
-    k_unet_update<<<nblk(n, 256), 256, 0, st>>>(d, u->delta, u->alpha, p_r, p_b);
-    u->launches += 4;
+    if (!u->dpk) {
+        UCK(cudaMalloc(&u->dpk, sizeof(float) * 2 * n));     // d (n) then a zero right-hand side (n)
+        UCK(cudaMemset(u->dpk, 0, sizeof(float) * 2 * n));
+    }
+    float *dr = u->dpk, *db = u->dpk + n / 2;
+    k_unet_delta<<<nblk(n, 256), 256, 0, st>>>(u->d0b.base(), d, u->params + u->w_off[HEAD], u->scales, dr, db);
+    ++u->launches;
     UCKL();
+    *d_r = dr;
+    *d_b = db;
+    *z_r = u->dpk + n;
+    *z_b = u->dpk + n + n / 2;
     if (launches) *launches += u->launches - l0;
     return BLZ_OK;
 }
+
+int unet_combine(blz_unet *u, const blz_params &P, const float *rhs_r, const float *rhs_b, float *p_r, float *p_b,
+                 cudaStream_t st, long long *launches) {
+    const GridInfo g = grid_info(P);
+    const LDims &d = u->L[0];
+    const long long n = (long long)d.W * d.H * d.D;
+    const float *dr = u->dpk, *db = u->dpk + n / 2;
+    k_unet_project<<<kNormBlocks, kNormThreads, 0, st>>>(g, CellArr{rhs_r, rhs_b}, CellArr{p_r, p_b},
+                                                         CellArr{dr, db}, u->partials);
+    k_unet_alpha<<<1, 256, 0, st>>>(u->partials, kNormBlocks, u->alpha);
+    k_unet_update<<<nblk(n / 2, 256), 256, 0, st>>>(n / 2, dr, db, u->alpha, p_r, p_b);
+    u->launches += 3;
+    if (launches) *launches += 3;
+    UCKL();
+    return BLZ_OK;
+}
+
+int unet_smoothing(const blz_unet *u) { return u->smooth; }
 int unet_timeout_flag(blz_unet *u, cudaStream_t st) { return sync_conv_flag(u, st); }
 } // namespace blz
 
@@ -1138,6 +1154,12 @@ int blz_unet_destroy(blz_unet *u) {
 long long blz_unet_num_params(const blz_unet *u) { return u ? (long long)u->n_params : 0; }
 
 long long blz_unet_kernel_launches(const blz_unet *u) { return u ? u->launches : 0; }
+
+int blz_unet_set_smoothing(blz_unet *u, int sweeps) {
+    if (!u || sweeps < 0) return ufail(BLZ_ERR_ARG, "bad smoothing sweep count");
+    u->smooth = sweeps;
+    return BLZ_OK;
+}
 
 float blz_unet_last_alpha(const blz_unet *u) {
     float a = 0.0f;

@@ -351,13 +351,16 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t acc = tmem + (uint32_t)((it & 1) * N);
-#pragma unroll 1
+            // slots of padded planes z, z+1, z+2 (taps dz = -1, 0, +1)
+            const uint32_t sz[3] = {aS + (uint32_t)((z % kZmSlots) * kSlot),
+                                    aS + (uint32_t)(((z + 1) % kZmSlots) * kSlot),
+                                    aS + (uint32_t)(((z + 2) % kZmSlots) * kSlot)};
+#pragma unroll
             for (int ch = 0; ch < CH; ++ch) {
-#pragma unroll 1
+#pragma unroll
                 for (int t = 0; t < 27; ++t) {
-                    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-                    const uint32_t slot = aS + (uint32_t)(((z + 1 + dz) % kZmSlots) * kSlot);
-                    const uint64_t ad = umma_desc(slot + ch * 3 * kRowBytes + (dy + 1) * kRowBytes + (dx + 1) * 16,
+                    const int dzi = t / 9, dyi = (t / 3) % 3, dxi = t % 3;
+                    const uint64_t ad = umma_desc(sz[dzi] + ch * 3 * kRowBytes + dyi * kRowBytes + dxi * 16,
                                                   kKgBytes, 128);
                     const uint64_t bd = umma_desc(bS + (ch * 27 + t) * N * 32, N * 16, 128);
                     const uint32_t accum = (ch > 0 || t > 0) ? 1u : 0u;

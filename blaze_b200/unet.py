@@ -138,6 +138,10 @@ class WarmStartUNet:
         """Step alpha of the last warm start (p + alpha d)."""
         return float(self._lib.blz_unet_last_alpha(self._h))
 
+    def set_smoothing(self, sweeps):
+        """Sweeps of p and d before the warm start's step is chosen."""
+        check(self._lib.blz_unet_set_smoothing(self._h, int(sweeps)))
+
     def tensor(self, name):
         """FP32 host copy of an internal tensor, padded (D+2, H+2, W+2, C)."""
         i = TENSOR_NAMES.index(name)
