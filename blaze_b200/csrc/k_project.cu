@@ -111,18 +111,6 @@ __global__ void k_rbgs_half(Geom g, SolveParams sp, const float *__restrict__ rh
 // 128-bit loads of the rhs row segment, of the other colour's segments in
 // rows j-1, j, j+1 and planes k-1, k+1, plus one scalar for the x neighbour
 // that falls outside the segment; 128-bit store.
-__device__ __forceinline__ float gs_den(const SolveParams &sp, bool has_xm, bool has_xp, bool has_ym,
-                                        bool has_yp, bool has_zm, bool has_zp, bool dir) {
-    float d = 0.0f;
-    d += has_xm ? 1.0f : (dir && sp.open.xlo ? 1.0f : 0.0f);
-    d += has_xp ? 1.0f : (dir && sp.open.xhi ? 1.0f : 0.0f);
-    d += has_ym ? 1.0f : (dir && sp.open.ylo ? 1.0f : 0.0f);
-    d += has_yp ? 1.0f : (dir && sp.open.yhi ? 1.0f : 0.0f);
-    d += has_zm ? 1.0f : (dir && sp.open.zlo ? 1.0f : 0.0f);
-    d += has_zp ? 1.0f : (dir && sp.open.zhi ? 1.0f : 0.0f);
-    return d;
-}
-
 __device__ __forceinline__ float4 ld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
 
 // Updates four consecutive packed cells m0..m0+3 of one row: o is the other
@@ -140,23 +128,36 @@ __device__ __forceinline__ float4 gs_segment(const SolveParams &sp, int s, bool 
         xl[0] = o.x; xl[1] = o.y; xl[2] = o.z; xl[3] = o.w;
         xr[0] = o.y; xr[1] = o.z; xr[2] = o.w; xr[3] = xe;
     }
+    // A missing neighbour arrives as 0 (the caller passes zero4 and xe = 0),
+    // so the sum is branch free and in the reference's order; only the
+    // neighbour count differs, and it is the same for every cell of the quad
+    // except the one at a row end, so the count and its reciprocal are formed
+    // three times per quad rather than per cell.
     const bool dir = sp.dirichlet;
+    const float den_b = 2.0f + (has_ym ? 1.0f : (dir && sp.open.ylo ? 1.0f : 0.0f)) +
+                        (has_yp ? 1.0f : (dir && sp.open.yhi ? 1.0f : 0.0f)) +
+                        (has_zm ? 1.0f : (dir && sp.open.zlo ? 1.0f : 0.0f)) +
+                        (has_zp ? 1.0f : (dir && sp.open.zhi ? 1.0f : 0.0f));
+    const float den0 = (s == 0 && first) ? den_b - 1.0f + (dir && sp.open.xlo ? 1.0f : 0.0f) : den_b;
+    const float den3 = (s == 1 && last) ? den_b - 1.0f + (dir && sp.open.xhi ? 1.0f : 0.0f) : den_b;
+    const float inv_b = inv_count(den_b), inv0 = inv_count(den0), inv3 = inv_count(den3);
     const float ra[4] = {r.x, r.y, r.z, r.w};
     const float yma[4] = {ym.x, ym.y, ym.z, ym.w}, ypa[4] = {yp.x, yp.y, yp.z, yp.w};
     const float zma[4] = {zm.x, zm.y, zm.z, zm.w}, zpa[4] = {zp.x, zp.y, zp.z, zp.w};
     float out[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-        const bool has_xm = !(s == 0 && first && t == 0);
-        const bool has_xp = !(s == 1 && last && t == 3);
         float num = sp.scale * ra[t];
-        if (has_xm) num += xl[t];
-        if (has_xp) num += xr[t];
-        if (has_ym) num += yma[t];
-        if (has_yp) num += ypa[t];
-        if (has_zm) num += zma[t];
-        if (has_zp) num += zpa[t];
-        out[t] = div_count(num, gs_den(sp, has_xm, has_xp, has_ym, has_yp, has_zm, has_zp, dir));
+        num += xl[t];
+        num += xr[t];
+        num += yma[t];
+        num += ypa[t];
+        num += zma[t];
+        num += zpa[t];
+        const float den = t == 0 ? den0 : t == 3 ? den3 : den_b;
+        const float inv = t == 0 ? inv0 : t == 3 ? inv3 : inv_b;
+        const float q0 = num * inv;
+        out[t] = fmaf(fmaf(-q0, den, num), inv, q0);
     }
     return make_float4(out[0], out[1], out[2], out[3]);
 }
