@@ -219,6 +219,11 @@ def main(argv=None):
     ap.add_argument("--crop", type=int, default=128)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--perturb", type=float, default=0.5)
+    ap.add_argument("--harvest", default=None,
+                    help="harvest schedule 'kind:seeds:frames:stride,...' (kind plain or policy; seed lists "
+                         "use '/' between items), all harvested before one training round; overrides "
+                         "--plain-seeds/--policy-seeds/--rounds")
+    ap.add_argument("--keep-kappa", action="store_true", help="keep the --init weights' kappa")
     ap.add_argument("--init", default=None, help="start from these weights (npz)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", required=True)
@@ -247,18 +252,33 @@ def main(argv=None):
     rounds = []
     plain_seeds = _seed_list(args.plain_seeds)
     policy_seeds = _seed_list(args.policy_seeds)
-    schedule = ([("plain", plain_seeds)] if plain_seeds else []) + [("policy", policy_seeds)] * args.rounds
-    for r, (kind, seeds) in enumerate(schedule):
-        if kind == "policy" and not args.init and r == 0:
-            raise SystemExit("on-policy rounds need a network: give --plain-seeds or --init")
-        t0 = time.time()
-        new, rat = harvest(n, seeds, args.frames, args.warmup, args.tol, args.target_tol, args.max_iter,
-                           args.check_every, log, policy=full if kind == "policy" else None,
-                           extra_cap=args.extra_cap, stride=args.stride)
-        t_harvest += time.time() - t0
+    if args.harvest:
+        # one round that trains on every harvested group
+        groups = []
+        for item in args.harvest.split(","):
+            kind, seeds, frames, stride = item.split(":")
+            groups.append((kind, _seed_list(seeds.replace("/", ",")), int(frames), int(stride)))
+        schedule = [groups]
+    else:
+        schedule = ([[("plain", plain_seeds, args.frames, args.stride)]] if plain_seeds else []) + \
+                   [[("policy", policy_seeds, args.frames, args.stride)]] * args.rounds
+    init_kappa = kappa
+    for r, round_groups in enumerate(schedule):
+        new = []
+        for kind, seeds, frames, stride in round_groups:
+            if kind == "policy" and not args.init and r == 0:
+                raise SystemExit("on-policy rounds need a network: give --plain-seeds or --init")
+            t0 = time.time()
+            got, rat = harvest(n, seeds, frames, args.warmup, args.tol, args.target_tol, args.max_iter,
+                               args.check_every, log, policy=full if kind == "policy" else None,
+                               extra_cap=args.extra_cap, stride=stride)
+            t_harvest += time.time() - t0
+            new += got
+            ratios += rat
+        kind = "+".join(sorted({g[0] for g in round_groups}))
+        seeds = [x for g in round_groups for x in g[1]]
         pairs += new
-        ratios += rat
-        kappa = float(np.mean(ratios)) if ratios else 1.0
+        kappa = init_kappa if (args.keep_kappa and args.init) else (float(np.mean(ratios)) if ratios else 1.0)
         log(f"round {r} ({kind}): {len(new)} new pairs, {len(pairs)} in all, kappa {kappa:.4f}")
         net = WarmStartUNet(crop, full.get_params(), kappa=kappa)
         lr = args.lr if (r == 0 and not args.init) else 0.3 * args.lr
@@ -279,6 +299,7 @@ def main(argv=None):
     sweep_ratio, time_ratio, conv = _ratios(rows)
     summary = {
         "grid": n, "plain_seeds": args.plain_seeds, "policy_seeds": args.policy_seeds, "rounds": rounds,
+        "harvest": args.harvest, "keep_kappa": args.keep_kappa,
         "eval_seeds": args.eval_seeds, "frames": args.frames, "stride": args.stride, "warmup": args.warmup,
         "tol": args.tol,
         "target_tol": args.target_tol, "extra_cap": args.extra_cap, "iters": args.iters, "crop": crop[0],

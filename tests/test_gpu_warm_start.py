@@ -23,13 +23,15 @@ def test_trained_network_halves_the_sweeps():
     assert os.path.exists(path), "trained weights missing"
     net = WarmStartUNet((256, 256, 256)).load(path)
     trained_on = set()
+    for rnd in net.meta.get("rounds", []):
+        trained_on.update(int(x) for x in rnd.get("seeds", []))
     for key in ("plain_seeds", "policy_seeds", "train_seeds"):
         spec = net.meta.get(key) or ""
         for part in str(spec).split(","):
             if "-" in part:
                 a, b = part.split("-")
                 trained_on.update(range(int(a), int(b) + 1))
-    assert SEED not in trained_on
+    assert trained_on and SEED not in trained_on
     scn, parts = family_scene(n=256, seed=SEED, tol=1e-4, max_iter=60000, check_every=20)
     tmr = Timer()
     solver = FluidSolver(tmr, scn, particles=parts)
