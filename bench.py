@@ -40,8 +40,8 @@ MAX_ITER = 40000
 CHECK_EVERY = 20
 # Sweeps per frame the reference arm runs (maxIterSolve): the mean the plain
 # RBGS step needs on this scene and frame window (frames 5-14 of seed 3 at
-# 256^3: 12150 sweeps), measured on a B200.
-REF_EQUAL_WORK_SWEEPS = int(os.environ.get("BLZ_REF_SWEEPS", "12150"))
+# 256^3: 26074 sweeps), measured on a B200.
+REF_EQUAL_WORK_SWEEPS = int(os.environ.get("BLZ_REF_SWEEPS", "26074"))
 
 
 def load_peaks():
