@@ -488,21 +488,28 @@ static int choose_variant(blz_solver *s) {
     CK(s, cudaMemcpyAsync(tr, s->p_r, half * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
     CK(s, cudaMemcpyAsync(tb, s->p_b, half * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
     const SolveParams sp = solve_params(s->P);
-    int best = 0;
-    float best_ms = 1e30f;
     long long dummy = 0;
-    for (int v = 0; v < nv; ++v) {
-        // 4 + 8 sweeps: whole passes for the temporal-blocking variants
+    // An untimed round over every variant first (the SM clock ramps up under
+    // load, which would favour whichever variant is timed last), then two
+    // timed rounds in opposite orders; each variant keeps its faster time.
+    // 4 and 8 sweeps: whole passes for the temporal-blocking variants.
+    for (int v = 0; v < nv; ++v)
         launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 4, s->st, &dummy, v, q_r(s), q_b(s));
-        CK(s, cudaEventRecord(s->ev[6], s->st));
-        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 8, s->st, &dummy, v, q_r(s), q_b(s));
-        CK(s, cudaEventRecord(s->ev[7], s->st));
-        CKL(s);
-        CK(s, cudaEventSynchronize(s->ev[7]));
-        float ms = 0.0f;
-        CK(s, cudaEventElapsedTime(&ms, s->ev[6], s->ev[7]));
-        if (ms < best_ms) { best_ms = ms; best = v; }
-    }
+    CKL(s);
+    std::vector<float> t_min(nv, 1e30f);
+    for (int round = 0; round < 2; ++round)
+        for (int i = 0; i < nv; ++i) {
+            const int v = round == 0 ? i : nv - 1 - i;
+            CK(s, cudaEventRecord(s->ev[6], s->st));
+            launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 8, s->st, &dummy, v, q_r(s), q_b(s));
+            CK(s, cudaEventRecord(s->ev[7], s->st));
+            CKL(s);
+            CK(s, cudaEventSynchronize(s->ev[7]));
+            float ms = 0.0f;
+            CK(s, cudaEventElapsedTime(&ms, s->ev[6], s->ev[7]));
+            t_min[v] = std::min(t_min[v], ms);
+        }
+    const int best = (int)(std::min_element(t_min.begin(), t_min.end()) - t_min.begin());
     s->launches += dummy;
     s->variant = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
