@@ -7,6 +7,7 @@
 // all rows contiguous; red cells of a row are even or odd i according to the
 // row parity (j+k)&1.
 #include <algorithm>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -113,13 +114,38 @@ __global__ void k_rbgs_half(Geom g, SolveParams sp, const float *__restrict__ rh
 // that falls outside the segment; 128-bit store.
 __device__ __forceinline__ float4 ld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
 
-// Updates four consecutive packed cells m0..m0+3 of one row: o is the other
-// colour at the same packed indices, xe its value just outside the segment
-// (m0-1 when the row's cells sit at even i, m0+4 when odd), ym/yp/zm/zp the
-// other colour in rows j-1, j+1 and planes k-1, k+1.
-__device__ __forceinline__ float4 gs_segment(const SolveParams &sp, int s, bool first, bool last, float4 r,
-                                             float4 o, float xe, float4 ym, float4 yp, float4 zm, float4 zp,
-                                             bool has_ym, bool has_yp, bool has_zm, bool has_zp) {
+// Neighbour counts of a quad and their reciprocals: the count is the same
+// for every cell of the quad except the one at a row end (cell 0 when the
+// row's cells sit at even i and the quad starts the row, cell 3 when odd
+// and it ends the row), so it is formed three times per quad, not per cell.
+struct QuadDen {
+    float d0, i0, db, ib, d3, i3;
+};
+
+__device__ __forceinline__ QuadDen quad_den(const SolveParams &sp, int s, bool first, bool last, bool has_ym,
+                                            bool has_yp, bool has_zm, bool has_zp) {
+    const bool dir = sp.dirichlet;
+    QuadDen q;
+    q.db = 2.0f + (has_ym ? 1.0f : (dir && sp.open.ylo ? 1.0f : 0.0f)) +
+           (has_yp ? 1.0f : (dir && sp.open.yhi ? 1.0f : 0.0f)) +
+           (has_zm ? 1.0f : (dir && sp.open.zlo ? 1.0f : 0.0f)) +
+           (has_zp ? 1.0f : (dir && sp.open.zhi ? 1.0f : 0.0f));
+    q.d0 = (s == 0 && first) ? q.db - 1.0f + (dir && sp.open.xlo ? 1.0f : 0.0f) : q.db;
+    q.d3 = (s == 1 && last) ? q.db - 1.0f + (dir && sp.open.xhi ? 1.0f : 0.0f) : q.db;
+    q.ib = inv_count(q.db);
+    q.i0 = inv_count(q.d0);
+    q.i3 = inv_count(q.d3);
+    return q;
+}
+
+// Updates four consecutive packed cells m0..m0+3 of one row given their
+// neighbour counts: o is the other colour at the same packed indices, xe its
+// value just outside the segment (m0-1 when the row's cells sit at even i,
+// m0+4 when odd), ym/yp/zm/zp the other colour in rows j-1, j+1 and planes
+// k-1, k+1.  A missing neighbour arrives as 0 (the caller passes zero4 and
+// xe = 0), so the sum is branch free and in the reference's order.
+__device__ __forceinline__ float4 gs_quad(float scale, int s, float4 r, float4 o, float xe, float4 ym, float4 yp,
+                                          float4 zm, float4 zp, const QuadDen &q) {
     float xl[4], xr[4];
     if (s == 0) {
         xl[0] = xe; xl[1] = o.x; xl[2] = o.y; xl[3] = o.z;
@@ -128,38 +154,32 @@ __device__ __forceinline__ float4 gs_segment(const SolveParams &sp, int s, bool 
         xl[0] = o.x; xl[1] = o.y; xl[2] = o.z; xl[3] = o.w;
         xr[0] = o.y; xr[1] = o.z; xr[2] = o.w; xr[3] = xe;
     }
-    // A missing neighbour arrives as 0 (the caller passes zero4 and xe = 0),
-    // so the sum is branch free and in the reference's order; only the
-    // neighbour count differs, and it is the same for every cell of the quad
-    // except the one at a row end, so the count and its reciprocal are formed
-    // three times per quad rather than per cell.
-    const bool dir = sp.dirichlet;
-    const float den_b = 2.0f + (has_ym ? 1.0f : (dir && sp.open.ylo ? 1.0f : 0.0f)) +
-                        (has_yp ? 1.0f : (dir && sp.open.yhi ? 1.0f : 0.0f)) +
-                        (has_zm ? 1.0f : (dir && sp.open.zlo ? 1.0f : 0.0f)) +
-                        (has_zp ? 1.0f : (dir && sp.open.zhi ? 1.0f : 0.0f));
-    const float den0 = (s == 0 && first) ? den_b - 1.0f + (dir && sp.open.xlo ? 1.0f : 0.0f) : den_b;
-    const float den3 = (s == 1 && last) ? den_b - 1.0f + (dir && sp.open.xhi ? 1.0f : 0.0f) : den_b;
-    const float inv_b = inv_count(den_b), inv0 = inv_count(den0), inv3 = inv_count(den3);
     const float ra[4] = {r.x, r.y, r.z, r.w};
     const float yma[4] = {ym.x, ym.y, ym.z, ym.w}, ypa[4] = {yp.x, yp.y, yp.z, yp.w};
     const float zma[4] = {zm.x, zm.y, zm.z, zm.w}, zpa[4] = {zp.x, zp.y, zp.z, zp.w};
     float out[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-        float num = sp.scale * ra[t];
+        float num = scale * ra[t];
         num += xl[t];
         num += xr[t];
         num += yma[t];
         num += ypa[t];
         num += zma[t];
         num += zpa[t];
-        const float den = t == 0 ? den0 : t == 3 ? den3 : den_b;
-        const float inv = t == 0 ? inv0 : t == 3 ? inv3 : inv_b;
+        const float den = t == 0 ? q.d0 : t == 3 ? q.d3 : q.db;
+        const float inv = t == 0 ? q.i0 : t == 3 ? q.i3 : q.ib;
         const float q0 = num * inv;
         out[t] = fmaf(fmaf(-q0, den, num), inv, q0);
     }
     return make_float4(out[0], out[1], out[2], out[3]);
+}
+
+__device__ __forceinline__ float4 gs_segment(const SolveParams &sp, int s, bool first, bool last, float4 r,
+                                             float4 o, float xe, float4 ym, float4 yp, float4 zm, float4 zp,
+                                             bool has_ym, bool has_yp, bool has_zm, bool has_zp) {
+    return gs_quad(sp.scale, s, r, o, xe, ym, yp, zm, zp,
+                   quad_den(sp, s, first, last, has_ym, has_yp, has_zm, has_zp));
 }
 
 // Half sweep, four packed cells per thread along x (W % 8 == 0), KZ
@@ -220,29 +240,58 @@ k_rbgs_seg(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float 
 // level 0 updates red on plane t, level 1 black on t-1, level 2 red on t-2,
 // level 3 black on t-3, each level over a region one row and one plane
 // narrower than the one before, so every update reads exactly the values
-// the in-place sweeps would (the z neighbours from the thread's own
-// registers, the in-plane neighbours from shared memory, four plane slots
-// per colour).  Per cell the arithmetic is gs_segment's, so a pass equals
-// two sweeps of the segment kernel bit for bit.  HBM traffic per pass is
-// about 10 B/cell instead of 24 B/cell for two unblocked sweeps; the price is
-// recomputing the halo.
+// the in-place sweeps would.  Per cell the arithmetic is gs_quad's, so a
+// pass equals two sweeps of the segment kernel bit for bit.  HBM traffic
+// per pass is about 10 B/cell instead of 24 B/cell for two unblocked sweeps;
+// the price is recomputing the halo.
+//
+// A thread owns one quad in each of two adjacent rows (A = 2y, B = 2y + 1)
+// and carries both rows' plane windows in registers: the z neighbours, and
+// the y neighbour inside the pair, come from registers; the y neighbour
+// outside the pair and the rhs come from shared memory; the x neighbour
+// beyond the quad comes from a warp shuffle when a warp spans exactly one
+// row (W = 256), else from shared memory.
+//
+// One barrier per step suffices: in step t every level reads only planes
+// written in step t-1 (level 0 the black input staged then, level 1 red
+// t-1 from level 0, level 2 black t-2 from level 1, level 3 red t-3 from
+// level 2), and the slots written in step t (red t and t-2, black t+1 and
+// t-1) are, modulo the four-slot rings, none of the slots read in it (red
+// t-1 and t-3, black t and t-2); every slot's previous contents were last
+// read in step t-1.
+//
+// Missing neighbours read zeros instead of being selected away: the p
+// slots start zero-filled and rows outside the domain are never written
+// (their register windows stay zero); the row pads hold the x neighbour
+// beyond either row end; and a plane outside the domain is zero in the
+// register windows (the staged input reads zero there and level 0 sets zero
+// past the last plane).  Adding +0 is what the segment kernel does for a
+// missing neighbour, so the sums are the same bits; only the neighbour
+// counts of the two end planes differ from the interior ones.
 // ---------------------------------------------------------------------------
-constexpr int kTbThreads = 768;
+constexpr int kTbThreads = 384;
+constexpr int kTbSlots = 18;
+constexpr int kTbSmemMax = 227 * 1024;
 
+// Rows of output per CTA: as many as the thread budget (one thread per quad
+// of a row pair; TY + 8 rows with the halo, rounded up to a whole pair) and
+// the shared memory (18 plane slots of rows of Wq + 1 float4, the last a
+// zero pad) allow.
 __host__ __device__ inline int tb_rows_tile(int Wq, int H) {
-    const int ty = kTbThreads / Wq - 8;
+    const int by_threads = 2 * (kTbThreads / Wq);
+    const int by_smem = kTbSmemMax / (kTbSlots * (Wq + 1) * 16);
+    const int ty = ((by_threads < by_smem ? by_threads : by_smem) & ~1) - 8;
     return ty < H ? ty : H;
 }
+__host__ __device__ inline int tb_rows_alloc(int TY) { return (TY + 8 + 1) & ~1; }
 
-__device__ __forceinline__ void cp_async16_tb(float4 *dst, const float *src) {
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-
+template <bool WARPROW>
 __global__ void __launch_bounds__(kTbThreads, 1)
 k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float *__restrict__ rhs_b,
            const float *__restrict__ pin_b, float *__restrict__ pout_r, float *__restrict__ pout_b, int TY, int ZC) {
-    // Shared memory, in units of one plane slot (rows x Wq float4):
+    // Shared memory, in units of one plane slot (2*blockDim.y rows of
+    // Wq + 1 float4; the last float4 of each row is a zero pad), addressed
+    // by 32-bit byte offsets:
     //   [0, 8)   p, colour c and plane k at slot c*4 + (k & 3)
     //   [8, 12)  red rhs, plane k at 8 + (k & 3)
     //   [12, 16) black rhs, plane k at 12 + (k & 3)
@@ -250,83 +299,185 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     // rhs and staged input are prefetched one step ahead with cp.async and
     // only ever read back by the thread that loaded them.
     extern __shared__ float4 sm4[];
-    const int Wh = g.W >> 1, Wq = Wh >> 2;
+    char *const smc = reinterpret_cast<char *>(sm4);
+    const uint32_t sm_base = static_cast<uint32_t>(__cvta_generic_to_shared(sm4));
+    const int Wh = g.W >> 1, Wq = Wh >> 2, D = g.D;
     const int rows = TY + 8;
-    const int mq = threadIdx.x, r = threadIdx.y;
+    const int mq = threadIdx.x, rA = 2 * threadIdx.y, rB = rA + 1;
     const int j0 = blockIdx.x * TY, z0 = blockIdx.y * ZC;
-    const int z1 = z0 + ZC < g.D ? z0 + ZC : g.D;
-    const int j = j0 - 4 + r;
-    const bool row_ok = j >= 0 && j < g.H;
+    const int z1 = z0 + ZC < D ? z0 + ZC : D;
+    const int jA = j0 - 4 + rA, jB = jA + 1;
+    const bool okA = jA >= 0 && jA < g.H, okB = rB < rows && jB >= 0 && jB < g.H;
     const int m0 = 4 * mq;
-    const size_t pl = (size_t)Wh * g.H;
-    const size_t rowoff = (size_t)m0 + (size_t)Wh * (size_t)(row_ok ? j : 0);
+    const long long pl = (long long)Wh * g.H;
+    const long long offA = (long long)m0 + (long long)Wh * (okA ? jA : 0);
+    const long long offB = (long long)m0 + (long long)Wh * (okB ? jB : 0);
     const bool first = m0 == 0, last = m0 + 4 == Wh;
-    const bool has_ym = j > 0, has_yp = j < g.H - 1;
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    const size_t slot = (size_t)rows * Wq;
-    auto S = [&](int colour, int plane, int row) -> float4 * {
-        return sm4 + (size_t)(colour * 4 + (plane & 3)) * slot + (size_t)row * Wq;
+    const int rowb = (Wq + 1) * 16, slotb = 2 * (int)blockDim.y * rowb;
+    const int ownA = rA * rowb + mq * 16, ownB = ownA + rowb;
+    auto slot = [&](int c, int k) { return (c * 4 + (k & 3)) * slotb; };
+    auto lds4 = [&](int off) { return *reinterpret_cast<const float4 *>(smc + off); };
+    auto lds1 = [&](int off) { return *reinterpret_cast<const float *>(smc + off); };
+    auto sts4 = [&](int off, float4 v) { *reinterpret_cast<float4 *>(smc + off) = v; };
+    auto cp16 = [&](int off, const float *src) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sm_base + (uint32_t)off), "l"(src)
+                     : "memory");
     };
-    float4 *own = sm4 + (size_t)r * Wq + mq;                 // this thread's element of slot 0
-    auto RR = [&](int plane) { return own + (size_t)(8 + (plane & 3)) * slot; };
-    auto RB = [&](int plane) { return own + (size_t)(12 + (plane & 3)) * slot; };
-    auto ST = [&](int plane) { return own + (size_t)(16 + (plane & 1)) * slot; };
-    auto valid = [&](int k) { return row_ok && k >= 0 && k < g.D; };
+#pragma unroll
+    for (int sl = 0; sl < 8; ++sl) {
+        sts4(sl * slotb + ownA, zero4);
+        sts4(sl * slotb + ownB, zero4);
+        if (last) {                                   // the rows' pads
+            sts4(sl * slotb + ownA + 16, zero4);
+            sts4(sl * slotb + ownB + 16, zero4);
+        }
+    }
+    // Rows on which level h updates: bit h (the halo shrinks by one row per
+    // level; level 3's rows are the CTA's output rows).
+    auto rowmask = [&](int r, bool ok) {
+        return ok ? ((r >= 1 && r < rows - 1 ? 1u : 0u) | (r >= 2 && r < rows - 2 ? 2u : 0u) |
+                     (r >= 3 && r < rows - 3 ? 4u : 0u) | (r >= 4 && r < rows - 4 ? 8u : 0u))
+                  : 0u;
+    };
+    const unsigned mA = rowmask(rA, okA), mB = rowmask(rB, okB);
+    auto kact = [&](int h, int k) { return k >= z0 - 3 + h && k < z1 + 3 - h && k >= 0 && k < D; };
+    auto kin = [&](int k) { return k >= 0 && k < D; };
+    // Neighbour counts of each row's quad on planes with both z neighbours,
+    // for row parity s = 0 and 1.
+    const bool hymA = jA > 0, hypA = jA < g.H - 1, hymB = jB > 0, hypB = jB < g.H - 1;
+    const QuadDen qA0 = quad_den(sp, 0, first, last, hymA, hypA, true, true);
+    const QuadDen qA1 = quad_den(sp, 1, first, last, hymA, hypA, true, true);
+    const QuadDen qB0 = quad_den(sp, 0, first, last, hymB, hypB, true, true);
+    const QuadDen qB1 = quad_den(sp, 1, first, last, hymB, hypB, true, true);
+    const int RR = 8 * slotb, RB = 12 * slotb, STG = 16 * slotb;
     auto prefetch = [&](int k_red, int k_black, int k_in) {
         // red rhs: levels 0 and 2 cover planes [z0-3, z1+3); black rhs: levels 1 and 3 cover [z0-2, z1+2)
-        if (valid(k_red) && k_red >= z0 - 3 && k_red < z1 + 3) cp_async16_tb(RR(k_red), rhs_r + rowoff + (size_t)k_red * pl);
-        if (valid(k_black) && k_black >= z0 - 2 && k_black < z1 + 2) cp_async16_tb(RB(k_black), rhs_b + rowoff + (size_t)k_black * pl);
-        if (valid(k_in) && k_in < z1 + 4) cp_async16_tb(ST(k_in), pin_b + rowoff + (size_t)k_in * pl);
+        if (kin(k_red) && k_red >= z0 - 3 && k_red < z1 + 3) {
+            const int o = RR + (k_red & 3) * slotb;
+            if (okA) cp16(o + ownA, rhs_r + offA + k_red * pl);
+            if (okB) cp16(o + ownB, rhs_r + offB + k_red * pl);
+        }
+        if (kin(k_black) && k_black >= z0 - 2 && k_black < z1 + 2) {
+            const int o = RB + (k_black & 3) * slotb;
+            if (okA) cp16(o + ownA, rhs_b + offA + k_black * pl);
+            if (okB) cp16(o + ownB, rhs_b + offB + k_black * pl);
+        }
+        if (kin(k_in) && k_in < z1 + 4) {
+            const int o = STG + (k_in & 1) * slotb;
+            if (okA) cp16(o + ownA, pin_b + offA + k_in * pl);
+            if (okB) cp16(o + ownB, pin_b + offB + k_in * pl);
+        }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    // One level: the colour `c` cells of this thread's quad on plane k.
-    auto update = [&](int c, int k, float4 o, float4 zm, float4 zp) -> float4 {
-        const int oc = c ^ 1;
-        const float4 *so = S(oc, k, r);
-        const float4 ym = has_ym ? S(oc, k, r - 1)[mq] : zero4;
-        const float4 yp = has_yp ? S(oc, k, r + 1)[mq] : zero4;
-        const int s = (j + k + c) & 1;
-        const float *sf = reinterpret_cast<const float *>(so);
-        const float xe = s == 0 ? (first ? 0.0f : sf[m0 - 1]) : (last ? 0.0f : sf[m0 + 4]);
-        const bool has_zm = k > 0, has_zp = k < g.D - 1;
-        const float4 rv = c ? *RB(k) : *RR(k);
-        return gs_segment(sp, s, first, last, rv, o, xe, ym, yp, has_zm ? zm : zero4, has_zp ? zp : zero4,
-                          has_ym, has_yp, has_zm, has_zp);
-    };
-    auto active = [&](int h, int k) {
-        return row_ok && r >= 1 + h && r < rows - 1 - h && k >= z0 - 3 + h && k < z1 + 3 - h && k >= 0 &&
-               k < g.D;
-    };
-    // register windows: black planes t-3..t+1, red planes t-4..t
-    float4 bm3 = zero4, bm2 = zero4, bp1;
-    float4 bm1 = valid(z0 - 4) ? ld4(pin_b + rowoff + (size_t)(z0 - 4) * pl) : zero4;
-    float4 b0 = valid(z0 - 3) ? ld4(pin_b + rowoff + (size_t)(z0 - 3) * pl) : zero4;
-    float4 rm4 = zero4, rm3 = zero4, rm2 = zero4, rm1 = zero4, r0 = zero4;
-    S(1, z0 - 4, r)[mq] = bm1;
-    S(1, z0 - 3, r)[mq] = b0;
+    // register windows of each row: black planes t-3..t+1, red planes t-4..t
+    float4 bm3A = zero4, bm2A = zero4, bp1A, rm4A = zero4, rm3A = zero4, rm2A = zero4, rm1A = zero4, r0A = zero4;
+    float4 bm3B = zero4, bm2B = zero4, bp1B, rm4B = zero4, rm3B = zero4, rm2B = zero4, rm1B = zero4, r0B = zero4;
+    float4 bm1A = okA && kin(z0 - 4) ? ld4(pin_b + offA + (z0 - 4) * pl) : zero4;
+    float4 b0A = okA && kin(z0 - 3) ? ld4(pin_b + offA + (z0 - 3) * pl) : zero4;
+    float4 bm1B = okB && kin(z0 - 4) ? ld4(pin_b + offB + (z0 - 4) * pl) : zero4;
+    float4 b0B = okB && kin(z0 - 3) ? ld4(pin_b + offB + (z0 - 3) * pl) : zero4;
+    sts4(slot(1, z0 - 4) + ownA, bm1A);
+    sts4(slot(1, z0 - 3) + ownA, b0A);
+    sts4(slot(1, z0 - 4) + ownB, bm1B);
+    sts4(slot(1, z0 - 3) + ownB, b0B);
     prefetch(z0 - 3, z0 - 4, z0 - 2);                 // what the first step reads
+    // One quad update of row parity S: colour c on plane k, `own` the row's
+    // element offset, o the other colour's own quad, ym/yp/zm/zp its
+    // neighbours.
+    auto update = [&](auto s_c, int c, int k, int own, float4 o, float4 ym, float4 yp, float4 zm, float4 zp,
+                      const QuadDen &qi, bool hym, bool hyp) -> float4 {
+        constexpr int S = decltype(s_c)::value;
+        float xe;
+        if constexpr (WARPROW) {
+            const float v = S == 0 ? __shfl_up_sync(0xffffffffu, o.w, 1) : __shfl_down_sync(0xffffffffu, o.x, 1);
+            xe = (S == 0 ? first : last) ? 0.0f : v;
+        } else {
+            const int b = slot(c ^ 1, k) + own;
+            xe = S == 0 ? lds1(b - 4) : lds1(b + 16);
+        }
+        const float4 rv = lds4((c ? RB : RR) + (k & 3) * slotb + own);
+        if (k > 0 && k < D - 1) return gs_quad(sp.scale, S, rv, o, xe, ym, yp, zm, zp, qi);
+        return gs_quad(sp.scale, S, rv, o, xe, ym, yp, zm, zp, quad_den(sp, S, first, last, hym, hyp, k > 0, k < D - 1));
+    };
+    // The four levels of step t.  Every level of a step has, in row A, row
+    // parity (jA + t) & 1 (level h: plane t - h, colour h & 1), row B the
+    // other one.
+    auto levels = [&](int t, auto sa_c) {
+        constexpr int SA = decltype(sa_c)::value, SB = 1 - SA;
+        const std::integral_constant<int, SA> sA{};
+        const std::integral_constant<int, SB> sB{};
+        const QuadDen &qa = SA ? qA1 : qA0;
+        const QuadDen &qb = SB ? qB1 : qB0;
+        if (kact(0, t)) {
+            const int b = slot(1, t);
+            if (mA & 1u) {
+                r0A = update(sA, 0, t, ownA, b0A, lds4(b + ownA - rowb), b0B, bm1A, bp1A, qa, hymA, hypA);
+                sts4(slot(0, t) + ownA, r0A);
+            }
+            if (mB & 1u) {
+                r0B = update(sB, 0, t, ownB, b0B, b0A, lds4(b + ownB + rowb), bm1B, bp1B, qb, hymB, hypB);
+                sts4(slot(0, t) + ownB, r0B);
+            }
+        }
+        if (t >= D) { r0A = zero4; r0B = zero4; }
+        if (kact(1, t - 1)) {
+            const int b = slot(0, t - 1), w = slot(1, t - 1);
+            if (mA & 2u) {
+                bm1A = update(sA, 1, t - 1, ownA, rm1A, lds4(b + ownA - rowb), rm1B, rm2A, r0A, qa, hymA, hypA);
+                sts4(w + ownA, bm1A);
+            }
+            if (mB & 2u) {
+                bm1B = update(sB, 1, t - 1, ownB, rm1B, rm1A, lds4(b + ownB + rowb), rm2B, r0B, qb, hymB, hypB);
+                sts4(w + ownB, bm1B);
+            }
+        }
+        if (kact(2, t - 2)) {
+            const int b = slot(1, t - 2), w = slot(0, t - 2);
+            if (mA & 4u) {
+                rm2A = update(sA, 0, t - 2, ownA, bm2A, lds4(b + ownA - rowb), bm2B, bm3A, bm1A, qa, hymA, hypA);
+                sts4(w + ownA, rm2A);
+            }
+            if (mB & 4u) {
+                rm2B = update(sB, 0, t - 2, ownB, bm2B, bm2A, lds4(b + ownB + rowb), bm3B, bm1B, qb, hymB, hypB);
+                sts4(w + ownB, rm2B);
+            }
+        }
+        const int k3 = t - 3;
+        if (kact(3, k3)) {
+            const int b = slot(0, k3);
+            const bool outp = k3 >= z0;
+            if (mA & 8u) {
+                bm3A = update(sA, 1, k3, ownA, rm3A, lds4(b + ownA - rowb), rm3B, rm4A, rm2A, qa, hymA, hypA);
+                if (outp) {
+                    *reinterpret_cast<float4 *>(pout_r + offA + k3 * pl) = rm3A;
+                    *reinterpret_cast<float4 *>(pout_b + offA + k3 * pl) = bm3A;
+                }
+            }
+            if (mB & 8u) {
+                bm3B = update(sB, 1, k3, ownB, rm3B, rm3A, lds4(b + ownB + rowb), rm4B, rm2B, qb, hymB, hypB);
+                if (outp) {
+                    *reinterpret_cast<float4 *>(pout_r + offB + k3 * pl) = rm3B;
+                    *reinterpret_cast<float4 *>(pout_b + offB + k3 * pl) = bm3B;
+                }
+            }
+        }
+    };
     for (int t = z0 - 3; t < z1 + 3; ++t) {
         prefetch(t + 1, t, t + 2);                    // what the next step reads
         asm volatile("cp.async.wait_group 1;" ::: "memory");
-        bp1 = valid(t + 1) ? *ST(t + 1) : zero4;
-        S(1, t + 1, r)[mq] = bp1;
+        const int st = STG + ((t + 1) & 1) * slotb;
+        bp1A = okA && kin(t + 1) ? lds4(st + ownA) : zero4;
+        bp1B = okB && kin(t + 1) ? lds4(st + ownB) : zero4;
         __syncthreads();
-        if (active(0, t)) { r0 = update(0, t, b0, bm1, bp1); S(0, t, r)[mq] = r0; }
-        __syncthreads();
-        if (active(1, t - 1)) { bm1 = update(1, t - 1, rm1, rm2, r0); S(1, t - 1, r)[mq] = bm1; }
-        __syncthreads();
-        if (active(2, t - 2)) { rm2 = update(0, t - 2, bm2, bm3, bm1); S(0, t - 2, r)[mq] = rm2; }
-        __syncthreads();
-        const int k3 = t - 3;
-        if (active(3, k3)) {
-            bm3 = update(1, k3, rm3, rm4, rm2);
-            if (k3 >= z0 && r >= 4 && r < 4 + TY) {
-                *reinterpret_cast<float4 *>(pout_r + rowoff + (size_t)k3 * pl) = rm3;
-                *reinterpret_cast<float4 *>(pout_b + rowoff + (size_t)k3 * pl) = bm3;
-            }
-        }
-        rm4 = rm3; rm3 = rm2; rm2 = rm1; rm1 = r0;
-        bm3 = bm2; bm2 = bm1; bm1 = b0; b0 = bp1;
+        sts4(slot(1, t + 1) + ownA, bp1A);
+        sts4(slot(1, t + 1) + ownB, bp1B);
+        if ((jA + t) & 1) levels(t, std::integral_constant<int, 1>{});
+        else levels(t, std::integral_constant<int, 0>{});
+        rm4A = rm3A; rm3A = rm2A; rm2A = rm1A; rm1A = r0A;
+        bm3A = bm2A; bm2A = bm1A; bm1A = b0A; b0A = bp1A;
+        rm4B = rm3B; rm3B = rm2B; rm2B = rm1B; rm1B = r0B;
+        bm3B = bm2B; bm2B = bm1B; bm1B = b0B; b0B = bp1B;
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
@@ -337,28 +488,54 @@ static bool tb_supported(const Geom &g) {
     return Wq <= 48 && tb_rows_tile(Wq, g.H) >= 1;
 }
 
-static size_t tb_smem(const Geom &g, int TY) { return sizeof(float4) * 18 * (size_t)(TY + 8) * (g.W >> 3); }
+static size_t tb_smem(const Geom &g, int TY) {
+    return sizeof(float4) * kTbSlots * (size_t)tb_rows_alloc(TY) * ((g.W >> 3) + 1);
+}
 
-// One pass = two sweeps from (p_in) into (p_out).
+static int device_sm_count() {
+    static int cache[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (cache[dev] == 0) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cache[dev] = n > 0 ? n : 1;
+    }
+    return cache[dev];
+}
+
+// One pass = two sweeps from (p_in) into (p_out).  ZC <= 0: planes per CTA
+// chosen so that the row bands times the z chunks fill the SMs in one wave
+// (one CTA per SM: its shared memory is most of the SM's), at least 8
+// planes.
 static void launch_tb_pass(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
                            const float *pin_b, float *pout_r, float *pout_b, int ZC, cudaStream_t st) {
     const int Wq = g.W >> 3, TY = tb_rows_tile(Wq, g.H);
     const size_t smem = tb_smem(g, TY);
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_rbgs_tb2, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(k_rbgs_tb2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_rbgs_tb2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
         attr_set = true;
     }
-    const dim3 b(Wq, TY + 8, 1);
+    if (ZC <= 0) {
+        const int bands = (g.H + TY - 1) / TY;
+        const int chunks = std::max(1, device_sm_count() / bands);
+        ZC = std::max(8, (g.D + chunks - 1) / chunks);
+    }
+    const dim3 b(Wq, tb_rows_alloc(TY) / 2, 1);
     const dim3 gr((g.H + TY - 1) / TY, (g.D + ZC - 1) / ZC, 1);
-    k_rbgs_tb2<<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC);
+    if (Wq == 32) k_rbgs_tb2<true><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC);
+    else k_rbgs_tb2<false><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC);
 }
 
 // (planes per thread, rows per block) of each segment-kernel variant; the
-// variants after them are the temporal-blocking pass with ZC planes per CTA.
+// variants after them are the temporal-blocking pass with ZC planes per CTA
+// (0: sized to fill the SMs).
 static const int kVariantKZ[kSegVariants] = {1, 2, 4, 8, 2, 4};
 static const int kVariantBY[kSegVariants] = {8, 8, 4, 4, 4, 8};
-static const int kVariantZC[kSweepVariants - kSegVariants] = {16, 32};
+static const int kVariantZC[kSweepVariants - kSegVariants] = {16, 32, 0};
 
 int sweep_variant_count(const Geom &g) {
     if ((g.W & 7) != 0) return 0;

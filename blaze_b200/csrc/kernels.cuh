@@ -63,7 +63,7 @@ void launch_divergence(const Geom &g, const float *U, const float *V, const floa
 // sweeps per pass; all give identical results.  Other W use the one-cell
 // kernel.  sweep_variant_count: variants available for this grid (0: W % 8).
 constexpr int kSegVariants = 6;
-constexpr int kSweepVariants = 8;
+constexpr int kSweepVariants = 9;
 int  sweep_variant_count(const Geom &g);
 void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                         const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,

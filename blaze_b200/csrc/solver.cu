@@ -454,11 +454,11 @@ static int residual_sync(blz_solver *s, double *r, double *b) {
     return BLZ_OK;
 }
 
-// Sweep launch-shape autotuner: each variant of the segment kernel runs a few
-// sweeps on scratch copies of p (the solver's state is untouched; rhs is only
-// read), timed with CUDA events; the fastest is kept per (device, grid dims)
-// for the life of the process.  BLZ_SWEEP_VARIANT or params.sweep_variant
-// forces a choice.
+// Sweep launch-shape autotuner: each variant (segment-kernel shapes and the
+// temporal-blocking passes) runs sweeps on scratch copies of p (the solver's
+// state is untouched; rhs is only read), timed with CUDA events around a
+// graph launch; the fastest is kept per (device, grid dims) for the life of
+// the process.  BLZ_SWEEP_VARIANT or params.sweep_variant forces a choice.
 // Scratch pressure of the temporal-blocking sweeps (slot 4 of the six
 // T-sized scratch arrays; the autotuner's copy of p uses slots 0-1).
 static float *q_r(blz_solver *s) { return s->scratch + 4 * n_of(s->P, 0); }
@@ -489,27 +489,61 @@ static int choose_variant(blz_solver *s) {
     CK(s, cudaMemcpyAsync(tb, s->p_b, half * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
     const SolveParams sp = solve_params(s->P);
     long long dummy = 0;
-    // An untimed round over every variant first (the SM clock ramps up under
-    // load, which would favour whichever variant is timed last), then two
-    // timed rounds in opposite orders; each variant keeps its faster time.
-    // 4 and 8 sweeps: whole passes for the temporal-blocking variants.
+    // Direct launches first: they set the kernels' attributes outside any
+    // capture and warm the SM clock.
     for (int v = 0; v < nv; ++v)
         launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 4, s->st, &dummy, v, q_r(s), q_b(s));
     CKL(s);
+    CK(s, cudaStreamSynchronize(s->st));
+    // Each variant is timed as the solve runs it: kTuneSweeps sweeps (one
+    // residual-check interval at the default) captured in a CUDA graph, so
+    // the launch count of a variant does not count against it.  An untimed
+    // round, then two timed rounds in opposite orders (the SM clock ramps up
+    // under load); each variant keeps its faster time.
+    constexpr int kTuneSweeps = 20;
+    cudaStream_t ts = nullptr;
+    CK(s, cudaStreamCreateWithFlags(&ts, cudaStreamNonBlocking));
+    std::vector<cudaGraphExec_t> ex(nv, nullptr);
+    std::vector<long long> per_graph(nv, 0);
     std::vector<float> t_min(nv, 1e30f);
-    for (int round = 0; round < 2; ++round)
-        for (int i = 0; i < nv; ++i) {
+    cudaError_t err = cudaSuccess;
+    for (int v = 0; v < nv && err == cudaSuccess; ++v) {
+        cudaGraph_t gph = nullptr;
+        err = cudaStreamBeginCapture(ts, cudaStreamCaptureModeThreadLocal);
+        if (err != cudaSuccess) break;
+        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, kTuneSweeps, ts, &per_graph[v], v, q_r(s),
+                           q_b(s));
+        err = cudaStreamEndCapture(ts, &gph);
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&ex[v], gph, 0);
+        if (gph) cudaGraphDestroy(gph);
+    }
+    for (int v = 0; v < nv && err == cudaSuccess; ++v) {
+        err = cudaGraphLaunch(ex[v], ts);
+        if (err == cudaSuccess) dummy += per_graph[v];
+    }
+    for (int round = 0; round < 2 && err == cudaSuccess; ++round)
+        for (int i = 0; i < nv && err == cudaSuccess; ++i) {
             const int v = round == 0 ? i : nv - 1 - i;
-            CK(s, cudaEventRecord(s->ev[6], s->st));
-            launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, tr, tb, 8, s->st, &dummy, v, q_r(s), q_b(s));
-            CK(s, cudaEventRecord(s->ev[7], s->st));
-            CKL(s);
-            CK(s, cudaEventSynchronize(s->ev[7]));
             float ms = 0.0f;
-            CK(s, cudaEventElapsedTime(&ms, s->ev[6], s->ev[7]));
-            t_min[v] = std::min(t_min[v], ms);
+            err = cudaEventRecord(s->ev[6], ts);
+            if (err == cudaSuccess) err = cudaGraphLaunch(ex[v], ts);
+            if (err == cudaSuccess) dummy += per_graph[v];
+            if (err == cudaSuccess) err = cudaEventRecord(s->ev[7], ts);
+            if (err == cudaSuccess) err = cudaEventSynchronize(s->ev[7]);
+            if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, s->ev[6], s->ev[7]);
+            if (err == cudaSuccess) t_min[v] = std::min(t_min[v], ms);
         }
+    cudaStreamSynchronize(ts);
+    for (auto e : ex)
+        if (e) cudaGraphExecDestroy(e);
+    cudaStreamDestroy(ts);
+    if (err != cudaSuccess) return fail(s, BLZ_ERR_CUDA, "sweep autotuner: %s", cudaGetErrorString(err));
     const int best = (int)(std::min_element(t_min.begin(), t_min.end()) - t_min.begin());
+    if (std::getenv("BLZ_TUNE_VERBOSE")) {
+        std::fprintf(stderr, "sweep autotuner %dx%dx%d, us per sweep:", s->g.W, s->g.H, s->g.D);
+        for (int v = 0; v < nv; ++v) std::fprintf(stderr, " v%d=%.2f", v, 1e3f * t_min[v] / kTuneSweeps);
+        std::fprintf(stderr, " -> v%d\n", best);
+    }
     s->launches += dummy;
     s->variant = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
