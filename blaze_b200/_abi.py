@@ -92,6 +92,30 @@ class BlzConvDesc(C.Structure):
                 ("relu", C.c_int), ("out_f32", C.c_int)]
 
 
+BLZ_MAX_LIGHTS = 10
+BLZ_MAX_RAMP = 10
+
+
+class BlzRenderParams(C.Structure):
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int),
+        ("cam_focal", C.c_float), ("cam_aperture", C.c_float),
+        ("cam_u", C.c_float * 3), ("cam_v", C.c_float * 3), ("cam_w", C.c_float * 3),
+        ("cam_trans", C.c_float * 3),
+        ("p_step", C.c_float), ("s_step", C.c_float), ("cutoff", C.c_float),
+        ("density_scale", C.c_float), ("shadow_density_scale", C.c_float), ("absorption", C.c_float),
+        ("scattering", C.c_float * 3), ("volume_color", C.c_float * 3),
+        ("gain", C.c_float), ("emission_scale", C.c_float), ("temp_range", C.c_float * 2),
+        ("ramp_size", C.c_int), ("ramp_keys", C.c_float * BLZ_MAX_RAMP),
+        ("ramp_colors", (C.c_float * 3) * BLZ_MAX_RAMP),
+        ("multi_scatter_scale", C.c_float), ("multi_scatter_density_mask", C.c_float * 2),
+        ("multi_scatter_color", C.c_float * 3), ("multi_scatter_blur_iter", C.c_int),
+        ("light_count", C.c_int),
+        ("light_dir", (C.c_float * 3) * BLZ_MAX_LIGHTS), ("light_color", (C.c_float * 3) * BLZ_MAX_LIGHTS),
+        ("light_intensity", C.c_float * BLZ_MAX_LIGHTS), ("light_exposure", C.c_float * BLZ_MAX_LIGHTS),
+    ]
+
+
 # Every entry point declared in include/blaze_b200.h, with its ctypes signature.
 _P = C.POINTER
 EXPORTS = {
@@ -144,6 +168,18 @@ EXPORTS = {
     "blz_batch_solve": (C.c_int, [C.c_void_p, _P(BlzStepStats)]),
     "blz_batch_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "blz_batch_last_ms": (C.c_float, [C.c_void_p]),
+    "blz_render_create": (C.c_int, [_P(BlzRenderParams), _P(BlzParams), _P(C.c_void_p)]),
+    "blz_render_destroy": (C.c_int, [C.c_void_p]),
+    "blz_render_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "blz_render": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "blz_render_solver": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "blz_render_get_image": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "blz_render_write": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "blz_image_write": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int]),
+    "blz_render_sample_temp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "blz_render_last_ms": (C.c_float, [C.c_void_p]),
+    "blz_render_kernel_launches": (C.c_longlong, [C.c_void_p]),
+    "blz_render_last_error": (C.c_char_p, [C.c_void_p]),
     "blz_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "blz_last_error": (C.c_char_p, [C.c_void_p]),
 }

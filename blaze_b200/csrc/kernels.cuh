@@ -137,6 +137,8 @@ void launch_batch_check(const BatchSim *sims, const int *blk0, int nsims, int to
 void solver_batch_view(blz_solver *s, BatchSim *out, const blz_params **P);
 void solver_flip_front(blz_solver *s);
 void solver_add_launches(blz_solver *s, long long n);
+cudaStream_t solver_stream(blz_solver *s);
+const blz_params *solver_params(blz_solver *s);
 
 // -- learned warm start: tensor-core convolution (unet_conv.cu) -------------
 struct ConvDesc {

@@ -869,4 +869,6 @@ void solver_batch_view(blz_solver *s, BatchSim *out, const blz_params **P) {
 }
 void solver_flip_front(blz_solver *s) { s->cur ^= 1; }
 void solver_add_launches(blz_solver *s, long long n) { s->launches += n; }
+cudaStream_t solver_stream(blz_solver *s) { return s->st; }
+const blz_params *solver_params(blz_solver *s) { return &s->P; }
 } // namespace blz

@@ -2,11 +2,12 @@
 
 ``load_blz`` reads the solver fields the reference's Parser::sceneParse reads
 (src/Parser.h:41-171) into a SceneSettings; renderer fields are kept in
-``extra``.  ``particle_file`` applies the reference's animated-source naming
-(src/Parser.h:181-188), and ``run`` is the frame loop of src/main.cu:89-106
-without the renderer:
+``extra`` (``render.render_params_from_blz`` turns them into the renderer's
+parameters).  ``particle_file`` applies the reference's animated-source
+naming (src/Parser.h:181-188), and ``run`` is the frame loop of
+src/main.cu:89-106, rendering the frames in renderRange when asked:
 
-    python -m blaze_b200.scenefile scene.blz [--frames N]
+    python -m blaze_b200.scenefile scene.blz [--frames N] [--render]
 """
 import argparse
 import json
@@ -72,29 +73,42 @@ def load_blz(path):
                      render_range, d)
 
 
-def run(scene, frames=None, on_frame=None):
-    """The reference's frame loop (main.cu:89-106) minus rendering: frames
-    run from sourceRange.x to renderRange.y; while iter <= sourceRange.y a
-    frame sources particles first; a static source's file is read once
-    (FluidSolver.cu:775-794).  Returns the per-frame step statistics."""
+def run(scene, frames=None, on_frame=None, render=False):
+    """The reference's frame loop (main.cu:89-106): frames run from
+    sourceRange.x to renderRange.y; while iter <= sourceRange.y a frame
+    sources particles first; a static source's file is read once
+    (FluidSolver.cu:775-794); with `render`, a frame inside renderRange is
+    rendered and written under the reference's file name (main.cu:96-99).
+    Returns the per-frame step statistics."""
     from .solver import FluidSolver
     tmr = Timer(iter=scene.source_range[0], time=0.0)
     last = scene.render_range[1] if frames is None else scene.source_range[0] + frames - 1
     stats = []
     loaded = False
-    with FluidSolver(tmr, scene.settings) as solver:
-        while tmr.iter <= last:
-            if tmr.iter <= scene.source_range[1]:
-                if scene.animated or not loaded:
-                    solver.setParticles(read_part(scene.particle_file(tmr.iter)))
-                    loaded = True
-                solver.addSource()
-            st = solver.step()
-            stats.append(st)
-            if on_frame is not None:
-                on_frame(tmr.iter, solver, st)
-            tmr.iter += 1
-            tmr.time += scene.settings.dt
+    engine = None
+    if render:
+        from .render import RenderEngine, render_params_from_blz
+        engine = RenderEngine(tmr, scene.settings, render_params_from_blz(scene.raw))
+    try:
+        with FluidSolver(tmr, scene.settings) as solver:
+            while tmr.iter <= last:
+                if tmr.iter <= scene.source_range[1]:
+                    if scene.animated or not loaded:
+                        solver.setParticles(read_part(scene.particle_file(tmr.iter)))
+                        loaded = True
+                    solver.addSource()
+                st = solver.step()
+                if engine is not None and scene.render_range[0] <= tmr.iter <= scene.render_range[1]:
+                    st["ms_render"] = engine.render(solver)
+                    st["render_file"] = engine.writeToDisk(scene)
+                stats.append(st)
+                if on_frame is not None:
+                    on_frame(tmr.iter, solver, st)
+                tmr.iter += 1
+                tmr.time += scene.settings.dt
+    finally:
+        if engine is not None:
+            engine.close()
     return stats
 
 
@@ -102,9 +116,10 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description="Run a Blaze .blz scene through the B200 fluid step")
     ap.add_argument("scene")
     ap.add_argument("--frames", type=int, default=None)
+    ap.add_argument("--render", action="store_true", help="render frames in renderRange (main.cu:96-99)")
     a = ap.parse_args(argv)
     sc = load_blz(a.scene)
-    for n, st in enumerate(run(sc, a.frames)):
+    for n, st in enumerate(run(sc, a.frames, render=a.render)):
         print(f"frame {sc.source_range[0] + n:04d}: {st['ms_total']:.2f} ms, "
               f"{st['iterations']} sweeps, rel. residual {st['rel_residual']:.2e}")
     return 0

@@ -18,6 +18,11 @@
  *   struct SceneSettings (solver fields)    src/SceneSettings.h:32-71   -> blz_params
  *   Timer::iter / Timer::time               src/Timer.h:35-36           -> time argument of blz_step
  *   Parser::sourceParticleParse records     src/Parser.h:196-209        -> rec8 layout of blz_set_particles
+ *   class RenderEngine           src/RenderEngine.h:46-95
+ *     RenderEngine(Timer*, SceneSettings)   src/RenderEngine.cu:250-293 -> blz_render_create
+ *     render(Grid**)                        src/RenderEngine.cu:306-365 -> blz_render / blz_render_solver
+ *     writeToDisk()                         src/RenderEngine.cu:367-476 -> blz_render_write
+ *   struct SceneSettings (renderer fields)  src/SceneSettings.h:73-107  -> blz_render_params
  *   checkCudaErrors -> exit()               src/utils/helper_cuda.h:577 -> negative return codes
  *
  * Grid layout (identical to the reference so fields can be exchanged as is):
@@ -337,6 +342,75 @@ int  blz_batch_step(blz_batch *b, const float *times, blz_step_stats *stats);
 int  blz_batch_solve(blz_batch *b, blz_step_stats *stats);
 long long blz_batch_kernel_launches(const blz_batch *b);
 float blz_batch_last_ms(const blz_batch *b);             /* device ms of the last step/solve */
+
+/* ---- volume renderer ---------------------------------------------------------- */
+/* Replaces class RenderEngine (src/RenderEngine.h:46-95, RenderEngine.cu:
+ * 50-365): the temperature field rendered as an emissive, absorbing and
+ * single-scattering volume under directional lights, with an optional
+ * blurred quarter-resolution multiple-scattering term.  The fields are the
+ * renderer's part of SceneSettings (src/SceneSettings.h:73-107, parsed by
+ * Parser.h:109-170); light_samples is parsed by the reference and unused by
+ * its renderer, so it is not carried.                                      */
+#define BLZ_MAX_LIGHTS 10
+#define BLZ_MAX_RAMP   10
+
+typedef struct blz_render_params {
+    int   width, height;                       /* renderRes (pixels)                 */
+    float cam_focal, cam_aperture;             /* cam.focal, cam.aperture            */
+    float cam_u[3], cam_v[3], cam_w[3];        /* cam.rotMat rows                    */
+    float cam_trans[3];                        /* cam.t (camera origin, world)       */
+    float p_step, s_step, cutoff;              /* primarySampleRate, shadowSamplingRate,
+                                                  cutoff                             */
+    float density_scale, shadow_density_scale; /* densityScale, shadowDensityScale   */
+    float absorption;                          /* absorption                         */
+    float scattering[3], volume_color[3];      /* scatteringColor, volumeColor       */
+    float gain;                                /* gain (shadow-ray falloff)          */
+    float emission_scale;                      /* emissionScale                      */
+    float temp_range[2];                       /* shaderTempRange                    */
+    int   ramp_size;                           /* shaderColorRamp.count (1..10)      */
+    float ramp_keys[BLZ_MAX_RAMP];
+    float ramp_colors[BLZ_MAX_RAMP][3];
+    float multi_scatter_scale;                 /* multiScatterScale (0: off)         */
+    float multi_scatter_density_mask[2];
+    float multi_scatter_color[3];
+    int   multi_scatter_blur_iter;
+    int   light_count;                         /* 0..10 directional lights           */
+    float light_dir[BLZ_MAX_LIGHTS][3];
+    float light_color[BLZ_MAX_LIGHTS][3];
+    float light_intensity[BLZ_MAX_LIGHTS];
+    float light_exposure[BLZ_MAX_LIGHTS];
+} blz_render_params;
+
+typedef struct blz_renderer blz_renderer;
+/* RenderEngine(Timer*, SceneSettings) (RenderEngine.cu:250-293): `grid`
+ * gives the T dims (each >= 4), dx and the domain box.                      */
+int  blz_render_create(const blz_render_params *rp, const blz_params *grid, blz_renderer **out);
+int  blz_render_destroy(blz_renderer *r);
+int  blz_render_set_stream(blz_renderer *r, void *cuda_stream);
+/* RenderEngine::render(Grid**) (RenderEngine.cu:306-365): renders the
+ * temperature field `temp` (device memory, reference layout i + j*W + k*W*H,
+ * the grid's dims) into the renderer's frame buffer.  Synchronises.        */
+int  blz_render(blz_renderer *r, const float *temp);
+/* The same for a solver's current temperature field.                        */
+int  blz_render_solver(blz_renderer *r, blz_solver *s);
+/* The frame buffer: width*height RGB float triples, row 0 at the top
+ * (framebuffer[i + width*j] of RenderEngine.cu:185).                       */
+int  blz_render_get_image(const blz_renderer *r, float *rgb, int on_device);
+/* RenderEngine::writeToDisk (RenderEngine.cu:367-476): writes the frame
+ * buffer to `path`, format by extension: .ppm (ASCII P3, 255.99 scaling as
+ * the reference), .png (8-bit RGBA, clamped), .exr (32-bit float B, G, R
+ * scanlines, uncompressed).                                                 */
+int  blz_render_write(const blz_renderer *r, const char *path);
+/* The writer alone, on any host RGB buffer (width*height float triples, row
+ * 0 at the top); host code only, no GPU needed.                            */
+int  blz_image_write(const char *path, const float *rgb, int width, int height);
+/* Test hook: copies `temp` into the renderer's T volume and samples it at
+ * n texel coordinates pos3 (device memory, x y z per sample) through the
+ * renderer's filtered texture into out (device memory).                    */
+int  blz_render_sample_temp(blz_renderer *r, const float *temp, const float *pos3, int n, float *out);
+float blz_render_last_ms(const blz_renderer *r);          /* device ms of the last render */
+long long blz_render_kernel_launches(const blz_renderer *r);
+const char *blz_render_last_error(const blz_renderer *r);
 
 /* Number of kernels this solver launched since creation.                    */
 long long blz_kernel_launches(const blz_solver *s);

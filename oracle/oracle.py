@@ -21,8 +21,8 @@ _lib = None
 
 
 def build(force=False):
-    src = os.path.join(HERE, "blaze_oracle.cpp")
-    if force or not os.path.exists(LIB) or os.path.getmtime(src) > os.path.getmtime(LIB):
+    srcs = [os.path.join(HERE, f) for f in ("blaze_oracle.cpp", "render_oracle.cpp")]
+    if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
         subprocess.run(["make", "-s", "-C", HERE, "lib/liboracle.so"] + (["-B"] if force else []), check=True)
     return LIB
 
@@ -52,6 +52,11 @@ def load():
                 fn = getattr(lib, f"orc_{name}_{suf}")
                 fn.restype = None
                 fn.argtypes = args
+        F = C.POINTER(C.c_float)
+        lib.orc_tex_sample.restype = None
+        lib.orc_tex_sample.argtypes = [F, C.c_int, C.c_int, C.c_int, F, C.c_int, F, C.c_int]
+        lib.orc_render.restype = None
+        lib.orc_render.argtypes = [C.POINTER(_abi.BlzRenderParams), P, F, F, C.c_int]
         lib.orc_perlin.restype = C.c_float
         lib.orc_perlin.argtypes = [C.c_float] * 4 + [C.c_int]
         lib.orc_num_threads.restype = C.c_int
@@ -141,3 +146,24 @@ def perlin(x, y, z, scale, seed):
 
 def num_threads():
     return load().orc_num_threads()
+
+
+def tex_sample(T, pos3, quant=3):
+    """The texture sampler of the reference's renderer restated (trilinear,
+    clamped, weights quantised per `quant`, render_oracle.cpp; 3 is the rule
+    measured on B200) on T shaped (z, y, x) at texel coordinates pos3 (n, 3)."""
+    T = np.ascontiguousarray(T, np.float32)
+    pos = np.ascontiguousarray(pos3, np.float32).reshape(-1, 3)
+    out = np.empty(len(pos), np.float32)
+    D, H, W = T.shape
+    load().orc_tex_sample(_ptr(T), W, H, D, _ptr(pos), len(pos), _ptr(out), quant)
+    return out
+
+
+def render(rp, grid, T, quant=3):
+    """The reference's render pass restated (render_oracle.cpp): image of T
+    (z, y, x) shaped (height, width, 3), row 0 at the top."""
+    T = np.ascontiguousarray(T, np.float32)
+    out = np.empty((rp.height, rp.width, 3), np.float32)
+    load().orc_render(C.byref(rp), C.byref(grid), _ptr(T), _ptr(out), quant)
+    return out

@@ -41,6 +41,10 @@ def load():
             ("ref_get_field", C.c_int, [C.c_void_p, C.c_int, F]),
             ("ref_set_field", C.c_int, [C.c_void_p, C.c_int, F]),
             ("ref_perlin", C.c_int, [F, C.c_int, C.c_float, C.c_int, F]),
+            ("ref_render_create", C.c_void_p, [C.c_void_p, C.POINTER(_abi.BlzRenderParams)]),
+            ("ref_render", C.c_int, [C.c_void_p, C.c_void_p, F]),
+            ("ref_render_get", C.c_int, [C.c_void_p, F]),
+            ("ref_render_destroy", None, [C.c_void_p]),
         ]:
             fn = getattr(lib, name)
             fn.restype = res
@@ -113,3 +117,36 @@ def perlin(pos3, scale, seed):
     _chk(load().ref_perlin(a.ctypes.data_as(C.POINTER(C.c_float)), len(a), scale, seed,
                            out.ctypes.data_as(C.POINTER(C.c_float))), "perlin")
     return out
+
+
+class RefRenderer:
+    """The reference's RenderEngine on a RefSolver's temperature field."""
+
+    def __init__(self, sim, rp):
+        self.sim, self.rp = sim, rp
+        self.lib = sim.lib
+        self.h = self.lib.ref_render_create(sim.h, C.byref(rp))
+        if not self.h:
+            raise RuntimeError("ref_render_create failed")
+
+    def render(self):
+        """Renders the solver's current T; returns device milliseconds."""
+        ms = C.c_float()
+        _chk(self.lib.ref_render(self.sim.h, self.h, C.byref(ms)), "render")
+        return ms.value
+
+    def image(self):
+        out = np.empty((self.rp.height, self.rp.width, 3), np.float32)
+        _chk(self.lib.ref_render_get(self.h, out.ctypes.data_as(C.POINTER(C.c_float))), "render_get")
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.ref_render_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

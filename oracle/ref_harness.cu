@@ -2,7 +2,9 @@
 //
 // TEST INFRASTRUCTURE ONLY.  Built by `make -C oracle ref` into
 // oracle/_ref/libblaze_ref.so, which compiles the reference's
-// src/FluidSolver.cu where it lies (unmodified; included below) with the
+// src/FluidSolver.cu and src/RenderEngine.cu where they lie (unmodified;
+// included below; lodepng.cpp, which the renderer's PNG writer calls, is
+// compiled from the reference's thirdparty/ tree) with the
 // reference's documented flags.  It serves as (a) a parity pin: the tests run
 // the reference's kernels on seeded inputs and compare the oracle with them,
 // and (b) the reference timing arm of bench.py.  Nothing in the product links
@@ -34,8 +36,23 @@
 
 #include "../include/blaze_b200.h"
 
+// Standard headers the reference's renderer and its image libraries
+// (lodepng, tinyexr) use, included before `private` is redefined.
+#include <algorithm>
+#include <cfloat>
+#include <cstdint>
+#include <limits>
+#include <map>
+#include <set>
+#include <utility>
+
+// Ray.h calls uint_as_float, a device function older CUDA releases declared
+// and CUDA 12.9 no longer does; this maps it to the current intrinsic.
+__device__ __forceinline__ float uint_as_float(unsigned int u) { return __uint_as_float(u); }
+
 #define private public
 #include "FluidSolver.cu"
+#include "RenderEngine.cu"
 #undef private
 
 namespace {
@@ -227,6 +244,84 @@ int ref_set_field(void *h, int f, const float *src) {
     if (!n) return -2;
     float *dst = f == 4 ? r->fs->d_mP : f == 5 ? r->fs->d_mRhs : front_of(r, f);
     return cudaMemcpy(dst, src, n * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess ? 0 : -1;
+}
+
+// The reference's RenderEngine (RenderEngine.cu:250-365) on the harness
+// solver's temperature field: the renderer fields of blz_render_params are
+// copied into the simulation's SceneSettings, which RenderEngine reads.
+void *ref_render_create(void *h, const blz_render_params *rp) {
+    RefSim *r = (RefSim *)h;
+    SceneSettings &s = r->scn;
+    s.renderRes = make_int2(rp->width, rp->height);
+    s.camFocal = rp->cam_focal;
+    s.camAperture = rp->cam_aperture;
+    s.camU = make_float3(rp->cam_u[0], rp->cam_u[1], rp->cam_u[2]);
+    s.camV = make_float3(rp->cam_v[0], rp->cam_v[1], rp->cam_v[2]);
+    s.camW = make_float3(rp->cam_w[0], rp->cam_w[1], rp->cam_w[2]);
+    s.camTrans = make_float3(rp->cam_trans[0], rp->cam_trans[1], rp->cam_trans[2]);
+    s.rndrPStep = rp->p_step;
+    s.rndrSStep = rp->s_step;
+    s.rndrCutoff = rp->cutoff;
+    s.shaderDensityScale = rp->density_scale;
+    s.shaderShadowDensityScale = rp->shadow_density_scale;
+    s.shaderAbsorption = rp->absorption;
+    s.shaderScattering = make_float3(rp->scattering[0], rp->scattering[1], rp->scattering[2]);
+    s.shaderVolumeColor = make_float3(rp->volume_color[0], rp->volume_color[1], rp->volume_color[2]);
+    s.shaderGain = rp->gain;
+    s.shaderEmissionScale = rp->emission_scale;
+    s.shaderTempRampSize = rp->ramp_size;
+    s.shaderTempRange = make_float2(rp->temp_range[0], rp->temp_range[1]);
+    for (int i = 0; i < rp->ramp_size; ++i) {
+        s.shaderColorRampKeys[i] = rp->ramp_keys[i];
+        s.shaderColorRampColors[i] = make_float3(rp->ramp_colors[i][0], rp->ramp_colors[i][1], rp->ramp_colors[i][2]);
+    }
+    s.multiScatterScale = rp->multi_scatter_scale;
+    s.multiScatterDensityMask = make_float2(rp->multi_scatter_density_mask[0], rp->multi_scatter_density_mask[1]);
+    s.multiScatterColor = make_float3(rp->multi_scatter_color[0], rp->multi_scatter_color[1], rp->multi_scatter_color[2]);
+    s.multiScatterBlurIter = rp->multi_scatter_blur_iter;
+    s.lightCount = rp->light_count;
+    for (int i = 0; i < rp->light_count; ++i) {
+        s.lightExposure[i] = rp->light_exposure[i];
+        s.lightIntensity[i] = rp->light_intensity[i];
+        s.lightSamples[i] = 1;
+        s.lightDir[i] = make_float3(rp->light_dir[i][0], rp->light_dir[i][1], rp->light_dir[i][2]);
+        s.lightColor[i] = make_float3(rp->light_color[i][0], rp->light_color[i][1], rp->light_color[i][2]);
+    }
+    std::snprintf(s.renderFile, sizeof s.renderFile, "render_####.exr");
+    RenderEngine *e = new RenderEngine(&r->tmr, s);
+    return cudaDeviceSynchronize() == cudaSuccess ? e : nullptr;
+}
+
+// One render of the solver's current T; device milliseconds in *ms.
+int ref_render(void *h, void *eng, float *ms) {
+    RefSim *r = (RefSim *)h;
+    RenderEngine *e = (RenderEngine *)eng;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a);
+    e->render(r->fs->getTempGrid());
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (ms) *ms = t;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// The frame buffer (mRdrWidth * mRdrHeight float3, row 0 at the top).
+int ref_render_get(void *eng, float *rgb) {
+    RenderEngine *e = (RenderEngine *)eng;
+    if (cudaDeviceSynchronize() != cudaSuccess) return -1;
+    std::memcpy(rgb, e->mFrameBuffer, sizeof(float) * 3 * (size_t)e->mRdrWidth * e->mRdrHeight);
+    return 0;
+}
+
+void ref_render_destroy(void *eng) {
+    delete (RenderEngine *)eng;
+    cudaDeviceSynchronize();
 }
 
 int ref_perlin(const float *pos3, int n, float scale, int seed, float *out) {
