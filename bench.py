@@ -512,6 +512,149 @@ def run_reference(args, ws, rank, local):
     }
 
 
+RENDER_RES = (1280, 720)
+
+
+def plume_field(n, seed=SEED):
+    """A seeded synthetic temperature field shaped like the plume family at
+    frame 12: three columns rising from the lower half with mushroom caps,
+    smooth, zero elsewhere, with 10 % multiplicative noise; (z, y, x), float32."""
+    rng = np.random.default_rng(seed)
+    ax = (np.arange(n, dtype=np.float32) + 0.5) / n
+    z, y, x = ax[:, None, None], ax[None, :, None], ax[None, None, :]
+    T = np.zeros((n, n, n), np.float32)
+    for _ in range(3):
+        cx, cz = rng.uniform(0.25, 0.75, 2)
+        top, r = rng.uniform(0.35, 0.7), rng.uniform(0.06, 0.1)
+        yy = 1.0 - y                                   # grid y runs down from the top
+        d2 = (x - cx) ** 2 + (z - cz) ** 2
+        stem = np.exp(-d2 / (2 * (0.3 * r) ** 2)) * ((yy < top) & (yy > 0.02))
+        cap = np.exp(-(d2 / (2 * r * r) + (yy - top) ** 2 / (2 * (0.6 * r) ** 2)))
+        T += (1.5 * stem + 2.0 * cap).astype(np.float32)
+    T *= (1.0 + 0.1 * rng.standard_normal(T.shape)).astype(np.float32)
+    T[T < 1e-3] = 0.0
+    return T
+
+
+def _render_setup(args):
+    from blaze_b200.render import default_render_params
+    from blaze_b200.scenes import SceneSettings
+    n = args.grid
+    scn = SceneSettings(gridRes=(n, n, n), dx=1.0 / n)
+    rp = default_render_params(scn, width=RENDER_RES[0], height=RENDER_RES[1], lights=1, multi_scatter=True)
+    return scn, rp, plume_field(n)
+
+
+def _render_config(args, rp):
+    return {"workload": f"volume render of a {args.grid}^3 temperature field (seeded synthetic plumes) at "
+                        f"{rp.width}x{rp.height}, 1 directional light with shadow rays, multiple scattering "
+                        f"(3 blur passes), primary step dx, shadow step 2 dx",
+            "grid": [args.grid] * 3, "image": [rp.width, rp.height], "lights": rp.light_count,
+            "l2": "T (67 MB) exceeds L2 when uploaded; the render reads it through a 3-D texture"}
+
+
+def run_render(args, ws, rank, local):
+    """The renderer (RenderEngine::render, src/RenderEngine.cu:306-365): value
+    = renders/s of the device pass (T resident); e2e = T uploaded from pinned
+    host memory and the image read back every step, through RenderEngine."""
+    import torch
+    from blaze_b200.render import RenderEngine
+    from blaze_b200.scenes import Timer
+    torch.cuda.set_device(local)
+    scn, rp, T = _render_setup(args)
+    Td = torch.from_numpy(T).cuda()
+    eng = RenderEngine(Timer(), scn, rp)
+    for _ in range(args.warmup):
+        eng.render(Td)
+    if ws > 1:
+        torch.distributed.barrier()
+    l0 = eng.kernel_launches
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ms_each = [eng.render(Td) for _ in range(args.steps)]
+        torch.cuda.synchronize()
+    ms = float(sum(ms_each))
+    launches = eng.kernel_launches - l0
+    img = eng.image()
+    e2e = None
+    if not args.no_e2e:
+        host = torch.from_numpy(T).pin_memory()
+        e0 = time.perf_counter()
+        for _ in range(args.steps):
+            Td.copy_(host, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            eng.render(Td)
+            eng.image()
+        e2e = args.steps / (time.perf_counter() - e0)
+    eng.close()
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t[0].item())
+    if rank != 0:
+        return None
+    cpu = None
+    if not args.no_cpu:
+        from oracle import oracle
+        from blaze_b200 import _abi
+        g = scn.to_params()
+        sub = _abi.BlzRenderParams()
+        C_ = __import__("ctypes")
+        C_.pointer(sub)[0] = rp
+        sub.width, sub.height = rp.width // 8, rp.height // 8          # 1/64 of the pixels, same camera
+        c0 = time.perf_counter()
+        oracle.render(sub, g, T)
+        cs = time.perf_counter() - c0
+        cpu = {"value": 1.0 / (cs * 64.0), "unit": "renders/s", "cores": oracle.num_threads(), "kind": "port",
+               "sample": f"the oracle's render pass (render_oracle.cpp) at {sub.width}x{sub.height}, the same "
+                         f"camera, scaled by the pixel count to {rp.width}x{rp.height} ({cs:.1f} s)"}
+    value = ws * args.steps / (ms * 1e-3)
+    return {"metric": f"{args.grid}³ volume renders/s at {rp.width}x{rp.height}", "value": value,
+            "unit": "renders/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": _render_config(args, rp),
+            "render_ms": ms_each, "image_mean": float(img.mean()), "image_max": float(img.max()),
+            "roofline": None,
+            "roofline_note": "k_render is bound by texture-filter issue and the latency of dependent ray "
+                             "steps, not by HBM bytes or tensor FLOPs (profiles/k_render_256.md)",
+            "cpu_baseline": cpu,
+            "e2e": None if e2e is None else {"value": ws * e2e, "unit": "renders/s",
+                                             "h2d_bytes_per_step": int(T.nbytes),
+                                             "d2h_bytes_per_step": int(img.nbytes)},
+            "gpu_launches": int(launches), "clocks": clk.summary()}
+
+
+def run_render_reference(args, ws, rank, local):
+    """The reference's RenderEngine (built from its sources into oracle/_ref)
+    on the same field, camera and settings, timed with CUDA events."""
+    if rank != 0:
+        return None
+    import torch
+    from oracle import ref
+    if not ref.available():
+        return {"impl": "reference", "unavailable": "reference CUDA build (oracle/_ref) not built"}
+    torch.cuda.set_device(local)
+    scn, rp, T = _render_setup(args)
+    with ref.RefSolver(scn.to_params()) as sim:
+        sim.set("T", T)
+        with ref.RefRenderer(sim, rp) as rr:
+            for _ in range(args.warmup):
+                rr.render()
+            with ClockSampler(local) as clk:
+                ms_each = [rr.render() for _ in range(args.steps)]
+    ms = float(sum(ms_each))
+    value = args.steps / (ms * 1e-3)
+    return {"metric": f"{args.grid}³ volume renders/s at {rp.width}x{rp.height}", "impl": "reference",
+            "value": value, "unit": "renders/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": _render_config(args, rp), "render_ms": ms_each,
+            "cpu_baseline": {"value": value, "unit": "renders/s", "cores": 1, "kind": "reference",
+                             "sample": "the reference's RenderEngine (src/RenderEngine.cu, -O3 --use_fast_math, "
+                                       "sm_100a) on the same B200 (it has no CPU path)"},
+            "e2e": {"value": value, "unit": "renders/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": clk.summary()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -522,8 +665,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) pass")
     ap.add_argument("--max-iter", type=int, default=MAX_ITER, help="GS sweep cap per frame (profiling runs)")
-    ap.add_argument("--workload", default="plume", choices=["plume", "batch"],
-                    help="plume: the 256^3 step (default); batch: 64 uneven simulations in one batch")
+    ap.add_argument("--workload", default="plume", choices=["plume", "batch", "render"],
+                    help="plume: the 256^3 step (default); batch: 64 uneven simulations in one batch; "
+                         "render: the volume renderer on a 256^3 field")
     ap.add_argument("--batch-sims", type=int, default=64)
     ap.add_argument("--plain-only", action="store_true", help="skip the learned warm-start pass")
     ap.add_argument("--weights", default=None, help="warm-start network weights (npz)")
@@ -533,7 +677,7 @@ def main():
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         # rank 0 alone runs the reference; the other ranks exit without work
-        line = run_reference(args, ws, rank, local)
+        line = (run_render_reference if args.workload == "render" else run_reference)(args, ws, rank, local)
         if line is not None:
             print(json.dumps(line), flush=True)
         return
@@ -545,6 +689,8 @@ def main():
     try:
         if args.workload == "batch":
             line = run_batch(args, ws, rank, local)
+        elif args.workload == "render":
+            line = run_render(args, ws, rank, local)
         else:
             line = run_ours(args, ws, rank, local)
     finally:

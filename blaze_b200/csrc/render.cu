@@ -71,6 +71,14 @@ struct RenderArgs {
     float skip_p, skip_s;
 };
 
+// Per-light and ramp tables, read with uniform loads (a kernel parameter
+// array indexed by a loop counter would be copied to local memory).
+struct Tables {
+    float3 l_dir[BLZ_MAX_LIGHTS], l_illum[BLZ_MAX_LIGHTS];
+    float ramp_keys[BLZ_MAX_RAMP];
+    float3 ramp_colors[BLZ_MAX_RAMP];
+};
+
 __device__ __forceinline__ float3 f3(float a, float b, float c) { return make_float3(a, b, c); }
 __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
 __device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
@@ -97,7 +105,7 @@ __device__ __forceinline__ Ray make_ray(float3 o, float3 d) {
     Ray r;
     r.o = o;
     r.d = d;
-    r.inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    r.inv = f3(fdiv(1.0f, d.x), fdiv(1.0f, d.y), fdiv(1.0f, d.z));
     r.sx = r.inv.x < 0.0f; r.sy = r.inv.y < 0.0f; r.sz = r.inv.z < 0.0f;
     r.t0 = 0.0f;
     r.t1 = __int_as_float(0x7f800000);
@@ -129,31 +137,34 @@ __device__ bool box_hit(Ray &r, float3 lo, float3 hi) {
 
 // World position -> texel coordinates of T, y measured down from the top of
 // the domain (Grid.h:292-296).
-__device__ __forceinline__ float3 world_to_grid(const RenderArgs &a, float3 p) {
-    return f3(fdiv(p.x - a.dmin.x, a.dx), fdiv(a.dsize.y - (p.y - a.dmin.y), a.dx), fdiv(p.z - a.dmin.z, a.dx));
+// inv_dx = fdiv(1, dx): the fast-math quotient x / dx is x times the
+// approximate reciprocal of dx, formed once per thread here.
+__device__ __forceinline__ float3 world_to_grid(const RenderArgs &a, float inv_dx, float3 p) {
+    return f3((p.x - a.dmin.x) * inv_dx, (a.dsize.y - (p.y - a.dmin.y)) * inv_dx, (p.z - a.dmin.z) * inv_dx);
 }
 
 // Temperature ramp (ColorRamp.h:57-79): piecewise-linear over keys in
 // [0, 1] after remapping [t_in, t_out].
-__device__ float3 ramp_color(const RenderArgs &a, float temp) {
-    const float x = fminf(fmaxf((temp - a.t_in) / (a.t_out - a.t_in), 0.0f), 1.0f);
-    if (a.ramp_n == 1) return a.ramp_colors[0];
+__device__ float3 ramp_color(const RenderArgs &a, const Tables *__restrict__ tb, float temp) {
+    const float x = fminf(fmaxf(fdiv(temp - a.t_in, a.t_out - a.t_in), 0.0f), 1.0f);
+    if (a.ramp_n == 1) return tb->ramp_colors[0];
     int prev = 0, next = 0;
     for (int i = 0; i < a.ramp_n; ++i) {
-        if (a.ramp_keys[i] <= x) {
+        if (tb->ramp_keys[i] <= x) {
             prev = i;
         } else {
             next = i;
             break;
         }
     }
-    const float range = a.ramp_keys[next] - a.ramp_keys[prev];
-    const float blend = (x - a.ramp_keys[prev]) / range;
-    return a.ramp_colors[prev] + blend * (a.ramp_colors[next] - a.ramp_colors[prev]);
+    const float range = tb->ramp_keys[next] - tb->ramp_keys[prev];
+    const float blend = fdiv(x - tb->ramp_keys[prev], range);
+    const float3 cp = tb->ramp_colors[prev], cn = tb->ramp_colors[next];
+    return cp + blend * (cn - cp);
 }
 
 __device__ __forceinline__ float smooth_step(float e0, float e1, float x) {
-    const float y = fmaxf(0.0f, fminf((x - e0) / (e1 - e0), 1.0f));
+    const float y = fmaxf(0.0f, fminf(fdiv(x - e0, e1 - e0), 1.0f));
     return y * y * (3.0f - (2.0f * y));
 }
 
@@ -174,23 +185,31 @@ __global__ void k_macro_max(const float *__restrict__ T, int W, int H, int D, in
     out[m] = v;
 }
 
-__device__ __forceinline__ float macro_at(const RenderArgs &a, const float *__restrict__ macro, float3 g) {
-    const int mx = min(max((int)floorf(g.x * (1.0f / kMacro)), 0), a.mW - 1);
-    const int my = min(max((int)floorf(g.y * (1.0f / kMacro)), 0), a.mH - 1);
-    const int mz = min(max((int)floorf(g.z * (1.0f / kMacro)), 0), a.mD - 1);
-    return __ldg(macro + mx + a.mW * (my + a.mH * mz));
+// The cell maximum at texel coordinates g: a point-filtered, clamped 3-D
+// texture of the cells, sampled at g / kMacro (the texture unit forms floor
+// and clamp; measured faster than forming the cell index in registers and
+// reloading only on a change of cell).
+__device__ __forceinline__ float macro_at(cudaTextureObject_t mtex, float3 g) {
+    return tex3D<float>(mtex, g.x * (1.0f / kMacro), g.y * (1.0f / kMacro), g.z * (1.0f / kMacro));
 }
 
-// Light intensities color * intensity * 2^exposure (Light.h:44-47), formed
-// once per renderer on the device as the reference's Light constructor does.
-__global__ void k_light_setup(RenderArgs a, float3 *__restrict__ illum) {
-    if (threadIdx.x == 0 && blockIdx.x == 0)
-        for (int l = 0; l < a.n_lights; ++l) illum[l] = a.l_color[l] * a.l_intensity[l] * powf(2.0f, a.l_exposure[l]);
+// The tables; light intensities color * intensity * 2^exposure (Light.h:
+// 44-47) are formed on the device as the reference's Light constructor does.
+__global__ void k_tables_setup(RenderArgs a, Tables *__restrict__ tb) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int l = 0; l < a.n_lights; ++l) {
+        tb->l_dir[l] = a.l_dir[l];
+        tb->l_illum[l] = a.l_color[l] * a.l_intensity[l] * powf(2.0f, a.l_exposure[l]);
+    }
+    for (int i = 0; i < a.ramp_n; ++i) {
+        tb->ramp_keys[i] = a.ramp_keys[i];
+        tb->ramp_colors[i] = a.ramp_colors[i];
+    }
 }
 
 __global__ void __launch_bounds__(64) k_render(RenderArgs a, cudaTextureObject_t temp_tex,
-                                               cudaTextureObject_t scatter_tex, const float3 *__restrict__ illum,
-                                               const float *__restrict__ macro, float *__restrict__ fb) {
+                                               cudaTextureObject_t scatter_tex, cudaTextureObject_t macro_tex,
+                                               const Tables *__restrict__ tb, float *__restrict__ fb) {
     const int i = threadIdx.x + blockIdx.x * blockDim.x;
     const int j = threadIdx.y + blockIdx.y * blockDim.y;
     if (i >= a.res_x || j >= a.res_y) return;
@@ -198,29 +217,32 @@ __global__ void __launch_bounds__(64) k_render(RenderArgs a, cudaTextureObject_t
     out[0] = out[1] = out[2] = 0.0f;
 
     // camera (Camera.h:41-60)
-    const float aspect = (float)a.res_x / (float)a.res_y;
+    const float aspect = fdiv((float)a.res_x, (float)a.res_y);
     const float half_w = 0.5f * a.aperture;
-    const float half_h = half_w / aspect;
+    const float half_h = fdiv(half_w, aspect);
     const float3 top_left = a.cam_o - a.focal * a.cam_w - half_w * a.cam_u + half_h * a.cam_v;
     const float3 horiz = 2.0f * half_w * a.cam_u;
     const float3 vert = -2.0f * half_h * a.cam_v;
-    const float3 v = top_left + ((i + 0.5f) / a.res_x) * horiz + ((j + 0.5f) / a.res_y) * vert - a.cam_o;
+    const float3 v = top_left + fdiv(i + 0.5f, (float)a.res_x) * horiz + fdiv(j + 0.5f, (float)a.res_y) * vert - a.cam_o;
     const float3 dir = v * rsqrtf(dot3(v, v));
     Ray pr = make_ray(a.cam_o, dir);
     if (!box_hit(pr, a.dmin, a.dmax)) return;
 
     // shader constants (Shader.h:53-67)
-    const float3 albedo = (a.volume_color * a.scattering) / (a.scattering + f3(a.absorption, a.absorption, a.absorption));
+    const float3 sa = a.scattering + f3(a.absorption, a.absorption, a.absorption);
+    const float3 vs = a.volume_color * a.scattering;
+    const float3 albedo = f3(fdiv(vs.x, sa.x), fdiv(vs.y, sa.y), fdiv(vs.z, sa.z));
     const float3 ext = (a.scattering + f3(a.absorption, a.absorption, a.absorption)) * -1.0f;
     const float3 one = f3(1.0f, 1.0f, 1.0f);
+    const float inv_dx = fdiv(1.0f, a.dx);
 
     float3 lumi = f3(0.0f, 0.0f, 0.0f);
     float3 trans = f3(1.0f, 1.0f, 1.0f);
     int np = 0;
     for (float pt = pr.t0 + a.dx * 0.5f; pt <= pr.t1 && np < a.max_p_steps; pt += a.p_step, ++np) {
         const float3 ppos = pr.o + pt * pr.d;
-        const float3 pg = world_to_grid(a, ppos);
-        if (macro_at(a, macro, pg) < a.skip_p) continue;
+        const float3 pg = world_to_grid(a, inv_dx, ppos);
+        if (macro_at(macro_tex, pg) < a.skip_p) continue;
         const float temp = tex3D<float>(temp_tex, pg.x, pg.y, pg.z);
         const float density = temp * a.density_scale;
         if (density < a.cutoff) continue;
@@ -231,25 +253,25 @@ __global__ void __launch_bounds__(64) k_render(RenderArgs a, cudaTextureObject_t
 
         float3 emission = f3(0.0f, 0.0f, 0.0f);
         if (a.emission_scale > 0.0f)
-            emission = ramp_color(a, temp) * a.emission_scale +
+            emission = ramp_color(a, tb, temp) * a.emission_scale +
                        a.ms_color * scat * a.ms_scale * smooth_step(a.ms_mask0, a.ms_mask1, temp);
         const float3 dT = exp3(ext * density * a.p_step);
 
         for (int l = 0; l < a.n_lights; ++l) {
             // directional light (Light.h:37-54)
-            Ray sr = make_ray(ppos, -1.0f * a.l_dir[l]);
+            Ray sr = make_ray(ppos, -1.0f * tb->l_dir[l]);
             box_hit(sr, a.dmin, a.dmax);
             float3 s_trans = f3(1.0f, 1.0f, 1.0f);
             int ns = 0;
             for (float st = sr.t0 + a.dx * 0.5f; st <= sr.t1 && ns < a.max_s_steps; st += a.s_step, ++ns) {
-                const float3 sg = world_to_grid(a, sr.o + st * sr.d);
-                if (macro_at(a, macro, sg) < a.skip_s) continue;
+                const float3 sg = world_to_grid(a, inv_dx, sr.o + st * sr.d);
+                if (macro_at(macro_tex, sg) < a.skip_s) continue;
                 const float sd = tex3D<float>(temp_tex, sg.x, sg.y, sg.z) * a.density_scale * a.shadow_density_scale;
                 if (sd < a.cutoff) continue;
                 s_trans = s_trans * exp3((ext * sd * a.s_step) * fdiv(1.0f, 1.0f + st * a.gain));
                 if (sqlen(s_trans) < a.cutoff) break;
             }
-            lumi = lumi + albedo * s_trans * trans * illum[l] * (one - dT);
+            lumi = lumi + albedo * s_trans * trans * tb->l_illum[l] * (one - dT);
         }
         lumi = lumi + trans * emission * (one - dT);
         trans = trans * dT;
@@ -328,8 +350,10 @@ struct blz_renderer {
     cudaTextureObject_t t_tex = 0, s_tex = 0;
     float *s_buf[2] = {nullptr, nullptr};
     float *fb = nullptr;
-    float3 *illum = nullptr;
+    Tables *tables = nullptr;
     float *macro = nullptr;
+    cudaArray_t m_arr = nullptr;
+    cudaTextureObject_t m_tex = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     float last_ms = 0.0f;
     long long launches = 0;
@@ -365,21 +389,24 @@ static void render_release(blz_renderer *r) {
     cudaFree(r->s_buf[0]);
     cudaFree(r->s_buf[1]);
     cudaFree(r->fb);
-    cudaFree(r->illum);
+    cudaFree(r->tables);
     cudaFree(r->macro);
+    if (r->m_tex) cudaDestroyTextureObject(r->m_tex);
+    if (r->m_arr) cudaFreeArray(r->m_arr);
     if (r->e0) cudaEventDestroy(r->e0);
     if (r->e1) cudaEventDestroy(r->e1);
     if (r->own_stream && r->st) cudaStreamDestroy(r->st);
 }
 
-static int make_volume(blz_renderer *r, int w, int h, int d, cudaArray_t *arr, cudaTextureObject_t *tex) {
+static int make_volume(blz_renderer *r, int w, int h, int d, cudaArray_t *arr, cudaTextureObject_t *tex,
+                       cudaTextureFilterMode filter = cudaFilterModeLinear) {
     const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<float>();
     RCK(r, cudaMalloc3DArray(arr, &fmt, make_cudaExtent(w, h, d)));
     cudaResourceDesc res{};
     res.resType = cudaResourceTypeArray;
     res.res.array.array = *arr;
     cudaTextureDesc td{};
-    td.filterMode = cudaFilterModeLinear;
+    td.filterMode = filter;
     td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
     td.readMode = cudaReadModeElementType;
     td.normalizedCoords = 0;
@@ -610,11 +637,12 @@ int blz_render_create(const blz_render_params *rp, const blz_params *grid, blz_r
     step(cudaMalloc(&r->s_buf[0], sn * sizeof(float)), "cudaMalloc(scatter)");
     step(cudaMalloc(&r->s_buf[1], sn * sizeof(float)), "cudaMalloc(scatter)");
     step(cudaMalloc(&r->fb, (size_t)3 * rp->width * rp->height * sizeof(float)), "cudaMalloc(frame buffer)");
-    step(cudaMalloc(&r->illum, BLZ_MAX_LIGHTS * sizeof(float3)), "cudaMalloc(lights)");
+    step(cudaMalloc(&r->tables, sizeof(Tables)), "cudaMalloc(tables)");
     step(cudaMalloc(&r->macro, (size_t)a.mW * a.mH * a.mD * sizeof(float)), "cudaMalloc(empty-space cells)");
+    if (rc == BLZ_OK) rc = make_volume(r, a.mW, a.mH, a.mD, &r->m_arr, &r->m_tex, cudaFilterModePoint);
     if (rc == BLZ_OK) {
-        k_light_setup<<<1, 1, 0, r->st>>>(r->a, r->illum);
-        step(cudaGetLastError(), "k_light_setup");
+        k_tables_setup<<<1, 1, 0, r->st>>>(r->a, r->tables);
+        step(cudaGetLastError(), "k_tables_setup");
         r->launches += 1;
     }
     step(cudaEventCreate(&r->e0), "cudaEventCreate");
@@ -678,9 +706,12 @@ int blz_render(blz_renderer *r, const float *temp) {
     }
     const int nm = r->a.mW * r->a.mH * r->a.mD;
     k_macro_max<<<(nm + 127) / 128, 128, 0, r->st>>>(temp, r->W, r->H, r->D, r->a.mW, r->a.mH, r->a.mD, r->macro);
+    RCK(r, cudaGetLastError());
+    rc = copy_to_volume(r, r->macro, r->a.mW, r->a.mH, r->a.mD, r->m_arr);
+    if (rc != BLZ_OK) return rc;
     const dim3 b(8, 8, 1);
     const dim3 g((r->a.res_x + 7) / 8, (r->a.res_y + 7) / 8, 1);
-    k_render<<<g, b, 0, r->st>>>(r->a, r->t_tex, r->s_tex, r->illum, r->macro, r->fb);
+    k_render<<<g, b, 0, r->st>>>(r->a, r->t_tex, r->s_tex, r->m_tex, r->tables, r->fb);
     RCK(r, cudaGetLastError());
     r->launches += 2;
     RCK(r, cudaEventRecord(r->e1, r->st));
