@@ -632,7 +632,24 @@ void launch_plane_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_
 // ---------------------------------------------------------------------------
 constexpr int kResThreads = 256;
 
+// Tiles of the z-marching residual (W % 8 == 0 and W <= 2048): a block of
+// kResThreads threads covers kResThreads / Wq rows of quads and kResKZ planes.
+constexpr int kResKZ = 8;
+
+__host__ __device__ inline bool residual_tiled(const Geom &g) { return (g.W & 7) == 0 && (g.W >> 3) <= kResThreads; }
+__host__ __device__ inline int residual_tile_rows(const Geom &g) { return kResThreads / (g.W >> 3); }
+__host__ __device__ inline int residual_tiles_y(const Geom &g) {
+    const int R = residual_tile_rows(g);
+    return (g.H + R - 1) / R;
+}
+
+__host__ __device__ inline int residual_tiles(const Geom &g) {
+    return residual_tiles_y(g) * ((g.D + kResKZ - 1) / kResKZ);
+}
+
+// Partial sums one residual of g produces: one per tile, else one per block.
 int residual_blocks(const Geom &g) {
+    if (residual_tiled(g)) return residual_tiles(g);
     const long long items = (long long)(g.W >> 1) * g.H * g.D / ((g.W & 7) == 0 ? 4 : 1);
     return (int)std::min<long long>((items + kResThreads - 1) / kResThreads, 148 * 8);
 }
@@ -735,11 +752,81 @@ __device__ __forceinline__ void residual_seg_block(const Geom &g, const SolvePar
     }
 }
 
+__device__ __forceinline__ void block_pair_sum(double r2, double b2, double *__restrict__ out) {
+    __shared__ double s_r[kResThreads / 32], s_b[kResThreads / 32];
+    r2 = warp_sum(r2);
+    b2 = warp_sum(b2);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { s_r[wid] = r2; s_b[wid] = b2; }
+    __syncthreads();
+    if (wid == 0) {
+        r2 = lane < kResThreads / 32 ? s_r[lane] : 0.0;
+        b2 = lane < kResThreads / 32 ? s_b[lane] : 0.0;
+        r2 = warp_sum(r2);
+        b2 = warp_sum(b2);
+        if (lane == 0) { out[0] = r2; out[1] = b2; }
+    }
+    __syncthreads();                                  // s_r / s_b are reused by the block's next tile
+}
+
+// Tile `blk` of the z-marching residual: each thread takes one quad of a row
+// through kResKZ planes, carrying both colours' quads of planes k-1, k, k+1
+// in registers (one new plane of each per step), red cells then black cells
+// per plane; the block's FP64 sums go to partials[2*blk], [2*blk + 1].
+__device__ __forceinline__ void residual_tile_block(const Geom &g, const SolveParams &sp, double scale,
+                                                    const float *__restrict__ rr, const float *__restrict__ rb,
+                                                    const float *__restrict__ pr, const float *__restrict__ pb,
+                                                    int blk, double *__restrict__ partials) {
+    const int Wh = g.W >> 1, Wq = Wh >> 2;
+    const int R = residual_tile_rows(g), ty = residual_tiles_y(g);
+    const int t = threadIdx.x;
+    const int mq = t % Wq, jr = t / Wq;
+    const int j = (blk % ty) * R + jr, k0 = (blk / ty) * kResKZ;
+    double r2 = 0.0, b2 = 0.0;
+    if (jr < R && j < g.H) {
+        const size_t pl = (size_t)Wh * g.H;
+        const size_t row = (size_t)4 * mq + (size_t)Wh * j;
+        const bool has_ym = j > 0, has_yp = j < g.H - 1;
+        const bool first = mq == 0, last = 4 * mq + 4 == Wh;
+        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 rm = k0 > 0 ? ld4(pr + row + (k0 - 1) * pl) : zero4, bm = k0 > 0 ? ld4(pb + row + (k0 - 1) * pl) : zero4;
+        float4 rc = ld4(pr + row + k0 * pl), bc = ld4(pb + row + k0 * pl);
+        const int k1 = k0 + kResKZ < g.D ? k0 + kResKZ : g.D;
+        for (int k = k0; k < k1; ++k) {
+            const size_t q = row + (size_t)k * pl;
+            const bool has_zm = k > 0, has_zp = k < g.D - 1;
+            const float4 rp = has_zp ? ld4(pr + q + pl) : zero4, bp = has_zp ? ld4(pb + q + pl) : zero4;
+            const int sr = (j + k) & 1, sb = sr ^ 1;
+            residual_segment(sp, scale, sr, first, last, ld4(rr + q), rc, bc,
+                             sr == 0 ? (first ? 0.f : __ldg(pb + q - 1)) : (last ? 0.f : __ldg(pb + q + 4)),
+                             has_ym ? ld4(pb + q - Wh) : zero4, has_yp ? ld4(pb + q + Wh) : zero4, bm, bp,
+                             has_ym, has_yp, has_zm, has_zp, r2, b2);
+            residual_segment(sp, scale, sb, first, last, ld4(rb + q), bc, rc,
+                             sb == 0 ? (first ? 0.f : __ldg(pr + q - 1)) : (last ? 0.f : __ldg(pr + q + 4)),
+                             has_ym ? ld4(pr + q - Wh) : zero4, has_yp ? ld4(pr + q + Wh) : zero4, rm, rp,
+                             has_ym, has_yp, has_zm, has_zp, r2, b2);
+            rm = rc; rc = rp; bm = bc; bc = bp;
+        }
+    }
+    block_pair_sum(r2, b2, partials + 2 * (size_t)blk);
+}
+
+// The residual blocks of one grid (residual_blocks(g) of them): tiles when
+// residual_tiled(g), else the grid-stride segments.
+__device__ __forceinline__ void residual_block(const Geom &g, const SolveParams &sp, double scale,
+                                               const float *__restrict__ rr, const float *__restrict__ rb,
+                                               const float *__restrict__ pr, const float *__restrict__ pb, int blk,
+                                               int nblk, double *__restrict__ partials) {
+    if (residual_tiled(g)) residual_tile_block(g, sp, scale, rr, rb, pr, pb, blk, partials);
+    else residual_seg_block(g, sp, scale, rr, rb, pr, pb, blk, nblk, partials);
+}
+
+// One block per tile when residual_tiled(g), else grid-stride segments.
 __global__ void __launch_bounds__(kResThreads)
 k_residual_seg(Geom g, SolveParams sp, double scale, const float *__restrict__ rr,
                const float *__restrict__ rb, const float *__restrict__ pr, const float *__restrict__ pb,
                double *__restrict__ partials) {
-    residual_seg_block(g, sp, scale, rr, rb, pr, pb, blockIdx.x, gridDim.x, partials);
+    residual_block(g, sp, scale, rr, rb, pr, pb, blockIdx.x, gridDim.x, partials);
 }
 
 // One packed pair per item (any even W).
@@ -817,13 +904,15 @@ __global__ void __launch_bounds__(1024) k_reduce_pairs(const double *__restrict_
 int launch_residual(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
                     const float *p_r, const float *p_b, double *partials, int max_partials,
                     double *out2, cudaStream_t st) {
-    const int blocks = std::min(residual_blocks(g), max_partials);
+    // max_partials is residual_blocks(g) (the partials buffer of the solver)
+    const int parts = std::min(residual_blocks(g), max_partials);
     const double scale = (double)sp.scale_d;
-    if ((g.W & 7) == 0)
-        k_residual_seg<<<blocks, kResThreads, 0, st>>>(g, sp, scale, rhs_r, rhs_b, p_r, p_b, partials);
-    else
-        k_residual<<<blocks, kResThreads, 0, st>>>(g, sp, scale, rhs_r, rhs_b, p_r, p_b, partials);
-    k_reduce_pairs<<<1, 1024, 0, st>>>(partials, blocks, out2);
+    if ((g.W & 7) == 0) {
+        k_residual_seg<<<parts, kResThreads, 0, st>>>(g, sp, scale, rhs_r, rhs_b, p_r, p_b, partials);
+    } else {
+        k_residual<<<parts, kResThreads, 0, st>>>(g, sp, scale, rhs_r, rhs_b, p_r, p_b, partials);
+    }
+    k_reduce_pairs<<<1, 1024, 0, st>>>(partials, parts, out2);
     return 2;
 }
 
@@ -1029,8 +1118,8 @@ k_batch_residual(const BatchSim *__restrict__ sims, const int *__restrict__ blk0
     if (!ctl[s].active) return;
     const BatchSim &S = sims[s];
     const int b0 = __ldg(blk0 + s);
-    residual_seg_block(S.g, S.sp, S.sp.scale_d, S.rhs_r, S.rhs_b, S.p_r, S.p_b, blockIdx.x - b0,
-                       __ldg(blk0 + s + 1) - b0, partials + 2 * (size_t)b0);
+    residual_block(S.g, S.sp, S.sp.scale_d, S.rhs_r, S.rhs_b, S.p_r, S.p_b, blockIdx.x - b0,
+                   __ldg(blk0 + s + 1) - b0, partials + 2 * (size_t)b0);
 }
 
 // One block per grid: its residual totals and the single-grid loop's decision.
