@@ -9,6 +9,8 @@
 #include <algorithm>
 #include <type_traits>
 
+#include <cuda.h>   // CUtensorMap and its enums; the encoder comes from cudaGetDriverEntryPoint
+
 #include "kernels.cuh"
 
 namespace blz {
@@ -271,7 +273,9 @@ k_rbgs_seg(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float 
 // ---------------------------------------------------------------------------
 constexpr int kTbThreads = 384;
 constexpr int kTbSlots = 18;
-constexpr int kTbSmemMax = 227 * 1024;
+// Dynamic shared memory of one pass at most: the 227 KB a block may opt into,
+// less room for the static shared memory (the TMA variant's mbarriers).
+constexpr int kTbSmemMax = 227 * 1024 - 1024;
 
 // Rows of output per CTA: as many as the thread budget (one thread per quad
 // of a row pair; TY + 8 rows with the halo, rounded up to a whole pair) and
@@ -285,10 +289,40 @@ __host__ __device__ inline int tb_rows_tile(int Wq, int H) {
 }
 __host__ __device__ inline int tb_rows_alloc(int TY) { return (TY + 8 + 1) & ~1; }
 
-template <bool WARPROW>
+// TMA staging: the rhs and input planes arrive as bulk tensor copies (one
+// box of Wh floats x the CTA's rows x 1 plane per copy) into dense ring
+// slots, completing on one mbarrier per slot.  Rows and planes outside the
+// grid arrive as zeros (the copies' out-of-bounds fill).  Every wait is
+// bounded: a wait that gives up counts in g_tb_timeouts and the pass goes
+// on (its result is then wrong, and the solver reports the timeout).
+constexpr int kTbDenseSlots = 10;                 // 4 red rhs, 4 black rhs, 2 input
+__device__ unsigned int g_tb_timeouts;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void tb_wait(uint32_t bar, uint32_t parity) {
+    for (int it = 0; it < (1 << 24); ++it) {
+        uint32_t done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return;
+    }
+    atomicAdd(&g_tb_timeouts, 1u);
+}
+
+__host__ __device__ inline int tb_dense_slot_bytes(int Wq, int rows_alloc) {
+    return (rows_alloc * Wq * 16 + 127) & ~127;
+}
+
+template <bool WARPROW, bool TMA>
 __global__ void __launch_bounds__(kTbThreads, 1)
 k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float *__restrict__ rhs_b,
-           const float *__restrict__ pin_b, float *__restrict__ pout_r, float *__restrict__ pout_b, int TY, int ZC) {
+           const float *__restrict__ pin_b, float *__restrict__ pout_r, float *__restrict__ pout_b, int TY, int ZC,
+           const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_b,
+           const __grid_constant__ CUtensorMap map_in) {
     // Shared memory, in units of one plane slot (2*blockDim.y rows of
     // Wq + 1 float4; the last float4 of each row is a zero pad), addressed
     // by 32-bit byte offsets:
@@ -298,10 +332,20 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     //   [16, 18) black p input staging, plane k at 16 + (k & 1)
     // rhs and staged input are prefetched one step ahead with cp.async and
     // only ever read back by the thread that loaded them.
-    extern __shared__ float4 sm4[];
-    char *const smc = reinterpret_cast<char *>(sm4);
-    const uint32_t sm_base = static_cast<uint32_t>(__cvta_generic_to_shared(sm4));
+    //
+    // With TMA the rhs and input slots are dense rows of Wq float4 (only
+    // their owner reads them) in a region of kTbDenseSlots 128-byte-aligned
+    // slots ahead of the p slots: red rhs k at (k & 3), black rhs k at
+    // 4 + (k & 3), input k at 8 + (k & 1).
+    extern __shared__ __align__(128) float4 sm4[];
+    __shared__ __align__(8) uint64_t tbar[kTbDenseSlots];
     const int Wh = g.W >> 1, Wq = Wh >> 2, D = g.D;
+    const int rows_alloc = 2 * (int)blockDim.y;
+    const int dslot = TMA ? tb_dense_slot_bytes(Wq, rows_alloc) : 0;
+    char *const raw = reinterpret_cast<char *>(sm4);
+    char *const dbase = TMA ? raw + ((128u - (smem_addr(raw) & 127u)) & 127u) : raw;
+    char *const smc = dbase + (TMA ? kTbDenseSlots * dslot : 0);
+    const uint32_t sm_base = static_cast<uint32_t>(__cvta_generic_to_shared(smc));
     const int rows = TY + 8;
     const int mq = threadIdx.x, rA = 2 * threadIdx.y, rB = rA + 1;
     const int j0 = blockIdx.x * TY, z0 = blockIdx.y * ZC;
@@ -316,6 +360,7 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const int rowb = (Wq + 1) * 16, slotb = 2 * (int)blockDim.y * rowb;
     const int ownA = rA * rowb + mq * 16, ownB = ownA + rowb;
+    const int denA = (rA * Wq + mq) * 16, denB = denA + Wq * 16;       // dense-slot offsets (TMA)
     auto slot = [&](int c, int k) { return (c * 4 + (k & 3)) * slotb; };
     auto lds4 = [&](int off) { return *reinterpret_cast<const float4 *>(smc + off); };
     auto lds1 = [&](int off) { return *reinterpret_cast<const float *>(smc + off); };
@@ -351,7 +396,34 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     const QuadDen qB0 = quad_den(sp, 0, first, last, hymB, hypB, true, true);
     const QuadDen qB1 = quad_den(sp, 1, first, last, hymB, hypB, true, true);
     const int RR = 8 * slotb, RB = 12 * slotb, STG = 16 * slotb;
+    const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
+    const uint32_t dbase_u = smem_addr(dbase);
+    // TMA: one bulk tensor copy of plane k into dense slot ds.
+    auto tma_fill = [&](const CUtensorMap &m, int ds, int k) {
+        const uint32_t bar = smem_addr(&tbar[ds]);
+        const uint32_t bytes = (uint32_t)(rows_alloc * Wh * 4);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                     " [%0], [%1, {%2, %3, %4}], [%5];"
+                     ::"r"(dbase_u + (uint32_t)(ds * dslot)), "l"(reinterpret_cast<uint64_t>(&m)), "r"(0),
+                       "r"(j0 - 4), "r"(k), "r"(bar)
+                     : "memory");
+    };
+    // Fill order: red planes z0-3.. in slots k & 3, black planes z0-2.. in
+    // 4 + (k & 3), input planes z0-2.. in 8 + (k & 1); the n-th fill of a
+    // slot completes its mbarrier's phase n.
+    auto wait_red = [&](int k) { tb_wait(smem_addr(&tbar[k & 3]), ((k - (z0 - 3)) >> 2) & 1); };
+    auto wait_black = [&](int k) { tb_wait(smem_addr(&tbar[4 + (k & 3)]), ((k - (z0 - 2)) >> 2) & 1); };
+    auto wait_in = [&](int k) { tb_wait(smem_addr(&tbar[8 + (k & 1)]), ((k - (z0 - 2)) >> 1) & 1); };
     auto prefetch = [&](int k_red, int k_black, int k_in) {
+        if constexpr (TMA) {
+            if (!leader) return;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (k_red >= z0 - 3 && k_red < z1 + 3) tma_fill(map_r, k_red & 3, k_red);
+            if (k_black >= z0 - 2 && k_black < z1 + 2) tma_fill(map_b, 4 + (k_black & 3), k_black);
+            if (k_in >= z0 - 2 && k_in < z1 + 4) tma_fill(map_in, 8 + (k_in & 1), k_in);
+            return;
+        }
         // red rhs: levels 0 and 2 cover planes [z0-3, z1+3); black rhs: levels 1 and 3 cover [z0-2, z1+2)
         if (kin(k_red) && k_red >= z0 - 3 && k_red < z1 + 3) {
             const int o = RR + (k_red & 3) * slotb;
@@ -370,6 +442,20 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
+    // rhs of colour c, plane k, for the row whose element offsets are
+    // (own, den): from its padded slot (cp.async) or its dense slot (TMA).
+    auto rhs_ld = [&](int c, int k, int own, int den) -> float4 {
+        if constexpr (TMA) return lds4((int)(dbase - smc) + ((c ? 4 : 0) + (k & 3)) * dslot + den);
+        return lds4((c ? RB : RR) + (k & 3) * slotb + own);
+    };
+    if constexpr (TMA) {
+        if (leader) {
+            for (int i = 0; i < kTbDenseSlots; ++i)
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&tbar[i])) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+    }
     // register windows of each row: black planes t-3..t+1, red planes t-4..t
     float4 bm3A = zero4, bm2A = zero4, bp1A, rm4A = zero4, rm3A = zero4, rm2A = zero4, rm1A = zero4, r0A = zero4;
     float4 bm3B = zero4, bm2B = zero4, bp1B, rm4B = zero4, rm3B = zero4, rm2B = zero4, rm1B = zero4, r0B = zero4;
@@ -385,8 +471,8 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     // One quad update of row parity S: colour c on plane k, `own` the row's
     // element offset, o the other colour's own quad, ym/yp/zm/zp its
     // neighbours.
-    auto update = [&](auto s_c, int c, int k, int own, float4 o, float4 ym, float4 yp, float4 zm, float4 zp,
-                      const QuadDen &qi, bool hym, bool hyp) -> float4 {
+    auto update = [&](auto s_c, int c, int k, int own, int den, float4 o, float4 ym, float4 yp, float4 zm,
+                      float4 zp, const QuadDen &qi, bool hym, bool hyp) -> float4 {
         constexpr int S = decltype(s_c)::value;
         float xe;
         if constexpr (WARPROW) {
@@ -396,7 +482,7 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
             const int b = slot(c ^ 1, k) + own;
             xe = S == 0 ? lds1(b - 4) : lds1(b + 16);
         }
-        const float4 rv = lds4((c ? RB : RR) + (k & 3) * slotb + own);
+        const float4 rv = rhs_ld(c, k, own, den);
         if (k > 0 && k < D - 1) return gs_quad(sp.scale, S, rv, o, xe, ym, yp, zm, zp, qi);
         return gs_quad(sp.scale, S, rv, o, xe, ym, yp, zm, zp, quad_den(sp, S, first, last, hym, hyp, k > 0, k < D - 1));
     };
@@ -412,11 +498,11 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
         if (kact(0, t)) {
             const int b = slot(1, t);
             if (mA & 1u) {
-                r0A = update(sA, 0, t, ownA, b0A, lds4(b + ownA - rowb), b0B, bm1A, bp1A, qa, hymA, hypA);
+                r0A = update(sA, 0, t, ownA, denA, b0A, lds4(b + ownA - rowb), b0B, bm1A, bp1A, qa, hymA, hypA);
                 sts4(slot(0, t) + ownA, r0A);
             }
             if (mB & 1u) {
-                r0B = update(sB, 0, t, ownB, b0B, b0A, lds4(b + ownB + rowb), bm1B, bp1B, qb, hymB, hypB);
+                r0B = update(sB, 0, t, ownB, denB, b0B, b0A, lds4(b + ownB + rowb), bm1B, bp1B, qb, hymB, hypB);
                 sts4(slot(0, t) + ownB, r0B);
             }
         }
@@ -424,22 +510,22 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
         if (kact(1, t - 1)) {
             const int b = slot(0, t - 1), w = slot(1, t - 1);
             if (mA & 2u) {
-                bm1A = update(sA, 1, t - 1, ownA, rm1A, lds4(b + ownA - rowb), rm1B, rm2A, r0A, qa, hymA, hypA);
+                bm1A = update(sA, 1, t - 1, ownA, denA, rm1A, lds4(b + ownA - rowb), rm1B, rm2A, r0A, qa, hymA, hypA);
                 sts4(w + ownA, bm1A);
             }
             if (mB & 2u) {
-                bm1B = update(sB, 1, t - 1, ownB, rm1B, rm1A, lds4(b + ownB + rowb), rm2B, r0B, qb, hymB, hypB);
+                bm1B = update(sB, 1, t - 1, ownB, denB, rm1B, rm1A, lds4(b + ownB + rowb), rm2B, r0B, qb, hymB, hypB);
                 sts4(w + ownB, bm1B);
             }
         }
         if (kact(2, t - 2)) {
             const int b = slot(1, t - 2), w = slot(0, t - 2);
             if (mA & 4u) {
-                rm2A = update(sA, 0, t - 2, ownA, bm2A, lds4(b + ownA - rowb), bm2B, bm3A, bm1A, qa, hymA, hypA);
+                rm2A = update(sA, 0, t - 2, ownA, denA, bm2A, lds4(b + ownA - rowb), bm2B, bm3A, bm1A, qa, hymA, hypA);
                 sts4(w + ownA, rm2A);
             }
             if (mB & 4u) {
-                rm2B = update(sB, 0, t - 2, ownB, bm2B, bm2A, lds4(b + ownB + rowb), bm3B, bm1B, qb, hymB, hypB);
+                rm2B = update(sB, 0, t - 2, ownB, denB, bm2B, bm2A, lds4(b + ownB + rowb), bm3B, bm1B, qb, hymB, hypB);
                 sts4(w + ownB, rm2B);
             }
         }
@@ -448,14 +534,14 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
             const int b = slot(0, k3);
             const bool outp = k3 >= z0;
             if (mA & 8u) {
-                bm3A = update(sA, 1, k3, ownA, rm3A, lds4(b + ownA - rowb), rm3B, rm4A, rm2A, qa, hymA, hypA);
+                bm3A = update(sA, 1, k3, ownA, denA, rm3A, lds4(b + ownA - rowb), rm3B, rm4A, rm2A, qa, hymA, hypA);
                 if (outp) {
                     *reinterpret_cast<float4 *>(pout_r + offA + k3 * pl) = rm3A;
                     *reinterpret_cast<float4 *>(pout_b + offA + k3 * pl) = bm3A;
                 }
             }
             if (mB & 8u) {
-                bm3B = update(sB, 1, k3, ownB, rm3B, rm3A, lds4(b + ownB + rowb), rm4B, rm2B, qb, hymB, hypB);
+                bm3B = update(sB, 1, k3, ownB, denB, rm3B, rm3A, lds4(b + ownB + rowb), rm4B, rm2B, qb, hymB, hypB);
                 if (outp) {
                     *reinterpret_cast<float4 *>(pout_r + offB + k3 * pl) = rm3B;
                     *reinterpret_cast<float4 *>(pout_b + offB + k3 * pl) = bm3B;
@@ -464,12 +550,26 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
         }
     };
     for (int t = z0 - 3; t < z1 + 3; ++t) {
-        prefetch(t + 1, t, t + 2);                    // what the next step reads
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
-        const int st = STG + ((t + 1) & 1) * slotb;
-        bp1A = okA && kin(t + 1) ? lds4(st + ownA) : zero4;
-        bp1B = okB && kin(t + 1) ? lds4(st + ownB) : zero4;
-        __syncthreads();
+        if constexpr (TMA) {
+            // this step's copies were issued in the previous one; slots are
+            // overwritten only after the barrier (their last readers were in
+            // the previous step)
+            wait_red(t);
+            if (t - 1 >= z0 - 2) wait_black(t - 1);
+            wait_in(t + 1);
+            const int st = (int)(dbase - smc) + (8 + ((t + 1) & 1)) * dslot;
+            bp1A = okA && kin(t + 1) ? lds4(st + denA) : zero4;
+            bp1B = okB && kin(t + 1) ? lds4(st + denB) : zero4;
+            __syncthreads();
+            prefetch(t + 1, t, t + 2);
+        } else {
+            prefetch(t + 1, t, t + 2);                // what the next step reads
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            const int st = STG + ((t + 1) & 1) * slotb;
+            bp1A = okA && kin(t + 1) ? lds4(st + ownA) : zero4;
+            bp1B = okB && kin(t + 1) ? lds4(st + ownB) : zero4;
+            __syncthreads();
+        }
         sts4(slot(1, t + 1) + ownA, bp1A);
         sts4(slot(1, t + 1) + ownB, bp1B);
         if ((jA + t) & 1) levels(t, std::integral_constant<int, 1>{});
@@ -479,7 +579,7 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
         rm4B = rm3B; rm3B = rm2B; rm2B = rm1B; rm1B = r0B;
         bm3B = bm2B; bm2B = bm1B; bm1B = b0B; b0B = bp1B;
     }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    if constexpr (!TMA) asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 static bool tb_supported(const Geom &g) {
@@ -490,6 +590,56 @@ static bool tb_supported(const Geom &g) {
 
 static size_t tb_smem(const Geom &g, int TY) {
     return sizeof(float4) * kTbSlots * (size_t)tb_rows_alloc(TY) * ((g.W >> 3) + 1);
+}
+
+// TMA layout: alignment slack, the dense slots, the 8 padded p slots (never
+// more than tb_smem for the 9 or more rows a tile has).
+static size_t tb_smem_tma(const Geom &g, int TY) {
+    const int Wq = g.W >> 3, ra = tb_rows_alloc(TY);
+    return 128 + (size_t)kTbDenseSlots * tb_dense_slot_bytes(Wq, ra) + sizeof(float4) * 8 * (size_t)ra * (Wq + 1);
+}
+
+typedef CUresult (*TensorMapEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                      const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static TensorMapEncodeFn tensor_map_encoder() {
+    static TensorMapEncodeFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<TensorMapEncodeFn>(p);
+    }
+    return fn;
+}
+
+// Tensor map of one colour-packed plane stack (Wh x H x D floats) with a box
+// of Wh x rows x 1: whole rows from x = 0, so every copy starts 16-byte
+// aligned; out-of-range rows and planes read as zeros.
+static bool tb_tensor_map(CUtensorMap *m, const float *base, const Geom &g, int rows) {
+    TensorMapEncodeFn enc = tensor_map_encoder();
+    if (!enc) return false;
+    const int Wh = g.W >> 1;
+    const cuuint64_t dims[3] = {(cuuint64_t)Wh, (cuuint64_t)g.H, (cuuint64_t)g.D};
+    const cuuint64_t strides[2] = {(cuuint64_t)Wh * 4, (cuuint64_t)Wh * g.H * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)Wh, (cuuint32_t)rows, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || Wh > 256 || rows > 256) return false;
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Timeouts counted by the TMA waits since the last call (then reset).
+unsigned int tb_take_timeouts() {
+    unsigned int n = 0, zero = 0;
+    if (cudaMemcpyFromSymbol(&n, g_tb_timeouts, sizeof n) != cudaSuccess) return 0;
+    if (n) cudaMemcpyToSymbol(g_tb_timeouts, &zero, sizeof zero);
+    return n;
 }
 
 static int device_sm_count() {
@@ -510,32 +660,49 @@ static int device_sm_count() {
 // (one CTA per SM: its shared memory is most of the SM's), at least 8
 // planes.
 static void launch_tb_pass(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
-                           const float *pin_b, float *pout_r, float *pout_b, int ZC, cudaStream_t st) {
+                           const float *pin_b, float *pout_r, float *pout_b, int ZC, bool tma, cudaStream_t st) {
     const int Wq = g.W >> 3, TY = tb_rows_tile(Wq, g.H);
-    const size_t smem = tb_smem(g, TY);
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_rbgs_tb2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
-        cudaFuncSetAttribute(k_rbgs_tb2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_rbgs_tb2<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_rbgs_tb2<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_rbgs_tb2<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_rbgs_tb2<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
         attr_set = true;
     }
+    CUtensorMap mr{}, mb{}, mi{};
+    const int ra = tb_rows_alloc(TY);
+    if (tma) tma = tb_tensor_map(&mr, rhs_r, g, ra) && tb_tensor_map(&mb, rhs_b, g, ra) && tb_tensor_map(&mi, pin_b, g, ra);
+    const size_t smem = tma ? tb_smem_tma(g, TY) : tb_smem(g, TY);
     if (ZC <= 0) {
         const int bands = (g.H + TY - 1) / TY;
         const int chunks = std::max(1, device_sm_count() / bands);
         ZC = std::max(8, (g.D + chunks - 1) / chunks);
     }
-    const dim3 b(Wq, tb_rows_alloc(TY) / 2, 1);
+    const dim3 b(Wq, ra / 2, 1);
     const dim3 gr((g.H + TY - 1) / TY, (g.D + ZC - 1) / ZC, 1);
-    if (Wq == 32) k_rbgs_tb2<true><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC);
-    else k_rbgs_tb2<false><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC);
+    if (tma) {
+        if (Wq == 32)
+            k_rbgs_tb2<true, true><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC, mr, mb, mi);
+        else
+            k_rbgs_tb2<false, true><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC, mr, mb, mi);
+    } else {
+        if (Wq == 32)
+            k_rbgs_tb2<true, false><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC, mr, mb, mi);
+        else
+            k_rbgs_tb2<false, false><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC, mr, mb,
+                                                         mi);
+    }
 }
 
 // (planes per thread, rows per block) of each segment-kernel variant; the
 // variants after them are the temporal-blocking pass with ZC planes per CTA
-// (0: sized to fill the SMs).
+// (0: sized to fill the SMs), the last with its rhs and input planes staged
+// by TMA.
 static const int kVariantKZ[kSegVariants] = {1, 2, 4, 8, 2, 4};
 static const int kVariantBY[kSegVariants] = {8, 8, 4, 4, 4, 8};
-static const int kVariantZC[kSweepVariants - kSegVariants] = {16, 32, 0};
+static const int kVariantZC[kSweepVariants - kSegVariants] = {16, 32, 0, 0};
+static const bool kVariantTMA[kSweepVariants - kSegVariants] = {false, false, false, true};
 
 int sweep_variant_count(const Geom &g) {
     if ((g.W & 7) != 0) return 0;
@@ -550,9 +717,10 @@ void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r
         // result lands in p; the remaining sweeps run unblocked.
         const int passes = (sweeps / 4) * 2;
         const int zc = kVariantZC[variant - kSegVariants];
+        const bool tma = kVariantTMA[variant - kSegVariants];
         for (int i = 0; i < passes; ++i) {
-            if ((i & 1) == 0) launch_tb_pass(g, sp, rhs_r, rhs_b, p_b, q_r, q_b, zc, st);
-            else launch_tb_pass(g, sp, rhs_r, rhs_b, q_b, p_r, p_b, zc, st);
+            if ((i & 1) == 0) launch_tb_pass(g, sp, rhs_r, rhs_b, p_b, q_r, q_b, zc, tma, st);
+            else launch_tb_pass(g, sp, rhs_r, rhs_b, q_b, p_r, p_b, zc, tma, st);
         }
         *launches += passes;
         sweeps -= 2 * passes;

@@ -63,8 +63,11 @@ void launch_divergence(const Geom &g, const float *U, const float *V, const floa
 // sweeps per pass; all give identical results.  Other W use the one-cell
 // kernel.  sweep_variant_count: variants available for this grid (0: W % 8).
 constexpr int kSegVariants = 6;
-constexpr int kSweepVariants = 9;
+constexpr int kSweepVariants = 10;
 int  sweep_variant_count(const Geom &g);
+// Bounded TMA waits of the temporal-blocking pass that gave up since the last
+// call (then reset); nonzero means a pass produced a wrong result.
+unsigned int tb_take_timeouts();
 void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                         const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
                         long long *launches, int variant = 0, float *q_r = nullptr, float *q_b = nullptr);

@@ -601,6 +601,15 @@ static int solve_device_loop(blz_solver *s, blz_step_stats *st) {
 
 static int solve_body(blz_solver *s, blz_step_stats *st);
 
+// The TMA-staged pass counts bounded waits that gave up; after work that may
+// have used it, a nonzero count is reported (that pass's result is wrong).
+static int check_tb_timeouts(blz_solver *s) {
+    if (s->variant != kSweepVariants - 1) return BLZ_OK;
+    CK(s, cudaStreamSynchronize(s->st));
+    if (tb_take_timeouts()) return fail(s, BLZ_ERR_TIMEOUT, "temporal-blocking pass: a bounded TMA wait gave up");
+    return BLZ_OK;
+}
+
 int blz_solve(blz_solver *s, blz_step_stats *st) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     const blz_params &P = s->P;
@@ -632,6 +641,7 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
     }
     int rc = solve_body(s, st);
     if (rc != BLZ_OK) return rc;
+    if ((rc = check_tb_timeouts(s)) != BLZ_OK) return rc;
     if (s->warm) {
         if ((rc = unet_timeout_flag(s->warm, s->st)) != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
         if (st) {
@@ -722,7 +732,8 @@ static int solve_body(blz_solver *s, blz_step_stats *st) {
 int blz_sweeps(blz_solver *s, int n) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     if (n < 0) return fail(s, BLZ_ERR_ARG, "negative sweep count %d", n);
-    return n > 0 ? sweeps(s, n) : BLZ_OK;
+    const int rc = n > 0 ? sweeps(s, n) : BLZ_OK;
+    return rc != BLZ_OK ? rc : check_tb_timeouts(s);
 }
 
 int blz_gradient(blz_solver *s) {

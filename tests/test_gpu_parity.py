@@ -274,7 +274,7 @@ def test_device_loop_hits_the_cap():
 def test_sweep_variants_are_bitwise_identical():
     """Every launch shape of the segment sweep kernel gives the same bits."""
     ref = None
-    for v in range(9):
+    for v in range(10):
         gpu, _ = pair(scene(dims=(64, 20, 18), bc_mode=BLZ_BC_FREE_SURFACE, sweep_variant=v), 65)
         gpu.sweeps(7)
         p = gpu.get("P")
@@ -295,7 +295,7 @@ def test_fixed_sweeps_match_oracle():
 def test_sweep_variants_identical_full_width_rows():
     """W = 256: a warp spans a whole packed row (32 segments of 4)."""
     ref = None
-    for v in range(9):
+    for v in range(10):
         gpu, _ = pair(scene(dims=(256, 6, 8), bc_mode=BLZ_BC_FREE_SURFACE, sweep_variant=v), 67)
         gpu.sweeps(5)
         p = gpu.get("P")
@@ -310,14 +310,15 @@ def test_sweep_variants_identical_full_width_rows():
 @pytest.mark.parametrize("dims,bc", [((64, 200, 70), BLZ_BC_FREE_SURFACE), ((256, 40, 40), BLZ_BC_FREE_SURFACE),
                                      ((384, 20, 12), BLZ_BC_REF_COMPAT), ((128, 48, 33), BLZ_BC_FREE_SURFACE)])
 def test_temporal_blocking_equals_plain_sweeps(dims, bc):
-    """The two-sweeps-per-pass kernels (variants 6, 7, 8: several row bands and
-    z chunks here) give the plain segment kernel's bits."""
+    """The two-sweeps-per-pass kernels (variants 6-9, 9 with TMA-staged rhs and
+    input planes: several row bands and z chunks here) give the plain segment
+    kernel's bits."""
     out = {}
-    for v in (0, 6, 7, 8):
+    for v in (0, 6, 7, 8, 9):
         gpu, _ = pair(scene(dims=dims, bc_mode=bc, sweep_variant=v), 68)
         gpu.sweeps(10)
         out[v] = gpu.get("P")
         gpu.close()
     assert np.isfinite(out[0]).all() and np.abs(out[0]).max() > 0
-    for v in (6, 7, 8):
+    for v in (6, 7, 8, 9):
         np.testing.assert_array_equal(out[v], out[0], err_msg=f"variant {v}")
