@@ -37,7 +37,8 @@ GRID = 256
 SEED = 3
 TOL = 1e-4
 MAX_ITER = 40000
-CHECK_EVERY = 20
+CHECK_EVERY = 20          # residual-check interval of the batched simulations
+CHECK_AUTO = -1           # the 256^3 step: interval chosen per frame (blz_params.check_every < 0)
 # Sweeps per frame the reference arm runs (maxIterSolve): the mean the plain
 # RBGS step needs on this scene and frame window (frames 5-14 of seed 3 at
 # 256^3: 26074 sweeps), measured on a B200.
@@ -159,7 +160,8 @@ def run_ours(args, ws, rank, local):
     from blaze_b200 import FluidSolver, Timer, family_scene
 
     torch.cuda.set_device(local)
-    scn, parts = family_scene(n=args.grid, seed=SEED + rank, tol=TOL, max_iter=args.max_iter, check_every=CHECK_EVERY)
+    check = CHECK_AUTO if args.max_iter % 320 == 0 else CHECK_EVERY
+    scn, parts = family_scene(n=args.grid, seed=SEED + rank, tol=TOL, max_iter=args.max_iter, check_every=check)
     if args.host_loop:
         scn.device_loop = 0
     W, H, D = scn.gridRes
@@ -322,7 +324,10 @@ def run_ours(args, ws, rank, local):
                                f"wind {scn.extra['wind_cells_per_step']:.2f} cells/step), "
                                f"{'learned warm start + ' if head_learned else 'plain '}RBGS with free-surface "
                                f"top to FP64 relative residual {TOL:g} per frame",
-                   "grid": [W, H, D], "particles": int(len(parts)), "tol": TOL, "check_every": CHECK_EVERY,
+                   "grid": [W, H, D], "particles": int(len(parts)), "tol": TOL,
+                   "check_every": "auto: per frame from 20..320, minimising checks plus sweeps past convergence"
+                   if check < 0 else check,
+                   "check_intervals": [int(x["check_interval"]) for x in (st_learn if head_learned else st_plain)],
                    "max_iter": args.max_iter, "mean_sweeps": head["mean_sweeps"],
                    "sweeps_per_frame": head["sweeps_per_frame"], "max_rel_residual": head["max_rel_residual"],
                    "all_converged": head["all_converged"],

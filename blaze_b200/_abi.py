@@ -77,7 +77,7 @@ class BlzStepStats(C.Structure):
         ("ms_solve", C.c_float), ("ms_gradient", C.c_float), ("ms_advect", C.c_float),
         ("ms_total", C.c_float), ("ms_sweeps", C.c_float), ("residual_checks", C.c_int),
         ("sweep_variant", C.c_int), ("device_loop", C.c_int), ("ms_checks", C.c_float),
-        ("ms_warm_start", C.c_float), ("warm_started", C.c_int),
+        ("ms_warm_start", C.c_float), ("warm_started", C.c_int), ("check_interval", C.c_int),
     ]
 
     def as_dict(self):

@@ -44,10 +44,19 @@ struct blz_solver {
     long long launches = 0;
     blz_unet *warm = nullptr;                   // learned warm start (caller owned)
     int variant = -2;                           // sweep launch shape (-2: not chosen yet)
-    // device-loop solve: instantiated graph and its control block
-    cudaGraphExec_t solve_exec = nullptr;
+    // device-loop solve: instantiated graphs (one per check interval used)
+    // and their control block
+    struct SolveGraph {
+        int chunk = 0;
+        cudaGraphExec_t exec = nullptr;
+        int body = 0, prologue = 0;
+    };
+    SolveGraph graphs[8];
     SolveCtl *ctl = nullptr, *h_ctl = nullptr;
-    int graph_body = 0, graph_prologue = 0;
+    // automatic check interval (check_every < 0): the last solve's sweeps and
+    // its measured cost of one residual check in sweeps
+    int last_iters = 0;
+    double check_ratio = 0.0;
     std::string err;
 };
 
@@ -154,7 +163,8 @@ static void release(blz_solver *s) {
     cudaFree(s->parts); cudaFree(s->boxes); cudaFree(s->bin_start); cudaFree(s->bin_list); cudaFree(s->active);
     cudaFree(s->partials); cudaFree(s->d_norm2);
     if (s->h_norm2) cudaFreeHost(s->h_norm2);
-    if (s->solve_exec) cudaGraphExecDestroy(s->solve_exec);
+    for (auto &gr : s->graphs)
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
     cudaFree(s->ctl);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
@@ -172,8 +182,8 @@ int blz_create(const blz_params *p, blz_solver **out) {
         return fail(nullptr, BLZ_ERR_ARG, "grid too large for 32-bit packed indexing");
     if (!(p->dx > 0.0f) || !(p->dt > 0.0f) || !(p->density > 0.0f))
         return fail(nullptr, BLZ_ERR_ARG, "dx, dt and density must be positive");
-    if (p->max_iter < 0 || p->check_every < 0 || p->max_particles < 0)
-        return fail(nullptr, BLZ_ERR_ARG, "negative max_iter, check_every or max_particles");
+    if (p->max_iter < 0 || p->max_particles < 0)
+        return fail(nullptr, BLZ_ERR_ARG, "negative max_iter or max_particles");
     if (p->bc_mode != BLZ_BC_REF_COMPAT && p->bc_mode != BLZ_BC_FREE_SURFACE)
         return fail(nullptr, BLZ_ERR_ARG, "bad bc_mode %d", p->bc_mode);
     if (p->gs_order != BLZ_GS_RB3D && p->gs_order != BLZ_GS_PLANE)
@@ -566,22 +576,55 @@ static int sweeps(blz_solver *s, int n) {
 }
 
 // The residual-controlled solve as one graph launch (graph_solve.cu).
-static int solve_device_loop(blz_solver *s, blz_step_stats *st) {
+// Residual checks are a stopping test: every `chunk` sweeps the FP64
+// residual decides whether the solve goes on.  With check_every < 0 the
+// interval is chosen per solve from 20, 40, ..., 320 (those dividing
+// max_iter) to minimise the expected cost of the checks plus the sweeps
+// past convergence, (N / c) * r + c / 2 in sweeps, with N the previous
+// solve's sweep count and r the measured cost of one check in sweeps (1.5
+// before any measurement).  The stopping rule itself is unchanged.
+static int check_chunk(const blz_solver *s) {
+    const blz_params &P = s->P;
+    if (P.check_every >= 1) return P.check_every;
+    if (P.check_every == 0) return 1;
+    constexpr int kBase = 20;
+    if (s->last_iters <= 0) return kBase;
+    const double r = s->check_ratio > 0.0 ? s->check_ratio : 1.5;
+    int best = kBase;
+    double best_cost = 1e300;
+    for (int c = kBase; c <= 16 * kBase; c *= 2) {
+        if (P.max_iter % c != 0) continue;
+        const double cost = s->last_iters / (double)c * r + 0.5 * c;
+        if (cost < best_cost) { best_cost = cost; best = c; }
+    }
+    return best;
+}
+
+static int solve_device_loop(blz_solver *s, blz_step_stats *st, int chunk) {
     const blz_params &P = s->P;
     int rc = choose_variant(s);
     if (rc != BLZ_OK) return rc;
-    if (!s->solve_exec) {
+    blz_solver::SolveGraph *gr = nullptr;
+    for (auto &x : s->graphs)
+        if (x.exec && x.chunk == chunk) gr = &x;
+    if (!gr) {
+        for (auto &x : s->graphs)
+            if (!x.exec) { gr = &x; break; }
+        if (!gr) return fail(s, BLZ_ERR_STATE, "too many check intervals");
         cudaError_t e = build_solve_graph(s->g, solve_params(P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->partials,
-                                          s->n_partials, s->d_norm2, s->ctl, std::max(1, P.check_every), P.max_iter,
-                                          P.tol, s->variant, s->st, &s->solve_exec, &s->graph_body,
-                                          &s->graph_prologue, q_r(s), q_b(s));
+                                          s->n_partials, s->d_norm2, s->ctl, chunk, P.max_iter, P.tol, s->variant,
+                                          s->st, &gr->exec, &gr->body, &gr->prologue, q_r(s), q_b(s));
         if (e != cudaSuccess) return fail(s, BLZ_ERR_CUDA, "building the solve graph failed: %s", cudaGetErrorString(e));
+        gr->chunk = chunk;
     }
-    CK(s, cudaGraphLaunch(s->solve_exec, s->st));
+    CK(s, cudaGraphLaunch(gr->exec, s->st));
     CK(s, cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s->st));
     CK(s, cudaStreamSynchronize(s->st));
     const SolveCtl &c = *s->h_ctl;
-    s->launches += s->graph_prologue + (long long)(c.checks - 1) * s->graph_body;
+    s->launches += gr->prologue + (long long)(c.checks - 1) * gr->body;
+    s->last_iters = c.iters;
+    if (c.iters > 0 && c.checks > 0 && c.sweep_ns > 0)
+        s->check_ratio = ((double)c.check_ns / c.checks) / ((double)c.sweep_ns / c.iters);
     if (st) {
         const double r = std::sqrt(c.r2), b = std::sqrt(c.b2);
         st->iterations = c.iters;
@@ -594,6 +637,7 @@ static int solve_device_loop(blz_solver *s, blz_step_stats *st) {
         st->residual_checks = c.checks;
         st->sweep_variant = s->variant;
         st->device_loop = 1;
+        st->check_interval = chunk;
         if (!std::isfinite(r)) return fail(s, BLZ_ERR_NAN, "non-finite residual after %d sweeps", c.iters);
     }
     return BLZ_OK;
@@ -671,9 +715,9 @@ int blz_set_warm_start(blz_solver *s, blz_unet *u) {
 
 static int solve_body(blz_solver *s, blz_step_stats *st) {
     const blz_params &P = s->P;
-    const int chunk_sz = std::max(1, P.check_every);
-    if (P.device_loop && P.tol > 0.0 && P.gs_order == BLZ_GS_RB3D && P.max_iter % chunk_sz == 0)
-        return solve_device_loop(s, st);
+    const int chunk = check_chunk(s);
+    if (P.device_loop && P.tol > 0.0 && P.gs_order == BLZ_GS_RB3D && P.max_iter % chunk == 0)
+        return solve_device_loop(s, st, chunk);
     int done = 0, rc, checks = 0;
     double r = 0.0, b = 0.0;
     bool have = false;
@@ -695,7 +739,6 @@ static int solve_body(blz_solver *s, blz_step_stats *st) {
         if ((rc = timed_sweeps(P.max_iter)) != BLZ_OK) return rc;
         done = P.max_iter;
     } else {
-        const int chunk = std::max(1, P.check_every);
         if ((rc = residual_sync(s, &r, &b)) != BLZ_OK) return rc;
         ++checks;
         while (done < P.max_iter && !(b == 0.0 || r / b <= P.tol)) {
@@ -708,6 +751,7 @@ static int solve_body(blz_solver *s, blz_step_stats *st) {
         }
         have = true;
     }
+    s->last_iters = done;
     if (st) {
         if (!have) {
             if ((rc = residual_sync(s, &r, &b)) != BLZ_OK) return rc;
@@ -723,6 +767,7 @@ static int solve_body(blz_solver *s, blz_step_stats *st) {
         st->residual_checks = checks;
         st->sweep_variant = s->variant;
         st->device_loop = 0;
+        st->check_interval = chunk;
         st->ms_checks = 0.0f;
         if (!std::isfinite(r)) return fail(s, BLZ_ERR_NAN, "non-finite residual after %d sweeps", done);
     }

@@ -103,7 +103,11 @@ typedef struct blz_params {
     int    max_iter;              /* maxIterSolve: sweep cap                 */
     double tol;                   /* relative FP64 residual target; <= 0 runs
                                      exactly max_iter sweeps (reference)     */
-    int    check_every;           /* sweeps between residual checks (>= 1)   */
+    int    check_every;           /* sweeps between residual checks (>= 1;
+                                     0 counts as 1; < 0: chosen per solve
+                                     from 20, 40, ..., 320 to minimise checks
+                                     plus sweeps past convergence, given the
+                                     previous solve's sweep count)          */
     int    bc_mode;               /* BLZ_BC_*                                */
     int    gs_order;              /* BLZ_GS_*                                */
     int    reset_pressure;        /* 1: p = 0 before every solve (the
@@ -147,6 +151,7 @@ typedef struct blz_step_stats {
     float  ms_warm_start;         /* device time of the learned warm start
                                      (inside ms_solve; 0 without a network)  */
     int    warm_started;          /* 1 if a network set the initial pressure  */
+    int    check_interval;        /* sweeps between residual checks used      */
 } blz_step_stats;
 
 typedef struct blz_solver blz_solver;
