@@ -21,6 +21,8 @@ BLZ_GS_PLANE = 1
 BLZ_ADVECT_RK3 = 0
 BLZ_ADVECT_EULER = 1
 BLZ_ADVECT_RK2 = 2
+BLZ_WARM_STEP_RESIDUAL = 0
+BLZ_WARM_STEP_ENERGY = 1
 
 FIELD_T, FIELD_U, FIELD_V, FIELD_W, FIELD_P, FIELD_RHS = range(6)
 FIELD_NAMES = {"T": FIELD_T, "U": FIELD_U, "V": FIELD_V, "W": FIELD_W, "P": FIELD_P, "RHS": FIELD_RHS}
@@ -148,6 +150,7 @@ EXPORTS = {
     "blz_unet_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "blz_unet_last_alpha": (C.c_float, [C.c_void_p]),
     "blz_unet_set_smoothing": (C.c_int, [C.c_void_p, C.c_int]),
+    "blz_unet_set_step": (C.c_int, [C.c_void_p, C.c_int]),
     "blz_unet_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "blz_unet_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "blz_unet_get_grads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),

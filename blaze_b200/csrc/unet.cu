@@ -14,12 +14,15 @@
 // Output: delta = head(features) and the correction d = kappa*rms(r)*delta.
 // The solver then sweeps p and d alike k times (d with a zero right-hand
 // side; Gauss-Seidel is affine, so S^k(p + alpha d) = S^k(p) + alpha M^k d
-// for every alpha) and adds alpha M^k d with alpha minimising the residual
-// norm ||b - A (S^k(p) + alpha M^k d)||: the combination chosen on what the
-// stopping rule measures, after the smoother has removed the error it removes
-// anyway; a useless d gets alpha ~ 0.  rms() and the inner products run over
-// the whole grid in FP64; kappa is a constant of the trained weights (the
-// training set's mean rms(p* - p_prev) / rms(r)).
+// for every alpha; default k = 40) and adds alpha M^k d.  By default alpha
+// minimises the residual norm ||b - A (S^k(p) + alpha M^k d)||: the
+// combination chosen on what the stopping rule measures, after the smoother
+// has removed the error it removes anyway.  The other choice
+// (blz_unet_set_step) minimises the error's energy norm, alpha =
+// <d, r> / <d, A d>, which weighs the smooth error Gauss-Seidel removes
+// slowest as the sweep count does.  A useless d gets alpha ~ 0.  rms() and
+// the inner products run over the whole grid in FP64; kappa is a constant of
+// the trained weights (the training set's mean rms(p* - p_prev) / rms(r)).
 //
 // The 3x3x3 convolutions (forward and data gradient) run on the tcgen05 tensor
 // cores (unet_conv.cu).  Pooling, the transposed convolutions, weight gradients,
@@ -503,12 +506,13 @@ __global__ void k_unet_delta(const bf16 *__restrict__ d0b, LDims d, const float 
     (((i + j + k) & 1) ? db : dr)[pidx(i, j, k, d.W >> 1, d.H)] = __ldg(scales + 3) * head_out(d0b, pvox(d, i, j, k), head, f);
 }
 
-// Step 3: <r, q> and <q, q> (FP64) with r = b - A p and q = A d, one pair per block.
+// Step 3: <r, q>, <q, q>, <d, r> and <d, q> (FP64) with r = b - A p and
+// q = A d, one quadruple per block.
 __global__ void __launch_bounds__(kNormThreads)
 k_unet_project(GridInfo g, CellArr rhs, CellArr p, CellArr dl, double *partials) {
     const long long n = (long long)g.W * g.H * g.D;
     const GridInfo g0{g.W, g.H, g.D, g.open, g.dirichlet, 0.0f};
-    double rq = 0.0, qq = 0.0;
+    double rq = 0.0, qq = 0.0, dr = 0.0, dq = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t % g.W);
         const long long jk = t / g.W;
@@ -518,38 +522,49 @@ k_unet_project(GridInfo g, CellArr rhs, CellArr p, CellArr dl, double *partials)
         cell_brp(g0, rhs, dl, i, j, k, zb, dc, mq);      // with b = 0: mq = -(A d)
         rq -= (double)r * (double)mq;
         qq += (double)mq * (double)mq;
+        dr += (double)dc * (double)r;
+        dq -= (double)dc * (double)mq;
     }
-    __shared__ double s[2][kNormThreads / 32];
-    rq = warp_sum_d(rq);
-    qq = warp_sum_d(qq);
+    __shared__ double s[4][kNormThreads / 32];
+    double a[4] = {rq, qq, dr, dq};
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0) { s[0][w] = rq; s[1][w] = qq; }
-    __syncthreads();
-    if (w == 0) {
-        rq = lane < kNormThreads / 32 ? s[0][lane] : 0.0;
-        qq = lane < kNormThreads / 32 ? s[1][lane] : 0.0;
-        rq = warp_sum_d(rq);
-        qq = warp_sum_d(qq);
-        if (lane == 0) { partials[2 * blockIdx.x] = rq; partials[2 * blockIdx.x + 1] = qq; }
+    for (int q = 0; q < 4; ++q) {
+        a[q] = warp_sum_d(a[q]);
+        if (lane == 0) s[q][w] = a[q];
     }
+    __syncthreads();
+    if (w == 0)
+        for (int q = 0; q < 4; ++q) {
+            double v = lane < kNormThreads / 32 ? s[q][lane] : 0.0;
+            v = warp_sum_d(v);
+            if (lane == 0) partials[4 * blockIdx.x + q] = v;
+        }
 }
 
-// alpha = <r, A d> / <A d, A d>: the step along d that minimises the
-// residual norm ||b - A (p + alpha d)|| (0 when A d is 0).
-__global__ void k_unet_alpha(const double *partials, int nblk, float *alpha) {
-    __shared__ double s[2][32];
-    double a[2] = {0.0, 0.0};
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) { a[0] += partials[2 * b]; a[1] += partials[2 * b + 1]; }
+// The step along d:
+//   BLZ_WARM_STEP_RESIDUAL  alpha = <r, A d> / <A d, A d>, minimising the
+//                           residual norm ||b - A (p + alpha d)||;
+//   BLZ_WARM_STEP_ENERGY    alpha = <d, r> / <d, A d>, minimising the error's
+//                           energy norm ||e - alpha d||_A (A symmetric
+//                           positive definite: a Dirichlet face or more).
+// Either is 0 when its denominator is 0.
+__global__ void k_unet_alpha(const double *partials, int nblk, int mode, float *alpha) {
+    __shared__ double s[4][32];
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+        for (int q = 0; q < 4; ++q) a[q] += partials[4 * b + q];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < 4; ++q) {
         a[q] = warp_sum_d(a[q]);
         if (lane == 0) s[q][w] = a[q];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double rq = 0.0, qq = 0.0;
-        for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i) { rq += s[0][i]; qq += s[1][i]; }
-        *alpha = qq > 0.0 ? (float)(rq / qq) : 0.0f;
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i)
+            for (int q = 0; q < 4; ++q) t[q] += s[q][i];
+        if (mode == BLZ_WARM_STEP_ENERGY) *alpha = t[3] > 0.0 ? (float)(t[2] / t[3]) : 0.0f;
+        else *alpha = t[1] > 0.0 ? (float)(t[0] / t[1]) : 0.0f;
     }
 }
 
@@ -709,6 +724,7 @@ struct blz_unet {
     float *scales = nullptr;
     float *dpk = nullptr, *alpha = nullptr;     // warm start: packed correction + zero rhs; its step
     int smooth = 40;                            // sweeps of p and d before the step is chosen
+    int step_mode = BLZ_WARM_STEP_RESIDUAL;     // how the step along d is chosen
     int *err = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;
@@ -1059,7 +1075,7 @@ int unet_combine(blz_unet *u, const blz_params &P, const float *rhs_r, const flo
     const float *dr = u->dpk, *db = u->dpk + n / 2;
     k_unet_project<<<kNormBlocks, kNormThreads, 0, st>>>(g, CellArr{rhs_r, rhs_b}, CellArr{p_r, p_b},
                                                          CellArr{dr, db}, u->partials);
-    k_unet_alpha<<<1, 256, 0, st>>>(u->partials, kNormBlocks, u->alpha);
+    k_unet_alpha<<<1, 256, 0, st>>>(u->partials, kNormBlocks, u->step_mode, u->alpha);
     k_unet_update<<<nblk(n / 2, 256), 256, 0, st>>>(n / 2, dr, db, u->alpha, p_r, p_b);
     u->launches += 3;
     if (launches) *launches += 3;
@@ -1116,7 +1132,7 @@ int blz_unet_create(int width, int height, int depth, blz_unet **out) {
     if (rc == BLZ_OK) ck(cudaMemset(u->params, 0, off * sizeof(float)), "cudaMemset params");
     ck(cudaMalloc(&u->wf, bf * sizeof(bf16)), "cudaMalloc wf");
     ck(cudaMalloc(&u->wd, bf * sizeof(bf16)), "cudaMalloc wd");
-    ck(cudaMalloc(&u->partials, 3 * kNormBlocks * sizeof(double)), "cudaMalloc partials");
+    ck(cudaMalloc(&u->partials, 4 * kNormBlocks * sizeof(double)), "cudaMalloc partials");
     ck(cudaMalloc(&u->sums, 2 * sizeof(double)), "cudaMalloc sums");
     ck(cudaMallocHost(&u->h_sums, 2 * sizeof(double)), "cudaMallocHost");
     ck(cudaMalloc(&u->scales, 4 * sizeof(float)), "cudaMalloc scales");
@@ -1158,6 +1174,13 @@ long long blz_unet_kernel_launches(const blz_unet *u) { return u ? u->launches :
 int blz_unet_set_smoothing(blz_unet *u, int sweeps) {
     if (!u || sweeps < 0) return ufail(BLZ_ERR_ARG, "bad smoothing sweep count");
     u->smooth = sweeps;
+    return BLZ_OK;
+}
+
+int blz_unet_set_step(blz_unet *u, int mode) {
+    if (!u || (mode != BLZ_WARM_STEP_RESIDUAL && mode != BLZ_WARM_STEP_ENERGY))
+        return ufail(BLZ_ERR_ARG, "bad warm-start step mode");
+    u->step_mode = mode;
     return BLZ_OK;
 }
 

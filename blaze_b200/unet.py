@@ -138,6 +138,11 @@ class WarmStartUNet:
         """Step alpha of the last warm start (p + alpha d)."""
         return float(self._lib.blz_unet_last_alpha(self._h))
 
+    def set_step(self, mode):
+        """_abi.BLZ_WARM_STEP_RESIDUAL or BLZ_WARM_STEP_ENERGY (blz_unet_set_step)."""
+        check(self._lib.blz_unet_set_step(self._h, int(mode)))
+        return self
+
     def set_smoothing(self, sweeps):
         """Sweeps of p and d before the warm start's step is chosen."""
         check(self._lib.blz_unet_set_smoothing(self._h, int(sweeps)))

@@ -169,12 +169,14 @@ def test_unet_training_lowers_the_loss():
     net.close()
 
 
-def test_warm_start_through_the_solver():
+@pytest.mark.parametrize("mode", ["residual", "energy"])
+def test_warm_start_through_the_solver(mode):
     """Without smoothing, blz_solve with a network attached starts from
-    p + alpha d, d = kappa rms(r) delta, alpha = <r, A d> / <A d, A d>."""
+    p + alpha d, d = kappa rms(r) delta, with alpha = <r, A d> / <A d, A d>
+    (residual-norm step) or <d, r> / <d, A d> (energy-norm step)."""
     import torch
     from oracle import unet_oracle as uo
-    from blaze_b200 import FluidSolver, Timer
+    from blaze_b200 import FluidSolver, Timer, _abi
     from blaze_b200.scenes import SceneSettings
     from blaze_b200.unet import WarmStartUNet
     W, H, D = 16, 16, 16
@@ -184,6 +186,7 @@ def test_warm_start_through_the_solver():
     params = _net_params(8)
     net = WarmStartUNet((W, H, D), params, kappa=0.6)
     net.set_smoothing(0)
+    net.set_step(_abi.BLZ_WARM_STEP_RESIDUAL if mode == "residual" else _abi.BLZ_WARM_STEP_ENERGY)
     g = scn.to_params()
     delta = net.forward(g, torch.from_numpy(rhs).cuda(), torch.from_numpy(p).cuda()).cpu().numpy()
     so = uo.scales(g, rhs, p, 0.6)[3]
@@ -197,7 +200,8 @@ def test_warm_start_through_the_solver():
     d = float(so) * delta.astype(np.float64)
     _, _, r = uo.residual_parts(g, rhs, p)
     Ad = -uo.residual_parts(g, np.zeros_like(rhs), d.astype(np.float32))[2].astype(np.float64)
-    alpha = float(np.sum(r * Ad) / np.sum(Ad * Ad))
+    r = r.astype(np.float64)
+    alpha = float(np.sum(r * Ad) / np.sum(Ad * Ad)) if mode == "residual" else float(np.sum(d * r) / np.sum(d * Ad))
     assert abs(net.last_alpha() - alpha) <= 1e-4 * abs(alpha), (net.last_alpha(), alpha)
     want = p.astype(np.float64) + net.last_alpha() * d
     assert np.abs(got - want).max() <= 1e-5 * np.abs(want - p).max() + 1e-6
@@ -210,8 +214,9 @@ def test_warm_start_through_the_solver():
 
 
 def test_smoothed_warm_start_never_raises_the_residual():
-    """With k smoothing sweeps the warm start's residual is at most that of k
-    plain sweeps from the same pressure (alpha = 0 is among the choices)."""
+    """With k smoothing sweeps and the residual-norm step the warm start's
+    residual is at most that of k plain sweeps from the same pressure
+    (alpha = 0 is among the choices)."""
     from blaze_b200 import FluidSolver, Timer
     from blaze_b200.scenes import SceneSettings
     from blaze_b200.unet import WarmStartUNet
@@ -219,8 +224,10 @@ def test_smoothed_warm_start_never_raises_the_residual():
     scn = SceneSettings(gridRes=(W, H, D), dx=1.0 / W, closedBounds=(1, 1, 1, 0, 1, 1), bc_mode=1,
                         maxIterSolve=0, tol=0.0, device_loop=0)
     rhs, p, _ = _fields(W, H, D, 9)
+    from blaze_b200 import _abi
     net = WarmStartUNet((W, H, D), _net_params(10), kappa=0.6)
     net.set_smoothing(40)
+    net.set_step(_abi.BLZ_WARM_STEP_RESIDUAL)
     out = []
     for warm in (False, True):
         solver = FluidSolver(Timer(), scn)
