@@ -621,7 +621,7 @@ def run_render(args, ws, rank, local):
             "render_ms": ms_each, "image_mean": float(img.mean()), "image_max": float(img.max()),
             "roofline": None,
             "roofline_note": "k_render is bound by texture-filter issue and the latency of dependent ray "
-                             "steps, not by HBM bytes or tensor FLOPs (profiles/k_render_256.md)",
+                             "steps, not by HBM bytes or tensor FLOPs (see the k_render ncu summary under profiles/)",
             "cpu_baseline": cpu,
             "e2e": None if e2e is None else {"value": ws * e2e, "unit": "renders/s",
                                              "h2d_bytes_per_step": int(T.nbytes),
