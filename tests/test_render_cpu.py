@@ -193,3 +193,41 @@ def test_render_params_from_blz_keys():
     assert (rp.width, rp.height, rp.ramp_size, rp.light_count, rp.multi_scatter_blur_iter) == (32, 16, 2, 1, 2)
     assert rp.cam_trans[2] == 3.0 and rp.scattering[2] == pytest.approx(0.7) and rp.light_dir[0][1] == -1.0
     assert rp.ramp_colors[1][1] == pytest.approx(0.5) and rp.temp_range[1] == 2.0
+
+
+@pytest.mark.parametrize("field,value,msg", [
+    ("width", 0, "bad render resolution"),
+    ("height", -3, "bad render resolution"),
+    ("p_step", 0.0, "steps and dx must be positive"),
+    ("s_step", float("nan"), "steps and dx must be positive"),
+    ("ramp_size", 0, "ramp_size must be 1..10"),
+    ("ramp_size", 11, "ramp_size must be 1..10"),
+    ("light_count", -1, "light_count must be 0..10"),
+    ("light_count", 11, "light_count must be 0..10"),
+    ("multi_scatter_blur_iter", -1, "negative multi_scatter_blur_iter"),
+])
+def test_renderer_rejects_bad_parameters(field, value, msg):
+    """blz_render_create checks its arguments before touching the device, and
+    leaves the handle null on failure."""
+    from blaze_b200._lib import load
+    lib = load()
+    s, g = _scene()
+    rp = default_render_params(s, width=8, height=8)
+    setattr(rp, field, value)
+    h = C.c_void_p(1)
+    assert lib.blz_render_create(C.byref(rp), C.byref(g), C.byref(h)) == _abi.BLZ_ERR_ARG
+    assert h.value is None
+    assert msg in lib.blz_render_last_error(None).decode()
+
+
+def test_renderer_rejects_small_grids_and_null_arguments():
+    from blaze_b200._lib import load
+    lib = load()
+    s, g = _scene()
+    rp = default_render_params(s, width=8, height=8)
+    g.depth = 3
+    h = C.c_void_p()
+    assert lib.blz_render_create(C.byref(rp), C.byref(g), C.byref(h)) == _abi.BLZ_ERR_ARG
+    assert "grid dims must be >= 4" in lib.blz_render_last_error(None).decode()
+    assert lib.blz_render_create(None, C.byref(g), C.byref(h)) == _abi.BLZ_ERR_ARG
+    assert "null argument" in lib.blz_render_last_error(None).decode()
