@@ -83,5 +83,41 @@ def test_argument_checks_need_no_gpu(lib):
     assert lib.blz_set_particles(None, None, 0) == _abi.BLZ_ERR_ARG
 
 
+def _err(lib):
+    return lib.blz_last_error(None).decode()
+
+
+def test_warm_start_and_batch_argument_checks_need_no_gpu(lib):
+    """The network's and the batch's entry points reject bad arguments before
+    any device call, and say why in the thread's last error."""
+    _abi.bind(lib)
+    h = C.c_void_p(1)
+    for dims in ((0, 8, 8), (12, 16, 16), (16, 16, 4), (-8, 8, 8)):
+        assert lib.blz_unet_create(*dims, C.byref(h)) == _abi.BLZ_ERR_ARG
+        assert h.value is None and "multiples of 8" in _err(lib)
+    assert lib.blz_unet_create(8, 8, 8, None) == _abi.BLZ_ERR_ARG
+    assert lib.blz_unet_set_smoothing(None, 10) == _abi.BLZ_ERR_ARG
+    assert lib.blz_unet_set_step(None, _abi.BLZ_WARM_STEP_ENERGY) == _abi.BLZ_ERR_ARG
+    assert "step mode" in _err(lib)
+    assert lib.blz_unet_set_kappa(None, 0.5) == _abi.BLZ_ERR_ARG
+    assert lib.blz_unet_set_params(None, None, 0) == _abi.BLZ_ERR_ARG
+    assert lib.blz_unet_get_params(None, None, 0) == _abi.BLZ_ERR_ARG
+    assert lib.blz_unet_get_grads(None, None, 0) == _abi.BLZ_ERR_ARG
+    info = (C.c_longlong * 6)()
+    for layer in (-1, 10 ** 6):
+        assert lib.blz_unet_layer_info(layer, info) == _abi.BLZ_ERR_ARG
+        assert f"no layer {layer}" in _err(lib)
+    assert lib.blz_unet_layer_info(0, info) == 0 and (info[0], info[3]) == (0, 27) and info[1] > 0
+    assert lib.blz_batch_create(None, 0, C.byref(h)) == _abi.BLZ_ERR_ARG
+    assert "at least one solver" in _err(lib)
+    sims = (C.c_void_p * 2)(None, None)
+    assert lib.blz_batch_create(sims, 2, C.byref(h)) == _abi.BLZ_ERR_ARG
+    assert "solver 0 is null" in _err(lib)
+    assert lib.blz_batch_add_source(None) == _abi.BLZ_ERR_ARG
+    assert lib.blz_batch_solve(None, None) == _abi.BLZ_ERR_ARG
+    assert lib.blz_batch_step(None, None, None) == _abi.BLZ_ERR_ARG
+    assert "null batch" in _err(lib)
+
+
 def test_oracle_library_loads(oracle_mod):
     assert oracle_mod.num_threads() >= 1
