@@ -118,6 +118,41 @@ class BlzRenderParams(C.Structure):
     ]
 
 
+# Noise functions (blz_noise): ids 0-8 are cuda-noise's basisFunction values.
+NOISE_FUNCS = ["checker", "discrete", "linearvalue", "fadedvalue", "cubicvalue", "perlin", "simplex", "worley",
+               "spots", "repeater_perlin", "repeater_perlin_bounded", "repeater_perlin_abs", "repeater_simplex",
+               "repeater_simplex_abs", "repeater_simplex_bounded", "repeater", "fractal_simplex", "turbulence",
+               "repeater_turbulence"]
+BLZ_NOISE = {name: i for i, name in enumerate(NOISE_FUNCS)}
+BLZ_SHAPE_STEP, BLZ_SHAPE_LINEAR, BLZ_SHAPE_QUADRATIC = 0, 1, 2
+
+
+class BlzNoiseArgs(C.Structure):
+    _fields_ = [
+        ("func", C.c_int), ("seed", C.c_int), ("scale", C.c_float), ("scale_out", C.c_float),
+        ("size", C.c_float), ("jitter", C.c_float), ("min_num", C.c_int), ("max_num", C.c_int),
+        ("shape", C.c_int), ("octaves", C.c_int), ("lacunarity", C.c_float), ("decay", C.c_float),
+        ("threshold", C.c_float), ("du", C.c_float), ("strength", C.c_float),
+        ("basis", C.c_int), ("basis_out", C.c_int),
+    ]
+
+
+def noise_args(func, **kw):
+    """A BlzNoiseArgs for function `func` (name or id); bases may be given by
+    name.  Unset fields take the library's usual values (scale 1, octaves 4,
+    lacunarity 2, decay 0.5, size 1, jitter 1, 4 points per cell)."""
+    a = BlzNoiseArgs()
+    a.func = BLZ_NOISE[func] if isinstance(func, str) else int(func)
+    a.scale = a.scale_out = a.size = a.jitter = 1.0
+    a.min_num = a.max_num = a.octaves = 4
+    a.lacunarity, a.decay = 2.0, 0.5
+    for k, v in kw.items():
+        if k in ("basis", "basis_out") and isinstance(v, str):
+            v = BLZ_NOISE[v]
+        setattr(a, k, v)
+    return a
+
+
 # Every entry point declared in include/blaze_b200.h, with its ctypes signature.
 _P = C.POINTER
 EXPORTS = {
@@ -141,6 +176,7 @@ EXPORTS = {
     "blz_field_size": (C.c_size_t, [C.c_void_p, C.c_int]),
     "blz_field_ptr": (C.c_void_p, [C.c_void_p, C.c_int]),
     "blz_perlin": (C.c_int, [_P(C.c_float), C.c_int, C.c_float, C.c_int, _P(C.c_float)]),
+    "blz_noise": (C.c_int, [_P(BlzNoiseArgs), C.c_void_p, C.c_longlong, C.c_void_p, C.c_int, C.c_void_p]),
     "blz_residual_noalloc": (C.c_int, [_P(BlzParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "blz_conv3d": (C.c_int, [_P(BlzConvDesc), C.c_void_p, C.c_void_p, _P(C.c_float), C.c_void_p, C.c_void_p]),
     "blz_unet_layer_info": (C.c_int, [C.c_int, _P(C.c_longlong)]),

@@ -102,9 +102,13 @@ __device__ __forceinline__ float len3(float x, float y, float z) { return sqrtf(
 // ---------------------------------------------------------------------------
 // Gradient noise: cudaNoise's perlinNoise (reference thirdparty/cuda-noise/
 // cuda_noise.cuh:570-615) evaluated with explicitly rounded operations, so the
-// result is independent of FMA contraction and equals the oracle's FP32 value
-// bit for bit.  The lattice hash (46-57) takes a float sum of the corner
-// coordinates (120-124) truncated to unsigned (cvt.rzi.u32 saturates).
+// result is independent of this build's FMA contraction and equals the
+// oracle's FP32 value bit for bit.  Where the library's source has a multiply
+// feeding an add in one expression, the reference build fuses the two (the
+// left product when both operands are products), and so does this code; the
+// result then equals the reference build's bit for bit.  The lattice hash
+// (46-57) takes a float sum of the corner coordinates (120-124) truncated to
+// unsigned (cvt.rzi.u32 saturates).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t lattice_hash(uint32_t s) {
     s = (s + 0x7ed55d16u) + (s << 12);
@@ -140,14 +144,16 @@ __device__ __forceinline__ float lattice_grad(int h, float x, float y, float z) 
     }
 }
 
+// fade (204-207): t^3 (t (6t - 15) + 10), the inner polynomial fused.
 __device__ __forceinline__ float fade5(float t) {
     const float a = __fmul_rn(__fmul_rn(t, t), t);
-    const float b = __fadd_rn(__fmul_rn(t, __fsub_rn(__fmul_rn(t, 6.0f), 15.0f)), 10.0f);
+    const float b = __fmaf_rn(t, __fmaf_rn(t, 6.0f, -15.0f), 10.0f);
     return __fmul_rn(a, b);
 }
 
+// lerp (167-170): a (1 - r) + b r with the left product fused.
 __device__ __forceinline__ float lerp_rn(float a, float b, float r) {
-    return __fadd_rn(__fmul_rn(a, __fsub_rn(1.0f, r)), __fmul_rn(b, r));
+    return __fmaf_rn(a, __fsub_rn(1.0f, r), __fmul_rn(b, r));
 }
 
 __device__ __forceinline__ float perlin(float px, float py, float pz, float scale, int seed) {

@@ -216,6 +216,62 @@ void *blz_field_ptr(blz_solver *s, int field);
  * the host array out.  Lets callers check the noise without a solver.       */
 int  blz_perlin(const float *pos3, int n, float scale, int seed, float *out);
 
+/* The rest of the reference's noise library (thirdparty/cuda-noise/
+ * cuda_noise.cuh), evaluated at positions {x,y,z}.  Ids 0-8 are the
+ * library's basisFunction values (cuda_noise.cuh:13-23); the others are its
+ * derived functions.  Each function reads the blz_noise_args fields named
+ * beside it, with the library's argument meaning.                           */
+#define BLZ_NOISE_CHECKER                  0   /* checker(scale, seed), 324-335          */
+#define BLZ_NOISE_DISCRETE                 1   /* discreteNoise(scale, seed), 472-480    */
+#define BLZ_NOISE_LINEARVALUE              2   /* linearValue(scale, seed), 482-515      */
+#define BLZ_NOISE_FADEDVALUE               3   /* fadedValue(scale, seed), 517-550       */
+#define BLZ_NOISE_CUBICVALUE               4   /* cubicValue(scale, seed), 552-568       */
+#define BLZ_NOISE_PERLIN                   5   /* perlinNoise(scale, seed), 570-615      */
+#define BLZ_NOISE_SIMPLEX                  6   /* simplexNoise(scale, seed), 230-321     */
+#define BLZ_NOISE_WORLEY                   7   /* worleyNoise(scale, seed, size, min_num,
+                                                  max_num, jitter), 395-436              */
+#define BLZ_NOISE_SPOTS                    8   /* spots(... as worley, shape), 337-393   */
+#define BLZ_NOISE_REPEATER_PERLIN          9   /* (scale, seed, octaves, lacunarity, decay), 620-633 */
+#define BLZ_NOISE_REPEATER_PERLIN_BOUNDED 10   /* (... , threshold), 636-656             */
+#define BLZ_NOISE_REPEATER_PERLIN_ABS     11   /* 659-673                                */
+#define BLZ_NOISE_REPEATER_SIMPLEX        12   /* 676-690                                */
+#define BLZ_NOISE_REPEATER_SIMPLEX_ABS    13   /* 693-707                                */
+#define BLZ_NOISE_REPEATER_SIMPLEX_BOUNDED 14  /* (... , threshold), 710-731             */
+#define BLZ_NOISE_REPEATER                15   /* repeater(... , basis), 734-779         */
+#define BLZ_NOISE_FRACTAL_SIMPLEX         16   /* (scale, seed, du, octaves, lacunarity,
+                                                  decay), 782-801                        */
+#define BLZ_NOISE_TURBULENCE              17   /* (scale = scaleIn, scale_out, seed,
+                                                  strength, basis, basis_out), 804-865   */
+#define BLZ_NOISE_REPEATER_TURBULENCE     18   /* (as turbulence, octaves), 867-874      */
+#define BLZ_NOISE_COUNT                   19
+
+#define BLZ_SHAPE_STEP      0                  /* spots' profileShape, 26-30             */
+#define BLZ_SHAPE_LINEAR    1
+#define BLZ_SHAPE_QUADRATIC 2
+
+typedef struct blz_noise_args {
+    int   func;                 /* BLZ_NOISE_*                                     */
+    int   seed;
+    float scale;                /* turbulence: scaleIn                             */
+    float scale_out;            /* turbulence: scaleOut                            */
+    float size, jitter;         /* worley, spots                                   */
+    int   min_num, max_num;     /* feature points per cell (worley, spots)        */
+    int   shape;                /* spots: BLZ_SHAPE_*                              */
+    int   octaves;              /* repeaters, fractal: n                           */
+    float lacunarity, decay;
+    float threshold;            /* bounded repeaters                               */
+    float du;                   /* fractal simplex: smallest feature size          */
+    float strength;             /* turbulence                                      */
+    int   basis, basis_out;     /* repeater / turbulence bases (BLZ_NOISE_0..8)    */
+} blz_noise_args;
+
+/* Evaluates a->func at n positions pos3 into out (both device memory when
+ * on_device, else host memory), on `stream` (NULL: the legacy default
+ * stream) for device buffers.  Host buffers are copied through the device
+ * and the call returns when out is written.  BLZ_ERR_ARG for an unknown
+ * function or basis, octaves outside 0..64, min_num > max_num or n < 0.     */
+int  blz_noise(const blz_noise_args *a, const float *pos3, long long n, float *out, int on_device, void *stream);
+
 /* FP64 residual norms without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc (a host
  * application or plugin host that owns all device memory through its own

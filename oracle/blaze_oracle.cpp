@@ -62,7 +62,8 @@ static inline uint32_t f2u_sat(float x) {
 // fma(z, 149812, fma(x, 1723, y*93241)), then adds 3824 and seed; once a
 // product exceeds 2^24 the contraction changes the rounded value and with it
 // the hashed lattice gradient, so the oracle forms it the same way.  Pinned
-// bit for bit against the reference build's own noise (tests/golden/perlin.npz).
+// bit for bit against the reference build's own noise (tests/golden/perlin.npz,
+// tests/golden/noise.npz).
 static inline uint32_t lattice_seed(float x, float y, float z, float seed) {
     float acc = std::fma(x, 1723.0f, y * 93241.0f);
     acc = std::fma(z, 149812.0f, acc);
@@ -85,11 +86,14 @@ static inline float lattice_grad(int h, float x, float y, float z) {
     }
 }
 
-static inline float fade5(float t) {           // cuda_noise.cuh:204-207
-    return t * t * t * (t * (t * 6.0f - 15.0f) + 10.0f);
+// fade and lerp (cuda_noise.cuh:204-207, 167-170) as the reference's CUDA
+// build evaluates them: a multiply feeding an add in the same expression is
+// one fused multiply-add (the left product when both operands are products).
+static inline float fade5(float t) {
+    return t * t * t * std::fma(t, std::fma(t, 6.0f, -15.0f), 10.0f);
 }
-static inline float lerpf(float a, float b, float r) {  // cuda_noise.cuh:167-170
-    return a * (1.0f - r) + b * r;
+static inline float lerpf(float a, float b, float r) {
+    return std::fma(a, 1.0f - r, b * r);
 }
 
 // perlinNoise, cuda_noise.cuh:570-615.

@@ -59,6 +59,10 @@ def load():
         lib.orc_render.argtypes = [C.POINTER(_abi.BlzRenderParams), P, F, F, C.c_int]
         lib.orc_perlin.restype = C.c_float
         lib.orc_perlin.argtypes = [C.c_float] * 4 + [C.c_int]
+        lib.orc_noise.restype = C.c_int
+        lib.orc_noise_set_lattice_patterns.restype = C.c_int
+        lib.orc_noise_set_lattice_patterns.argtypes = [C.POINTER(C.c_ulonglong), C.c_int]
+        lib.orc_noise.argtypes = [C.POINTER(_abi.BlzNoiseArgs), C.c_void_p, C.c_longlong, C.c_void_p]
         lib.orc_num_threads.restype = C.c_int
         _lib = lib
     return _lib
@@ -142,6 +146,27 @@ class State:
 
 def perlin(x, y, z, scale, seed):
     return load().orc_perlin(x, y, z, scale, seed)
+
+
+def noise(args, pos3, lattice_patterns=()):
+    """The noise library's function args.func (a BlzNoiseArgs) restated
+    (noise_oracle.cpp), at positions pos3 (n x 3 float32).  lattice_patterns
+    selects, per value-noise lattice blend and lattice point, the other
+    contraction of the hash sum (the test hook
+    orc_noise_set_lattice_patterns; empty is the standalone form)."""
+    a = np.ascontiguousarray(pos3, np.float32).reshape(-1, 3)
+    out = np.empty(len(a), np.float32)
+    lib = load()
+    pats = (C.c_ulonglong * max(1, len(lattice_patterns)))(*lattice_patterns)
+    if lib.orc_noise_set_lattice_patterns(pats, len(lattice_patterns)) != 0:
+        raise ValueError("at most 16 lattice patterns")
+    try:
+        rc = lib.orc_noise(C.byref(args), a.ctypes.data, len(a), out.ctypes.data)
+    finally:
+        lib.orc_noise_set_lattice_patterns(pats, 0)
+    if rc != 0:
+        raise ValueError(f"orc_noise: bad arguments ({rc})")
+    return out
 
 
 def num_threads():

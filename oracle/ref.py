@@ -41,6 +41,7 @@ def load():
             ("ref_get_field", C.c_int, [C.c_void_p, C.c_int, F]),
             ("ref_set_field", C.c_int, [C.c_void_p, C.c_int, F]),
             ("ref_perlin", C.c_int, [F, C.c_int, C.c_float, C.c_int, F]),
+            ("ref_noise", C.c_int, [C.POINTER(_abi.BlzNoiseArgs), F, C.c_int, F]),
             ("ref_render_create", C.c_void_p, [C.c_void_p, C.POINTER(_abi.BlzRenderParams)]),
             ("ref_render", C.c_int, [C.c_void_p, C.c_void_p, F]),
             ("ref_render_get", C.c_int, [C.c_void_p, F]),
@@ -150,3 +151,13 @@ class RefRenderer:
 
     def __exit__(self, *a):
         self.close()
+
+
+def noise(args, pos3):
+    """The reference library's noise function args.func (a BlzNoiseArgs) at
+    positions pos3, computed by the reference build on the GPU."""
+    a = np.ascontiguousarray(pos3, np.float32).reshape(-1, 3)
+    out = np.empty(len(a), np.float32)
+    _chk(load().ref_noise(C.byref(args), a.ctypes.data_as(C.POINTER(C.c_float)), len(a),
+                          out.ctypes.data_as(C.POINTER(C.c_float))), "noise")
+    return out

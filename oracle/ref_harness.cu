@@ -336,3 +336,68 @@ int ref_perlin(const float *pos3, int n, float scale, int seed, float *out) {
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// The reference's noise library (thirdparty/cuda-noise/cuda_noise.cuh, which
+// FluidSolver.cu includes) at n positions: one function, selected by
+// a.func, per launch.  Used to generate tests/golden/noise.npz.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void ref_noise_kernel(blz_noise_args a, const float *pos, int n, float *out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    using namespace cudaNoise;
+    const float3 p = make_float3(pos[3 * t], pos[3 * t + 1], pos[3 * t + 2]);
+    const basisFunction bi = (basisFunction)a.basis, bo = (basisFunction)a.basis_out;
+    float v = 0.0f;
+    switch (a.func) {
+    case BLZ_NOISE_CHECKER: v = checker(p, a.scale, a.seed); break;
+    case BLZ_NOISE_DISCRETE: v = discreteNoise(p, a.scale, a.seed); break;
+    case BLZ_NOISE_LINEARVALUE: v = linearValue(p, a.scale, a.seed); break;
+    case BLZ_NOISE_FADEDVALUE: v = fadedValue(p, a.scale, a.seed); break;
+    case BLZ_NOISE_CUBICVALUE: v = cubicValue(p, a.scale, a.seed); break;
+    case BLZ_NOISE_PERLIN: v = perlinNoise(p, a.scale, a.seed); break;
+    case BLZ_NOISE_SIMPLEX: v = simplexNoise(p, a.scale, a.seed); break;
+    case BLZ_NOISE_WORLEY: v = worleyNoise(p, a.scale, a.seed, a.size, a.min_num, a.max_num, a.jitter); break;
+    case BLZ_NOISE_SPOTS:
+        v = spots(p, a.scale, a.seed, a.size, a.min_num, a.max_num, a.jitter, (profileShape)a.shape);
+        break;
+    case BLZ_NOISE_REPEATER_PERLIN: v = repeaterPerlin(p, a.scale, a.seed, a.octaves, a.lacunarity, a.decay); break;
+    case BLZ_NOISE_REPEATER_PERLIN_BOUNDED:
+        v = repeaterPerlinBounded(p, a.scale, a.seed, a.octaves, a.lacunarity, a.decay, a.threshold);
+        break;
+    case BLZ_NOISE_REPEATER_PERLIN_ABS: v = repeaterPerlinAbs(p, a.scale, a.seed, a.octaves, a.lacunarity, a.decay); break;
+    case BLZ_NOISE_REPEATER_SIMPLEX: v = repeaterSimplex(p, a.scale, a.seed, a.octaves, a.lacunarity, a.decay); break;
+    case BLZ_NOISE_REPEATER_SIMPLEX_ABS:
+        v = repeaterSimplexAbs(p, a.scale, a.seed, a.octaves, a.lacunarity, a.decay);
+        break;
+    case BLZ_NOISE_REPEATER_SIMPLEX_BOUNDED:
+        v = repeaterSimplexBounded(p, a.scale, a.seed, a.octaves, a.lacunarity, a.decay, a.threshold);
+        break;
+    case BLZ_NOISE_REPEATER: v = repeater(p, a.scale, a.seed, a.octaves, a.lacunarity, a.decay, bi); break;
+    case BLZ_NOISE_FRACTAL_SIMPLEX:
+        v = fractalSimplex(p, a.scale, a.seed, a.du, a.octaves, a.lacunarity, a.decay);
+        break;
+    case BLZ_NOISE_TURBULENCE: v = turbulence(p, a.scale, a.scale_out, a.seed, a.strength, bi, bo); break;
+    case BLZ_NOISE_REPEATER_TURBULENCE:
+        v = repeaterTurbulence(p, a.scale, a.scale_out, a.seed, a.strength, a.octaves, bi, bo);
+        break;
+    default: break;
+    }
+    out[t] = v;
+}
+} // namespace
+
+extern "C" int ref_noise(const blz_noise_args *a, const float *pos3, int n, float *out) {
+    if (n <= 0) return 0;
+    if (!a || a->func < 0 || a->func >= BLZ_NOISE_COUNT || a->basis < 0 || a->basis > 8 || a->basis_out < 0 ||
+        a->basis_out > 8 || a->min_num > a->max_num || a->octaves < 0 || a->octaves > 64)
+        return -2;
+    float *d = nullptr;
+    if (cudaMalloc(&d, sizeof(float) * 4 * (size_t)n) != cudaSuccess) return -1;
+    cudaMemcpy(d, pos3, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice);
+    ref_noise_kernel<<<(n + 127) / 128, 128>>>(*a, d, n, d + 3 * (size_t)n);
+    const cudaError_t e = cudaMemcpy(out, d + 3 * (size_t)n, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? 0 : -1;
+}

@@ -45,10 +45,13 @@ def test_struct_layout_matches_c(tmp_path):
     src = tmp_path / "layout.c"
     fields = [f for f, _ in _abi.BlzParams._fields_]
     sfields = [f for f, _ in _abi.BlzStepStats._fields_]
+    nfields = [f for f, _ in _abi.BlzNoiseArgs._fields_]
     body = "".join(f'printf("p {f} %zu\\n", offsetof(blz_params, {f}));' for f in fields)
     body += "".join(f'printf("s {f} %zu\\n", offsetof(blz_step_stats, {f}));' for f in sfields)
+    body += "".join(f'printf("n {f} %zu\\n", offsetof(blz_noise_args, {f}));' for f in nfields)
     src.write_text(f'#include <stdio.h>\n#include <stddef.h>\n#include "blaze_b200.h"\nint main(void){{'
-                   f'printf("P %zu\\nS %zu\\n", sizeof(blz_params), sizeof(blz_step_stats));{body} return 0;}}\n')
+                   f'printf("P %zu\\nS %zu\\nN %zu\\n", sizeof(blz_params), sizeof(blz_step_stats), '
+                   f'sizeof(blz_noise_args));{body} return 0;}}\n')
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
@@ -65,6 +68,9 @@ def test_struct_layout_matches_c(tmp_path):
         assert got[("p", f)] == getattr(_abi.BlzParams, f).offset, f
     for f in sfields:
         assert got[("s", f)] == getattr(_abi.BlzStepStats, f).offset, f
+    assert got["N"] == C.sizeof(_abi.BlzNoiseArgs)
+    for f in nfields:
+        assert got[("n", f)] == getattr(_abi.BlzNoiseArgs, f).offset, f
 
 
 def test_argument_checks_need_no_gpu(lib):
