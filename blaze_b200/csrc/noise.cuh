@@ -19,6 +19,10 @@
 namespace blz {
 namespace noise {
 
+// Integer sums wrap, as the reference's do on the GPU (cell indices come from
+// saturating conversions and may sit at INT_MAX).
+__device__ __forceinline__ int wadd(int a, int b) { return (int)((uint32_t)a + (uint32_t)b); }
+
 __device__ __forceinline__ float unit_rand(uint32_t s) {            // randomFloat, 68-74
     return __fmul_rn(__uint2float_rn(lattice_hash(s)), 2.3283064365386963e-10f);
 }
@@ -106,8 +110,8 @@ __device__ inline float simplex(float px, float py, float pz, float scale, int s
 }
 
 __device__ __forceinline__ float checker(float px, float py, float pz, float scale) {     // 324-335
-    const int s = __float2int_rz(__fmul_rn(px, scale)) + __float2int_rz(__fmul_rn(py, scale)) +
-                  __float2int_rz(__fmul_rn(pz, scale));
+    const int s = wadd(wadd(__float2int_rz(__fmul_rn(px, scale)), __float2int_rz(__fmul_rn(py, scale))),
+                       __float2int_rz(__fmul_rn(pz, scale)));
     return s % 2 == 0 ? 1.0f : -1.0f;
 }
 
@@ -158,7 +162,7 @@ __device__ inline float spots(float px, float py, float pz, float scale, int see
     for (int x = -1; x < 2; ++x)
         for (int y = -1; y < 2; ++y)
             for (int z = -1; z < 2; ++z) {
-                const int a = ix + x, b = iy + y, c = iz + z;
+                const int a = wadd(ix, x), b = wadd(iy, y), c = wadd(iz, z);
                 const int count = feature_count(seed, a, b, c, 823452.0f, 3234874.0f, lo, hi);
                 const float uu = __fsub_rn(u, (float)x), vv = __fsub_rn(v, (float)y), ww = __fsub_rn(w, (float)z);
                 for (int i = 0; i < count; ++i) {
@@ -189,7 +193,7 @@ __device__ inline float worley(float px, float py, float pz, float scale, int se
     for (int x = -1; x < 2; ++x)
         for (int y = -1; y < 2; ++y)
             for (int z = -1; z < 2; ++z) {
-                const int a = ix + x, b = iy + y, c = iz + z;
+                const int a = wadd(ix, x), b = wadd(iy, y), c = wadd(iz, z);
                 const int count = feature_count(seed, a, b, c, 67262.0f, 0.0f, lo, hi);
                 const float uu = __fsub_rn(u, (float)x), vv = __fsub_rn(v, (float)y), ww = __fsub_rn(w, (float)z);
                 for (int i = 0; i < count; ++i) best = fminf(best, feature_dist(seed, a, b, c, i, uu, vv, ww, jitter).d2);
@@ -205,9 +209,9 @@ __device__ inline float tricubic(int x, int y, int z, float u, float v, float w)
         float xs[4];
 #pragma unroll
         for (int dy = 0; dy < 4; ++dy) {
-            const int yy = y - 1 + dy, zz = z - 1 + dz;
-            xs[dy] = cubic(grid_rand(x - 1, yy, zz, 0), grid_rand(x, yy, zz, 0), grid_rand(x + 1, yy, zz, 0),
-                           grid_rand(x + 2, yy, zz, 0), u);
+            const int yy = wadd(y, dy - 1), zz = wadd(z, dz - 1);
+            xs[dy] = cubic(grid_rand(wadd(x, -1), yy, zz, 0), grid_rand(x, yy, zz, 0), grid_rand(wadd(x, 1), yy, zz, 0),
+                           grid_rand(wadd(x, 2), yy, zz, 0), u);
         }
         ys[dz] = cubic(xs[0], xs[1], xs[2], xs[3], v);
     }
@@ -221,10 +225,11 @@ __device__ __forceinline__ float discrete(float px, float py, float pz, float sc
 
 // Trilinear blend of the eight lattice values of cell (ix, iy, iz).
 __device__ __forceinline__ float value_lerp(int ix, int iy, int iz, int seed, float u, float v, float w) {
-    const float x00 = lerp(grid_rand(ix, iy, iz, seed), grid_rand(ix + 1, iy, iz, seed), u);
-    const float x10 = lerp(grid_rand(ix, iy + 1, iz, seed), grid_rand(ix + 1, iy + 1, iz, seed), u);
-    const float x01 = lerp(grid_rand(ix, iy, iz + 1, seed), grid_rand(ix + 1, iy, iz + 1, seed), u);
-    const float x11 = lerp(grid_rand(ix, iy + 1, iz + 1, seed), grid_rand(ix + 1, iy + 1, iz + 1, seed), u);
+    const int jx = wadd(ix, 1), jy = wadd(iy, 1), jz = wadd(iz, 1);
+    const float x00 = lerp(grid_rand(ix, iy, iz, seed), grid_rand(jx, iy, iz, seed), u);
+    const float x10 = lerp(grid_rand(ix, jy, iz, seed), grid_rand(jx, jy, iz, seed), u);
+    const float x01 = lerp(grid_rand(ix, iy, jz, seed), grid_rand(jx, iy, jz, seed), u);
+    const float x11 = lerp(grid_rand(ix, jy, jz, seed), grid_rand(jx, jy, jz, seed), u);
     return lerp(lerp(x00, x10, v), lerp(x01, x11, v), w);
 }
 

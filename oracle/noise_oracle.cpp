@@ -279,7 +279,7 @@ static float tricubic(int x, int y, int z, float u, float v, float w) {
         for (int dy = 0; dy < 4; ++dy) {
             float p[4];
             for (int dx = 0; dx < 4; ++dx) {
-                const int xx = x - 1 + dx, yy = y - 1 + dy, zz = z - 1 + dz;
+                const int xx = wadd(x, dx - 1), yy = wadd(y, dy - 1), zz = wadd(z, dz - 1);
                 p[dx] = grid_rand_p(xx, yy, zz, 0, (pat >> (dx + 4 * dy + 16 * dz)) & 1u);
             }
             xs[dy] = cubic(p[0], p[1], p[2], p[3], u);
@@ -297,7 +297,7 @@ float discrete(float px, float py, float pz, float scale, int seed) {       // 4
 static inline float value_lerp(int ix, int iy, int iz, int seed, float u, float v, float w) {
     const uint64_t p = next_pattern();
     auto g = [&](int dx, int dy, int dz) {
-        return grid_rand_p(ix + dx, iy + dy, iz + dz, seed, (p >> (dx + 2 * dy + 4 * dz)) & 1u);
+        return grid_rand_p(wadd(ix, dx), wadd(iy, dy), wadd(iz, dz), seed, (p >> (dx + 2 * dy + 4 * dz)) & 1u);
     };
     const float x00 = lerp(g(0, 0, 0), g(1, 0, 0), u);
     const float x10 = lerp(g(0, 1, 0), g(1, 1, 0), u);
