@@ -6,7 +6,7 @@
 //
 // It restates, stage by stage, the algorithm of the Blaze reference
 // (asiroisvigneux/Blaze; paths below are inside that project) in plain C++,
-// templated on the arithmetic type: the FP64 instantiation is the judge of the
+// templated on the arithmetic type: the FP64 instantiation is the yardstick for the
 // FP32 CUDA kernels, the FP32 one mirrors the reference's own arithmetic for
 // comparisons against the reference's CUDA build.  Float constants of the
 // reference (1.001f, 1e-20f, 1e-5) keep their float values in both.
