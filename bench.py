@@ -39,10 +39,11 @@ TOL = 1e-4
 MAX_ITER = 40000
 CHECK_EVERY = 20          # residual-check interval of the batched simulations
 CHECK_AUTO = -1           # the 256^3 step: interval chosen per frame (blz_params.check_every < 0)
-# Sweeps per frame the reference arm runs (maxIterSolve): the mean the plain
-# RBGS step needs on this scene and frame window (frames 5-14 of seed 3 at
-# 256^3: 26074 sweeps), measured on a B200.
-REF_EQUAL_WORK_SWEEPS = int(os.environ.get("BLZ_REF_SWEEPS", "26074"))
+# The reference arm runs, frame by frame, the sweep count (maxIterSolve) the
+# plain RBGS step needs on the same frame, measured by a plain-only run of
+# this script in a child process just before (BLZ_REF_SWEEPS=<n> fixes n
+# sweeps per frame instead, for short runs).
+REF_SWEEPS_ENV = "BLZ_REF_SWEEPS"
 
 
 def load_peaks():
@@ -279,6 +280,7 @@ def run_ours(args, ws, rank, local):
                "max_rel_residual": float(rel.max()), "all_converged": all(s["converged"] for s in st_),
                "hbm_gbs_step": float(np.mean([step_bytes(W, H, D, a, c) for a, c in zip(sw, ck)]))
                / (ms_ / args.steps * 1e-3) / 1e9,
+               "ms_per_sweep": float(sum(s["ms_sweeps"] for s in st_) / max(1.0, sw.sum())),
                "stage_ms": {k: float(np.mean([s[k] for s in st_])) for k in
                             ("ms_forces", "ms_divergence", "ms_solve", "ms_gradient", "ms_advect", "ms_sweeps",
                              "ms_checks", "ms_warm_start")}}
@@ -466,6 +468,27 @@ def run_batch(args, ws, rank, local):
             "gpu_launches": int(launches), "clocks": clk.summary()}
 
 
+def plain_sweeps_per_frame(args, local):
+    """Sweeps per frame of the plain RBGS step on the timed frames, from a
+    plain-only run of this script (same grid, steps and warm-up) in a child
+    process, so the reference process itself loads no code of this
+    repository's library.  Returns (per-frame list, how)."""
+    fixed = os.environ.get(REF_SWEEPS_ENV)
+    if fixed:
+        return [int(fixed)] * args.steps, f"{REF_SWEEPS_ENV}={fixed} sweeps per frame"
+    cmd = [sys.executable, os.path.abspath(__file__), "--plain-only", "--no-cpu", "--no-e2e", "--grid",
+           str(args.grid), "--steps", str(args.steps), "--warmup", str(args.warmup), "--max-iter", str(args.max_iter)]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        env.pop(k, None)
+    res = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
+    lines = [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+    if res.returncode != 0 or not lines:
+        raise RuntimeError("plain run for the reference's sweep counts failed:\n" + res.stderr[-2000:])
+    plain = json.loads(lines[-1])["plain"]
+    return [int(x) for x in plain["sweeps_per_frame"]], "measured by a plain-only run of this script just before"
+
+
 def run_reference(args, ws, rank, local):
     if rank != 0:
         return None
@@ -474,15 +497,18 @@ def run_reference(args, ws, rank, local):
     from blaze_b200 import family_scene, BLZ_BC_REF_COMPAT
     if not ref.available():
         return {"impl": "reference", "unavailable": "reference CUDA build (oracle/_ref) not built"}
+    sweeps, how = plain_sweeps_per_frame(args, local)
+    mean_sweeps = float(np.mean(sweeps))
     torch.cuda.set_device(local)
-    scn, parts = family_scene(n=args.grid, seed=SEED, tol=0.0, max_iter=REF_EQUAL_WORK_SWEEPS,
+    scn, parts = family_scene(n=args.grid, seed=SEED, tol=0.0, max_iter=int(round(mean_sweeps)),
                               bc_mode=BLZ_BC_REF_COMPAT)
     p = scn.to_params()
     r = ref.RefSolver(p)
     it, t = 0, 0.0
 
-    def frame():
+    def frame(n_sweeps):
         nonlocal it, t
+        r.set_max_iter(n_sweeps)
         r.set_time(it, t)
         r.set_particles(parts)
         r.add_source()
@@ -491,12 +517,12 @@ def run_reference(args, ws, rank, local):
         t += scn.dt
 
     for _ in range(args.warmup):
-        frame()
+        frame(int(round(mean_sweeps)))
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         w0 = time.perf_counter()
-        for _ in range(args.steps):
-            frame()
+        for f in range(args.steps):
+            frame(sweeps[f])
         torch.cuda.synchronize()
         wall = time.perf_counter() - w0
     r.close()
@@ -507,8 +533,11 @@ def run_reference(args, ws, rank, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"plume-family {args.grid}^3 scene (seed {SEED}) through the reference's "
                                f"own CUDA build (src/FluidSolver.cu, -O3 --use_fast_math, sm_100a), "
-                               f"maxIterSolve={REF_EQUAL_WORK_SWEEPS} (equal sweep count; the reference "
-                               f"has no residual control)", "grid": [args.grid] * 3},
+                               f"maxIterSolve per frame = the plain RBGS step's sweeps on that frame "
+                               f"(mean {mean_sweeps:.0f}; equal sweep count, the reference has no residual "
+                               f"control)", "grid": [args.grid] * 3,
+                   "sweeps_per_frame": sweeps, "mean_sweeps": mean_sweeps, "sweep_counts": how},
+        "ms_per_sweep": wall * 1e3 / float(sum(sweeps)),
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference",
                          "sample": "the reference's CUDA build on the same B200 (it has no CPU path); "
                                    "its frame includes the .part file read of an animated source"},

@@ -293,24 +293,39 @@ __host__ __device__ inline int tb_rows_alloc(int TY) { return (TY + 8 + 1) & ~1;
 // box of Wh floats x the CTA's rows x 1 plane per copy) into dense ring
 // slots, completing on one mbarrier per slot.  Rows and planes outside the
 // grid arrive as zeros (the copies' out-of-bounds fill).  Every wait is
-// bounded: a wait that gives up counts in g_tb_timeouts and the pass goes
-// on (its result is then wrong, and the solver reports the timeout).
+// bounded in time (kTbWaitNs on the device's global timer).  When a wait of
+// any thread gives up, the whole CTA stops the pass: it counts the failure in
+// g_tb_timeouts, waits once more (bounded) for the copies it issued last so
+// that none lands in shared memory after the CTA has exited, and returns
+// without computing on unfilled slots.  The pass's output is then incomplete
+// and the solver reports BLZ_ERR_TIMEOUT.
 constexpr int kTbDenseSlots = 10;                 // 4 red rhs, 4 black rhs, 2 input
+constexpr unsigned long long kTbWaitNs = 10ull * 1000ull * 1000ull;   // 10 ms; a normal wait takes microseconds
 __device__ unsigned int g_tb_timeouts;
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ void tb_wait(uint32_t bar, uint32_t parity) {
-    for (int it = 0; it < (1 << 24); ++it) {
-        uint32_t done;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                     " selp.u32 %0, 1, 0, p;\n}\n"
-                     : "=r"(done) : "r"(bar), "r"(parity) : "memory");
-        if (done) return;
+__device__ __forceinline__ unsigned long long tb_now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for phase `parity` of the mbarrier at `bar`; false after kTbWaitNs.
+__device__ __forceinline__ bool tb_wait(uint32_t bar, uint32_t parity) {
+    const unsigned long long t0 = tb_now_ns();
+    for (;;) {
+        for (int it = 0; it < 64; ++it) {
+            uint32_t done;
+            asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                         " selp.u32 %0, 1, 0, p;\n}\n"
+                         : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+            if (done) return true;
+        }
+        if (tb_now_ns() - t0 > kTbWaitNs) return false;
     }
-    atomicAdd(&g_tb_timeouts, 1u);
 }
 
 __host__ __device__ inline int tb_dense_slot_bytes(int Wq, int rows_alloc) {
@@ -412,9 +427,9 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     // Fill order: red planes z0-3.. in slots k & 3, black planes z0-2.. in
     // 4 + (k & 3), input planes z0-2.. in 8 + (k & 1); the n-th fill of a
     // slot completes its mbarrier's phase n.
-    auto wait_red = [&](int k) { tb_wait(smem_addr(&tbar[k & 3]), ((k - (z0 - 3)) >> 2) & 1); };
-    auto wait_black = [&](int k) { tb_wait(smem_addr(&tbar[4 + (k & 3)]), ((k - (z0 - 2)) >> 2) & 1); };
-    auto wait_in = [&](int k) { tb_wait(smem_addr(&tbar[8 + (k & 1)]), ((k - (z0 - 2)) >> 1) & 1); };
+    auto wait_red = [&](int k) { return tb_wait(smem_addr(&tbar[k & 3]), ((k - (z0 - 3)) >> 2) & 1); };
+    auto wait_black = [&](int k) { return tb_wait(smem_addr(&tbar[4 + (k & 3)]), ((k - (z0 - 2)) >> 2) & 1); };
+    auto wait_in = [&](int k) { return tb_wait(smem_addr(&tbar[8 + (k & 1)]), ((k - (z0 - 2)) >> 1) & 1); };
     auto prefetch = [&](int k_red, int k_black, int k_in) {
         if constexpr (TMA) {
             if (!leader) return;
@@ -554,9 +569,19 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
             // this step's copies were issued in the previous one; slots are
             // overwritten only after the barrier (their last readers were in
             // the previous step)
-            wait_red(t);
-            if (t - 1 >= z0 - 2) wait_black(t - 1);
-            wait_in(t + 1);
+            bool ok = wait_red(t);
+            if (t - 1 >= z0 - 2) ok = wait_black(t - 1) && ok;
+            ok = wait_in(t + 1) && ok;
+            if (__syncthreads_or(!ok)) {
+                // CTA-uniform: stop the pass.  The copies issued in the
+                // previous step are the only ones that can still be in
+                // flight; wait for them once more before exiting.
+                if (leader) atomicAdd(&g_tb_timeouts, 1u);
+                wait_red(t);
+                if (t - 1 >= z0 - 2) wait_black(t - 1);
+                wait_in(t + 1);
+                return;
+            }
             const int st = (int)(dbase - smc) + (8 + ((t + 1) & 1)) * dslot;
             bp1A = okA && kin(t + 1) ? lds4(st + denA) : zero4;
             bp1B = okB && kin(t + 1) ? lds4(st + denB) : zero4;
@@ -753,6 +778,56 @@ void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r
             k_rbgs_half<<<gr, b, 0, st>>>(g, sp, rhs_r, p_b, p_r, 0);
             k_rbgs_half<<<gr, b, 0, st>>>(g, sp, rhs_b, p_r, p_b, 1);
         }
+    }
+    *launches += 2LL * sweeps;
+}
+
+// Red-black successive over-relaxation: each half sweep moves a cell from
+// its value v to v + omega (g - v), g its Gauss-Seidel update (gs_segment).
+// omega = 1 is Gauss-Seidel; 1 < omega < 2 converges in O(N) sweeps on an
+// N^3 Poisson problem instead of O(N^2) (Young's theory of SOR for
+// consistently ordered matrices).  Not a step of the fluid solve (which is
+// Gauss-Seidel, as the reference's): it computes tightly converged
+// pressures, the targets the warm-start network is trained on.
+__global__ void __launch_bounds__(256)
+k_sor_seg(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float *__restrict__ p_o,
+          float *__restrict__ p_c, int colour, float omega) {
+    const int Wq = g.W >> 3, Wh = g.W >> 1;
+    const int mq = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (mq >= Wq || j >= g.H || k >= g.D) return;
+    const int m0 = mq * 4;
+    const size_t pl = (size_t)Wh * g.H;
+    const size_t q = (size_t)m0 + (size_t)Wh * (size_t)j + (size_t)k * pl;
+    const bool has_ym = j > 0, has_yp = j < g.H - 1, has_zm = k > 0, has_zp = k < g.D - 1;
+    const bool first = m0 == 0, last = m0 + 4 == Wh;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 zm = has_zm ? ld4(p_o + q - pl) : zero4;
+    const float4 zp = has_zp ? ld4(p_o + q + pl) : zero4;
+    const float4 ym = has_ym ? ld4(p_o + q - Wh) : zero4;
+    const float4 yp = has_yp ? ld4(p_o + q + Wh) : zero4;
+    const int s = (j + k + colour) & 1;
+    const float xe = s == 0 ? (first ? 0.0f : __ldg(p_o + q - 1)) : (last ? 0.0f : __ldg(p_o + q + 4));
+    const float4 gs = gs_segment(sp, s, first, last, ld4(rhs_c + q), ld4(p_o + q), xe, ym, yp, zm, zp, has_ym,
+                                 has_yp, has_zm, has_zp);
+    float4 v = *reinterpret_cast<const float4 *>(p_c + q);
+    v.x = fmaf(omega, gs.x - v.x, v.x);
+    v.y = fmaf(omega, gs.y - v.y, v.y);
+    v.z = fmaf(omega, gs.z - v.z, v.z);
+    v.w = fmaf(omega, gs.w - v.w, v.w);
+    *reinterpret_cast<float4 *>(p_c + q) = v;
+}
+
+void launch_sor_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b, float *p_r,
+                       float *p_b, int sweeps, float omega, cudaStream_t st, long long *launches) {
+    const int Wq = g.W >> 3;
+    const int bx = std::min(32, Wq);
+    const dim3 b(bx, std::max(1, 256 / bx), 1);
+    const dim3 gr((Wq + b.x - 1) / b.x, (g.H + b.y - 1) / b.y, g.D);
+    for (int it = 0; it < sweeps; ++it) {
+        k_sor_seg<<<gr, b, 0, st>>>(g, sp, rhs_r, p_b, p_r, 0, omega);
+        k_sor_seg<<<gr, b, 0, st>>>(g, sp, rhs_b, p_r, p_b, 1, omega);
     }
     *launches += 2LL * sweeps;
 }

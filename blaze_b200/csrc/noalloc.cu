@@ -135,6 +135,10 @@ int blz_residual_noalloc(const blz_params *prm, const float *rhs_dev, const floa
         return noalloc_fail(BLZ_ERR_ARG, "grid too large for 32-bit plane indexing");
     if (!(prm->dt > 0.0f) || !(prm->density > 0.0f) || !(prm->dx > 0.0f))
         return noalloc_fail(BLZ_ERR_ARG, "dx, dt and density must be positive");
+    // The same check as blz_create: an unknown boundary mode is an error, not
+    // a silent Neumann solve.
+    if (prm->bc_mode != BLZ_BC_REF_COMPAT && prm->bc_mode != BLZ_BC_FREE_SURFACE)
+        return noalloc_fail(BLZ_ERR_ARG, "bad bc_mode");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return noalloc_fail(BLZ_ERR_CUDA, "cudaGetDevice", e);

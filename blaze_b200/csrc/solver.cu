@@ -781,6 +781,16 @@ int blz_sweeps(blz_solver *s, int n) {
     return rc != BLZ_OK ? rc : check_tb_timeouts(s);
 }
 
+int blz_sor_sweeps(blz_solver *s, int n, float omega) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    if (n < 0) return fail(s, BLZ_ERR_ARG, "negative sweep count");
+    if (!(omega > 0.0f && omega < 2.0f)) return fail(s, BLZ_ERR_ARG, "omega must lie in (0, 2)");
+    if ((s->g.W & 7) != 0) return fail(s, BLZ_ERR_ARG, "SOR sweeps need width %% 8 == 0");
+    launch_sor_sweeps(s->g, solve_params(s->P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, omega, s->st, &s->launches);
+    CKL(s);
+    return BLZ_OK;
+}
+
 int blz_gradient(blz_solver *s) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     const int c = s->cur;

@@ -85,6 +85,10 @@ class FluidSolver:
     def sweeps(self, n):
         check(self._lib.blz_sweeps(self._h, int(n)), self._h)
 
+    def sor_sweeps(self, n, omega):
+        """n red-black SOR sweeps (training targets; not the fluid solve)."""
+        check(self._lib.blz_sor_sweeps(self._h, int(n), C.c_float(omega)), self._h)
+
     def gradient(self):
         check(self._lib.blz_gradient(self._h), self._h)
 

@@ -196,6 +196,14 @@ int  blz_advect(blz_solver *s);                        /* + swap               *
  * gs_solve_kernel, FluidSolver.cu:526-597, run n times).                    */
 int  blz_sweeps(blz_solver *s, int n);
 
+/* n red-black successive over-relaxation sweeps, relaxation omega in (0, 2)
+ * (omega = 1 is Gauss-Seidel; near 2 - 2 pi / N it converges in O(N) sweeps on
+ * an N^3 grid instead of O(N^2)), on the current rhs and p, no residual
+ * checks; width % 8 == 0.  No counterpart in the reference, and not a step of
+ * the fluid solve (which stays Gauss-Seidel): it computes tightly converged
+ * pressures, the targets the learned warm start is trained on.              */
+int  blz_sor_sweeps(blz_solver *s, int n, float omega);
+
 /* FP64 ||b - A p||_2 and ||b||_2 of the current rhs and p.                  */
 int  blz_residual(blz_solver *s, double *res_norm, double *rhs_norm);
 

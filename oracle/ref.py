@@ -35,6 +35,7 @@ def load():
         for name, res, args in [
             ("ref_create", C.c_void_p, [P]), ("ref_destroy", None, [C.c_void_p]),
             ("ref_set_time", None, [C.c_void_p, C.c_int, C.c_float]),
+            ("ref_set_max_iter", None, [C.c_void_p, C.c_int]),
             ("ref_set_particles", C.c_int, [C.c_void_p, F, C.c_int]),
             ("ref_add_source", C.c_int, [C.c_void_p]), ("ref_step", C.c_int, [C.c_void_p]),
             ("ref_project", C.c_int, [C.c_void_p]), ("ref_stage", C.c_int, [C.c_void_p, C.c_int]),
@@ -82,6 +83,10 @@ class RefSolver:
 
     def set_time(self, it, time):
         self.lib.ref_set_time(self.h, it, time)
+
+    def set_max_iter(self, n):
+        """maxIterSolve of the following solves."""
+        self.lib.ref_set_max_iter(self.h, int(n))
 
     def set_particles(self, rec8):
         a = np.ascontiguousarray(rec8, np.float32).reshape(-1, 8)

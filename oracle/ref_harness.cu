@@ -151,6 +151,11 @@ void ref_destroy(void *h) {
     delete r;
 }
 
+// The sweep count of the next solves (FluidSolver::mMaxIter, set from
+// SceneSettings::maxIterSolve by the constructor, FluidSolver.cu:676 and
+// read by project(), 841).
+void ref_set_max_iter(void *h, int n) { ((RefSim *)h)->fs->mMaxIter = n; }
+
 void ref_set_time(void *h, int iter, float time) {
     RefSim *r = (RefSim *)h;
     r->tmr.iter = iter;

@@ -125,5 +125,24 @@ def test_warm_start_and_batch_argument_checks_need_no_gpu(lib):
     assert "null batch" in _err(lib)
 
 
+def test_noalloc_residual_argument_checks_need_no_gpu(lib):
+    """The allocation-free residual refuses what blz_create refuses (an
+    unknown bc_mode, bad dims, non-positive dx/dt/density) and grids deeper
+    than its static scratch, before any device call."""
+    _abi.bind(lib)
+    p = _abi.BlzParams()
+    assert lib.blz_default_params(C.byref(p)) == 0
+    p.width, p.height, p.depth = 16, 16, 16
+    dummy = C.c_void_p(256)                               # never dereferenced: rejected first
+    for bad, words in ((dict(bc_mode=7), "bc_mode"), (dict(bc_mode=-1), "bc_mode"), (dict(width=3), ">= 4"),
+                       (dict(dt=0.0), "positive"), (dict(depth=4097), "4096")):
+        q = p.copy()
+        for k, v in bad.items():
+            setattr(q, k, v)
+        assert lib.blz_residual_noalloc(C.byref(q), dummy, dummy, dummy, None) == _abi.BLZ_ERR_ARG
+        assert words in _err(lib), (bad, _err(lib))
+    assert lib.blz_residual_noalloc(C.byref(p), None, dummy, dummy, None) == _abi.BLZ_ERR_ARG
+
+
 def test_oracle_library_loads(oracle_mod):
     assert oracle_mod.num_threads() >= 1

@@ -1,0 +1,273 @@
+"""Whole-frame parity at the sizes the benchmark configurations name.
+
+The stage tests (test_gpu_parity.py, test_gpu_reference.py) pin every
+kernel on small seeded grids; these run the configurations themselves:
+
+* config 1 (64^3 smoke plume, 2000 particles, epsilon 0.3, beta 1, 80 GS
+  sweeps from p = 0, walls except a free-surface top) against the FP64
+  oracle after 1 and after 10 frames, in target mode (Dirichlet free surface)
+  and in ref-compat mode; and against the reference's own CUDA build (ref-
+  compat mode, the reference's plane schedule) within twice the spread the
+  reference shows between two runs of itself (its Gauss-Seidel races between
+  16x16 blocks: src/FluidSolver.cu:517-599).
+* config 2 (128^3 fire: four discs of 5000 particles, T ~ U[0.5, 1.5], curl
+  noise amplitude 0.5 with a 4-cell period, wind 0.2 cells/step, epsilon 0.5,
+  RBGS to relative residual 1e-4 with a cap of 400 sweeps) against the oracle
+  after 1 and 10 frames; and one frame solved to 1e-4 whose projected
+  velocity has FP64 relative divergence <= 1e-4 (divergence recomputed by
+  the oracle from the GPU's velocity).
+* one 256^3 frame of the benchmark scene (plume family, seed 3) against the
+  oracle: the GPU frame is solved to FP64 relative residual 1e-4, the oracle
+  runs the same frame with the GPU's sweep count, and every field is
+  compared; the oracle also recomputes the residual of the GPU's pressure.
+
+Per-field error = relative L2 and max-abs / max(1, max|oracle|).  Tolerances
+are written beside each comparison; the measured errors are printed (run with
+-s) and, when BLZ_PARITY_REPORT names a file, appended to it as JSON lines.
+Reference: src/FluidSolver.cu:858-955 (step) and 823-856 (project).
+"""
+import json
+import os
+import time
+
+import numpy as np
+import pytest
+
+from blaze_b200 import (BLZ_BC_FREE_SURFACE, BLZ_BC_REF_COMPAT, BLZ_GS_PLANE, BLZ_GS_RB3D, Timer,
+                        family_scene, fire_scene, plume_scene)
+from conftest import max_abs, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("T", "U", "V", "W", "P")
+
+
+def report(name, **kw):
+    line = {"case": name, **kw}
+    print(json.dumps(line))
+    path = os.environ.get("BLZ_PARITY_REPORT")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(line) + "\n")
+
+
+def errors(got, want, fields=FIELDS):
+    out = {}
+    for f in fields:
+        g, r = got[f], want[f]
+        scale = max(1.0, float(np.max(np.abs(r))))
+        out[f] = (rel_l2(g, r), max_abs(g, r) / scale)
+    return out
+
+
+def check(errs, rel, absol, what):
+    for f, (e_rel, e_abs) in errs.items():
+        assert e_rel <= rel and e_abs <= absol, f"{what} {f}: rel_l2 {e_rel:.3e} (<= {rel:g}), " \
+                                                f"scaled max {e_abs:.3e} (<= {absol:g})"
+
+
+def fmt(errs):
+    return {f: [float("%.3g" % a), float("%.3g" % b)] for f, (a, b) in errs.items()}
+
+
+def gpu_frames(scn, parts, frames, checkpoints, fields=FIELDS):
+    """Frames of the CUDA path through the public API; fields at the
+    checkpoints (frame counts) and per-frame solve stats."""
+    from blaze_b200 import FluidSolver
+    tmr = Timer()
+    out, stats = {}, []
+    with FluidSolver(tmr, scn, particles=parts) as s:
+        for n in range(1, frames + 1):
+            s.addSource()
+            stats.append(s.step(tmr.time))
+            tmr.iter += 1
+            tmr.time += scn.dt
+            if n in checkpoints:
+                out[n] = {f: s.get(f) for f in fields}
+    return out, stats
+
+
+def oracle_frames(scn, parts, frames, checkpoints, sweeps=None):
+    """The same frames in the FP64 oracle; `sweeps` (per frame) fixes the
+    sweep count of each solve instead of the scene's residual control."""
+    from oracle import oracle
+    p = scn.to_params()
+    ref = oracle.State(p, np.float64)
+    out, its = {}, []
+    t = 0.0
+    for n in range(1, frames + 1):
+        if sweeps is not None:
+            p.tol, p.max_iter = 0.0, int(sweeps[n - 1])
+            ref.p = p
+        ref.add_source(parts)
+        its.append(ref.step(t)[0])
+        t += scn.dt
+        if n in checkpoints:
+            out[n] = {f: getattr(ref, f).copy() for f in FIELDS}
+    return out, its
+
+
+# ---------------------------------------------------------------------------
+# config 1: 64^3 smoke plume, 80 sweeps from p = 0
+# ---------------------------------------------------------------------------
+def config1(bc, order=BLZ_GS_RB3D, seed=1):
+    scn, parts = plume_scene(n=64, seed=seed, particles=2000)
+    scn.bc_mode, scn.gs_order = bc, order
+    assert scn.maxIterSolve == 80 and scn.reset_pressure == 1 and scn.tol == 0.0
+    return scn, parts
+
+
+@pytest.mark.parametrize("bc", [BLZ_BC_FREE_SURFACE, BLZ_BC_REF_COMPAT], ids=["target", "ref_compat"])
+def test_config1_64_against_oracle(bc):
+    """Per-field error after 1 frame <= 2e-5 relative L2 / 2e-4 scaled max
+    (FP32 against FP64 over 80 sweeps and every stage); after 10 frames
+    <= 2e-3 / 2e-2 (the flow's chaotic growth of rounding differences)."""
+    scn, parts = config1(bc)
+    got, st = gpu_frames(scn, parts, 10, (1, 10))
+    want, its = oracle_frames(scn, parts, 10, (1, 10))
+    assert all(x["iterations"] == 80 for x in st) and its == [80] * 10
+    e1, e10 = errors(got[1], want[1]), errors(got[10], want[10])
+    report(f"config1_64_oracle_bc{bc}", after_1=fmt(e1), after_10=fmt(e10))
+    check(e1, 2e-5, 2e-4, "after 1 frame")
+    check(e10, 2e-3, 2e-2, "after 10 frames")
+
+
+def ref_frames(scn, parts, frames, checkpoints):
+    """The reference's FluidSolver (its own CUDA build) on the same frames,
+    pressure zeroed before every step (the configuration's "from zero
+    pressure"; the reference keeps p between frames, FluidSolver.cu:715)."""
+    from oracle import ref
+    p = scn.to_params()
+    out = {}
+    with ref.RefSolver(p) as r:
+        zero = np.zeros(p.field_shape("P"), np.float32)
+        t = 0.0
+        for n in range(1, frames + 1):
+            r.set_time(n - 1, t)
+            r.set_particles(parts)
+            r.add_source()
+            r.set("P", zero)
+            r.step()
+            t += scn.dt
+            if n in checkpoints:
+                out[n] = {f: r.get(f) for f in FIELDS}
+    return out
+
+
+def test_config1_64_against_reference_build():
+    """Ref-compat mode with the reference's plane schedule (BLZ_GS_PLANE)
+    against two runs of the reference build: the error against the first run
+    must stay within twice the larger of the reference's run-to-run spread and
+    the per-stage floor (1e-5 relative L2, 1e-4 scaled max: fast math and
+    float atomics reorder sums), after 1 and after 10 frames."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference build not present")
+    scn, parts = config1(BLZ_BC_REF_COMPAT, BLZ_GS_PLANE)
+    got, _ = gpu_frames(scn, parts, 10, (1, 10))
+    ra = ref_frames(scn, parts, 10, (1, 10))
+    rb = ref_frames(scn, parts, 10, (1, 10))
+    rows, errs = {}, {}
+    for n in (1, 10):
+        spread = errors(rb[n], ra[n])
+        ours = errors(got[n], ra[n])
+        rows[n] = {"spread": fmt(spread), "ours": fmt(ours)}
+        errs[n] = (spread, ours)
+    report("config1_64_reference", after_1=rows[1], after_10=rows[10])
+    for n, (spread, ours) in errs.items():
+        for f in FIELDS:
+            lim_rel = 2.0 * max(spread[f][0], 1e-5)
+            lim_abs = 2.0 * max(spread[f][1], 1e-4)
+            assert ours[f][0] <= lim_rel and ours[f][1] <= lim_abs, \
+                f"after {n} frames, {f}: ours {ours[f]}, reference spread {spread[f]}"
+
+
+# ---------------------------------------------------------------------------
+# config 2: 128^3 fire and smoke
+# ---------------------------------------------------------------------------
+def config2():
+    scn, parts = fire_scene(n=128, seed=2, per_disc=5000)
+    scn.bc_mode = BLZ_BC_FREE_SURFACE
+    scn.check_every = 20
+    assert scn.maxIterSolve == 400 and scn.tol == 1e-4 and len(parts) == 20000
+    return scn, parts
+
+
+def test_config2_128_against_oracle():
+    """Both sides stop by the same rule (relative residual 1e-4, checked
+    every 20 sweeps, cap 400; from the frame's previous pressure), so they run
+    the same sweeps; per-field error after 1 frame <= 2e-5 / 2e-4, after 10
+    <= 2e-3 / 2e-2."""
+    scn, parts = config2()
+    got, st = gpu_frames(scn, parts, 10, (1, 10))
+    want, its = oracle_frames(scn, parts, 10, (1, 10))
+    assert [x["iterations"] for x in st] == its
+    e1, e10 = errors(got[1], want[1]), errors(got[10], want[10])
+    report("config2_128_oracle", sweeps=its, rel_residual=[float("%.3g" % x["rel_residual"]) for x in st],
+           after_1=fmt(e1), after_10=fmt(e10))
+    check(e1, 2e-5, 2e-4, "after 1 frame")
+    check(e10, 2e-3, 2e-2, "after 10 frames")
+
+
+def divergence_norm(p, U, V, W):
+    """||div||_2 in FP64 of a velocity field (the oracle's divergence stage,
+    FluidSolver.cu:475-515, on FP64 copies)."""
+    from oracle import oracle
+    st = oracle.State(p, np.float64)
+    st.U[...], st.V[...], st.W[...] = U, V, W
+    st.divergence()
+    return float(np.linalg.norm(st.RHS.ravel()))
+
+
+def test_config2_128_projection_divergence():
+    """One frame of config 2 with the sweep cap lifted: the solve reaches
+    relative residual 1e-4, and the projected velocity's FP64 divergence,
+    recomputed by the oracle from the GPU's fields, is <= 1e-4 of the
+    divergence before the projection (FP32 storage of the velocity adds at
+    most 1e-6 here)."""
+    from blaze_b200 import FluidSolver
+    scn, parts = config2()
+    scn.maxIterSolve = 40000
+    p = scn.to_params()
+    tmr = Timer()
+    with FluidSolver(tmr, scn, particles=parts) as s:
+        s.addSource()
+        s.forces(0.0)
+        s.divergence()
+        before = divergence_norm(p, s.get("U"), s.get("V"), s.get("W"))
+        st = s.solve()
+        s.gradient()
+        after = divergence_norm(p, s.get("U"), s.get("V"), s.get("W"))
+    rel = after / before
+    report("config2_128_divergence", sweeps=st["iterations"], rel_residual=st["rel_residual"], rel_divergence=rel)
+    assert st["converged"] and st["rel_residual"] <= 1e-4
+    assert rel <= 1e-4 + 1e-6, rel
+
+
+# ---------------------------------------------------------------------------
+# the 256^3 benchmark scene
+# ---------------------------------------------------------------------------
+def test_bench_scene_256_frame_against_oracle():
+    """Frame 1 of the 256^3 benchmark scene (plume family, seed 3, free-
+    surface top): the GPU solves to FP64 relative residual 1e-4; the oracle
+    runs the same frame with the GPU's sweep count.  Fields within 2e-4
+    relative L2 / 2e-3 scaled max (FP32 against FP64 over thousands of
+    sweeps); the oracle's FP64 residual of the GPU's pressure <= 1e-4."""
+    from oracle import oracle
+    scn, parts = family_scene(n=256, seed=3, tol=1e-4, max_iter=40000, check_every=20)
+    t0 = time.time()
+    got, st = gpu_frames(scn, parts, 1, (1,), fields=FIELDS + ("RHS",))
+    sweeps = st[0]["iterations"]
+    assert st[0]["converged"] and st[0]["rel_residual"] <= 1e-4
+    t1 = time.time()
+    want, _ = oracle_frames(scn, parts, 1, (1,), sweeps=[sweeps])
+    t2 = time.time()
+    # the oracle's FP64 residual of the GPU's pressure and rhs
+    chk = oracle.State(scn.to_params(), np.float64)
+    chk.RHS[...], chk.P[...] = got[1]["RHS"], got[1]["P"]
+    r, b = chk.residual_norms()
+    e = errors(got[1], want[1])
+    report("bench_256_frame1_oracle", sweeps=sweeps, rel_residual=st[0]["rel_residual"], oracle_rel_residual=r / b,
+           errors=fmt(e), gpu_s=round(t1 - t0, 1), oracle_s=round(t2 - t1, 1), oracle_threads=oracle.num_threads())
+    assert r / b <= 1e-4 * (1 + 1e-3)
+    check(e, 2e-4, 2e-3, "256^3 frame 1")
