@@ -24,8 +24,9 @@ BLZ_ADVECT_RK2 = 2
 BLZ_WARM_STEP_RESIDUAL = 0
 BLZ_WARM_STEP_ENERGY = 1
 
-FIELD_T, FIELD_U, FIELD_V, FIELD_W, FIELD_P, FIELD_RHS = range(6)
-FIELD_NAMES = {"T": FIELD_T, "U": FIELD_U, "V": FIELD_V, "W": FIELD_W, "P": FIELD_P, "RHS": FIELD_RHS}
+FIELD_T, FIELD_U, FIELD_V, FIELD_W, FIELD_P, FIELD_RHS, FIELD_DENSITY = range(7)
+FIELD_NAMES = {"T": FIELD_T, "U": FIELD_U, "V": FIELD_V, "W": FIELD_W, "P": FIELD_P, "RHS": FIELD_RHS,
+               "DENSITY": FIELD_DENSITY}
 
 
 class BlzParams(C.Structure):
@@ -45,6 +46,7 @@ class BlzParams(C.Structure):
         ("bc_mode", C.c_int), ("gs_order", C.c_int), ("reset_pressure", C.c_int),
         ("max_particles", C.c_int), ("temporal_block", C.c_int),
         ("device_loop", C.c_int), ("sweep_variant", C.c_int), ("advect_scheme", C.c_int),
+        ("density_field", C.c_int), ("buoyancy_alpha", C.c_float),
     ]
 
     def dims(self):
@@ -56,7 +58,7 @@ class BlzParams(C.Structure):
         if isinstance(f, str):
             f = FIELD_NAMES[f]
         return {FIELD_T: (D, H, W), FIELD_U: (D, H, W + 1), FIELD_V: (D, H + 1, W),
-                FIELD_W: (D + 1, H, W), FIELD_P: (D, H, W), FIELD_RHS: (D, H, W)}[f]
+                FIELD_W: (D + 1, H, W), FIELD_P: (D, H, W), FIELD_RHS: (D, H, W), FIELD_DENSITY: (D, H, W)}[f]
 
     def copy(self):
         p = BlzParams()
@@ -161,6 +163,7 @@ EXPORTS = {
     "blz_destroy": (C.c_int, [C.c_void_p]),
     "blz_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "blz_set_particles": (C.c_int, [C.c_void_p, _P(C.c_float), C.c_int]),
+    "blz_set_particles_ex": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "blz_add_source": (C.c_int, [C.c_void_p]),
     "blz_step": (C.c_int, [C.c_void_p, C.c_float, _P(BlzStepStats)]),
     "blz_forces": (C.c_int, [C.c_void_p, C.c_float]),

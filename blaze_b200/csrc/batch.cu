@@ -87,7 +87,17 @@ struct blz_batch {
     int prologue = 0, body = 0;               // kernels per graph part
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.0f;
+    // learned warm starts (solvers with an attached network): smoothing
+    // sweeps each ran before the batched loop, and the launches one solve
+    // graph replays for them
+    std::vector<int> pre;
+    long long warm_launches = 0;
 };
+
+// Sweep variant of the warm starts' smoothing sweeps inside a batch graph
+// (a segment-kernel shape: every variant gives the same bits, and the
+// solver's own autotuner cannot run inside a capture).
+constexpr int kBatchWarmVariant = 2;
 
 static thread_local std::string g_batch_err;
 
@@ -148,6 +158,15 @@ static int build_graph(blz_batch *b, bool with_stages, cudaGraphExec_t *out, lon
         for (auto *s : b->sims) {
             if ((rc = blz_forces(s, 0.0f)) != BLZ_OK || (rc = blz_divergence(s)) != BLZ_OK) break;
         }
+    if (rc == BLZ_OK) {
+        // Learned warm starts of the solvers that have a network, one after
+        // another on the batch stream (networks of equal dims may be shared).
+        long long w0 = launches_now();
+        for (int i = 0; i < b->n && rc == BLZ_OK; ++i)
+            if (solver_warm(b->sims[i])) rc = solver_warm_start(b->sims[i], kBatchWarmVariant, &b->pre[i]);
+            else b->pre[i] = 0;
+        b->warm_launches = launches_now() - w0;
+    }
     if (rc == BLZ_OK) {
         k_batch_begin<<<(b->n + 255) / 256, 256, 0, b->st>>>(b->d_ctl, b->n);
         launch_batch_check(b->d_sims, b->d_blk0, b->n, b->total_blocks, b->d_ctl, b->partials, 0, b->chunk, b->st);
@@ -278,6 +297,11 @@ static void release(blz_batch *b) {
 static int read_stats(blz_batch *b, blz_step_stats *stats, int loop_ran) {
     BCK(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BatchCtl) * b->n, cudaMemcpyDeviceToHost, b->st));
     BCK(cudaStreamSynchronize(b->st));
+    for (int i = 0; i < b->n; ++i)
+        if (blz_unet *u = solver_warm(b->sims[i])) {
+            const int rc = unet_timeout_flag(u, b->st);
+            if (rc != BLZ_OK) return bfail(rc, "simulation %d: a warm-start completion wait gave up", i);
+        }
     int max_checks = 0;
     for (int i = 0; i < b->n; ++i) max_checks = std::max(max_checks, b->h_ctl[i].checks);
     if (loop_ran) b->launches += b->prologue + (long long)std::max(0, max_checks - 1) * b->body;
@@ -297,8 +321,22 @@ static int read_stats(blz_batch *b, blz_step_stats *stats, int loop_ran) {
         st.residual_checks = c.checks;
         st.sweep_variant = b->kz;
         st.device_loop = 1;
+        if (solver_warm(b->sims[i])) {
+            st.warm_started = 1;
+            st.iterations += b->pre[i];
+        }
     }
     return BLZ_OK;
+}
+
+// The solve-only graph.  Capturing it counts the warm starts' launches into
+// their solvers once; they are counted per replay instead (warm_launches).
+static int build_solve_graph_of(blz_batch *b) {
+    std::vector<long long> before(b->n);
+    for (int i = 0; i < b->n; ++i) before[i] = blz_kernel_launches(b->sims[i]);
+    const int rc = build_graph(b, false, &b->solve_exec, nullptr);
+    for (int i = 0; i < b->n; ++i) solver_add_launches(b->sims[i], before[i] - blz_kernel_launches(b->sims[i]));
+    return rc;
 }
 
 extern "C" {
@@ -308,6 +346,7 @@ int blz_batch_create(blz_solver *const *sims, int n, blz_batch **out) {
     *out = nullptr;
     blz_batch *b = new blz_batch();
     b->n = n;
+    b->pre.assign(n, 0);
     std::vector<BatchSim> h(n);
     std::vector<long long> item0(4 * (size_t)(n + 1));
     std::vector<int> blk0(n + 1);
@@ -408,10 +447,11 @@ int blz_batch_solve(blz_batch *b, blz_step_stats *stats) {
     int rc = tune(b);
     if (rc != BLZ_OK) return rc;
     b->body = 2 * b->chunk + 2 + 1;
-    if (!b->solve_exec && (rc = build_graph(b, false, &b->solve_exec, nullptr)) != BLZ_OK) return rc;
+    if (!b->solve_exec && (rc = build_solve_graph_of(b)) != BLZ_OK) return rc;
     BCK(cudaEventRecord(b->ev0, b->st));
     BCK(cudaGraphLaunch(b->solve_exec, b->st));
     BCK(cudaEventRecord(b->ev1, b->st));
+    b->launches += b->warm_launches;
     return read_stats(b, stats, 1);
 }
 
@@ -444,8 +484,9 @@ int blz_batch_step(blz_batch *b, const float *times, blz_step_stats *stats) {
         b->launches += b->frame_stage_launches[par];
         return read_stats(b, stats, 1);
     }
-    if (!b->solve_exec && (rc = build_graph(b, false, &b->solve_exec, nullptr)) != BLZ_OK) return rc;
+    if (!b->solve_exec && (rc = build_solve_graph_of(b)) != BLZ_OK) return rc;
     BCK(cudaEventRecord(b->ev0, b->st));
+    b->launches += b->warm_launches;
     long long l0 = 0, l1 = 0;
     for (auto *s : b->sims) l0 += blz_kernel_launches(s);
     for (int i = 0; i < b->n; ++i) {

@@ -21,15 +21,13 @@ __device__ __forceinline__ void vel_at(const FieldRef &u, const FieldRef &v, con
 // RK3 (stages at 0.5 dt and 0.75 dt, weights 2/9, 3/9, 4/9;
 // FluidSolver.cu:431-456), forward Euler (392-407) or midpoint RK2
 // (409-429); then the tricubic sample at the departure point.
-template <bool CLAMP, int SCHEME>
-__device__ __forceinline__ float advect_one(const Geom &g, const FieldRef &src, const FieldRef &u,
-                                            const FieldRef &v, const FieldRef &w, int i, int j,
-                                            int k) {
+template <int SCHEME>
+__device__ __forceinline__ void departure(const Geom &g, const FieldRef &src, const FieldRef &u, const FieldRef &v,
+                                          const FieldRef &w, int i, int j, int k, float &qx, float &qy, float &qz) {
     const float r = g.inv_dx, dt = g.dt;
     const float px = ((float)i + src.ox) * g.dx, py = ((float)j + src.oy) * g.dx, pz = ((float)k + src.oz) * g.dx;
     float k1x, k1y, k1z;
     vel_at(u, v, w, r, px, py, pz, k1x, k1y, k1z);
-    float qx, qy, qz;
     if (SCHEME == BLZ_ADVECT_EULER) {
         qx = px - dt * k1x; qy = py - dt * k1y; qz = pz - dt * k1z;
     } else if (SCHEME == BLZ_ADVECT_RK2) {
@@ -47,21 +45,38 @@ __device__ __forceinline__ float advect_one(const Geom &g, const FieldRef &src, 
         qy = py - dt * (a * k1y + b * k2y + c * k3y);
         qz = pz - dt * (a * k1z + b * k2z + c * k3z);
     }
-    return tricubic<CLAMP>(src, r, qx, qy, qz);
 }
 
-template <int SCHEME>
+template <bool CLAMP, int SCHEME>
+__device__ __forceinline__ float advect_one(const Geom &g, const FieldRef &src, const FieldRef &u,
+                                            const FieldRef &v, const FieldRef &w, int i, int j,
+                                            int k) {
+    float qx, qy, qz;
+    departure<SCHEME>(g, src, u, v, w, i, j, k, qx, qy, qz);
+    return tricubic<CLAMP>(src, g.inv_dx, qx, qy, qz);
+}
+
+template <int SCHEME, bool DENS>
 __global__ void __launch_bounds__(256)
 k_advect(Geom g, const float *__restrict__ T, const float *__restrict__ U,
          const float *__restrict__ V, const float *__restrict__ W, float *__restrict__ Tn,
-         float *__restrict__ Un, float *__restrict__ Vn, float *__restrict__ Wn) {
+         float *__restrict__ Un, float *__restrict__ Vn, float *__restrict__ Wn,
+         const float *__restrict__ D, float *__restrict__ Dn) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z * blockDim.z + threadIdx.z;
     if (i > g.W || j > g.H || k > g.D) return;
     const FieldRef u = fU(U, g), v = fV(V, g), w = fW(W, g);
-    if (i < g.W && j < g.H && k < g.D)
-        Tn[lin(i, j, k, g.W, g.H)] = advect_one<true, SCHEME>(g, fT(T, g), u, v, w, i, j, k);
+    if (i < g.W && j < g.H && k < g.D) {
+        if (DENS) {                               // T and the density scalar share one backtrace
+            float qx, qy, qz;
+            departure<SCHEME>(g, fT(T, g), u, v, w, i, j, k, qx, qy, qz);
+            Tn[lin(i, j, k, g.W, g.H)] = tricubic<true>(fT(T, g), g.inv_dx, qx, qy, qz);
+            Dn[lin(i, j, k, g.W, g.H)] = tricubic<true>(fT(D, g), g.inv_dx, qx, qy, qz);
+        } else {
+            Tn[lin(i, j, k, g.W, g.H)] = advect_one<true, SCHEME>(g, fT(T, g), u, v, w, i, j, k);
+        }
+    }
     if (j < g.H && k < g.D)
         Un[lin(i, j, k, g.W + 1, g.H)] = advect_one<false, SCHEME>(g, u, u, v, w, i, j, k);
     if (i < g.W && k < g.D)
@@ -70,14 +85,21 @@ k_advect(Geom g, const float *__restrict__ T, const float *__restrict__ U,
         Wn[lin(i, j, k, g.W, g.H)] = advect_one<false, SCHEME>(g, w, u, v, w, i, j, k);
 }
 
-void launch_advect(const Geom &g, const float *T, const float *U, const float *V, const float *W,
-                   float *Tn, float *Un, float *Vn, float *Wn, cudaStream_t st, int scheme) {
-    if (scheme == BLZ_ADVECT_EULER)
-        k_advect<BLZ_ADVECT_EULER><<<face_grid(g), face_block(), 0, st>>>(g, T, U, V, W, Tn, Un, Vn, Wn);
-    else if (scheme == BLZ_ADVECT_RK2)
-        k_advect<BLZ_ADVECT_RK2><<<face_grid(g), face_block(), 0, st>>>(g, T, U, V, W, Tn, Un, Vn, Wn);
+template <int SCHEME>
+static void launch_scheme(const Geom &g, const float *T, const float *U, const float *V, const float *W, float *Tn,
+                          float *Un, float *Vn, float *Wn, cudaStream_t st, const float *D, float *Dn) {
+    if (D && Dn)
+        k_advect<SCHEME, true><<<face_grid(g), face_block(), 0, st>>>(g, T, U, V, W, Tn, Un, Vn, Wn, D, Dn);
     else
-        k_advect<BLZ_ADVECT_RK3><<<face_grid(g), face_block(), 0, st>>>(g, T, U, V, W, Tn, Un, Vn, Wn);
+        k_advect<SCHEME, false><<<face_grid(g), face_block(), 0, st>>>(g, T, U, V, W, Tn, Un, Vn, Wn, D, Dn);
+}
+
+void launch_advect(const Geom &g, const float *T, const float *U, const float *V, const float *W,
+                   float *Tn, float *Un, float *Vn, float *Wn, cudaStream_t st, int scheme, const float *D,
+                   float *Dn) {
+    if (scheme == BLZ_ADVECT_EULER) launch_scheme<BLZ_ADVECT_EULER>(g, T, U, V, W, Tn, Un, Vn, Wn, st, D, Dn);
+    else if (scheme == BLZ_ADVECT_RK2) launch_scheme<BLZ_ADVECT_RK2>(g, T, U, V, W, Tn, Un, Vn, Wn, st, D, Dn);
+    else launch_scheme<BLZ_ADVECT_RK3>(g, T, U, V, W, Tn, Un, Vn, Wn, st, D, Dn);
 }
 
 } // namespace blz

@@ -117,7 +117,7 @@ __device__ __forceinline__ bool vort_active(const Geom &g, int i, int j, int k) 
 __global__ void k_face_forces(Geom g, float *__restrict__ U, float *__restrict__ V,
                               float *__restrict__ W, const float *__restrict__ T,
                               const float *__restrict__ fx, const float *__restrict__ fy,
-                              const float *__restrict__ fz, ForceParams fp) {
+                              const float *__restrict__ fz, ForceParams fp, const float *__restrict__ Dn) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -154,7 +154,12 @@ __global__ void k_face_forces(Geom g, float *__restrict__ U, float *__restrict__
         if (fp.buoy_on) {
             const float px = ((float)i + 0.5f) * g.dx, py = (float)j * g.dx, pz = ((float)k + 0.5f) * g.dx;
             const float temp = trilinear(fT(T, g), g.inv_dx, px, py, pz);
-            v += g.dt * (fp.beta * temp * fp.grav);
+            if (fp.dens_on) {                         // target mode: the density's weight pulls down
+                const float rho = trilinear(fT(Dn, g), g.inv_dx, px, py, pz);
+                v += g.dt * ((fp.beta * temp - fp.alpha * rho) * fp.grav);
+            } else {
+                v += g.dt * (fp.beta * temp * fp.grav);
+            }
         }
         if (in_slab) v = v * one_m + (fp.wind_amp * nV) * g.dt;
         V[q] = v;
@@ -173,8 +178,8 @@ __global__ void k_face_forces(Geom g, float *__restrict__ U, float *__restrict__
 
 void launch_face_forces(const Geom &g, float *U, float *V, float *W, const float *T,
                         const float *fx, const float *fy, const float *fz, const ForceParams &fp,
-                        cudaStream_t st) {
-    k_face_forces<<<face_grid(g), face_block(), 0, st>>>(g, U, V, W, T, fx, fy, fz, fp);
+                        cudaStream_t st, const float *Dn) {
+    k_face_forces<<<face_grid(g), face_block(), 0, st>>>(g, U, V, W, T, fx, fy, fz, fp, Dn);
 }
 
 __device__ __forceinline__ float fit01(float v, float a, float b, float lo, float hi) {

@@ -16,6 +16,8 @@ struct ForceParams {
     float wind_amp, wind_turb_amp, wind_freq, wind_offset;
     float turb_amp, turb_freq, turb_offset;
     float tr0, tr1, vr0, vr1;
+    int   dens_on;                    // density scalar carried (target mode)
+    float alpha;                      // its buoyancy weight
 };
 
 struct SolveParams {
@@ -33,9 +35,15 @@ dim3 face_grid(const Geom &g);
 // -- sourcing ---------------------------------------------------------------
 // Cells per bin edge of the sourcing gather (one CTA of kSplatBin^3 threads).
 constexpr int kSplatBin = 8;
+// Ints per particle of the per-field index boxes: T, U, V, W and the density
+// scalar, 6 each.
+constexpr int kSplatBoxInts = 30;
+// dens (per kept particle) and Dn: the density scalar, both null when the
+// solver does not carry it.
 void launch_splat_gather(const Geom &g, const float *rec8, const int *boxes, const int *bin_start,
                          const int *bin_list, const int *active, int n_active, int nbx, int nby,
-                         float *T, float *U, float *V, float *W, cudaStream_t st);
+                         float *T, float *U, float *V, float *W, cudaStream_t st, const float *dens = nullptr,
+                         float *Dn = nullptr);
 
 // -- forces -------------------------------------------------------------------
 void launch_scale(float *a, size_t n, float s, cudaStream_t st);
@@ -46,7 +54,7 @@ void launch_vort_force(const Geom &g, const float *U, const float *V, const floa
                        float *fx, float *fy, float *fz, cudaStream_t st);
 void launch_face_forces(const Geom &g, float *U, float *V, float *W, const float *T,
                         const float *fx, const float *fy, const float *fz, const ForceParams &fp,
-                        cudaStream_t st);
+                        cudaStream_t st, const float *Dn = nullptr);
 void launch_turb_noise(const Geom &g, const float *T, const float *U, const float *V,
                        const float *W, float *nU, float *nV, float *nW, const ForceParams &fp,
                        cudaStream_t st);
@@ -180,12 +188,18 @@ int unet_correction(blz_unet *u, const blz_params &P, const float *rhs_r, const 
 int unet_combine(blz_unet *u, const blz_params &P, const float *rhs_r, const float *rhs_b, float *p_r, float *p_b,
                  cudaStream_t st, long long *launches);
 int unet_smoothing(const blz_unet *u);
+int unet_prepare(blz_unet *u, const blz_params &P);
+// The solver's attached network (null if none) and its warm start (solver.cu).
+blz_unet *solver_warm(blz_solver *s);
+int solver_warm_start(blz_solver *s, int variant, int *pre);
 // BLZ_ERR_TIMEOUT if a tensor-core completion wait of the last warm start
 // gave up (synchronises st).
 int unet_timeout_flag(blz_unet *u, cudaStream_t st);
 
 // -- advection ------------------------------------------------------------------
+// D/Dn: the density scalar and its advected copy (null when not carried).
 void launch_advect(const Geom &g, const float *T, const float *U, const float *V, const float *W,
-                   float *Tn, float *Un, float *Vn, float *Wn, cudaStream_t st, int scheme);
+                   float *Tn, float *Un, float *Vn, float *Wn, cudaStream_t st, int scheme,
+                   const float *D = nullptr, float *Dn = nullptr);
 
 } // namespace blz

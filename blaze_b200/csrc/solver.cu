@@ -28,12 +28,14 @@ struct blz_solver {
     bool own_stream = false;
     int device = 0;
     float *T[2]{}, *U[2]{}, *V[2]{}, *W[2]{};
+    float *Dn[2]{};                             // density scalar (density_field only)
     int cur = 0;                                // front = [cur]
     float *p_r = nullptr, *p_b = nullptr, *rhs_r = nullptr, *rhs_b = nullptr;
     float *scratch = nullptr;                   // 6 T-sized arrays (vorticity)
     // sourcing: compacted particle records, per-field index boxes and the
     // 8^3-cell bins (CSR) built on the host by blz_set_particles
     float *parts = nullptr;
+    float *pdens = nullptr;                     // per-particle density (density_field only)
     int *boxes = nullptr, *bin_start = nullptr, *bin_list = nullptr, *active = nullptr;
     int n_parts = 0, cap_parts = 0, cap_list = 0, n_active = 0;
     int nbx = 0, nby = 0, nbz = 0;
@@ -96,6 +98,7 @@ static size_t n_of(const blz_params &P, int f) {
     const size_t W = P.width, H = P.height, D = P.depth;
     switch (f) {
     case BLZ_FIELD_T: case BLZ_FIELD_P: case BLZ_FIELD_RHS: return W * H * D;
+    case BLZ_FIELD_DENSITY: return P.density_field ? W * H * D : 0;
     case BLZ_FIELD_U: return (W + 1) * H * D;
     case BLZ_FIELD_V: return W * (H + 1) * D;
     case BLZ_FIELD_W: return W * H * (D + 1);
@@ -157,7 +160,10 @@ size_t blz_field_size(const blz_solver *s, int field) { return s ? n_of(s->P, fi
 
 static void release(blz_solver *s) {
     if (!s) return;
-    for (int b = 0; b < 2; ++b) { cudaFree(s->T[b]); cudaFree(s->U[b]); cudaFree(s->V[b]); cudaFree(s->W[b]); }
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(s->T[b]); cudaFree(s->U[b]); cudaFree(s->V[b]); cudaFree(s->W[b]); cudaFree(s->Dn[b]);
+    }
+    cudaFree(s->pdens);
     cudaFree(s->p_r); cudaFree(s->p_b); cudaFree(s->rhs_r); cudaFree(s->rhs_b);
     cudaFree(s->scratch);
     cudaFree(s->parts); cudaFree(s->boxes); cudaFree(s->bin_start); cudaFree(s->bin_list); cudaFree(s->active);
@@ -190,6 +196,8 @@ int blz_create(const blz_params *p, blz_solver **out) {
         return fail(nullptr, BLZ_ERR_ARG, "bad gs_order %d", p->gs_order);
     if (p->advect_scheme < BLZ_ADVECT_RK3 || p->advect_scheme > BLZ_ADVECT_RK2)
         return fail(nullptr, BLZ_ERR_ARG, "bad advect_scheme %d", p->advect_scheme);
+    if (p->density_field != 0 && p->density_field != 1)
+        return fail(nullptr, BLZ_ERR_ARG, "density_field must be 0 or 1 (got %d)", p->density_field);
 
     blz_solver *s = new blz_solver();
     s->P = *p;
@@ -213,6 +221,7 @@ int blz_create(const blz_params *p, blz_solver **out) {
         ok = alloc(&s->T[b], nT) && alloc(&s->U[b], nU) && alloc(&s->V[b], nV) && alloc(&s->W[b], nW);
     ok = ok && alloc(&s->p_r, nT / 2) && alloc(&s->p_b, nT / 2) && alloc(&s->rhs_r, nT / 2) && alloc(&s->rhs_b, nT / 2);
     ok = ok && alloc(&s->scratch, 6 * nT);
+    if (p->density_field) ok = ok && alloc(&s->Dn[0], nT) && alloc(&s->Dn[1], nT);
     (void)nU; (void)nV; (void)nW;
     s->cap_parts = std::max(p->max_particles, 1);
     s->nbx = (g.W + kSplatBin) / kSplatBin;          // covers face index W
@@ -220,7 +229,8 @@ int blz_create(const blz_params *p, blz_solver **out) {
     s->nbz = (g.D + kSplatBin) / kSplatBin;
     const size_t nbins = (size_t)s->nbx * s->nby * s->nbz;
     ok = ok && alloc(&s->parts, 8 * (size_t)s->cap_parts);
-    ok = ok && cudaMalloc(&s->boxes, sizeof(int) * 24 * (size_t)s->cap_parts) == cudaSuccess;
+    if (p->density_field) ok = ok && alloc(&s->pdens, (size_t)s->cap_parts);
+    ok = ok && cudaMalloc(&s->boxes, sizeof(int) * kSplatBoxInts * (size_t)s->cap_parts) == cudaSuccess;
     ok = ok && cudaMalloc(&s->bin_start, sizeof(int) * (nbins + 1)) == cudaSuccess;
     ok = ok && cudaMalloc(&s->active, sizeof(int) * nbins) == cudaSuccess;
     s->n_partials = residual_blocks(g);
@@ -266,13 +276,17 @@ int blz_set_stream(blz_solver *s, void *stream) {
 // (Grid.h:319-324) in the same float operations, so host and device agree.
 static inline int trunc_box(float v) { return (int)std::fmin(std::fmax(v, -1.0e9f), 1.0e9f); }
 
-static void particle_boxes(const blz_params &P, const float *r, int out[24]) {
-    const float ox[4] = {0.5f, 0.0f, 0.5f, 0.5f}, oy[4] = {0.5f, 0.5f, 0.0f, 0.5f}, oz[4] = {0.5f, 0.5f, 0.5f, 0.0f};
+// Boxes 0-3: T, U, V, W; box 4: the density scalar (T grid, empty unless
+// the solver carries it), tested with the particle's density `dens`.
+static void particle_boxes(const blz_params &P, const float *r, float dens, int out[kSplatBoxInts]) {
+    const float ox[5] = {0.5f, 0.0f, 0.5f, 0.5f, 0.5f}, oy[5] = {0.5f, 0.5f, 0.0f, 0.5f, 0.5f};
+    const float oz[5] = {0.5f, 0.5f, 0.5f, 0.0f, 0.5f};
     const float dsy = P.domain_max[1] - P.domain_min[1];
     const float radius = r[6] / 2.0f, dx = P.dx;
-    for (int f = 0; f < 4; ++f) {
+    for (int f = 0; f < 5; ++f) {
         int *b = out + 6 * f;
-        const float value = f == 0 ? r[7] : r[2 + f];
+        if (f == 4 && !P.density_field) { for (int a = 0; a < 6; ++a) b[a] = 0; continue; }
+        const float value = f == 0 ? r[7] : f == 4 ? dens : r[2 + f];
         if (!(std::fabs(value) > 1e-5f)) { for (int a = 0; a < 6; ++a) b[a] = 0; continue; }
         const int w = P.width + (f == 1), h = P.height + (f == 2), d = P.depth + (f == 3);
         b[0] = std::max(trunc_box(((r[0] - radius) - P.domain_min[0]) / dx - ox[f]), 0);
@@ -285,26 +299,28 @@ static void particle_boxes(const blz_params &P, const float *r, int out[24]) {
     }
 }
 
-int blz_set_particles(blz_solver *s, const float *rec8, int n) {
-    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+static int set_particles(blz_solver *s, const float *rec8, const float *dens, int n) {
     if (n < 0 || (n > 0 && !rec8)) return fail(s, BLZ_ERR_ARG, "bad particle array (n=%d)", n);
     if (n > s->cap_parts) return fail(s, BLZ_ERR_ARG, "%d particles exceed max_particles=%d", n, s->cap_parts);
     const float half_dx = s->P.dx / 2.0f;
     // Keep the particles whose pscale passes the reference's cut
     // (FluidSolver.cu:83), in order, with their per-field boxes.
-    std::vector<float> keep;
+    std::vector<float> keep, keep_dens;
     std::vector<int> boxes;
     keep.reserve(8 * (size_t)n);
-    boxes.reserve(24 * (size_t)n);
+    boxes.reserve(kSplatBoxInts * (size_t)n);
     for (int p = 0; p < n; ++p) {
         const float *r = rec8 + 8 * (size_t)p;
         for (int c = 0; c < 8; ++c)
             if (!std::isfinite(r[c])) return fail(s, BLZ_ERR_NAN, "particle %d has a non-finite value", p);
+        const float d = dens ? dens[p] : 1.0f;
+        if (!std::isfinite(d)) return fail(s, BLZ_ERR_NAN, "particle %d has a non-finite density", p);
         if (!(r[6] > half_dx)) continue;
-        int b[24];
-        particle_boxes(s->P, r, b);
+        int b[kSplatBoxInts];
+        particle_boxes(s->P, r, d, b);
         keep.insert(keep.end(), r, r + 8);
-        boxes.insert(boxes.end(), b, b + 24);
+        if (s->P.density_field) keep_dens.push_back(d);
+        boxes.insert(boxes.end(), b, b + kSplatBoxInts);
     }
     const int m = (int)(keep.size() / 8);
     // Bin every kept particle into each 8^3 block its boxes overlap (CSR,
@@ -315,7 +331,7 @@ int blz_set_particles(blz_solver *s, const float *rec8, int n) {
     auto bin_range = [&](const int *b, int lo[3], int hi[3]) {
         lo[0] = lo[1] = lo[2] = 1 << 30; hi[0] = hi[1] = hi[2] = -1;
         bool any = false;
-        for (int f = 0; f < 4; ++f) {
+        for (int f = 0; f < 5; ++f) {
             const int *bb = b + 6 * f;
             if (bb[1] <= bb[0]) continue;
             any = true;
@@ -328,7 +344,7 @@ int blz_set_particles(blz_solver *s, const float *rec8, int n) {
     };
     for (int p = 0; p < m; ++p) {
         int lo[3], hi[3];
-        if (!bin_range(&boxes[24 * (size_t)p], lo, hi)) continue;
+        if (!bin_range(&boxes[kSplatBoxInts * (size_t)p], lo, hi)) continue;
         for (int z = lo[2]; z <= hi[2]; ++z)
             for (int y = lo[1]; y <= hi[1]; ++y)
                 for (int x = lo[0]; x <= hi[0]; ++x) count[(size_t)x + nbx * ((size_t)y + (size_t)nby * z) + 1]++;
@@ -338,7 +354,7 @@ int blz_set_particles(blz_solver *s, const float *rec8, int n) {
     std::vector<int> list(std::max(total, 1)), fillpos(count.begin(), count.end() - 1), active;
     for (int p = 0; p < m; ++p) {
         int lo[3], hi[3];
-        if (!bin_range(&boxes[24 * (size_t)p], lo, hi)) continue;
+        if (!bin_range(&boxes[kSplatBoxInts * (size_t)p], lo, hi)) continue;
         for (int z = lo[2]; z <= hi[2]; ++z)
             for (int y = lo[1]; y <= hi[1]; ++y)
                 for (int x = lo[0]; x <= hi[0]; ++x) list[fillpos[(size_t)x + nbx * ((size_t)y + (size_t)nby * z)]++] = p;
@@ -358,6 +374,9 @@ int blz_set_particles(blz_solver *s, const float *rec8, int n) {
     if (m > 0) {
         CK(s, cudaMemcpyAsync(s->parts, keep.data(), sizeof(float) * keep.size(), cudaMemcpyHostToDevice, s->st));
         CK(s, cudaMemcpyAsync(s->boxes, boxes.data(), sizeof(int) * boxes.size(), cudaMemcpyHostToDevice, s->st));
+        if (s->P.density_field)
+            CK(s, cudaMemcpyAsync(s->pdens, keep_dens.data(), sizeof(float) * keep_dens.size(),
+                                  cudaMemcpyHostToDevice, s->st));
     }
     CK(s, cudaMemcpyAsync(s->bin_start, count.data(), sizeof(int) * (nbins + 1), cudaMemcpyHostToDevice, s->st));
     if (total > 0) CK(s, cudaMemcpyAsync(s->bin_list, list.data(), sizeof(int) * (size_t)total, cudaMemcpyHostToDevice, s->st));
@@ -369,12 +388,23 @@ int blz_set_particles(blz_solver *s, const float *rec8, int n) {
     return BLZ_OK;
 }
 
+int blz_set_particles(blz_solver *s, const float *rec8, int n) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    return set_particles(s, rec8, nullptr, n);
+}
+
+int blz_set_particles_ex(blz_solver *s, const float *rec8, const float *density, int n) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    if (!s->P.density_field) return fail(s, BLZ_ERR_STATE, "particle densities need density_field = 1");
+    return set_particles(s, rec8, density, n);
+}
+
 int blz_add_source(blz_solver *s) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     if (s->n_active <= 0) return BLZ_OK;
     const int c = s->cur;
     launch_splat_gather(s->g, s->parts, s->boxes, s->bin_start, s->bin_list, s->active, s->n_active, s->nbx,
-                        s->nby, s->T[c], s->U[c], s->V[c], s->W[c], s->st);
+                        s->nby, s->T[c], s->U[c], s->V[c], s->W[c], s->st, s->pdens, s->Dn[c]);
     CKL(s);
     s->launches += 1;
     return BLZ_OK;
@@ -384,7 +414,9 @@ static ForceParams force_params(const blz_solver *s, float time) {
     const blz_params &P = s->P;
     ForceParams fp{};
     fp.vort_on = std::fabs(P.vorticity_conf) > 0.0f;
-    fp.buoy_on = std::fabs(P.buoyancy) > 0.0f;
+    fp.dens_on = P.density_field != 0;
+    fp.alpha = P.buoyancy_alpha;
+    fp.buoy_on = std::fabs(P.buoyancy) > 0.0f || (fp.dens_on && std::fabs(P.buoyancy_alpha) > 0.0f);
     fp.wind_on = P.wind_amp > 0.0f;
     fp.conf = P.vorticity_conf;
     fp.tiny = 1e-20f * (1.0f / (P.dx * P.dt));
@@ -432,7 +464,7 @@ int blz_forces(blz_solver *s, float time) {
         s->launches += 2;
     }
     if (fp.vort_on || fp.buoy_on || fp.wind_on) {
-        launch_face_forces(g, U, V, W, T, vf, vf + nT, vf + 2 * nT, fp, s->st); CKL(s);
+        launch_face_forces(g, U, V, W, T, vf, vf + nT, vf + 2 * nT, fp, s->st, s->Dn[c]); CKL(s);
         s->launches++;
     }
     if (P.turbulence_amp > 0.0f) {                                              // FluidSolver.cu:925-934
@@ -654,6 +686,37 @@ static int check_tb_timeouts(blz_solver *s) {
     return BLZ_OK;
 }
 
+// The learned warm start of the attached network, ordered on s->st with no
+// host synchronisation (so a batch can capture it in a graph): the network's
+// correction d, `pre` smoothing sweeps of p and of d (sweep variant
+// `variant`, or the solver's autotuned one when < 0), then p += alpha d.
+static int warm_start(blz_solver *s, int variant, int *pre) {
+    const blz_params &P = s->P;
+    float *d_r = nullptr, *d_b = nullptr;
+    const float *z_r = nullptr, *z_b = nullptr;
+    int rc = unet_correction(s->warm, P, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->st, &s->launches, &d_r, &d_b,
+                             &z_r, &z_b);
+    if (rc != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
+    *pre = unet_smoothing(s->warm);
+    if (*pre > 0 && P.gs_order == BLZ_GS_RB3D) {
+        if (variant < 0) {
+            if ((rc = sweeps(s, *pre)) != BLZ_OK) return rc;
+            variant = s->variant;
+        } else {
+            launch_rbgs_sweeps(s->g, solve_params(P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, *pre, s->st,
+                               &s->launches, variant, q_r(s), q_b(s));
+        }
+        launch_rbgs_sweeps(s->g, solve_params(P), z_r, z_b, d_r, d_b, *pre, s->st, &s->launches, variant, q_r(s),
+                           q_b(s));
+        CKL(s);
+    } else {
+        *pre = 0;
+    }
+    rc = unet_combine(s->warm, P, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->st, &s->launches);
+    if (rc != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
+    return BLZ_OK;
+}
+
 int blz_solve(blz_solver *s, blz_step_stats *st) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     const blz_params &P = s->P;
@@ -665,22 +728,8 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
     int pre = 0;                                 // sweeps of p before the solve proper
     if (s->warm) {
         CK(s, cudaEventRecord(s->ev[8], s->st));
-        float *d_r = nullptr, *d_b = nullptr;
-        const float *z_r = nullptr, *z_b = nullptr;
-        int rc = unet_correction(s->warm, P, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->st, &s->launches, &d_r, &d_b,
-                                 &z_r, &z_b);
-        if (rc != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
-        pre = unet_smoothing(s->warm);
-        if (pre > 0 && P.gs_order == BLZ_GS_RB3D) {
-            if ((rc = sweeps(s, pre)) != BLZ_OK) return rc;
-            launch_rbgs_sweeps(s->g, solve_params(P), z_r, z_b, d_r, d_b, pre, s->st, &s->launches,
-                               s->variant, q_r(s), q_b(s));
-            CKL(s);
-        } else {
-            pre = 0;
-        }
-        rc = unet_combine(s->warm, P, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->st, &s->launches);
-        if (rc != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
+        const int rc = warm_start(s, -1, &pre);
+        if (rc != BLZ_OK) return rc;
         CK(s, cudaEventRecord(s->ev[9], s->st));
     }
     int rc = solve_body(s, st);
@@ -708,6 +757,8 @@ int blz_set_warm_start(blz_solver *s, blz_unet *u) {
         if (blz_unet_num_params(u) <= 0) return fail(s, BLZ_ERR_ARG, "bad network");
         if (s->P.width % 8 || s->P.height % 8 || s->P.depth % 8)
             return fail(s, BLZ_ERR_ARG, "the warm start needs grid dims that are multiples of 8");
+        const int rc = unet_prepare(u, s->P);
+        if (rc != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
     }
     s->warm = u;
     return BLZ_OK;
@@ -812,7 +863,7 @@ int blz_advect(blz_solver *s) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     const int c = s->cur, b = c ^ 1;
     launch_advect(s->g, s->T[c], s->U[c], s->V[c], s->W[c], s->T[b], s->U[b], s->V[b], s->W[b], s->st,
-                  s->P.advect_scheme);
+                  s->P.advect_scheme, s->Dn[c], s->Dn[b]);
     CKL(s);
     s->launches++;
     s->cur = b;                                                                 // swap_grids_kernel
@@ -875,6 +926,7 @@ static float *front_of(blz_solver *s, int f) {
     case BLZ_FIELD_U: return s->U[c];
     case BLZ_FIELD_V: return s->V[c];
     case BLZ_FIELD_W: return s->W[c];
+    case BLZ_FIELD_DENSITY: return s->Dn[c];
     default: return nullptr;
     }
 }
@@ -920,6 +972,8 @@ int blz_set_field(blz_solver *s, int f, const float *src, int on_device) {
 } // extern "C"
 
 namespace blz {
+blz_unet *solver_warm(blz_solver *s) { return s->warm; }
+int solver_warm_start(blz_solver *s, int variant, int *pre) { return warm_start(s, variant, pre); }
 // What the batch (batch.cu) needs of a solver: its solve arrays and
 // parameters, and the front/back flip a replayed frame graph implies.
 void solver_batch_view(blz_solver *s, BatchSim *out, const blz_params **P) {

@@ -1036,6 +1036,18 @@ namespace blz {
 // zero right-hand side: Gauss-Seidel is affine, so this is exactly smoothing
 // p + alpha d for every alpha at once); unet_combine picks alpha minimising the
 // residual norm of p + alpha d and adds alpha d.
+// Allocates the correction buffers once (at attachment, so that a warm start
+// captured into a graph allocates nothing).
+int unet_prepare(blz_unet *u, const blz_params &P) {
+    (void)P;
+    if (u->dpk) return BLZ_OK;
+    const LDims &d = u->L[0];
+    const long long n = (long long)d.W * d.H * d.D;
+    UCK(cudaMalloc(&u->dpk, sizeof(float) * 2 * n));         // d (n) then a zero right-hand side (n)
+    UCK(cudaMemset(u->dpk, 0, sizeof(float) * 2 * n));
+    return BLZ_OK;
+}
+
 int unet_correction(blz_unet *u, const blz_params &P, const float *rhs_r, const float *rhs_b, const float *p_r,
                     const float *p_b, cudaStream_t st, long long *launches, float **d_r, float **d_b,
                     const float **z_r, const float **z_b) {
@@ -1051,10 +1063,7 @@ int unet_correction(blz_unet *u, const blz_params &P, const float *rhs_r, const 
     if ((rc = forward_core(u, st)) != BLZ_OK) return rc;
     const LDims &d = u->L[0];
     const long long n = (long long)d.W * d.H * d.D;
-    if (!u->dpk) {
-        UCK(cudaMalloc(&u->dpk, sizeof(float) * 2 * n));     // d (n) then a zero right-hand side (n)
-        UCK(cudaMemset(u->dpk, 0, sizeof(float) * 2 * n));
-    }
+    if ((rc = unet_prepare(u, P)) != BLZ_OK) return rc;
     float *dr = u->dpk, *db = u->dpk + n / 2;
     k_unet_delta<<<nblk(n, 256), 256, 0, st>>>(u->d0b.base(), d, u->params + u->w_off[HEAD], u->scales, dr, db);
     ++u->launches;

@@ -85,6 +85,10 @@ class SceneSettings:
     device_loop: int = 1
     sweep_variant: int = -1
     advect_scheme: int = _abi.BLZ_ADVECT_RK3
+    # Target mode: a smoke density scalar with buoyancy weight alpha
+    # (V += dt (beta T - alpha rho) g); the reference has neither.
+    density_field: int = 0
+    buoyancy_alpha: float = 0.0
     extra: dict = field(default_factory=dict)
 
     def to_params(self):
@@ -106,6 +110,7 @@ class SceneSettings:
         p.max_particles, p.temporal_block = self.sourceMaxParticleCount, self.temporal_block
         p.device_loop, p.sweep_variant = self.device_loop, self.sweep_variant
         p.advect_scheme = self.advect_scheme
+        p.density_field, p.buoyancy_alpha = int(self.density_field), float(self.buoyancy_alpha)
         return p
 
 
@@ -180,24 +185,31 @@ def disc_particles(rng, s, centre_cells, radius_cells, count, temp=(1.0, 1.0), p
     return out
 
 
-def plume_scene(n=64, seed=1, particles=2000):
+def plume_scene(n=64, seed=1, particles=2000, alpha=None):
     """Smoke plume: n^3, dx = 1/n, dt = 1/24, one ball of radius 6 cells at
     cells (n/2, n/8, n/2) (y up), T = 1, beta = 1, epsilon = 0.3, no noise,
-    walls except a free-surface top, 80 sweeps from p = 0."""
+    walls except a free-surface top, 80 sweeps from p = 0.  alpha (target
+    mode): carry the density scalar (density 1 per particle) with buoyancy
+    weight alpha (the configuration's 0.05)."""
     s = SceneSettings(gridRes=(n, n, n), dx=1.0 / n, dt=1.0 / 24,
                       closedBounds=(1, 1, 1, 0, 1, 1), maxIterSolve=80, buoyancy=1.0,
                       vorticityConf=0.3, reset_pressure=1)
+    if alpha is not None:
+        s.density_field, s.buoyancy_alpha = 1, float(alpha)
     rng = PCG32(seed)
     parts = sphere_particles(rng, s, (n / 2, n / 8, n / 2), 6.0, particles)
     s.sourceMaxParticleCount = max(particles, 1)
     return s, parts
 
 
-def fire_scene(n=128, seed=2, per_disc=5000):
+def fire_scene(n=128, seed=2, per_disc=5000, density_field=0, alpha=0.0):
     """Fire and smoke: n^3, four discs of radius 8 cells on the floor with
     5000 particles each, T ~ U[0.5, 1.5], pseudo-curl noise amplitude 0.5 with
     a 4-cell period, wind 0.2 cells/step along +x, epsilon = 0.5, walls except
-    the top, RBGS to relative residual 1e-4 with a cap of 400 sweeps."""
+    the top, RBGS to relative residual 1e-4 with a cap of 400 sweeps.  Every
+    particle's density ~ U[0.2, 1.0] (its own PCG32 stream, so the records do
+    not depend on it) is in extra["particle_density"]; density_field carries
+    it as the density scalar (target mode) with buoyancy weight alpha."""
     s = SceneSettings(gridRes=(n, n, n), dx=1.0 / n, dt=1.0 / 24,
                       closedBounds=(1, 1, 1, 0, 1, 1), maxIterSolve=400, tol=1e-4,
                       buoyancy=1.0, vorticityConf=0.5, turbulence_amp=0.5, turbulence_scale=4.0,
@@ -209,6 +221,9 @@ def fire_scene(n=128, seed=2, per_disc=5000):
         parts.append(disc_particles(rng, s, c, 8.0, per_disc, temp=(0.5, 1.5)))
     parts = np.concatenate(parts)
     s.sourceMaxParticleCount = len(parts)
+    drng = PCG32(seed, seq=0x5EED0D3E5)
+    s.extra = {"particle_density": np.array([drng.uniform(0.2, 1.0) for _ in range(len(parts))], np.float32)}
+    s.density_field, s.buoyancy_alpha = int(density_field), float(alpha)
     return s, parts
 
 

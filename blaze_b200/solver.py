@@ -20,7 +20,7 @@ from ._lib import BlazeError, check, load
 
 
 class FluidSolver:
-    def __init__(self, tmr, scn, particles=None, stream=None):
+    def __init__(self, tmr, scn, particles=None, stream=None, density=None):
         self._lib = load()
         self.tmr = tmr
         self.scn = scn
@@ -32,7 +32,7 @@ class FluidSolver:
         if stream is not None:
             check(self._lib.blz_set_stream(self._h, C.c_void_p(stream)), self._h)
         if particles is not None:
-            self.setParticles(particles)
+            self.setParticles(particles, density)
 
     # -- lifetime -------------------------------------------------------------
     def close(self):
@@ -53,9 +53,23 @@ class FluidSolver:
         self.close()
 
     # -- reference interface ----------------------------------------------------
-    def setParticles(self, rec8):
+    def setParticles(self, rec8, density=None):
+        """Particle records (8 floats each).  With the density scalar on
+        (scn.density_field), `density` gives each particle's density (default:
+        the scene's extra["particle_density"], else 1 per particle)."""
         a = np.ascontiguousarray(rec8, dtype=np.float32).reshape(-1, 8)
-        check(self._lib.blz_set_particles(self._h, a.ctypes.data_as(C.POINTER(C.c_float)), len(a)), self._h)
+        if not self.params.density_field:
+            check(self._lib.blz_set_particles(self._h, a.ctypes.data_as(C.POINTER(C.c_float)), len(a)), self._h)
+            return
+        if density is None:
+            density = getattr(self.scn, "extra", {}).get("particle_density")
+        d = None
+        if density is not None:
+            d = np.ascontiguousarray(density, dtype=np.float32).reshape(-1)
+            if len(d) != len(a):
+                raise BlazeError(_abi.BLZ_ERR_ARG, f"{len(d)} densities for {len(a)} particles")
+        check(self._lib.blz_set_particles_ex(self._h, a.ctypes.data_as(C.c_void_p),
+                                             None if d is None else d.ctypes.data_as(C.c_void_p), len(a)), self._h)
 
     def addSource(self):
         check(self._lib.blz_add_source(self._h), self._h)

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define BLZ_ABI_VERSION 1
+#define BLZ_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define BLZ_OK            0
@@ -76,6 +76,7 @@ extern "C" {
 #define BLZ_FIELD_W    3
 #define BLZ_FIELD_P    4   /* pressure, T dims (stored colour packed inside) */
 #define BLZ_FIELD_RHS  5   /* -div/dx with the wall fixes, T dims            */
+#define BLZ_FIELD_DENSITY 6 /* smoke density scalar, T dims (density_field)  */
 
 /* ---- solver parameters (SceneSettings' solver subset + new switches) ---- */
 typedef struct blz_params {
@@ -124,6 +125,13 @@ typedef struct blz_params {
     int    sweep_variant;         /* -1: autotune the sweep launch shape per
                                      grid size (first solve); >= 0: force one */
     int    advect_scheme;         /* BLZ_ADVECT_*: backtrace integrator       */
+    /* Target mode only (no counterpart in the reference, whose buoyancy is
+     * beta * T alone, FluidSolver.cu:142-156): a smoke density scalar on the
+     * T grid, splatted from the particles like T, advected like T (tricubic,
+     * clamped at 0), whose weight pulls down:
+     * V += dt * (beta * T - buoyancy_alpha * rho) * g.                       */
+    int    density_field;         /* 1: carry the density scalar            */
+    float  buoyancy_alpha;        /* alpha (density)                         */
 } blz_params;
 
 /* Backtrace integrators (FluidSolver.cu:392-456; the reference's step uses
@@ -172,6 +180,13 @@ int  blz_set_stream(blz_solver *s, void *cuda_stream);
 /* Particle upload (Parser::sourceParticleParse, Parser.h:174-210): n records
  * of 8 host floats {pos.xyz (world), vel.xyz, pscale, temperature}.         */
 int  blz_set_particles(blz_solver *s, const float *rec8, int n);
+
+/* blz_set_particles with a density per particle (target mode): density[p]
+ * is splatted into the density scalar by the same cubic pulse as the
+ * temperature (blz_set_particles gives every particle density 1).  density
+ * may be NULL (all 1).  No counterpart in the reference (its records carry
+ * no density); BLZ_ERR_STATE unless the solver has density_field set.     */
+int  blz_set_particles_ex(blz_solver *s, const float *rec8, const float *density, int n);
 
 /* The device half of FluidSolver::addSource (FluidSolver.cu:796-816):
  * cubic-pulse splat of the uploaded particles, then front = splat wherever

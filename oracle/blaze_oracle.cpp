@@ -259,11 +259,17 @@ static void sphere_to_grid(const Geo<R> &g, const Field<R> &f, R px, R py, R pz,
             }
 }
 
+// Dn (may be null): the density scalar of target mode (no counterpart in the
+// reference), on the T grid, splatted like T with each particle's density
+// dens[p] (null: 1 per particle) under the same |value| > 1e-5 rules.
 template <class R>
-void add_source(const blz_params *P, const float *rec, int n, R *T, R *U, R *V, R *W) {
+void add_source(const blz_params *P, const float *rec, int n, R *T, R *U, R *V, R *W, const float *dens = nullptr,
+                R *Dn = nullptr) {
     Geo<R> g(P);
     std::vector<R> bT(g.nT(), R(0)), bU(g.nU(), R(0)), bV(g.nV(), R(0)), bW(g.nW(), R(0));
+    std::vector<R> bD(Dn ? g.nT() : 0, R(0));
     Field<R> fT = g.T(bT.data()), fU = g.U(bU.data()), fV = g.V(bV.data()), fW = g.Wf(bW.data());
+    Field<R> fD = g.T(Dn ? bD.data() : bT.data());
     const R half_dx = (R)(P->dx / 2.0f);
     for (int p = 0; p < n; ++p) {
         const float *r = rec + 8 * (size_t)p;
@@ -273,12 +279,17 @@ void add_source(const blz_params *P, const float *rec, int n, R *T, R *U, R *V, 
         if (std::fabs(r[3]) > 1e-5) sphere_to_grid(g, fU, px, py, pz, ps, (R)r[3]);
         if (std::fabs(r[4]) > 1e-5) sphere_to_grid(g, fV, px, py, pz, ps, (R)r[4]);
         if (std::fabs(r[5]) > 1e-5) sphere_to_grid(g, fW, px, py, pz, ps, (R)r[5]);
+        if (Dn) {
+            const float d = dens ? dens[p] : 1.0f;
+            if (std::fabs(d) > 1e-5) sphere_to_grid(g, fD, px, py, pz, ps, (R)d);
+        }
     }
     auto apply = [](R *front, const std::vector<R> &back) {
         for (size_t i = 0; i < back.size(); ++i)
             if (std::fabs(back[i]) > R(1e-5)) front[i] = back[i];
     };
     apply(T, bT); apply(U, bU); apply(V, bV); apply(W, bW);
+    if (Dn) apply(Dn, bD);
 }
 
 // ---------------------------------------------------------------------------
@@ -383,9 +394,12 @@ static void vorticity(const Geo<R> &g, R *U, R *V, R *W, R conf) {
 }
 
 // add_buoyancy_kernel, FluidSolver.cu:142-156: V += dt*beta*T_lin*g at V faces.
+// With the density scalar of target mode (Dn, no reference counterpart):
+// V += dt*(beta*T_lin - alpha*rho_lin)*g, the smoke's weight pulling down.
 template <class R>
-static void buoyancy(const Geo<R> &g, const R *T, R *V, R beta, R grav) {
+static void buoyancy(const Geo<R> &g, const R *T, R *V, R beta, R grav, const R *Dn = nullptr, R alpha = R(0)) {
     Field<R> fT = g.T(const_cast<R *>(T)), fV = g.V(V);
+    Field<R> fD = g.T(const_cast<R *>(Dn ? Dn : T));
     const R dx = g.dx, dt = g.dt;
 #pragma omp parallel for schedule(static)
     for (int k = 0; k < g.D; ++k)
@@ -393,7 +407,12 @@ static void buoyancy(const Geo<R> &g, const R *T, R *V, R beta, R grav) {
             for (int i = 0; i < g.W; ++i) {
                 const R px = (R(i) + R(0.5)) * dx, py = R(j) * dx, pz = (R(k) + R(0.5)) * dx;
                 const R temp = trilinear(fT, dx, px, py, pz);
-                fV.at(i, j, k) += dt * (beta * temp * grav);
+                if (Dn) {
+                    const R rho = trilinear(fD, dx, px, py, pz);
+                    fV.at(i, j, k) += dt * ((beta * temp - alpha * rho) * grav);
+                } else {
+                    fV.at(i, j, k) += dt * (beta * temp * grav);
+                }
             }
 }
 
@@ -533,7 +552,7 @@ static void turbulence(const Geo<R> &g, const R *T, R *U, R *V, R *W, float time
 }
 
 template <class R>
-void forces(const blz_params *P, float time, R *T, R *U, R *V, R *W) {
+void forces(const blz_params *P, float time, R *T, R *U, R *V, R *W, const R *Dn = nullptr) {
     Geo<R> g(P);
     if (std::fabs(P->cooling_rate) > 0.0f) scale_all(T, g.nT(), R(1) - g.dt * (R)P->cooling_rate);
     if (P->drag > 0.0f) {
@@ -541,7 +560,10 @@ void forces(const blz_params *P, float time, R *T, R *U, R *V, R *W) {
         scale_all(U, g.nU(), s); scale_all(V, g.nV(), s); scale_all(W, g.nW(), s);
     }
     if (std::fabs(P->vorticity_conf) > 0.0f) vorticity(g, U, V, W, (R)P->vorticity_conf);
-    if (std::fabs(P->buoyancy) > 0.0f) buoyancy(g, T, V, (R)P->buoyancy, (R)P->gravity);
+    if (Dn && (std::fabs(P->buoyancy) > 0.0f || std::fabs(P->buoyancy_alpha) > 0.0f))
+        buoyancy(g, T, V, (R)P->buoyancy, (R)P->gravity, Dn, (R)P->buoyancy_alpha);
+    else if (std::fabs(P->buoyancy) > 0.0f)
+        buoyancy(g, T, V, (R)P->buoyancy, (R)P->gravity);
     if (P->wind_amp > 0.0f) wind(g, U, V, W, time);
     if (P->turbulence_amp > 0.0f) turbulence(g, T, U, V, W, time);
 }
@@ -770,10 +792,15 @@ static void advect_field(const Geo<R> &g, const Field<R> &U, const Field<R> &V, 
 }
 
 template <class R>
-void advect(const blz_params *P, R *T, R *U, R *V, R *W) {
+void advect(const blz_params *P, R *T, R *U, R *V, R *W, R *Dn = nullptr) {
     Geo<R> g(P);
     std::vector<R> nT(g.nT()), nU(g.nU()), nV(g.nV()), nW(g.nW());
     Field<R> fT = g.T(T), fU = g.U(U), fV = g.V(V), fW = g.Wf(W);
+    if (Dn) {                                     // the density scalar, clamped like T
+        std::vector<R> nD(g.nT());
+        advect_field(g, fU, fV, fW, g.T(Dn), nD.data(), true);
+        std::copy(nD.begin(), nD.end(), Dn);
+    }
     advect_field(g, fU, fV, fW, fT, nT.data(), true);
     advect_field(g, fU, fV, fW, fU, nU.data(), false);
     advect_field(g, fU, fV, fW, fV, nV.data(), false);
@@ -785,12 +812,12 @@ void advect(const blz_params *P, R *T, R *U, R *V, R *W) {
 // FluidSolver::step, FluidSolver.cu:858-955.
 template <class R>
 void step(const blz_params *P, float time, R *T, R *U, R *V, R *W, R *p, R *rhs,
-          int *iters, double *res, double *bn) {
-    forces(P, time, T, U, V, W);
+          int *iters, double *res, double *bn, R *Dn = nullptr) {
+    forces(P, time, T, U, V, W, Dn);
     divergence(P, U, V, W, rhs);
     solve(P, rhs, p, iters, res, bn);
     gradient(P, p, U, V, W);
-    advect(P, T, U, V, W);
+    advect(P, T, U, V, W, Dn);
 }
 
 } // namespace orc
@@ -806,9 +833,10 @@ float orc_perlin(float x, float y, float z, float scale, int seed) {
 
 #define ORC_EXPORT_ALL(SUF, R)                                                              \
     void orc_add_source_##SUF(const blz_params *P, const float *rec, int n, R *T, R *U,       \
-                              R *V, R *W) { orc::add_source<R>(P, rec, n, T, U, V, W); }     \
-    void orc_forces_##SUF(const blz_params *P, float time, R *T, R *U, R *V, R *W) {         \
-        orc::forces<R>(P, time, T, U, V, W); }                                               \
+                              R *V, R *W, const float *dens, R *Dn) {                        \
+        orc::add_source<R>(P, rec, n, T, U, V, W, dens, Dn); }                               \
+    void orc_forces_##SUF(const blz_params *P, float time, R *T, R *U, R *V, R *W,           \
+                          const R *Dn) { orc::forces<R>(P, time, T, U, V, W, Dn); }          \
     void orc_divergence_##SUF(const blz_params *P, const R *U, const R *V, const R *W,       \
                               R *rhs) { orc::divergence<R>(P, U, V, W, rhs); }               \
     void orc_gs_sweeps_##SUF(const blz_params *P, const R *rhs, R *p, int n) {               \
@@ -819,11 +847,11 @@ float orc_perlin(float x, float y, float z, float scale, int seed) {
                             double *bn) { orc::residual<R>(P, rhs, p, res, bn); }            \
     void orc_gradient_##SUF(const blz_params *P, const R *p, R *U, R *V, R *W) {             \
         orc::gradient<R>(P, p, U, V, W); }                                                   \
-    void orc_advect_##SUF(const blz_params *P, R *T, R *U, R *V, R *W) {                     \
-        orc::advect<R>(P, T, U, V, W); }                                                     \
+    void orc_advect_##SUF(const blz_params *P, R *T, R *U, R *V, R *W, R *Dn) {              \
+        orc::advect<R>(P, T, U, V, W, Dn); }                                                 \
     void orc_step_##SUF(const blz_params *P, float time, R *T, R *U, R *V, R *W, R *p,       \
-                        R *rhs, int *it, double *res, double *bn) {                          \
-        orc::step<R>(P, time, T, U, V, W, p, rhs, it, res, bn); }
+                        R *rhs, int *it, double *res, double *bn, R *Dn) {                   \
+        orc::step<R>(P, time, T, U, V, W, p, rhs, it, res, bn, Dn); }
 
 ORC_EXPORT_ALL(f64, double)
 ORC_EXPORT_ALL(f32, float)

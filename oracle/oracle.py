@@ -37,16 +37,16 @@ def load():
         for suf, ct in (("f64", C.c_double), ("f32", C.c_float)):
             R = C.POINTER(ct)
             sig = {
-                "add_source": [P, C.POINTER(C.c_float), C.c_int, R, R, R, R],
-                "forces": [P, C.c_float, R, R, R, R],
+                "add_source": [P, C.POINTER(C.c_float), C.c_int, R, R, R, R, C.POINTER(C.c_float), R],
+                "forces": [P, C.c_float, R, R, R, R, R],
                 "divergence": [P, R, R, R, R],
                 "gs_sweeps": [P, R, R, C.c_int],
                 "solve": [P, R, R, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)],
                 "residual": [P, R, R, C.POINTER(C.c_double), C.POINTER(C.c_double)],
                 "gradient": [P, R, R, R, R],
-                "advect": [P, R, R, R, R],
+                "advect": [P, R, R, R, R, R],
                 "step": [P, C.c_float, R, R, R, R, R, R, C.POINTER(C.c_int), C.POINTER(C.c_double),
-                         C.POINTER(C.c_double)],
+                         C.POINTER(C.c_double), R],
             }
             for name, args in sig.items():
                 fn = getattr(lib, f"orc_{name}_{suf}")
@@ -87,10 +87,18 @@ class State:
         z = lambda f: np.zeros(params.field_shape(f), self.dtype)
         self.T, self.U, self.V, self.W = z("T"), z("U"), z("V"), z("W")
         self.P, self.RHS = z("P"), z("RHS")
+        # the density scalar of target mode (params.density_field)
+        self.DENSITY = z("DENSITY") if params.density_field else None
         self.iterations, self.residual, self.rhs_norm = 0, 0.0, 0.0
 
     def fields(self):
-        return {"T": self.T, "U": self.U, "V": self.V, "W": self.W, "P": self.P, "RHS": self.RHS}
+        out = {"T": self.T, "U": self.U, "V": self.V, "W": self.W, "P": self.P, "RHS": self.RHS}
+        if self.DENSITY is not None:
+            out["DENSITY"] = self.DENSITY
+        return out
+
+    def _dn(self):
+        return None if self.DENSITY is None else _ptr(self.DENSITY)
 
     def load(self, **arrays):
         for k, v in arrays.items():
@@ -99,13 +107,17 @@ class State:
     def _fn(self, name):
         return getattr(load(), f"orc_{name}_{_suf(self.dtype)}")
 
-    def add_source(self, rec8):
+    def add_source(self, rec8, density=None):
+        """density: per-particle density for the density scalar (None: 1)."""
         a = np.ascontiguousarray(rec8, np.float32).reshape(-1, 8)
+        d = None if density is None else np.ascontiguousarray(density, np.float32).reshape(-1)
         self._fn("add_source")(C.byref(self.p), a.ctypes.data_as(C.POINTER(C.c_float)), len(a),
-                               _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W))
+                               _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W),
+                               None if d is None else d.ctypes.data_as(C.POINTER(C.c_float)), self._dn())
 
     def forces(self, time):
-        self._fn("forces")(C.byref(self.p), time, _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W))
+        self._fn("forces")(C.byref(self.p), time, _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W),
+                           self._dn())
 
     def divergence(self):
         self._fn("divergence")(C.byref(self.p), _ptr(self.U), _ptr(self.V), _ptr(self.W), _ptr(self.RHS))
@@ -128,7 +140,7 @@ class State:
         self._fn("gradient")(C.byref(self.p), _ptr(self.P), _ptr(self.U), _ptr(self.V), _ptr(self.W))
 
     def advect(self):
-        self._fn("advect")(C.byref(self.p), _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W))
+        self._fn("advect")(C.byref(self.p), _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W), self._dn())
 
     def project(self):
         self.divergence()
@@ -139,7 +151,7 @@ class State:
     def step(self, time):
         it, r, b = C.c_int(), C.c_double(), C.c_double()
         self._fn("step")(C.byref(self.p), time, _ptr(self.T), _ptr(self.U), _ptr(self.V), _ptr(self.W),
-                         _ptr(self.P), _ptr(self.RHS), C.byref(it), C.byref(r), C.byref(b))
+                         _ptr(self.P), _ptr(self.RHS), C.byref(it), C.byref(r), C.byref(b), self._dn())
         self.iterations, self.residual, self.rhs_norm = it.value, r.value, b.value
         return it.value, r.value, b.value
 

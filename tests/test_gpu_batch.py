@@ -88,3 +88,55 @@ def test_batch_rejects_mismatched_solvers():
     assert lib.blz_batch_create(arr2, 1, C.byref(h)) == -2          # width % 8 != 0
     for s in sims + [s2]:
         s.close()
+
+
+@pytest.mark.parametrize("turbulence", [False, True], ids=["frame-graph", "direct"])
+def test_batch_with_warm_start_equals_single(turbulence):
+    """Solvers with an attached network (one per grid size, shared by the
+    solvers of that size) warm-start inside the batch exactly as alone: same
+    sweeps, residuals and fields, bit for bit."""
+    from blaze_b200.batch import Batch
+    from blaze_b200.unet import WarmStartUNet, init_params
+    frames = 3
+    params = init_params(2)
+    nets = {}
+
+    def net_for(dims):
+        if dims not in nets:
+            nets[dims] = WarmStartUNet(dims, params, kappa=0.5)
+            nets[dims].set_smoothing(8)
+        return nets[dims]
+
+    runs = []
+    for batched in (False, True):
+        sims = _make(_scenes(turbulence))
+        for s in sims:
+            s.set_warm_start(net_for(tuple(s.scn.gridRes)))
+        stats = []
+        if batched:
+            batch = Batch(sims)
+            for f in range(frames):
+                batch.add_source()
+                stats.append(batch.step([f / 24.0] * len(sims)))
+            batch.close()
+        else:
+            for f in range(frames):
+                row = []
+                for s in sims:
+                    s.addSource()
+                    row.append(s.step(f / 24.0))
+                stats.append(row)
+        runs.append((stats, [{k: s.get(k) for k in FIELDS} for s in sims]))
+        for s in sims:
+            s.close()
+    (sa, fa), (sb, fb) = runs
+    for f in range(frames):
+        for i in range(len(sa[f])):
+            a, b = sa[f][i], sb[f][i]
+            assert a["warm_started"] == 1 and b["warm_started"] == 1
+            assert a["iterations"] == b["iterations"] and a["residual"] == b["residual"], (f, i, a, b)
+    for i in range(len(fa)):
+        for name in FIELDS:
+            assert np.array_equal(fa[i][name], fb[i][name]), (i, name)
+    for n in nets.values():
+        n.close()

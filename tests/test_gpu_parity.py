@@ -322,3 +322,80 @@ def test_temporal_blocking_equals_plain_sweeps(dims, bc):
     assert np.isfinite(out[0]).all() and np.abs(out[0]).max() > 0
     for v in (6, 7, 8, 9):
         np.testing.assert_array_equal(out[v], out[0], err_msg=f"variant {v}")
+
+
+# ---------------------------------------------------------------------------
+# Target mode's density scalar (no reference counterpart): sourcing,
+# buoyancy V += dt (beta T - alpha rho) g and advection against the oracle.
+# ---------------------------------------------------------------------------
+def dens_pair(scn, seed):
+    """pair() plus a random density field on both sides."""
+    gpu, ref = pair(scn, seed)
+    rng = np.random.default_rng(seed + 1000)
+    d = rng.uniform(0.0, 1.5, ref.DENSITY.shape).astype(np.float32)
+    gpu.set("DENSITY", d)
+    ref.DENSITY[...] = d
+    return gpu, ref
+
+
+def test_density_source_splat():
+    from blaze_b200 import FluidSolver
+    from oracle import oracle
+    scn = scene(density_field=1, buoyancy_alpha=0.05)
+    p = scn.to_params()
+    rng = np.random.default_rng(13)
+    n = 300
+    rec = np.zeros((n, 8), np.float32)
+    rec[:, :3] = rng.uniform(np.array(scn.domainBboxMin) - 0.05, np.array(scn.domainBboxMax) + 0.05, (n, 3))
+    rec[:, 6] = rng.uniform(0.0, 5.0, n) * p.dx
+    rec[:, 7] = rng.uniform(-0.5, 2.0, n)
+    dens = rng.uniform(0.0, 1.0, n).astype(np.float32)
+    dens[::7] = 0.0                                   # skipped channel
+    gpu = FluidSolver(Timer(), scn)
+    ref = oracle.State(p, np.float64)
+    gpu.setParticles(rec, dens)
+    gpu.addSource()
+    ref.add_source(rec, density=dens)
+    assert np.abs(ref.DENSITY).max() > 0.1
+    assert_close(gpu, ref, ("T", "DENSITY"), rel=1e-5, absol=1e-4)
+    # without explicit densities every particle carries 1
+    gpu2 = FluidSolver(Timer(), scn)
+    ref2 = oracle.State(p, np.float64)
+    gpu2.setParticles(rec)
+    gpu2.addSource()
+    ref2.add_source(rec)
+    assert_close(gpu2, ref2, ("DENSITY",), rel=1e-5, absol=1e-4)
+
+
+@pytest.mark.parametrize("beta,alpha", [(1.0, 0.05), (0.0, 0.7), (1.5, -0.3)])
+def test_density_buoyancy(beta, alpha):
+    gpu, ref = dens_pair(scene(buoyancy=beta, density_field=1, buoyancy_alpha=alpha, vorticityConf=0.2), 23)
+    gpu.forces(0.4)
+    ref.forces(0.4)
+    assert_close(gpu, ref, ("T", "U", "V", "W", "DENSITY"))
+
+
+def test_density_advect():
+    gpu, ref = dens_pair(scene(density_field=1, buoyancy_alpha=0.05), 83)
+    gpu.advect()
+    ref.advect()
+    assert_close(gpu, ref, ("T", "U", "V", "W", "DENSITY"))
+
+
+def test_density_off_is_the_reference_step():
+    """density_field = 1 with alpha = 0 changes no field of the reference's
+    step: the scalar is carried alongside, bit for bit the same T, U, V, W, P."""
+    from blaze_b200 import FluidSolver
+    out = []
+    for dens in (0, 1):
+        scn, parts = plume_scene(n=32, seed=4, particles=600)
+        scn.density_field, scn.buoyancy_alpha = dens, 0.0
+        tmr = Timer()
+        with FluidSolver(tmr, scn, particles=parts) as s:
+            for _ in range(3):
+                s.addSource()
+                s.step(tmr.time)
+                tmr.time += scn.dt
+            out.append({f: s.get(f) for f in ("T", "U", "V", "W", "P")})
+    for f in out[0]:
+        np.testing.assert_array_equal(out[0][f], out[1][f], err_msg=f)

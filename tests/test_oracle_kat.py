@@ -202,3 +202,33 @@ def test_fp32_and_fp64_oracles_agree(oracle_mod):
         s.step(p.dt)
     for f in ("T", "U", "V", "W", "P"):
         assert rel_l2(getattr(b, f), getattr(a, f)) < 2e-5, f
+
+
+def test_density_scalar_restates_temperature_buoyancy(oracle_mod):
+    """Target mode's density scalar (no reference counterpart): splatted with
+    each particle's density it follows T's sourcing rules, so with density =
+    temperature per particle the scalar equals T; and buoyancy
+    V += dt (beta T - alpha rho) g then equals the temperature-only buoyancy
+    with beta - alpha.  Advection carries it as it carries T."""
+    from blaze_b200 import SceneSettings
+    rng = np.random.default_rng(3)
+    n = 12
+    scn = SceneSettings(gridRes=(n, n, n), dx=1.0 / n, buoyancy=1.3, density_field=1, buoyancy_alpha=0.4)
+    p = scn.to_params()
+    rec = np.zeros((60, 8), np.float32)
+    rec[:, :3] = rng.uniform(0.1, 0.9, (60, 3))
+    rec[:, 6] = 3.0 / n
+    rec[:, 7] = rng.uniform(0.2, 1.5, 60)
+    st = oracle_mod.State(p, np.float64)
+    st.add_source(rec, density=rec[:, 7])
+    np.testing.assert_array_equal(st.DENSITY, st.T)
+    st.forces(0.0)
+    q = SceneSettings(gridRes=(n, n, n), dx=1.0 / n, buoyancy=1.3 - 0.4).to_params()
+    ref = oracle_mod.State(q, np.float64)
+    ref.add_source(rec)
+    ref.forces(0.0)
+    # beta and alpha are float32 parameters: 1.3f - 0.4f and 0.9f differ by 3e-8
+    np.testing.assert_allclose(st.V, ref.V, rtol=1e-7, atol=1e-12)
+    st.U[...] = rng.standard_normal(st.U.shape) * 0.3
+    st.advect()
+    np.testing.assert_array_equal(st.DENSITY, st.T)
