@@ -173,7 +173,7 @@ EXPORTS = {
     "blz_gradient": (C.c_int, [C.c_void_p]),
     "blz_advect": (C.c_int, [C.c_void_p]),
     "blz_sweeps": (C.c_int, [C.c_void_p, C.c_int]),
-    "blz_sor_sweeps": (C.c_int, [C.c_void_p, C.c_int, C.c_float]),
+    "blz_tight_solve": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_double, _P(C.c_int), _P(C.c_double)]),
     "blz_residual": (C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double)]),
     "blz_get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "blz_set_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),

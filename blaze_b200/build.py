@@ -14,7 +14,7 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libblaze_b200.so")
 SOURCES = ["k_source.cu", "k_forces.cu", "k_project.cu", "k_advect.cu", "graph_solve.cu", "solver.cu",
            "unet_conv.cu", "unet.cu", "batch.cu", "render.cu",
-           "noalloc.cu", "noise.cu"]
+           "noalloc.cu", "noise.cu", "tight.cu"]
 HEADERS = ["common.cuh", "kernels.cuh", "noise.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared"] + ARCH

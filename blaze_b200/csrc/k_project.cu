@@ -782,56 +782,6 @@ void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r
     *launches += 2LL * sweeps;
 }
 
-// Red-black successive over-relaxation: each half sweep moves a cell from
-// its value v to v + omega (g - v), g its Gauss-Seidel update (gs_segment).
-// omega = 1 is Gauss-Seidel; 1 < omega < 2 converges in O(N) sweeps on an
-// N^3 Poisson problem instead of O(N^2) (Young's theory of SOR for
-// consistently ordered matrices).  Not a step of the fluid solve (which is
-// Gauss-Seidel, as the reference's): it computes tightly converged
-// pressures, the targets the warm-start network is trained on.
-__global__ void __launch_bounds__(256)
-k_sor_seg(Geom g, SolveParams sp, const float *__restrict__ rhs_c, const float *__restrict__ p_o,
-          float *__restrict__ p_c, int colour, float omega) {
-    const int Wq = g.W >> 3, Wh = g.W >> 1;
-    const int mq = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
-    if (mq >= Wq || j >= g.H || k >= g.D) return;
-    const int m0 = mq * 4;
-    const size_t pl = (size_t)Wh * g.H;
-    const size_t q = (size_t)m0 + (size_t)Wh * (size_t)j + (size_t)k * pl;
-    const bool has_ym = j > 0, has_yp = j < g.H - 1, has_zm = k > 0, has_zp = k < g.D - 1;
-    const bool first = m0 == 0, last = m0 + 4 == Wh;
-    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 zm = has_zm ? ld4(p_o + q - pl) : zero4;
-    const float4 zp = has_zp ? ld4(p_o + q + pl) : zero4;
-    const float4 ym = has_ym ? ld4(p_o + q - Wh) : zero4;
-    const float4 yp = has_yp ? ld4(p_o + q + Wh) : zero4;
-    const int s = (j + k + colour) & 1;
-    const float xe = s == 0 ? (first ? 0.0f : __ldg(p_o + q - 1)) : (last ? 0.0f : __ldg(p_o + q + 4));
-    const float4 gs = gs_segment(sp, s, first, last, ld4(rhs_c + q), ld4(p_o + q), xe, ym, yp, zm, zp, has_ym,
-                                 has_yp, has_zm, has_zp);
-    float4 v = *reinterpret_cast<const float4 *>(p_c + q);
-    v.x = fmaf(omega, gs.x - v.x, v.x);
-    v.y = fmaf(omega, gs.y - v.y, v.y);
-    v.z = fmaf(omega, gs.z - v.z, v.z);
-    v.w = fmaf(omega, gs.w - v.w, v.w);
-    *reinterpret_cast<float4 *>(p_c + q) = v;
-}
-
-void launch_sor_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b, float *p_r,
-                       float *p_b, int sweeps, float omega, cudaStream_t st, long long *launches) {
-    const int Wq = g.W >> 3;
-    const int bx = std::min(32, Wq);
-    const dim3 b(bx, std::max(1, 256 / bx), 1);
-    const dim3 gr((Wq + b.x - 1) / b.x, (g.H + b.y - 1) / b.y, g.D);
-    for (int it = 0; it < sweeps; ++it) {
-        k_sor_seg<<<gr, b, 0, st>>>(g, sp, rhs_r, p_b, p_r, 0, omega);
-        k_sor_seg<<<gr, b, 0, st>>>(g, sp, rhs_b, p_r, p_b, 1, omega);
-    }
-    *launches += 2LL * sweeps;
-}
-
 // The reference's schedule made race free (FluidSolver.cu:517-599): plane by
 // plane, cells with (i+j) even first, then (i+j) odd.  In plane k the 2-D
 // colour (i+j)&1 equals the 3-D colour xor (k&1), so a 2-D half plane is one

@@ -79,10 +79,12 @@ unsigned int tb_take_timeouts();
 void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                         const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
                         long long *launches, int variant = 0, float *q_r = nullptr, float *q_b = nullptr);
-// Red-black SOR sweeps with relaxation factor omega (W % 8 == 0); computes
-// converged pressures for training targets, not a step of the fluid solve.
-void launch_sor_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b, float *p_r,
-                       float *p_b, int sweeps, float omega, cudaStream_t st, long long *launches);
+// The pressure system solved in FP64 (SOR, natural layout) to relative
+// residual tol, the result rounded into p (tight.cu).  Returns 0 or a
+// cudaError_t.
+int tight_solve(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b, float *p_r,
+                float *p_b, double tol, int max_sweeps, double omega, int check_every, cudaStream_t st, int *sweeps,
+                double *rel, long long *launches);
 void launch_plane_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r,
                          const float *rhs_b, float *p_r, float *p_b, int sweeps, cudaStream_t st,
                          long long *launches);

@@ -832,13 +832,20 @@ int blz_sweeps(blz_solver *s, int n) {
     return rc != BLZ_OK ? rc : check_tb_timeouts(s);
 }
 
-int blz_sor_sweeps(blz_solver *s, int n, float omega) {
+int blz_tight_solve(blz_solver *s, double tol, int max_sweeps, double omega, int *sweeps_out, double *rel_out) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
-    if (n < 0) return fail(s, BLZ_ERR_ARG, "negative sweep count");
-    if (!(omega > 0.0f && omega < 2.0f)) return fail(s, BLZ_ERR_ARG, "omega must lie in (0, 2)");
-    if ((s->g.W & 7) != 0) return fail(s, BLZ_ERR_ARG, "SOR sweeps need width %% 8 == 0");
-    launch_sor_sweeps(s->g, solve_params(s->P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, omega, s->st, &s->launches);
-    CKL(s);
+    if (!(tol > 0.0) || max_sweeps < 0 || !(omega > 0.0 && omega < 2.0))
+        return fail(s, BLZ_ERR_ARG, "tight solve needs tol > 0, max_sweeps >= 0 and omega in (0, 2)");
+    int sw = 0;
+    double rel = 0.0;
+    const int e = tight_solve(s->g, solve_params(s->P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, tol, max_sweeps, omega,
+                              50, s->st, &sw, &rel, &s->launches);
+    if (e != 0) {
+        cudaGetLastError();
+        return fail(s, BLZ_ERR_CUDA, "tight solve: %s", cudaGetErrorString((cudaError_t)e));
+    }
+    if (sweeps_out) *sweeps_out = sw;
+    if (rel_out) *rel_out = rel;
     return BLZ_OK;
 }
 

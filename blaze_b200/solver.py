@@ -99,9 +99,13 @@ class FluidSolver:
     def sweeps(self, n):
         check(self._lib.blz_sweeps(self._h, int(n)), self._h)
 
-    def sor_sweeps(self, n, omega):
-        """n red-black SOR sweeps (training targets; not the fluid solve)."""
-        check(self._lib.blz_sor_sweeps(self._h, int(n), C.c_float(omega)), self._h)
+    def tight_solve(self, tol, max_sweeps, omega):
+        """The pressure system solved in FP64 to relative residual tol (SOR,
+        training targets); returns (sweeps, FP64 relative residual)."""
+        n, r = C.c_int(), C.c_double()
+        check(self._lib.blz_tight_solve(self._h, float(tol), int(max_sweeps), float(omega), C.byref(n), C.byref(r)),
+              self._h)
+        return n.value, r.value
 
     def gradient(self):
         check(self._lib.blz_gradient(self._h), self._h)

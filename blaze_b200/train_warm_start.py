@@ -7,9 +7,10 @@
    deployed: RBGS to relative residual `--tol` every frame, either plain
    (warm-started from the previous frame's pressure) or with the current
    network's warm start ("on policy").  For each harvested frame the pair is
-   (rhs, p_prev) -> p*, where p* continues the frame's own solve with
-   red-black SOR sweeps (O(N) sweeps where Gauss-Seidel needs O(N^2))
-   towards `--target-tol`; the simulation then goes on from the
+   (rhs, p_prev) -> p*, where p* continues the frame's own solve in FP64
+   (blz_tight_solve: red-black SOR, O(N) sweeps where Gauss-Seidel needs
+   O(N^2), below the FP32 floor of ~1e-4 relative residual) to
+   `--target-tol`; the simulation then goes on from the
    `--tol` solution, so the next p_prev carries exactly the error a
    deployed solve leaves.  On-policy rounds (as in DAgger) add pairs from
    trajectories the network itself shaped, so it learns to correct its own
@@ -68,31 +69,6 @@ def sor_omega(dims):
     return 2.0 / (1.0 + math.sin(math.pi / (2.0 * n)))
 
 
-def _tighten(solver, target, cap, chunk=100, omega=None):
-    """Sweeps the current pressure on to relative residual `target` by
-    red-black SOR (blz_sor_sweeps), which needs O(N) sweeps where
-    Gauss-Seidel needs O(N^2); stops early when a chunk no longer lowers the
-    residual by 2 % (the FP32 floor)."""
-    done = 0
-    if omega is None:
-        p = solver.params
-        omega = sor_omega((p.width, p.height, p.depth))
-    r, b = solver.residual()
-    best = r
-    stall = 0
-    while b > 0 and r / b > target and done < cap:
-        solver.sor_sweeps(chunk, omega)
-        done += chunk
-        r, b = solver.residual()
-        if r < 0.98 * best:
-            best, stall = r, 0
-        else:
-            stall += 1
-            if stall >= 3:
-                break
-    return done, (r / b if b > 0 else 0.0)
-
-
 def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, log=print, policy=None,
             extra_cap=6000, stride=1):
     """List of dicts {rhs, p_prev, p_star} (device FP32, (D, H, W)) and the
@@ -119,7 +95,7 @@ def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, lo
             solver.set_warm_start(None)
             if keep:
                 p_tol = _field(solver, "P", shape)
-                extra, rel = _tighten(solver, target_tol, extra_cap)
+                extra, rel = solver.tight_solve(target_tol, extra_cap, sor_omega((n, n, n)))
                 p_star = _field(solver, "P", shape)
                 solver.set_device("P", p_tol.data_ptr())
                 d = (p_star - p_prev).double()
@@ -234,8 +210,8 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--eval-frames", type=int, default=8)
     ap.add_argument("--tol", type=float, default=1e-4)
-    ap.add_argument("--target-tol", type=float, default=1e-6)
-    ap.add_argument("--extra-cap", type=int, default=6000, help="SOR sweeps spent tightening each target")
+    ap.add_argument("--target-tol", type=float, default=1e-8)
+    ap.add_argument("--extra-cap", type=int, default=6000, help="FP64 SOR sweeps spent tightening each target")
     ap.add_argument("--max-iter", type=int, default=40000)
     ap.add_argument("--check-every", type=int, default=20)
     ap.add_argument("--iters", type=int, default=1500, help="Adam steps per training round")

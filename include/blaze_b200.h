@@ -211,13 +211,16 @@ int  blz_advect(blz_solver *s);                        /* + swap               *
  * gs_solve_kernel, FluidSolver.cu:526-597, run n times).                    */
 int  blz_sweeps(blz_solver *s, int n);
 
-/* n red-black successive over-relaxation sweeps, relaxation omega in (0, 2)
- * (omega = 1 is Gauss-Seidel; near 2 - 2 pi / N it converges in O(N) sweeps on
- * an N^3 grid instead of O(N^2)), on the current rhs and p, no residual
- * checks; width % 8 == 0.  No counterpart in the reference, and not a step of
- * the fluid solve (which stays Gauss-Seidel): it computes tightly converged
- * pressures, the targets the learned warm start is trained on.              */
-int  blz_sor_sweeps(blz_solver *s, int n, float omega);
+/* The current pressure system solved far past the FP32 floor: the iterate
+ * is held in FP64 (red-black SOR with relaxation omega, FP64 residual checks
+ * every 50 sweeps) until the FP64 relative residual is <= tol or max_sweeps
+ * ran, then rounded once into p.  With the pressure stored in FP32 the
+ * relative residual cannot go much below 2e-7 ||p|| / ||b|| (about 1e-4 on
+ * smooth 256^3 pressures), so this is how converged pressures are obtained.
+ * No counterpart in the reference and not a step of the fluid solve: it
+ * computes the targets the learned warm start is trained on.  Allocates
+ * 16 bytes per cell for the call; synchronises.                             */
+int  blz_tight_solve(blz_solver *s, double tol, int max_sweeps, double omega, int *sweeps, double *rel_residual);
 
 /* FP64 ||b - A p||_2 and ||b||_2 of the current rhs and p.                  */
 int  blz_residual(blz_solver *s, double *res_norm, double *rhs_norm);

@@ -399,3 +399,19 @@ def test_density_off_is_the_reference_step():
             out.append({f: s.get(f) for f in ("T", "U", "V", "W", "P")})
     for f in out[0]:
         np.testing.assert_array_equal(out[0][f], out[1][f], err_msg=f)
+
+
+def test_tight_solve_reaches_the_fp64_solution():
+    """blz_tight_solve (FP64 SOR, training targets) returns the pressure
+    system's solution: its FP64 relative residual meets tol, and the result
+    equals the FP64 oracle's converged Gauss-Seidel solution within FP32
+    rounding."""
+    from oracle import oracle
+    scn = scene(dims=(16, 16, 8), bc_mode=BLZ_BC_FREE_SURFACE, tol=1e-12, maxIterSolve=200000, check_every=200)
+    gpu, ref = pair(scn, 91)
+    sweeps, rel = gpu.tight_solve(1e-10, 20000, 1.8)
+    assert rel <= 1e-10 and 0 < sweeps <= 20000
+    it, r, b = ref.solve()
+    assert r / b <= 1e-12
+    p = gpu.get("P")
+    assert rel_l2(p, ref.P) <= 1e-6 and max_abs(p, ref.P) <= 1e-6 * np.abs(ref.P).max()
