@@ -33,6 +33,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "256³ steps/s: learned warm-start vs plain RBGS at equal residual; HBM GB/s"
+METRIC_FIRE = "384³ large-fire steps/s: learned warm-start vs plain RBGS at equal residual; HBM GB/s"
+
+
+def metric_of(args):
+    return METRIC_FIRE if args.workload == "fire384" else METRIC
 GRID = 256
 SEED = 3
 TOL = 1e-4
@@ -145,24 +150,60 @@ def cpu_baseline(scn, parts, mean_sweeps):
 
 
 def _load_net(args, W, H, D):
-    """The trained warm-start network for this grid, or (None, reason)."""
+    """The trained warm-start network for this grid, or (None, reason).  The
+    network is fully convolutional: without weights trained at this size the
+    256^3 weights are applied (and the line says so)."""
     from blaze_b200.unet import WarmStartUNet, weights_path
     if args.plain_only:
         return None, "disabled (--plain-only)"
     path = args.weights or weights_path(f"plume{W}.npz")
+    note = ""
+    if not os.path.exists(path) and not args.weights:
+        path, note = weights_path("plume256.npz"), f" (trained at 256^3, applied at {W}x{H}x{D})"
     if not os.path.exists(path):
         return None, f"no trained weights for {W}^3 ({os.path.relpath(path, ROOT)})"
     net = WarmStartUNet((W, H, D)).load(path)
-    return net, os.path.relpath(path, ROOT)
+    return net, os.path.relpath(path, ROOT) + note
+
+
+def make_workload(args, seed, tol=TOL, max_iter=None, check_every=None, bc_mode=None):
+    """(SceneSettings, frame_particles, description) of the --workload:
+    plume, the 256^3 plume-family benchmark scene (one static particle set);
+    fire384, the large fire scene (a static ground disc and two spheres
+    moving 1 cell per frame, re-sourced every frame as an animated source)."""
+    from blaze_b200 import family_scene
+    from blaze_b200.scenes import large_fire_scene
+    max_iter = args.max_iter if max_iter is None else max_iter
+    if check_every is None:
+        check_every = CHECK_AUTO if max_iter % 320 == 0 else CHECK_EVERY
+    if args.workload == "fire384":
+        scn, fp = large_fire_scene(n=args.grid if args.grid != GRID else 384, seed=5 + seed - SEED)
+        scn.tol, scn.maxIterSolve, scn.check_every = tol, max_iter, check_every
+        if bc_mode is not None:
+            scn.bc_mode = bc_mode
+            scn.defect_correction = 0 if bc_mode == 0 else scn.defect_correction
+        n = scn.gridRes[0]
+        desc = (f"large fire {n}^3 (ground disc of 30000 particles, two spheres moving 1 cell/frame as an "
+                f"animated source, curl noise 0.8 / 8 cells, wind 0.3 cells/step)")
+        return scn, fp, desc
+    scn, parts = family_scene(n=args.grid, seed=seed, tol=tol, max_iter=max_iter, check_every=check_every,
+                              **({} if bc_mode is None else {"bc_mode": bc_mode}))
+    if bc_mode is not None and bc_mode == 0:
+        scn.defect_correction = 0
+    desc = (f"plume-family {args.grid}^3 scene (seed {seed}, {scn.extra['sources']} sources, "
+            f"wind {scn.extra['wind_cells_per_step']:.2f} cells/step)")
+    return scn, (lambda f: parts), desc
 
 
 def run_ours(args, ws, rank, local):
     import torch
-    from blaze_b200 import FluidSolver, Timer, family_scene
+    from blaze_b200 import FluidSolver, Timer
 
     torch.cuda.set_device(local)
-    check = CHECK_AUTO if args.max_iter % 320 == 0 else CHECK_EVERY
-    scn, parts = family_scene(n=args.grid, seed=SEED + rank, tol=TOL, max_iter=args.max_iter, check_every=check)
+    scn, frame_parts, desc = make_workload(args, SEED + rank)
+    check = scn.check_every
+    animated = args.workload == "fire384"
+    parts = frame_parts(0)
     if args.host_loop:
         scn.device_loop = 0
     W, H, D = scn.gridRes
@@ -176,6 +217,8 @@ def run_ours(args, ws, rank, local):
     net, net_src = _load_net(args, W, H, D)
 
     def frame():
+        if animated:                                    # the reference re-reads an animated source every frame
+            solver.setParticles(frame_parts(tmr.iter))
         solver.addSource()
         st = solver.step(tmr.time)
         tmr.iter += 1
@@ -251,6 +294,8 @@ def run_ours(args, ws, rank, local):
         torch.cuda.synchronize()
         w0 = time.perf_counter()
         for _ in range(args.steps):
+            if animated:
+                pinned_parts.numpy()[...] = frame_parts(tmr.iter)
             solver.setParticles(pinned_parts.numpy())
             solver.addSource()
             solver.step(tmr.time)
@@ -319,13 +364,13 @@ def run_ours(args, ws, rank, local):
     value = ws * args.steps / (ms * 1e-3)
     head = learned if head_learned else plain
     line = {
-        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+        "metric": metric_of(args), "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"plume-family {W}^3 scene (seed {SEED}, {scn.extra['sources']} sources, "
-                               f"wind {scn.extra['wind_cells_per_step']:.2f} cells/step), "
+        "config": {"workload": f"{desc}, "
                                f"{'learned warm start + ' if head_learned else 'plain '}RBGS with free-surface "
-                               f"top to FP64 relative residual {TOL:g} per frame",
+                               f"top to FP64 relative residual {TOL:g} per frame"
+                               f"{' (defect correction: sweeps on the correction to the previous pressure)' if scn.defect_correction else ''}",
                    "grid": [W, H, D], "particles": int(len(parts)), "tol": TOL,
                    "check_every": "auto: per frame from 20..320, minimising checks plus sweeps past convergence"
                    if check < 0 else check,
@@ -374,23 +419,47 @@ def run_ours(args, ws, rank, local):
 
 
 def run_batch(args, ws, rank, local):
-    """Config 4: 64 independent plume simulations of uneven sizes stepped as one
-    batch; value = aggregate cells x steps / s (all ranks).  The same
-    simulations are also stepped one by one (each its own device-loop solve,
-    all on one stream) for the same frames: that pass is timed the same way
-    and every field of every simulation is compared bit for bit."""
+    """Config 4: one seeded set of 64 independent plume simulations of uneven
+    sizes, plain and learned mixed (every second simulation warm-started by
+    the network, one network instance per grid size, the 256^3 weights
+    applied at each size), stepped as one batch; value = aggregate cells x
+    steps / s.  With N ranks the set is split by cell count
+    (parallel.shard_sims: no data-path collective), so the total work is fixed
+    (strong scaling).  The same simulations are also stepped one by one (each
+    its own device-loop solve, all on one stream) for the same frames: that
+    pass is timed the same way and every field of every simulation is
+    compared bit for bit."""
     import torch
     from blaze_b200 import FluidSolver, Timer
     from blaze_b200.batch import Batch
+    from blaze_b200.parallel import shard_sims
     from blaze_b200.scenes import batch_scenes
+    from blaze_b200.unet import WarmStartUNet, weights_path
 
     torch.cuda.set_device(local)
-    scenes = batch_scenes(args.batch_sims, seed=4 + rank, tol=TOL, max_iter=MAX_ITER, check_every=CHECK_EVERY)
-    cells = sum(s.gridRes[0] * s.gridRes[1] * s.gridRes[2] for s, _ in scenes)
+    all_scenes = batch_scenes(args.batch_sims, seed=4, tol=TOL, max_iter=MAX_ITER, check_every=CHECK_EVERY)
+    all_cells = [s.gridRes[0] * s.gridRes[1] * s.gridRes[2] for s, _ in all_scenes]
+    mine = shard_sims(all_cells, ws)[rank]
+    scenes = [all_scenes[i] for i in mine]
+    cells = sum(all_cells[i] for i in mine)
+    total_cells = sum(all_cells)
     dt = scenes[0][0].dt
+    wpath = weights_path("plume256.npz")
+    nets = {}
+
+    def net_for(i, scn):
+        """Every second simulation (by its index in the whole set) is learned."""
+        if args.plain_only or mine[i] % 2 == 0 or not os.path.exists(wpath):
+            return None
+        dims = tuple(scn.gridRes)
+        if dims not in nets:
+            nets[dims] = WarmStartUNet(dims).load(wpath)
+        return nets[dims]
 
     # batched
     sims = [FluidSolver(Timer(), s, particles=p) for s, p in scenes]
+    for i, (sm, (s, _)) in enumerate(zip(sims, scenes)):
+        sm.set_warm_start(net_for(i, s))
     batch = Batch(sims)
 
     def frame(f):
@@ -422,6 +491,8 @@ def run_batch(args, ws, rank, local):
     # one by one, same frames
     alone_stream = torch.cuda.Stream()
     alone = [FluidSolver(Timer(), s, particles=p, stream=alone_stream.cuda_stream) for s, p in scenes]
+    for i, (sm, (s, _)) in enumerate(zip(alone, scenes)):
+        sm.set_warm_start(net_for(i, s))
 
     def frame_alone(f):
         for sm in alone:
@@ -441,6 +512,8 @@ def run_batch(args, ws, rank, local):
     agree = all(np.array_equal(sm.get(k), v) for sm, fd in zip(alone, fields) for k, v in fd.items())
     for sm in alone:
         sm.close()
+    for n_ in nets.values():
+        n_.close()
     if ws > 1:
         t = torch.tensor([ms, ms_alone], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -448,20 +521,27 @@ def run_batch(args, ws, rank, local):
     if rank != 0:
         return None
     sweeps = np.array([[x["iterations"] for x in fr] for fr in stats], float)
-    value = ws * cells * args.steps / (ms * 1e-3)
+    learned_mask = np.array([bool(x["warm_started"]) for x in stats[0]])
+    value = total_cells * args.steps / (ms * 1e-3)
     dims = {}
     for s, _ in scenes:
         dims[str(tuple(s.gridRes))] = dims.get(str(tuple(s.gridRes)), 0) + 1
     return {"metric": "batched simulations: aggregate cells x steps/s", "value": value, "unit": "cell-steps/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{len(scenes)} plume simulations of uneven sizes in one batch, RBGS to "
-                                   f"FP64 relative residual {TOL:g} each", "sims": len(scenes), "dims": dims,
-                       "cells": cells, "mean_sweeps": float(sweeps.mean()), "max_sweeps": float(sweeps.max()),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{len(all_scenes)} plume simulations of uneven sizes (seed 4), plain and learned "
+                                   f"mixed, in one batch per GPU, RBGS to FP64 relative residual {TOL:g} each",
+                       "sims": len(all_scenes), "sims_rank0": len(scenes), "dims_rank0": dims,
+                       "cells": total_cells, "cells_rank0": cells,
+                       "learned_sims_rank0": int(learned_mask.sum()),
+                       "learned_weights": os.path.relpath(wpath, ROOT) + " (trained at 256^3)" if nets else None,
+                       "mean_sweeps": float(sweeps.mean()), "max_sweeps": float(sweeps.max()),
+                       "mean_sweeps_plain_sims": float(sweeps[:, ~learned_mask].mean()) if (~learned_mask).any() else None,
+                       "mean_sweeps_learned_sims": float(sweeps[:, learned_mask].mean()) if learned_mask.any() else None,
                        "all_converged": all(x["converged"] for fr in stats for x in fr),
                        "per_sim_agreement_with_unbatched": "bitwise, all fields of all sims" if agree else "DIFFERS",
-                       "parallelism": f"replicas x{ws}"},
-            "unbatched": {"value": ws * cells * args.steps / (ms_alone * 1e-3), "ms_per_step": ms_alone / args.steps,
+                       "parallelism": f"simulations split over {ws} GPU(s) by cell count (parallel.shard_sims)"},
+            "unbatched": {"value": total_cells * args.steps / (ms_alone * 1e-3), "ms_per_step": ms_alone / args.steps,
                           "how": "the same simulations and frames, one solver after another on one stream, each "
                                  "with its own device-loop solve graph"},
             "batch_speedup": ms_alone / ms,
@@ -477,7 +557,8 @@ def plain_sweeps_per_frame(args, local):
     if fixed:
         return [int(fixed)] * args.steps, f"{REF_SWEEPS_ENV}={fixed} sweeps per frame"
     cmd = [sys.executable, os.path.abspath(__file__), "--plain-only", "--no-cpu", "--no-e2e", "--grid",
-           str(args.grid), "--steps", str(args.steps), "--warmup", str(args.warmup), "--max-iter", str(args.max_iter)]
+           str(args.grid), "--steps", str(args.steps), "--warmup", str(args.warmup), "--max-iter", str(args.max_iter),
+           "--workload", args.workload]
     env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
     for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
         env.pop(k, None)
@@ -494,14 +575,14 @@ def run_reference(args, ws, rank, local):
         return None
     import torch
     from oracle import ref
-    from blaze_b200 import family_scene, BLZ_BC_REF_COMPAT
+    from blaze_b200 import BLZ_BC_REF_COMPAT
     if not ref.available():
         return {"impl": "reference", "unavailable": "reference CUDA build (oracle/_ref) not built"}
     sweeps, how = plain_sweeps_per_frame(args, local)
     mean_sweeps = float(np.mean(sweeps))
     torch.cuda.set_device(local)
-    scn, parts = family_scene(n=args.grid, seed=SEED, tol=0.0, max_iter=int(round(mean_sweeps)),
-                              bc_mode=BLZ_BC_REF_COMPAT)
+    scn, frame_parts, desc = make_workload(args, SEED, tol=0.0, max_iter=int(round(mean_sweeps)),
+                                           check_every=20, bc_mode=BLZ_BC_REF_COMPAT)
     p = scn.to_params()
     r = ref.RefSolver(p)
     it, t = 0, 0.0
@@ -510,7 +591,7 @@ def run_reference(args, ws, rank, local):
         nonlocal it, t
         r.set_max_iter(n_sweeps)
         r.set_time(it, t)
-        r.set_particles(parts)
+        r.set_particles(frame_parts(it))
         r.add_source()
         r.step()
         it += 1
@@ -528,14 +609,14 @@ def run_reference(args, ws, rank, local):
     r.close()
     value = args.steps / wall
     return {
-        "metric": METRIC, "impl": "reference", "value": value, "unit": "steps/s", "n_gpus": 1,
+        "metric": metric_of(args), "impl": "reference", "value": value, "unit": "steps/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"plume-family {args.grid}^3 scene (seed {SEED}) through the reference's "
+        "config": {"workload": f"{desc} through the reference's "
                                f"own CUDA build (src/FluidSolver.cu, -O3 --use_fast_math, sm_100a), "
                                f"maxIterSolve per frame = the plain RBGS step's sweeps on that frame "
                                f"(mean {mean_sweeps:.0f}; equal sweep count, the reference has no residual "
-                               f"control)", "grid": [args.grid] * 3,
+                               f"control)", "grid": list(scn.gridRes),
                    "sweeps_per_frame": sweeps, "mean_sweeps": mean_sweeps, "sweep_counts": how},
         "ms_per_sweep": wall * 1e3 / float(sum(sweeps)),
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference",
@@ -699,9 +780,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) pass")
     ap.add_argument("--max-iter", type=int, default=MAX_ITER, help="GS sweep cap per frame (profiling runs)")
-    ap.add_argument("--workload", default="plume", choices=["plume", "batch", "render"],
-                    help="plume: the 256^3 step (default); batch: 64 uneven simulations in one batch; "
-                         "render: the volume renderer on a 256^3 field")
+    ap.add_argument("--workload", default="plume", choices=["plume", "fire384", "batch", "render"],
+                    help="plume: the 256^3 step (default); fire384: the 384^3 large fire with moving emitters; "
+                         "batch: 64 uneven simulations in one batch; render: the volume renderer on a 256^3 field")
     ap.add_argument("--batch-sims", type=int, default=64)
     ap.add_argument("--plain-only", action="store_true", help="skip the learned warm-start pass")
     ap.add_argument("--weights", default=None, help="warm-start network weights (npz)")
@@ -723,6 +804,8 @@ def main():
     try:
         if args.workload == "batch":
             line = run_batch(args, ws, rank, local)
+        elif args.workload == "fire384":
+            line = run_ours(args, ws, rank, local)
         elif args.workload == "render":
             line = run_render(args, ws, rank, local)
         else:

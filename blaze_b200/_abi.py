@@ -46,7 +46,7 @@ class BlzParams(C.Structure):
         ("bc_mode", C.c_int), ("gs_order", C.c_int), ("reset_pressure", C.c_int),
         ("max_particles", C.c_int), ("temporal_block", C.c_int),
         ("device_loop", C.c_int), ("sweep_variant", C.c_int), ("advect_scheme", C.c_int),
-        ("density_field", C.c_int), ("buoyancy_alpha", C.c_float),
+        ("density_field", C.c_int), ("buoyancy_alpha", C.c_float), ("defect_correction", C.c_int),
     ]
 
     def dims(self):

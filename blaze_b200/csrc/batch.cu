@@ -360,6 +360,10 @@ int blz_batch_create(blz_solver *const *sims, int n, blz_batch **out) {
             return bfail(BLZ_ERR_ARG, "solver %d: the batch needs width %% 8 == 0, 3-D red-black order, tol > 0 "
                                       "and max_iter a multiple of check_every >= 1", i);
         }
+        if (P->defect_correction) {
+            delete b;
+            return bfail(BLZ_ERR_ARG, "solver %d: the batch solves p directly (defect_correction must be 0)", i);
+        }
         if (i > 0 && P->check_every != b->params[0]->check_every) {
             delete b;
             return bfail(BLZ_ERR_ARG, "solver %d: all solvers of a batch need the same check_every", i);

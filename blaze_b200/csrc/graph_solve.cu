@@ -37,14 +37,16 @@ __global__ void k_ctl_mark(SolveCtl *c, int stop) {
 }
 
 // Reads {||r||^2, ||b||^2}, records them, and sets whether the loop goes on.
+// b2_ref (a defect-correction solve): the ||b||^2 of the frame's system, in
+// place of the defect's own norm.
 __global__ void k_ctl_check(SolveCtl *c, const double *__restrict__ norm2, cudaGraphConditionalHandle h,
-                            int after_sweeps, int chunk, int max_iter, double tol) {
+                            int after_sweeps, int chunk, int max_iter, double tol, const double *__restrict__ b2_ref) {
     if (after_sweeps) {
         c->iters += chunk;
         c->check_ns += global_ns() - c->t1;
     }
     c->checks += 1;
-    const double r2 = norm2[0], b2 = norm2[1];
+    const double r2 = norm2[0], b2 = b2_ref ? *b2_ref : norm2[1];
     c->r2 = r2;
     c->b2 = b2;
     const bool conv = b2 == 0.0 || sqrt(r2) / sqrt(b2) <= tol;
@@ -62,7 +64,7 @@ cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float 
                               float *p_r, float *p_b, double *partials, int n_partials, double *norm2,
                               SolveCtl *ctl, int chunk, int max_iter, double tol, int variant, cudaStream_t st,
                               cudaGraphExec_t *exec_out, int *body_kernels, int *prologue_kernels, float *q_r,
-                              float *q_b) {
+                              float *q_b, const double *b2_ref) {
     cudaError_t err = cudaSuccess;
     cudaGraph_t graph = nullptr, body = nullptr;
     cudaGraphConditionalHandle handle;
@@ -75,7 +77,7 @@ cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float 
     CKG(cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     k_ctl_begin<<<1, 1, 0, st>>>(ctl);
     *prologue_kernels = 1 + launch_residual(g, sp, rhs_r, rhs_b, p_r, p_b, partials, n_partials, norm2, st) + 1;
-    k_ctl_check<<<1, 1, 0, st>>>(ctl, norm2, handle, 0, chunk, max_iter, tol);
+    k_ctl_check<<<1, 1, 0, st>>>(ctl, norm2, handle, 0, chunk, max_iter, tol, b2_ref);
     {
         cudaStreamCaptureStatus status;
         const cudaGraphNode_t *deps = nullptr;
@@ -97,7 +99,7 @@ cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float 
     launch_rbgs_sweeps(g, sp, rhs_r, rhs_b, p_r, p_b, chunk, st, &dummy, variant, q_r, q_b);
     k_ctl_mark<<<1, 1, 0, st>>>(ctl, 1);
     *body_kernels = 2 + (int)dummy + launch_residual(g, sp, rhs_r, rhs_b, p_r, p_b, partials, n_partials, norm2, st) + 1;
-    k_ctl_check<<<1, 1, 0, st>>>(ctl, norm2, handle, 1, chunk, max_iter, tol);
+    k_ctl_check<<<1, 1, 0, st>>>(ctl, norm2, handle, 1, chunk, max_iter, tol, b2_ref);
     CKG(cudaStreamEndCapture(st, &body));
     CKG(cudaGraphInstantiate(exec_out, graph, 0));
 done:

@@ -1115,9 +1115,15 @@ int launch_residual(const Geom &g, const SolveParams &sp, const float *rhs_r, co
 // read after the update; the thread of the inner face writes both, so no
 // thread reads a face another thread writes), FREE_SURFACE applies the
 // gradient against the p = 0 ghost.
+// DEFECT: the pressure is p0 + delta (the defect-correction solve, p0 in
+// pr/pb and delta in dr/db); each difference is formed as
+// (p0_a - p0_b) + (delta_a - delta_b), so the gradient keeps the correction's
+// digits that p0 + delta rounded to FP32 would lose.
+template <bool DEFECT>
 __global__ void k_gradient(Geom g, SolveParams sp, float s, const float *__restrict__ pr,
                            const float *__restrict__ pb, float *__restrict__ U,
-                           float *__restrict__ V, float *__restrict__ W) {
+                           float *__restrict__ V, float *__restrict__ W, const float *__restrict__ dr,
+                           const float *__restrict__ db) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -1126,58 +1132,171 @@ __global__ void k_gradient(Geom g, SolveParams sp, float s, const float *__restr
     const OpenFaces &o = sp.open;
     const bool dir = sp.dirichlet;
     auto P = [&](int a, int b, int c) { return pval(pr, pb, a, b, c, Wh, H); };
+    // p(a) - p(b), and p(a) alone (the difference to a Dirichlet ghost)
+    auto dP = [&](int a1, int b1, int c1, int a2, int b2, int c2) -> float {
+        if (DEFECT)
+            return (P(a1, b1, c1) - P(a2, b2, c2)) + (pval(dr, db, a1, b1, c1, Wh, H) - pval(dr, db, a2, b2, c2, Wh, H));
+        return P(a1, b1, c1) - P(a2, b2, c2);
+    };
+    auto P1 = [&](int a, int b, int c) -> float {
+        if (DEFECT) return (P(a, b, c) - 0.0f) + (pval(dr, db, a, b, c, Wh, H) - 0.0f);
+        return P(a, b, c) - 0.0f;
+    };
+    auto P1n = [&](int a, int b, int c) -> float {       // 0 - p(a)
+        if (DEFECT) return (0.0f - P(a, b, c)) + (0.0f - pval(dr, db, a, b, c, Wh, H));
+        return 0.0f - P(a, b, c);
+    };
     if (j < g.H && k < g.D) {
         const size_t q = lin(i, j, k, g.W + 1, g.H);
         if (i > 0 && i < g.W) {
-            const float u = U[q] - s * (P(i, j, k) - P(i - 1, j, k));
+            const float u = U[q] - s * dP(i, j, k, i - 1, j, k);
             U[q] = u;
             if (!dir && i == 1 && o.xlo) U[q - 1] = u;
             if (!dir && i == g.W - 1 && o.xhi) U[q + 1] = u;
         } else if (i == 0) {
             if (!o.xlo) U[q] = 0.0f;
-            else if (dir) U[q] -= s * (P(0, j, k) - 0.0f);
+            else if (dir) U[q] -= s * P1(0, j, k);
         } else {
             if (!o.xhi) U[q] = 0.0f;
-            else if (dir) U[q] -= s * (0.0f - P(g.W - 1, j, k));
+            else if (dir) U[q] -= s * P1n(g.W - 1, j, k);
         }
     }
     if (i < g.W && k < g.D) {
         const size_t q = lin(i, j, k, g.W, g.H + 1);
         const size_t row = (size_t)g.W;
         if (j > 0 && j < g.H) {
-            const float v = V[q] - s * (P(i, j, k) - P(i, j - 1, k));
+            const float v = V[q] - s * dP(i, j, k, i, j - 1, k);
             V[q] = v;
             if (!dir && j == 1 && o.ylo) V[q - row] = v;
             if (!dir && j == g.H - 1 && o.yhi) V[q + row] = v;
         } else if (j == 0) {
             if (!o.ylo) V[q] = 0.0f;
-            else if (dir) V[q] -= s * (P(i, 0, k) - 0.0f);
+            else if (dir) V[q] -= s * P1(i, 0, k);
         } else {
             if (!o.yhi) V[q] = 0.0f;
-            else if (dir) V[q] -= s * (0.0f - P(i, g.H - 1, k));
+            else if (dir) V[q] -= s * P1n(i, g.H - 1, k);
         }
     }
     if (i < g.W && j < g.H) {
         const size_t q = lin(i, j, k, g.W, g.H);
         const size_t plane = (size_t)g.W * g.H;
         if (k > 0 && k < g.D) {
-            const float w = W[q] - s * (P(i, j, k) - P(i, j, k - 1));
+            const float w = W[q] - s * dP(i, j, k, i, j, k - 1);
             W[q] = w;
             if (!dir && k == 1 && o.zlo) W[q - plane] = w;
             if (!dir && k == g.D - 1 && o.zhi) W[q + plane] = w;
         } else if (k == 0) {
             if (!o.zlo) W[q] = 0.0f;
-            else if (dir) W[q] -= s * (P(i, j, 0) - 0.0f);
+            else if (dir) W[q] -= s * P1(i, j, 0);
         } else {
             if (!o.zhi) W[q] = 0.0f;
-            else if (dir) W[q] -= s * (0.0f - P(i, j, g.D - 1));
+            else if (dir) W[q] -= s * P1n(i, j, g.D - 1);
         }
     }
 }
 
 void launch_gradient(const Geom &g, const SolveParams &sp, float s, const float *p_r,
-                     const float *p_b, float *U, float *V, float *W, cudaStream_t st) {
-    k_gradient<<<face_grid(g), face_block(), 0, st>>>(g, sp, s, p_r, p_b, U, V, W);
+                     const float *p_b, float *U, float *V, float *W, cudaStream_t st, const float *d_r,
+                     const float *d_b) {
+    if (d_r && d_b)
+        k_gradient<true><<<face_grid(g), face_block(), 0, st>>>(g, sp, s, p_r, p_b, U, V, W, d_r, d_b);
+    else
+        k_gradient<false><<<face_grid(g), face_block(), 0, st>>>(g, sp, s, p_r, p_b, U, V, W, nullptr, nullptr);
+}
+
+// The defect of the current pressure, for the defect-correction solve: with
+// b = scale * rhs, r = b - A p0 evaluated in FP64 (the stencil in deviation
+// form on the FP32 p0, exact in FP64) and stored as the FP32 right-hand side
+// rhs' = r / scale of the system A delta = r that the sweeps then solve for
+// the correction delta.  Per-block partial sums of b^2 (FP64) go to
+// part[2 * block + 1] and of r^2 to part[2 * block]; k_defect_total sums them
+// in block order into out2 = {||r||^2, ||b||^2}.
+constexpr int kDefectThreads = 256;
+constexpr int kDefectBlocks = 1184;
+
+__global__ void __launch_bounds__(kDefectThreads)
+k_defect(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float *__restrict__ rhs_b,
+         const float *__restrict__ pr, const float *__restrict__ pb, float *__restrict__ def_r,
+         float *__restrict__ def_b, double *__restrict__ part) {
+    const int Wh = g.W >> 1, H = g.H;
+    const long long n = (long long)g.W * g.H * g.D;
+    const OpenFaces &o = sp.open;
+    const bool dir = sp.dirichlet;
+    double r2 = 0.0, b2 = 0.0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % g.W), j = (int)((c / g.W) % g.H), k = (int)(c / ((long long)g.W * g.H));
+        const size_t q = pidx(i, j, k, Wh, H);
+        const bool black = (i + j + k) & 1;
+        const double pc = (double)(black ? pb : pr)[q];
+        double d = 0.0;
+        if (i > 0) d += pc - (double)pval(pr, pb, i - 1, j, k, Wh, H); else if (dir && o.xlo) d += pc;
+        if (i < g.W - 1) d += pc - (double)pval(pr, pb, i + 1, j, k, Wh, H); else if (dir && o.xhi) d += pc;
+        if (j > 0) d += pc - (double)pval(pr, pb, i, j - 1, k, Wh, H); else if (dir && o.ylo) d += pc;
+        if (j < g.H - 1) d += pc - (double)pval(pr, pb, i, j + 1, k, Wh, H); else if (dir && o.yhi) d += pc;
+        if (k > 0) d += pc - (double)pval(pr, pb, i, j, k - 1, Wh, H); else if (dir && o.zlo) d += pc;
+        if (k < g.D - 1) d += pc - (double)pval(pr, pb, i, j, k + 1, Wh, H); else if (dir && o.zhi) d += pc;
+        const double b = sp.scale_d * (double)(black ? rhs_b : rhs_r)[q];
+        const double r = b - d;
+        (black ? def_b : def_r)[q] = (float)(r / sp.scale_d);
+        r2 += r * r;
+        b2 += b * b;
+    }
+    __shared__ double sr[kDefectThreads], sb[kDefectThreads];
+    sr[threadIdx.x] = r2;
+    sb[threadIdx.x] = b2;
+    __syncthreads();
+    for (int t = kDefectThreads / 2; t > 0; t >>= 1) {
+        if (threadIdx.x < t) { sr[threadIdx.x] += sr[threadIdx.x + t]; sb[threadIdx.x] += sb[threadIdx.x + t]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = sr[0]; part[2 * blockIdx.x + 1] = sb[0]; }
+}
+
+__global__ void k_defect_total(const double *__restrict__ part, int nb, double *__restrict__ out2) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double r2 = 0.0, b2 = 0.0;
+    for (int t = 0; t < nb; ++t) { r2 += part[2 * t]; b2 += part[2 * t + 1]; }
+    out2[0] = r2;
+    out2[1] = b2;
+}
+
+// p = RN(p + delta) and delta = (p + delta) - RN(p + delta), exactly (Knuth's
+// TwoSum: the rounding error of a float sum is itself a float), over both
+// colours: the folded pressure after a defect solve, with nothing lost.
+__device__ __forceinline__ void two_sum(float &a, float &b) {
+    const float s = __fadd_rn(a, b);
+    const float bp = __fsub_rn(s, a);
+    const float ap = __fsub_rn(s, bp);
+    b = __fadd_rn(__fsub_rn(a, ap), __fsub_rn(b, bp));
+    a = s;
+}
+__global__ void k_fold(long long n, float *__restrict__ pr, float *__restrict__ pb, float *__restrict__ dr,
+                       float *__restrict__ db) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        float a = pr[t], b = dr[t];
+        two_sum(a, b);
+        pr[t] = a;
+        dr[t] = b;
+        a = pb[t];
+        b = db[t];
+        two_sum(a, b);
+        pb[t] = a;
+        db[t] = b;
+    }
+}
+
+int launch_defect(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b, const float *p_r,
+                  const float *p_b, float *def_r, float *def_b, double *partials, int max_partials, double *out2,
+                  cudaStream_t st) {
+    const int nb = std::min(kDefectBlocks, max_partials);
+    k_defect<<<nb, kDefectThreads, 0, st>>>(g, sp, rhs_r, rhs_b, p_r, p_b, def_r, def_b, partials);
+    k_defect_total<<<1, 32, 0, st>>>(partials, nb, out2);
+    return 2;
+}
+
+void launch_fold(const Geom &g, float *p_r, float *p_b, float *d_r, float *d_b, cudaStream_t st) {
+    const long long n = (long long)g.W * g.H * g.D / 2;
+    k_fold<<<(int)std::min<long long>((n + 255) / 256, 4736), 256, 0, st>>>(n, p_r, p_b, d_r, d_b);
 }
 
 __global__ void k_pack(Geom g, const float *__restrict__ nat, float *__restrict__ red,

@@ -31,6 +31,17 @@ struct blz_solver {
     float *Dn[2]{};                             // density scalar (density_field only)
     int cur = 0;                                // front = [cur]
     float *p_r = nullptr, *p_b = nullptr, *rhs_r = nullptr, *rhs_b = nullptr;
+    // Defect-correction solve (params.defect_correction): the sweeps solve
+    // A delta = b - A p for the correction delta (dl) with the defect as
+    // right-hand side (df); afterwards p = RN(p + delta) and delta keeps the
+    // exact rounding remainder, so p + delta carries the solution past the
+    // FP32 floor.  sr/sx: the right-hand side and unknown the sweeps work on
+    // (df/dl, or rhs/p without defect correction).
+    float *df_r = nullptr, *df_b = nullptr, *dl_r = nullptr, *dl_b = nullptr;
+    const float *sr_r = nullptr, *sr_b = nullptr;
+    float *sx_r = nullptr, *sx_b = nullptr;
+    double *d_b2ref = nullptr;                  // ||b||^2 of the current defect solve (device)
+    bool defect_valid = false;                  // dl holds the remainder of the last solve
     float *scratch = nullptr;                   // 6 T-sized arrays (vorticity)
     // sourcing: compacted particle records, per-field index boxes and the
     // 8^3-cell bins (CSR) built on the host by blz_set_particles
@@ -165,6 +176,7 @@ static void release(blz_solver *s) {
     }
     cudaFree(s->pdens);
     cudaFree(s->p_r); cudaFree(s->p_b); cudaFree(s->rhs_r); cudaFree(s->rhs_b);
+    cudaFree(s->df_r); cudaFree(s->df_b); cudaFree(s->dl_r); cudaFree(s->dl_b); cudaFree(s->d_b2ref);
     cudaFree(s->scratch);
     cudaFree(s->parts); cudaFree(s->boxes); cudaFree(s->bin_start); cudaFree(s->bin_list); cudaFree(s->active);
     cudaFree(s->partials); cudaFree(s->d_norm2);
@@ -198,6 +210,8 @@ int blz_create(const blz_params *p, blz_solver **out) {
         return fail(nullptr, BLZ_ERR_ARG, "bad advect_scheme %d", p->advect_scheme);
     if (p->density_field != 0 && p->density_field != 1)
         return fail(nullptr, BLZ_ERR_ARG, "density_field must be 0 or 1 (got %d)", p->density_field);
+    if (p->defect_correction != 0 && p->defect_correction != 1)
+        return fail(nullptr, BLZ_ERR_ARG, "defect_correction must be 0 or 1 (got %d)", p->defect_correction);
 
     blz_solver *s = new blz_solver();
     s->P = *p;
@@ -220,6 +234,13 @@ int blz_create(const blz_params *p, blz_solver **out) {
     for (int b = 0; b < 2 && ok; ++b)
         ok = alloc(&s->T[b], nT) && alloc(&s->U[b], nU) && alloc(&s->V[b], nV) && alloc(&s->W[b], nW);
     ok = ok && alloc(&s->p_r, nT / 2) && alloc(&s->p_b, nT / 2) && alloc(&s->rhs_r, nT / 2) && alloc(&s->rhs_b, nT / 2);
+    if (p->defect_correction) {
+        ok = ok && alloc(&s->df_r, nT / 2) && alloc(&s->df_b, nT / 2) && alloc(&s->dl_r, nT / 2) && alloc(&s->dl_b, nT / 2);
+        ok = ok && cudaMalloc(&s->d_b2ref, sizeof(double)) == cudaSuccess;
+        s->sr_r = s->df_r; s->sr_b = s->df_b; s->sx_r = s->dl_r; s->sx_b = s->dl_b;
+    } else {
+        s->sr_r = s->rhs_r; s->sr_b = s->rhs_b; s->sx_r = s->p_r; s->sx_b = s->p_b;
+    }
     ok = ok && alloc(&s->scratch, 6 * nT);
     if (p->density_field) ok = ok && alloc(&s->Dn[0], nT) && alloc(&s->Dn[1], nT);
     (void)nU; (void)nV; (void)nW;
@@ -484,15 +505,33 @@ int blz_divergence(blz_solver *s) {
     return BLZ_OK;
 }
 
-static int residual_sync(blz_solver *s, double *r, double *b) {
+// FP64 residual norms of (rr/rb, pr/pb), synchronised to the host.
+static int residual_on(blz_solver *s, const float *rr, const float *rb, const float *pr, const float *pb, double *r,
+                       double *b) {
     const SolveParams sp = solve_params(s->P);
-    s->launches += launch_residual(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->partials, s->n_partials,
-                                   s->d_norm2, s->st);
+    s->launches += launch_residual(s->g, sp, rr, rb, pr, pb, s->partials, s->n_partials, s->d_norm2, s->st);
     CKL(s);
     CK(s, cudaMemcpyAsync(s->h_norm2, s->d_norm2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CK(s, cudaStreamSynchronize(s->st));
     *r = std::sqrt(s->h_norm2[0]);
     *b = std::sqrt(s->h_norm2[1]);
+    return BLZ_OK;
+}
+
+// ||b - A p|| and ||b|| of the current rhs and p.
+static int residual_sync(blz_solver *s, double *r, double *b) {
+    return residual_on(s, s->rhs_r, s->rhs_b, s->p_r, s->p_b, r, b);
+}
+
+// The residual the solve's stopping rule reads: of the system the sweeps
+// work on, relative to ||b|| of the frame (the defect solve's
+// ||b - A p - A delta|| equals the pressure's residual ||b - A (p + delta)||).
+static int solve_residual(blz_solver *s, double *r, double *b) {
+    int rc = residual_on(s, s->sr_r, s->sr_b, s->sx_r, s->sx_b, r, b);
+    if (rc != BLZ_OK || !s->P.defect_correction) return rc;
+    double b2 = 0.0;
+    CK(s, cudaMemcpy(&b2, s->d_b2ref, sizeof(double), cudaMemcpyDeviceToHost));
+    *b = std::sqrt(b2);
     return BLZ_OK;
 }
 
@@ -593,19 +632,21 @@ static int choose_variant(blz_solver *s) {
     return BLZ_OK;
 }
 
-static int sweeps(blz_solver *s, int n) {
+static int sweeps_on(blz_solver *s, int n, const float *rr, const float *rb, float *pr, float *pb) {
     const SolveParams sp = solve_params(s->P);
     if (s->P.gs_order == BLZ_GS_PLANE) {
-        launch_plane_sweeps(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, s->st, &s->launches);
+        launch_plane_sweeps(s->g, sp, rr, rb, pr, pb, n, s->st, &s->launches);
     } else {
         int rc = choose_variant(s);
         if (rc != BLZ_OK) return rc;
-        launch_rbgs_sweeps(s->g, sp, s->rhs_r, s->rhs_b, s->p_r, s->p_b, n, s->st, &s->launches, s->variant,
-                           q_r(s), q_b(s));
+        launch_rbgs_sweeps(s->g, sp, rr, rb, pr, pb, n, s->st, &s->launches, s->variant, q_r(s), q_b(s));
     }
     CKL(s);
     return BLZ_OK;
 }
+
+// Sweeps of the system the solve works on (sr, sx).
+static int sweeps(blz_solver *s, int n) { return sweeps_on(s, n, s->sr_r, s->sr_b, s->sx_r, s->sx_b); }
 
 // The residual-controlled solve as one graph launch (graph_solve.cu).
 // Residual checks are a stopping test: every `chunk` sweeps the FP64
@@ -643,9 +684,10 @@ static int solve_device_loop(blz_solver *s, blz_step_stats *st, int chunk) {
         for (auto &x : s->graphs)
             if (!x.exec) { gr = &x; break; }
         if (!gr) return fail(s, BLZ_ERR_STATE, "too many check intervals");
-        cudaError_t e = build_solve_graph(s->g, solve_params(P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->partials,
+        cudaError_t e = build_solve_graph(s->g, solve_params(P), s->sr_r, s->sr_b, s->sx_r, s->sx_b, s->partials,
                                           s->n_partials, s->d_norm2, s->ctl, chunk, P.max_iter, P.tol, s->variant,
-                                          s->st, &gr->exec, &gr->body, &gr->prologue, q_r(s), q_b(s));
+                                          s->st, &gr->exec, &gr->body, &gr->prologue, q_r(s), q_b(s),
+                                          P.defect_correction ? s->d_b2ref : nullptr);
         if (e != cudaSuccess) return fail(s, BLZ_ERR_CUDA, "building the solve graph failed: %s", cudaGetErrorString(e));
         gr->chunk = chunk;
     }
@@ -703,7 +745,7 @@ static int warm_start(blz_solver *s, int variant, int *pre) {
             if ((rc = sweeps(s, *pre)) != BLZ_OK) return rc;
             variant = s->variant;
         } else {
-            launch_rbgs_sweeps(s->g, solve_params(P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, *pre, s->st,
+            launch_rbgs_sweeps(s->g, solve_params(P), s->sr_r, s->sr_b, s->sx_r, s->sx_b, *pre, s->st,
                                &s->launches, variant, q_r(s), q_b(s));
         }
         launch_rbgs_sweeps(s->g, solve_params(P), z_r, z_b, d_r, d_b, *pre, s->st, &s->launches, variant, q_r(s),
@@ -712,7 +754,7 @@ static int warm_start(blz_solver *s, int variant, int *pre) {
     } else {
         *pre = 0;
     }
-    rc = unet_combine(s->warm, P, s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->st, &s->launches);
+    rc = unet_combine(s->warm, P, s->sr_r, s->sr_b, s->sx_r, s->sx_b, s->st, &s->launches);
     if (rc != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
     return BLZ_OK;
 }
@@ -725,6 +767,20 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
         CK(s, cudaMemsetAsync(s->p_r, 0, half * sizeof(float), s->st));
         CK(s, cudaMemsetAsync(s->p_b, 0, half * sizeof(float), s->st));
     }
+    if (P.defect_correction) {
+        // The correction starts at the previous solve's rounding remainder
+        // (zero when p was set or swept since); the defect b - A p is formed
+        // in FP64 and kept as the sweeps' right-hand side.
+        if (!s->defect_valid || P.reset_pressure) {
+            CK(s, cudaMemsetAsync(s->dl_r, 0, half * sizeof(float), s->st));
+            CK(s, cudaMemsetAsync(s->dl_b, 0, half * sizeof(float), s->st));
+        }
+        s->launches += launch_defect(s->g, solve_params(P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->df_r, s->df_b,
+                                     s->partials, s->n_partials, s->d_norm2, s->st);
+        CKL(s);
+        CK(s, cudaMemcpyAsync(s->d_b2ref, s->d_norm2 + 1, sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+        s->defect_valid = false;
+    }
     int pre = 0;                                 // sweeps of p before the solve proper
     if (s->warm) {
         CK(s, cudaEventRecord(s->ev[8], s->st));
@@ -735,6 +791,12 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
     int rc = solve_body(s, st);
     if (rc != BLZ_OK) return rc;
     if ((rc = check_tb_timeouts(s)) != BLZ_OK) return rc;
+    if (P.defect_correction) {                 // p = RN(p + delta), delta = the exact remainder
+        launch_fold(s->g, s->p_r, s->p_b, s->dl_r, s->dl_b, s->st);
+        CKL(s);
+        s->launches++;
+        s->defect_valid = true;
+    }
     if (s->warm) {
         if ((rc = unet_timeout_flag(s->warm, s->st)) != BLZ_OK) return fail(s, rc, "warm start: %s", g_thread_err.c_str());
         if (st) {
@@ -790,13 +852,13 @@ static int solve_body(blz_solver *s, blz_step_stats *st) {
         if ((rc = timed_sweeps(P.max_iter)) != BLZ_OK) return rc;
         done = P.max_iter;
     } else {
-        if ((rc = residual_sync(s, &r, &b)) != BLZ_OK) return rc;
+        if ((rc = solve_residual(s, &r, &b)) != BLZ_OK) return rc;
         ++checks;
         while (done < P.max_iter && !(b == 0.0 || r / b <= P.tol)) {
             const int n = std::min(chunk, P.max_iter - done);
             if ((rc = timed_sweeps(n)) != BLZ_OK) return rc;
             done += n;
-            if ((rc = residual_sync(s, &r, &b)) != BLZ_OK) return rc;
+            if ((rc = solve_residual(s, &r, &b)) != BLZ_OK) return rc;
             ++checks;
             add_elapsed();
         }
@@ -805,7 +867,7 @@ static int solve_body(blz_solver *s, blz_step_stats *st) {
     s->last_iters = done;
     if (st) {
         if (!have) {
-            if ((rc = residual_sync(s, &r, &b)) != BLZ_OK) return rc;
+            if ((rc = solve_residual(s, &r, &b)) != BLZ_OK) return rc;
             ++checks;
             if (done > 0) add_elapsed();
         }
@@ -828,7 +890,8 @@ static int solve_body(blz_solver *s, blz_step_stats *st) {
 int blz_sweeps(blz_solver *s, int n) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     if (n < 0) return fail(s, BLZ_ERR_ARG, "negative sweep count %d", n);
-    const int rc = n > 0 ? sweeps(s, n) : BLZ_OK;
+    s->defect_valid = false;                    // p changes on its own: drop the remainder
+    const int rc = n > 0 ? sweeps_on(s, n, s->rhs_r, s->rhs_b, s->p_r, s->p_b) : BLZ_OK;
     return rc != BLZ_OK ? rc : check_tb_timeouts(s);
 }
 
@@ -838,6 +901,7 @@ int blz_tight_solve(blz_solver *s, double tol, int max_sweeps, double omega, int
         return fail(s, BLZ_ERR_ARG, "tight solve needs tol > 0, max_sweeps >= 0 and omega in (0, 2)");
     int sw = 0;
     double rel = 0.0;
+    s->defect_valid = false;
     const int e = tight_solve(s->g, solve_params(s->P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, tol, max_sweeps, omega,
                               50, s->st, &sw, &rel, &s->launches);
     if (e != 0) {
@@ -853,7 +917,9 @@ int blz_gradient(blz_solver *s) {
     if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
     const int c = s->cur;
     const float sc = s->P.dt / (s->P.density * s->P.dx);                       // FluidSolver.cu:612
-    launch_gradient(s->g, solve_params(s->P), sc, s->p_r, s->p_b, s->U[c], s->V[c], s->W[c], s->st);
+    const bool dl = s->P.defect_correction && s->defect_valid;   // the pressure is p + delta
+    launch_gradient(s->g, solve_params(s->P), sc, s->p_r, s->p_b, s->U[c], s->V[c], s->W[c], s->st,
+                    dl ? s->dl_r : nullptr, dl ? s->dl_b : nullptr);
     CKL(s);
     s->launches++;
     return BLZ_OK;
@@ -963,6 +1029,7 @@ int blz_set_field(blz_solver *s, int f, const float *src, int on_device) {
     const size_t n = n_of(s->P, f);
     if (!n) return fail(s, BLZ_ERR_ARG, "bad field %d", f);
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (f == BLZ_FIELD_P) s->defect_valid = false;
     if (f == BLZ_FIELD_P || f == BLZ_FIELD_RHS) {
         float *tmp = s->scratch;
         CK(s, cudaMemcpyAsync(tmp, src, n * sizeof(float), kind, s->st));

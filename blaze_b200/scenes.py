@@ -14,6 +14,7 @@ reference build.
 """
 from dataclasses import dataclass, field
 import math
+import os
 
 import numpy as np
 
@@ -89,6 +90,9 @@ class SceneSettings:
     # (V += dt (beta T - alpha rho) g); the reference has neither.
     density_field: int = 0
     buoyancy_alpha: float = 0.0
+    # Solve for the correction to the previous pressure with an FP64 defect
+    # (removes the FP32 floor of the residual; see blz_params).
+    defect_correction: int = 0
     extra: dict = field(default_factory=dict)
 
     def to_params(self):
@@ -111,6 +115,7 @@ class SceneSettings:
         p.device_loop, p.sweep_variant = self.device_loop, self.sweep_variant
         p.advect_scheme = self.advect_scheme
         p.density_field, p.buoyancy_alpha = int(self.density_field), float(self.buoyancy_alpha)
+        p.defect_correction = int(self.defect_correction)
         return p
 
 
@@ -294,3 +299,61 @@ def batch_scenes(count=64, seed=4, tol=1e-4, max_iter=20000, check_every=20, dim
         s.sourceMaxParticleCount = len(parts)
         out.append((s, parts))
     return out
+
+
+def large_fire_scene(n=384, seed=5, defect_correction=1):
+    """Large fire (384^3 by default), dx = 1/n, dt = 1/24: a ground disc of
+    radius 40 cells with 30000 particles, and two spheres of radius 10 cells
+    (9259 particles each, the plume family's density) moving along seeded
+    straight paths at 1 cell per frame; T ~ U[1, 2]; curl noise amplitude 0.8
+    with an 8-cell period; wind 0.3 cells/step along +x; epsilon at the
+    family's 64^3 strength (0.3 * 64 / n); walls except a free-surface top;
+    RBGS to FP64 relative residual 1e-4 (defect correction on by default: at
+    384^3 the FP32 floor of a plain iterate is above 1e-4).
+
+    Returns (SceneSettings, frame_particles): frame_particles(f) gives the
+    records of frame f (the disc is the same every frame, the spheres have
+    moved f cells along their paths), as the per-frame .part files of an
+    animated source (write_animated_source) hold them."""
+    s = SceneSettings(gridRes=(n, n, n), dx=1.0 / n, dt=1.0 / 24, closedBounds=(1, 1, 1, 0, 1, 1),
+                      maxIterSolve=60000, tol=1e-4, check_every=-1, buoyancy=1.0,
+                      vorticityConf=FAMILY_EPSILON_64 * 64.0 / n, turbulence_amp=0.8, turbulence_scale=8.0,
+                      windDir=0, windAmp=0.3 * (1.0 / n) / (1.0 / 24), bc_mode=_abi.BLZ_BC_FREE_SURFACE,
+                      defect_correction=defect_correction)
+    rng = PCG32(seed)
+    disc = disc_particles(rng, s, (n / 2, 2.0, n / 2), 40.0, 30000, temp=(1.0, 2.0))
+    paths = []
+    for _ in range(2):
+        r = 10.0
+        start = np.array([rng.uniform(r + 20, n - r - 20), rng.uniform(r + 4, 0.3 * n), rng.uniform(r + 20, n - r - 20)])
+        a = rng.uniform(0.0, 2.0 * math.pi)
+        rise = rng.uniform(-0.3, 0.3)
+        v = np.array([math.cos(a), rise, math.sin(a)])
+        v /= np.linalg.norm(v)                       # 1 cell per frame
+        ball = sphere_particles(rng, s, (0.0, 0.0, 0.0), r, int(round(2000 * (r / 6.0) ** 3)), temp=(1.0, 2.0))
+        paths.append((start, v, ball))
+    n_parts = len(disc) + sum(len(b) for _, _, b in paths)
+    s.sourceMaxParticleCount = n_parts
+    s.extra = {"paths": [(p.tolist(), v.tolist()) for p, v, _ in paths]}
+
+    def frame_particles(f):
+        out = [disc]
+        for start, v, ball in paths:
+            c = np.clip(start + f * v, 10.0 + 1.0, n - 11.0)            # stays inside the domain
+            moved = ball.copy()
+            moved[:, :3] += np.array(_cell_to_world(s, c), np.float32) - np.array(_cell_to_world(s, (0, 0, 0)),
+                                                                                   np.float32)
+            out.append(moved)
+        return np.concatenate(out)
+
+    return s, frame_particles
+
+
+def write_animated_source(directory, stem, frame_particles, frames):
+    """The per-frame particle caches of an animated source, named as the
+    reference's parser looks them up (<stem>_%04d.part, src/Parser.h:181-188);
+    returns the particleFile value of frame 1 for a .blz scene."""
+    os.makedirs(directory, exist_ok=True)
+    for f in frames:
+        write_part(os.path.join(directory, f"{stem}_{f:04d}.part"), frame_particles(f))
+    return f"{stem}_0001.part"
