@@ -72,9 +72,9 @@ __device__ __forceinline__ float inv_count(float den) {
 }
 __device__ __forceinline__ float div_count(float num, float den) {
     const float inv = inv_count(den);
-    const float q0 = num * inv;
-    const float e = fmaf(-q0, den, num);
-    return fmaf(e, inv, q0);
+    const float q0 = __fmul_rn(num, inv);
+    const float e = __fmaf_rn(-q0, den, num);
+    return __fmaf_rn(e, inv, q0);
 }
 
 // One Gauss-Seidel update p = (scale*rhs + sum p_nb)/n_nb (FluidSolver.cu:
@@ -83,16 +83,24 @@ __device__ __forceinline__ float div_count(float num, float den) {
 __device__ __forceinline__ float gs_update(const Geom &g, const SolveParams &sp, float rhs,
                                            const float *__restrict__ po, size_t q, int i, int j,
                                            int k, int s, int Wh) {
-    float num = sp.scale * rhs;
+    // The same rounded operations as gs_quad (a missing neighbour adds +0):
+    // num = RN(scale * rhs + x-), then RN adds of x+, y-, y+, z-, z+.
     float den = 0.0f;
     const bool dir = sp.dirichlet;
-    if (i > 0) { num += __ldg(po + q - (s ? 0 : 1)); den += 1.0f; } else if (dir && sp.open.xlo) den += 1.0f;
-    if (i < g.W - 1) { num += __ldg(po + q + (s ? 1 : 0)); den += 1.0f; } else if (dir && sp.open.xhi) den += 1.0f;
-    if (j > 0) { num += __ldg(po + q - Wh); den += 1.0f; } else if (dir && sp.open.ylo) den += 1.0f;
-    if (j < g.H - 1) { num += __ldg(po + q + Wh); den += 1.0f; } else if (dir && sp.open.yhi) den += 1.0f;
+    float xm = 0.0f, xp = 0.0f, ym = 0.0f, yp = 0.0f, zm = 0.0f, zp = 0.0f;
+    if (i > 0) { xm = __ldg(po + q - (s ? 0 : 1)); den += 1.0f; } else if (dir && sp.open.xlo) den += 1.0f;
+    if (i < g.W - 1) { xp = __ldg(po + q + (s ? 1 : 0)); den += 1.0f; } else if (dir && sp.open.xhi) den += 1.0f;
+    if (j > 0) { ym = __ldg(po + q - Wh); den += 1.0f; } else if (dir && sp.open.ylo) den += 1.0f;
+    if (j < g.H - 1) { yp = __ldg(po + q + Wh); den += 1.0f; } else if (dir && sp.open.yhi) den += 1.0f;
     const size_t pl = (size_t)Wh * g.H;
-    if (k > 0) { num += __ldg(po + q - pl); den += 1.0f; } else if (dir && sp.open.zlo) den += 1.0f;
-    if (k < g.D - 1) { num += __ldg(po + q + pl); den += 1.0f; } else if (dir && sp.open.zhi) den += 1.0f;
+    if (k > 0) { zm = __ldg(po + q - pl); den += 1.0f; } else if (dir && sp.open.zlo) den += 1.0f;
+    if (k < g.D - 1) { zp = __ldg(po + q + pl); den += 1.0f; } else if (dir && sp.open.zhi) den += 1.0f;
+    float num = __fmaf_rn(sp.scale, rhs, xm);
+    num = __fadd_rn(num, xp);
+    num = __fadd_rn(num, ym);
+    num = __fadd_rn(num, yp);
+    num = __fadd_rn(num, zm);
+    num = __fadd_rn(num, zp);
     return div_count(num, den);
 }
 
@@ -162,19 +170,78 @@ __device__ __forceinline__ float4 gs_quad(float scale, int s, float4 r, float4 o
     float out[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-        float num = scale * ra[t];
-        num += xl[t];
-        num += xr[t];
-        num += yma[t];
-        num += ypa[t];
-        num += zma[t];
-        num += zpa[t];
+        // every rounding explicit, so the packed form (gs_quad_pk) has the
+        // same bits
+        float num = __fmaf_rn(scale, ra[t], xl[t]);
+        num = __fadd_rn(num, xr[t]);
+        num = __fadd_rn(num, yma[t]);
+        num = __fadd_rn(num, ypa[t]);
+        num = __fadd_rn(num, zma[t]);
+        num = __fadd_rn(num, zpa[t]);
         const float den = t == 0 ? q.d0 : t == 3 ? q.d3 : q.db;
         const float inv = t == 0 ? q.i0 : t == 3 ? q.i3 : q.ib;
-        const float q0 = num * inv;
-        out[t] = fmaf(fmaf(-q0, den, num), inv, q0);
+        const float q0 = __fmul_rn(num, inv);
+        out[t] = __fmaf_rn(__fmaf_rn(-q0, den, num), inv, q0);
     }
     return make_float4(out[0], out[1], out[2], out[3]);
+}
+
+// gs_quad on Blackwell's paired FP32 instructions: cells (0,1) and (2,3) of
+// the quad go through one fma/add/mul.rn.f32x2 each, every lane rounded as
+// IEEE FP32, in gs_quad's order, so the bits equal gs_quad's.  -q0 comes
+// from num times -inv (round to nearest is symmetric, so this is -RN(num
+// inv) exactly).
+typedef unsigned long long f2_t;
+__device__ __forceinline__ f2_t f2(float lo, float hi) {
+    f2_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_split(f2_t v, float &lo, float &hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
+    f2_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f2_t f2_add(f2_t a, f2_t b) {
+    f2_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
+    f2_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+__device__ __forceinline__ f2_t gs_pair(f2_t scale2, f2_t r, f2_t xl, f2_t xr, f2_t ym, f2_t yp, f2_t zm, f2_t zp,
+                                        f2_t den, f2_t inv, f2_t ninv) {
+    f2_t num = f2_fma(scale2, r, xl);
+    num = f2_add(num, xr);
+    num = f2_add(num, ym);
+    num = f2_add(num, yp);
+    num = f2_add(num, zm);
+    num = f2_add(num, zp);
+    const f2_t q0 = f2_mul(num, inv);
+    const f2_t nq0 = f2_mul(num, ninv);
+    return f2_fma(f2_fma(nq0, den, num), inv, q0);
+}
+
+__device__ __forceinline__ float4 gs_quad_pk(float scale, int s, float4 r, float4 o, float xe, float4 ym, float4 yp,
+                                             float4 zm, float4 zp, const QuadDen &q) {
+    const f2_t sc = f2(scale, scale);
+    const f2_t xl01 = s == 0 ? f2(xe, o.x) : f2(o.x, o.y), xl23 = s == 0 ? f2(o.y, o.z) : f2(o.z, o.w);
+    const f2_t xr01 = s == 0 ? f2(o.x, o.y) : f2(o.y, o.z), xr23 = s == 0 ? f2(o.z, o.w) : f2(o.w, xe);
+    const f2_t a = gs_pair(sc, f2(r.x, r.y), xl01, xr01, f2(ym.x, ym.y), f2(yp.x, yp.y), f2(zm.x, zm.y),
+                           f2(zp.x, zp.y), f2(q.d0, q.db), f2(q.i0, q.ib), f2(-q.i0, -q.ib));
+    const f2_t b = gs_pair(sc, f2(r.z, r.w), xl23, xr23, f2(ym.z, ym.w), f2(yp.z, yp.w), f2(zm.z, zm.w),
+                           f2(zp.z, zp.w), f2(q.db, q.d3), f2(q.ib, q.i3), f2(-q.ib, -q.i3));
+    float4 out;
+    f2_split(a, out.x, out.y);
+    f2_split(b, out.z, out.w);
+    return out;
 }
 
 __device__ __forceinline__ float4 gs_segment(const SolveParams &sp, int s, bool first, bool last, float4 r,
@@ -332,7 +399,7 @@ __host__ __device__ inline int tb_dense_slot_bytes(int Wq, int rows_alloc) {
     return (rows_alloc * Wq * 16 + 127) & ~127;
 }
 
-template <bool WARPROW, bool TMA>
+template <bool WARPROW, bool TMA, bool PK = false>
 __global__ void __launch_bounds__(kTbThreads, 1)
 k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float *__restrict__ rhs_b,
            const float *__restrict__ pin_b, float *__restrict__ pout_r, float *__restrict__ pout_b, int TY, int ZC,
@@ -498,6 +565,11 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
             xe = S == 0 ? lds1(b - 4) : lds1(b + 16);
         }
         const float4 rv = rhs_ld(c, k, own, den);
+        if constexpr (PK) {
+            if (k > 0 && k < D - 1) return gs_quad_pk(sp.scale, S, rv, o, xe, ym, yp, zm, zp, qi);
+            return gs_quad_pk(sp.scale, S, rv, o, xe, ym, yp, zm, zp,
+                              quad_den(sp, S, first, last, hym, hyp, k > 0, k < D - 1));
+        }
         if (k > 0 && k < D - 1) return gs_quad(sp.scale, S, rv, o, xe, ym, yp, zm, zp, qi);
         return gs_quad(sp.scale, S, rv, o, xe, ym, yp, zm, zp, quad_den(sp, S, first, last, hym, hyp, k > 0, k < D - 1));
     };
@@ -685,7 +757,8 @@ static int device_sm_count() {
 // (one CTA per SM: its shared memory is most of the SM's), at least 8
 // planes.
 static void launch_tb_pass(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
-                           const float *pin_b, float *pout_r, float *pout_b, int ZC, bool tma, cudaStream_t st) {
+                           const float *pin_b, float *pout_r, float *pout_b, int ZC, bool tma, bool pk,
+                           cudaStream_t st) {
     const int Wq = g.W >> 3, TY = tb_rows_tile(Wq, g.H);
     static bool attr_set = false;
     if (!attr_set) {
@@ -693,6 +766,8 @@ static void launch_tb_pass(const Geom &g, const SolveParams &sp, const float *rh
         cudaFuncSetAttribute(k_rbgs_tb2<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
         cudaFuncSetAttribute(k_rbgs_tb2<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
         cudaFuncSetAttribute(k_rbgs_tb2<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_rbgs_tb2<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_rbgs_tb2<false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
         attr_set = true;
     }
     CUtensorMap mr{}, mb{}, mi{};
@@ -711,6 +786,13 @@ static void launch_tb_pass(const Geom &g, const SolveParams &sp, const float *rh
             k_rbgs_tb2<true, true><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC, mr, mb, mi);
         else
             k_rbgs_tb2<false, true><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC, mr, mb, mi);
+    } else if (pk) {
+        if (Wq == 32)
+            k_rbgs_tb2<true, false, true><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC, mr,
+                                                               mb, mi);
+        else
+            k_rbgs_tb2<false, false, true><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC, mr,
+                                                                mb, mi);
     } else {
         if (Wq == 32)
             k_rbgs_tb2<true, false><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC, mr, mb, mi);
@@ -722,12 +804,15 @@ static void launch_tb_pass(const Geom &g, const SolveParams &sp, const float *rh
 
 // (planes per thread, rows per block) of each segment-kernel variant; the
 // variants after them are the temporal-blocking pass with ZC planes per CTA
-// (0: sized to fill the SMs), the last with its rhs and input planes staged
-// by TMA.
+// (0: sized to fill the SMs): 9 with its rhs and input planes staged by TMA,
+// 10 with the stencil on paired FP32 instructions (gs_quad_pk).
 static const int kVariantKZ[kSegVariants] = {1, 2, 4, 8, 2, 4};
 static const int kVariantBY[kSegVariants] = {8, 8, 4, 4, 4, 8};
-static const int kVariantZC[kSweepVariants - kSegVariants] = {16, 32, 0, 0};
-static const bool kVariantTMA[kSweepVariants - kSegVariants] = {false, false, false, true};
+static const int kVariantZC[kSweepVariants - kSegVariants] = {16, 32, 0, 0, 0};
+static const bool kVariantTMA[kSweepVariants - kSegVariants] = {false, false, false, true, false};
+static const bool kVariantPK[kSweepVariants - kSegVariants] = {false, false, false, false, true};
+
+bool sweep_variant_uses_tma(int v) { return v >= kSegVariants && v < kSweepVariants && kVariantTMA[v - kSegVariants]; }
 
 int sweep_variant_count(const Geom &g) {
     if ((g.W & 7) != 0) return 0;
@@ -742,10 +827,10 @@ void launch_rbgs_sweeps(const Geom &g, const SolveParams &sp, const float *rhs_r
         // result lands in p; the remaining sweeps run unblocked.
         const int passes = (sweeps / 4) * 2;
         const int zc = kVariantZC[variant - kSegVariants];
-        const bool tma = kVariantTMA[variant - kSegVariants];
+        const bool tma = kVariantTMA[variant - kSegVariants], pk = kVariantPK[variant - kSegVariants];
         for (int i = 0; i < passes; ++i) {
-            if ((i & 1) == 0) launch_tb_pass(g, sp, rhs_r, rhs_b, p_b, q_r, q_b, zc, tma, st);
-            else launch_tb_pass(g, sp, rhs_r, rhs_b, q_b, p_r, p_b, zc, tma, st);
+            if ((i & 1) == 0) launch_tb_pass(g, sp, rhs_r, rhs_b, p_b, q_r, q_b, zc, tma, pk, st);
+            else launch_tb_pass(g, sp, rhs_r, rhs_b, q_b, p_r, p_b, zc, tma, pk, st);
         }
         *launches += passes;
         sweeps -= 2 * passes;

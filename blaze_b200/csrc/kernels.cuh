@@ -71,8 +71,11 @@ void launch_divergence(const Geom &g, const float *U, const float *V, const floa
 // sweeps per pass; all give identical results.  Other W use the one-cell
 // kernel.  sweep_variant_count: variants available for this grid (0: W % 8).
 constexpr int kSegVariants = 6;
-constexpr int kSweepVariants = 10;
+constexpr int kSweepVariants = 11;
 int  sweep_variant_count(const Geom &g);
+// The temporal-blocking variant whose loads are TMA bulk copies (bounded
+// waits that may give up: tb_take_timeouts).
+bool sweep_variant_uses_tma(int v);
 // Bounded TMA waits of the temporal-blocking pass that gave up since the last
 // call (then reset); nonzero means a pass produced a wrong result.
 unsigned int tb_take_timeouts();

@@ -17,6 +17,8 @@
 #include <tuple>
 #include <vector>
 
+#include <sys/stat.h>
+
 #include "kernels.cuh"
 
 using namespace blz;
@@ -548,6 +550,63 @@ static float *q_b(blz_solver *s) { return s->scratch + 4 * n_of(s->P, 0) + n_of(
 static std::mutex g_tune_mu;
 static std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
 
+// The tuner's choices persist across processes in a small text file, one
+// line "<device name>|<W>|<H>|<D>|<variants offered>|<variant count> <choice>"
+// per grid: BLZ_TUNE_CACHE names the file ("off" or empty: none), default
+// $XDG_CACHE_HOME/blaze_b200/sweep_variants.txt or ~/.cache/... .
+static std::string tune_cache_path() {
+    if (const char *p = std::getenv("BLZ_TUNE_CACHE")) {
+        if (!*p || std::strcmp(p, "off") == 0) return std::string();
+        return p;
+    }
+    std::string base;
+    if (const char *x = std::getenv("XDG_CACHE_HOME")) base = x;
+    else if (const char *h = std::getenv("HOME")) base = std::string(h) + "/.cache";
+    else return std::string();
+    return base + "/blaze_b200/sweep_variants.txt";
+}
+
+static std::string tune_key(int device, const Geom &g, int offered) {
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return std::string();
+    char buf[400];
+    std::snprintf(buf, sizeof buf, "%s|%d|%d|%d|%d|%d", prop.name, g.W, g.H, g.D, offered, kSweepVariants);
+    for (char *c = buf; *c; ++c)
+        if (*c == ' ') *c = '_';
+    return buf;
+}
+
+static int tune_file_lookup(const std::string &key) {
+    const std::string path = tune_cache_path();
+    if (path.empty() || key.empty()) return -1;
+    FILE *f = std::fopen(path.c_str(), "r");
+    if (!f) return -1;
+    char line[512];
+    int found = -1;
+    while (std::fgets(line, sizeof line, f)) {
+        char k[450];
+        int v = -1;
+        if (std::sscanf(line, "%449s %d", k, &v) == 2 && key == k) found = v;   // the last entry wins
+    }
+    std::fclose(f);
+    return found;
+}
+
+static void tune_file_store(const std::string &key, int v) {
+    const std::string path = tune_cache_path();
+    if (path.empty() || key.empty()) return;
+    const size_t slash = path.rfind('/');
+    if (slash != std::string::npos && slash > 0) {
+        // create the directory chain (best effort)
+        for (size_t i = 1; i <= slash; ++i)
+            if (path[i] == '/' || i == slash) mkdir(path.substr(0, i == slash ? slash : i).c_str(), 0755);
+    }
+    if (FILE *f = std::fopen(path.c_str(), "a")) {
+        std::fprintf(f, "%s %d\n", key.c_str(), v);
+        std::fclose(f);
+    }
+}
+
 static int choose_variant(blz_solver *s) {
     if (s->variant != -2) return BLZ_OK;
     const int nv = s->P.temporal_block == 1 ? std::min(sweep_variant_count(s->g), kSegVariants)
@@ -559,10 +618,17 @@ static int choose_variant(blz_solver *s) {
         return BLZ_OK;
     }
     const auto key = std::make_tuple(s->device, s->g.W, s->g.H, s->g.D * 2 + (nv > kSegVariants ? 1 : 0));
+    const std::string fkey = tune_key(s->device, s->g, nv);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) { s->variant = it->second; return BLZ_OK; }
+        const int v = tune_file_lookup(fkey);
+        if (v >= 0 && v < nv) {
+            g_tune_cache[key] = v;
+            s->variant = v;
+            return BLZ_OK;
+        }
     }
     const size_t half = n_of(s->P, 0) / 2;
     float *tr = s->scratch, *tb = s->scratch + half;
@@ -629,6 +695,7 @@ static int choose_variant(blz_solver *s) {
     s->variant = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[key] = best;
+    tune_file_store(fkey, best);
     return BLZ_OK;
 }
 
@@ -722,7 +789,7 @@ static int solve_body(blz_solver *s, blz_step_stats *st);
 // The TMA-staged pass counts bounded waits that gave up; after work that may
 // have used it, a nonzero count is reported (that pass's result is wrong).
 static int check_tb_timeouts(blz_solver *s) {
-    if (s->variant != kSweepVariants - 1) return BLZ_OK;
+    if (!sweep_variant_uses_tma(s->variant)) return BLZ_OK;
     CK(s, cudaStreamSynchronize(s->st));
     if (tb_take_timeouts()) return fail(s, BLZ_ERR_TIMEOUT, "temporal-blocking pass: a bounded TMA wait gave up");
     return BLZ_OK;

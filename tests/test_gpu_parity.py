@@ -276,9 +276,11 @@ def test_device_loop_hits_the_cap():
 
 
 def test_sweep_variants_are_bitwise_identical():
-    """Every launch shape of the segment sweep kernel gives the same bits."""
+    """Every launch shape of the segment sweep kernel, and every temporal-
+    blocking pass (variants 6-10: TMA-staged, paired FP32), gives the same
+    bits."""
     ref = None
-    for v in range(10):
+    for v in range(11):
         gpu, _ = pair(scene(dims=(64, 20, 18), bc_mode=BLZ_BC_FREE_SURFACE, sweep_variant=v), 65)
         gpu.sweeps(7)
         p = gpu.get("P")
@@ -299,7 +301,7 @@ def test_fixed_sweeps_match_oracle():
 def test_sweep_variants_identical_full_width_rows():
     """W = 256: a warp spans a whole packed row (32 segments of 4)."""
     ref = None
-    for v in range(10):
+    for v in range(11):
         gpu, _ = pair(scene(dims=(256, 6, 8), bc_mode=BLZ_BC_FREE_SURFACE, sweep_variant=v), 67)
         gpu.sweeps(5)
         p = gpu.get("P")
@@ -314,17 +316,18 @@ def test_sweep_variants_identical_full_width_rows():
 @pytest.mark.parametrize("dims,bc", [((64, 200, 70), BLZ_BC_FREE_SURFACE), ((256, 40, 40), BLZ_BC_FREE_SURFACE),
                                      ((384, 20, 12), BLZ_BC_REF_COMPAT), ((128, 48, 33), BLZ_BC_FREE_SURFACE)])
 def test_temporal_blocking_equals_plain_sweeps(dims, bc):
-    """The two-sweeps-per-pass kernels (variants 6-9, 9 with TMA-staged rhs and
-    input planes: several row bands and z chunks here) give the plain segment
-    kernel's bits."""
+    """The two-sweeps-per-pass kernels (variants 6-10, 9 with TMA-staged rhs
+    and input planes, 10 with the stencil on paired FP32 instructions:
+    several row bands and z chunks here) give the plain segment kernel's
+    bits."""
     out = {}
-    for v in (0, 6, 7, 8, 9):
+    for v in (0, 6, 7, 8, 9, 10):
         gpu, _ = pair(scene(dims=dims, bc_mode=bc, sweep_variant=v), 68)
         gpu.sweeps(10)
         out[v] = gpu.get("P")
         gpu.close()
     assert np.isfinite(out[0]).all() and np.abs(out[0]).max() > 0
-    for v in (6, 7, 8, 9):
+    for v in (6, 7, 8, 9, 10):
         np.testing.assert_array_equal(out[v], out[0], err_msg=f"variant {v}")
 
 
@@ -486,3 +489,43 @@ def test_defect_correction_gradient_and_device_loop():
     assert out[0][:3] == out[1][:3]
     np.testing.assert_array_equal(out[0][3], out[1][3])
     np.testing.assert_array_equal(out[0][4], out[1][4])
+
+
+_TUNE_CHILD = r"""
+import sys, json
+sys.path.insert(0, sys.argv[1])
+from blaze_b200 import FluidSolver, SceneSettings, Timer, BLZ_BC_FREE_SURFACE
+scn = SceneSettings(gridRes=(256, 40, 40), dx=1.0 / 20, bc_mode=BLZ_BC_FREE_SURFACE, maxIterSolve=8)
+with FluidSolver(Timer(), scn) as s:
+    st = s.solve()
+print(json.dumps({"variant": st["sweep_variant"]}))
+"""
+
+
+def test_sweep_autotuner_choice_persists(tmp_path):
+    """The tuner's choice goes to the cache file (BLZ_TUNE_CACHE); a later
+    process with an entry for its device and grid takes that entry instead of
+    tuning (the last entry for a key wins)."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cache = tmp_path / "tune.txt"
+    env = dict(os.environ, BLZ_TUNE_CACHE=str(cache))
+    env.pop("BLZ_SWEEP_VARIANT", None)
+
+    def child():
+        r = subprocess.run([sys.executable, "-c", _TUNE_CHILD, root], env=env, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        return json.loads(r.stdout.strip().splitlines()[-1])["variant"]
+
+    first = child()
+    lines = cache.read_text().split("\n")
+    key, v = lines[0].split()
+    assert int(v) == first and key.endswith("|256|40|40|11|11")
+    forced = (first + 1) % 11
+    with open(cache, "a") as f:
+        f.write(f"{key} {forced}\n")
+    assert child() == forced
