@@ -37,16 +37,14 @@ __global__ void k_ctl_mark(SolveCtl *c, int stop) {
 }
 
 // Reads {||r||^2, ||b||^2}, records them, and sets whether the loop goes on.
-// b2_ref (a defect-correction solve): the ||b||^2 of the frame's system, in
-// place of the defect's own norm.
 __global__ void k_ctl_check(SolveCtl *c, const double *__restrict__ norm2, cudaGraphConditionalHandle h,
-                            int after_sweeps, int chunk, int max_iter, double tol, const double *__restrict__ b2_ref) {
+                            int after_sweeps, int chunk, int max_iter, double tol) {
     if (after_sweeps) {
         c->iters += chunk;
         c->check_ns += global_ns() - c->t1;
     }
     c->checks += 1;
-    const double r2 = norm2[0], b2 = b2_ref ? *b2_ref : norm2[1];
+    const double r2 = norm2[0], b2 = norm2[1];
     c->r2 = r2;
     c->b2 = b2;
     const bool conv = b2 == 0.0 || sqrt(r2) / sqrt(b2) <= tol;
@@ -64,20 +62,30 @@ cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float 
                               float *p_r, float *p_b, double *partials, int n_partials, double *norm2,
                               SolveCtl *ctl, int chunk, int max_iter, double tol, int variant, cudaStream_t st,
                               cudaGraphExec_t *exec_out, int *body_kernels, int *prologue_kernels, float *q_r,
-                              float *q_b, const double *b2_ref) {
+                              float *q_b, const DefectArrays *dfa) {
     cudaError_t err = cudaSuccess;
     cudaGraph_t graph = nullptr, body = nullptr;
     cudaGraphConditionalHandle handle;
     cudaGraphNode_t cond_node;
     long long dummy = 0;
     *exec_out = nullptr;
+    // The stopping test: the FP64 residual of (rhs, p); for a defect-
+    // correction solve (after sweeps) d folded into p and a fresh defect,
+    // whose norms are those of the pressure p + d.  Returns its launches.
+    auto check = [&](bool after) -> int {
+        if (!dfa) return launch_residual(g, sp, rhs_r, rhs_b, p_r, p_b, partials, n_partials, norm2, st);
+        int n = 0;
+        if (after) { launch_fold(g, dfa->p_r, dfa->p_b, dfa->d_r, dfa->d_b, st); ++n; }
+        return n + launch_defect(g, sp, dfa->rhs_r, dfa->rhs_b, dfa->p_r, dfa->p_b, dfa->d_r, dfa->d_b, dfa->df_r,
+                                 dfa->df_b, partials, n_partials, norm2, st);
+    };
     CKG(cudaGraphCreate(&graph, 0));
     CKG(cudaGraphConditionalHandleCreate(&handle, graph, 0, 0));
     // Prologue: reset the control block, check once before any sweep.
     CKG(cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     k_ctl_begin<<<1, 1, 0, st>>>(ctl);
-    *prologue_kernels = 1 + launch_residual(g, sp, rhs_r, rhs_b, p_r, p_b, partials, n_partials, norm2, st) + 1;
-    k_ctl_check<<<1, 1, 0, st>>>(ctl, norm2, handle, 0, chunk, max_iter, tol, b2_ref);
+    *prologue_kernels = 1 + check(false) + 1;
+    k_ctl_check<<<1, 1, 0, st>>>(ctl, norm2, handle, 0, chunk, max_iter, tol);
     {
         cudaStreamCaptureStatus status;
         const cudaGraphNode_t *deps = nullptr;
@@ -98,8 +106,8 @@ cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float 
     k_ctl_mark<<<1, 1, 0, st>>>(ctl, 0);
     launch_rbgs_sweeps(g, sp, rhs_r, rhs_b, p_r, p_b, chunk, st, &dummy, variant, q_r, q_b);
     k_ctl_mark<<<1, 1, 0, st>>>(ctl, 1);
-    *body_kernels = 2 + (int)dummy + launch_residual(g, sp, rhs_r, rhs_b, p_r, p_b, partials, n_partials, norm2, st) + 1;
-    k_ctl_check<<<1, 1, 0, st>>>(ctl, norm2, handle, 1, chunk, max_iter, tol, b2_ref);
+    *body_kernels = 2 + (int)dummy + check(true) + 1;
+    k_ctl_check<<<1, 1, 0, st>>>(ctl, norm2, handle, 1, chunk, max_iter, tol);
     CKG(cudaStreamEndCapture(st, &body));
     CKG(cudaGraphInstantiate(exec_out, graph, 0));
 done:

@@ -1289,40 +1289,46 @@ void launch_gradient(const Geom &g, const SolveParams &sp, float s, const float 
         k_gradient<false><<<face_grid(g), face_block(), 0, st>>>(g, sp, s, p_r, p_b, U, V, W, nullptr, nullptr);
 }
 
-// The defect of the current pressure, for the defect-correction solve: with
-// b = scale * rhs, r = b - A p0 evaluated in FP64 (the stencil in deviation
-// form on the FP32 p0, exact in FP64) and stored as the FP32 right-hand side
-// rhs' = r / scale of the system A delta = r that the sweeps then solve for
-// the correction delta.  Per-block partial sums of b^2 (FP64) go to
-// part[2 * block + 1] and of r^2 to part[2 * block]; k_defect_total sums them
-// in block order into out2 = {||r||^2, ||b||^2}.
+// The defect of the current pressure for the defect-correction solve, in
+// FP64 from the FP32 arrays: with b = scale * rhs, the sweeps' right-hand side
+// rhs' = (b - A p) / scale (stored FP32; the sweeps solve A delta = b - A p
+// for the correction delta) and the residual of the pressure p + delta,
+// r = b - A p - A delta (both stencils in deviation form, exact in FP64).
+// Per-block partial sums of r^2 and b^2 go to part[2 * block] and
+// part[2 * block + 1]; k_defect_total sums them in block order into
+// out2 = {||r||^2, ||b||^2}.
 constexpr int kDefectThreads = 256;
 constexpr int kDefectBlocks = 1184;
 
+__device__ __forceinline__ double stencil64(const float *__restrict__ pr, const float *__restrict__ pb, int i, int j,
+                                            int k, int W, int H, int D, int Wh, const OpenFaces &o, bool dir) {
+    const double pc = (double)pval(pr, pb, i, j, k, Wh, H);
+    double d = 0.0;
+    if (i > 0) d += pc - (double)pval(pr, pb, i - 1, j, k, Wh, H); else if (dir && o.xlo) d += pc;
+    if (i < W - 1) d += pc - (double)pval(pr, pb, i + 1, j, k, Wh, H); else if (dir && o.xhi) d += pc;
+    if (j > 0) d += pc - (double)pval(pr, pb, i, j - 1, k, Wh, H); else if (dir && o.ylo) d += pc;
+    if (j < H - 1) d += pc - (double)pval(pr, pb, i, j + 1, k, Wh, H); else if (dir && o.yhi) d += pc;
+    if (k > 0) d += pc - (double)pval(pr, pb, i, j, k - 1, Wh, H); else if (dir && o.zlo) d += pc;
+    if (k < D - 1) d += pc - (double)pval(pr, pb, i, j, k + 1, Wh, H); else if (dir && o.zhi) d += pc;
+    return d;
+}
+
 __global__ void __launch_bounds__(kDefectThreads)
 k_defect(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float *__restrict__ rhs_b,
-         const float *__restrict__ pr, const float *__restrict__ pb, float *__restrict__ def_r,
-         float *__restrict__ def_b, double *__restrict__ part) {
+         const float *__restrict__ pr, const float *__restrict__ pb, const float *__restrict__ dr,
+         const float *__restrict__ db, float *__restrict__ def_r, float *__restrict__ def_b,
+         double *__restrict__ part) {
     const int Wh = g.W >> 1, H = g.H;
     const long long n = (long long)g.W * g.H * g.D;
-    const OpenFaces &o = sp.open;
-    const bool dir = sp.dirichlet;
     double r2 = 0.0, b2 = 0.0;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(c % g.W), j = (int)((c / g.W) % g.H), k = (int)(c / ((long long)g.W * g.H));
         const size_t q = pidx(i, j, k, Wh, H);
         const bool black = (i + j + k) & 1;
-        const double pc = (double)(black ? pb : pr)[q];
-        double d = 0.0;
-        if (i > 0) d += pc - (double)pval(pr, pb, i - 1, j, k, Wh, H); else if (dir && o.xlo) d += pc;
-        if (i < g.W - 1) d += pc - (double)pval(pr, pb, i + 1, j, k, Wh, H); else if (dir && o.xhi) d += pc;
-        if (j > 0) d += pc - (double)pval(pr, pb, i, j - 1, k, Wh, H); else if (dir && o.ylo) d += pc;
-        if (j < g.H - 1) d += pc - (double)pval(pr, pb, i, j + 1, k, Wh, H); else if (dir && o.yhi) d += pc;
-        if (k > 0) d += pc - (double)pval(pr, pb, i, j, k - 1, Wh, H); else if (dir && o.zlo) d += pc;
-        if (k < g.D - 1) d += pc - (double)pval(pr, pb, i, j, k + 1, Wh, H); else if (dir && o.zhi) d += pc;
         const double b = sp.scale_d * (double)(black ? rhs_b : rhs_r)[q];
-        const double r = b - d;
-        (black ? def_b : def_r)[q] = (float)(r / sp.scale_d);
+        const double bp = b - stencil64(pr, pb, i, j, k, g.W, g.H, g.D, Wh, sp.open, sp.dirichlet);
+        (black ? def_b : def_r)[q] = (float)(bp / sp.scale_d);
+        const double r = bp - stencil64(dr, db, i, j, k, g.W, g.H, g.D, Wh, sp.open, sp.dirichlet);
         r2 += r * r;
         b2 += b * b;
     }
@@ -1371,10 +1377,10 @@ __global__ void k_fold(long long n, float *__restrict__ pr, float *__restrict__ 
 }
 
 int launch_defect(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b, const float *p_r,
-                  const float *p_b, float *def_r, float *def_b, double *partials, int max_partials, double *out2,
-                  cudaStream_t st) {
+                  const float *p_b, const float *d_r, const float *d_b, float *def_r, float *def_b, double *partials,
+                  int max_partials, double *out2, cudaStream_t st) {
     const int nb = std::min(kDefectBlocks, max_partials);
-    k_defect<<<nb, kDefectThreads, 0, st>>>(g, sp, rhs_r, rhs_b, p_r, p_b, def_r, def_b, partials);
+    k_defect<<<nb, kDefectThreads, 0, st>>>(g, sp, rhs_r, rhs_b, p_r, p_b, d_r, d_b, def_r, def_b, partials);
     k_defect_total<<<1, 32, 0, st>>>(partials, nb, out2);
     return 2;
 }

@@ -102,12 +102,19 @@ int  residual_blocks(const Geom &g);
 void launch_gradient(const Geom &g, const SolveParams &sp, float dt_over_rho_dx, const float *p_r,
                      const float *p_b, float *U, float *V, float *W, cudaStream_t st, const float *d_r = nullptr,
                      const float *d_b = nullptr);
-// Defect-correction solve: rhs' = (scale rhs - A p) / scale into def (FP64
-// stencil), out2 = {||scale rhs - A p||^2, ||scale rhs||^2}; returns the
-// launches (2).  launch_fold: p += d.
+// Defect-correction solve: rhs' = (b - A p) / scale into def and
+// out2 = {||b - A p - A d||^2, ||b||^2}, b = scale rhs (FP64 stencils);
+// returns the launches (2).  launch_fold: p = RN(p + d), d = the exact
+// remainder.
 int  launch_defect(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b, const float *p_r,
-                   const float *p_b, float *def_r, float *def_b, double *partials, int max_partials, double *out2,
-                   cudaStream_t st);
+                   const float *p_b, const float *d_r, const float *d_b, float *def_r, float *def_b, double *partials,
+                   int max_partials, double *out2, cudaStream_t st);
+// The arrays of a defect-correction solve (build_solve_graph): its checks
+// fold d into p and form a fresh defect instead of a plain residual.
+struct DefectArrays {
+    const float *rhs_r, *rhs_b;
+    float *p_r, *p_b, *d_r, *d_b, *df_r, *df_b;
+};
 void launch_fold(const Geom &g, float *p_r, float *p_b, float *d_r, float *d_b, cudaStream_t st);
 // Packed <-> natural layout.
 void launch_pack(const Geom &g, const float *nat, float *red, float *black, cudaStream_t st);
@@ -127,7 +134,7 @@ cudaError_t build_solve_graph(const Geom &g, const SolveParams &sp, const float 
                               float *p_r, float *p_b, double *partials, int n_partials, double *norm2,
                               SolveCtl *ctl, int chunk, int max_iter, double tol, int variant, cudaStream_t st,
                               cudaGraphExec_t *exec_out, int *body_kernels, int *prologue_kernels,
-                              float *q_r = nullptr, float *q_b = nullptr, const double *b2_ref = nullptr);
+                              float *q_r = nullptr, float *q_b = nullptr, const DefectArrays *dfa = nullptr);
 
 // -- batched solve over many grids (k_project.cu kernels, batch.cu graph) ---
 struct BatchSim {

@@ -42,7 +42,6 @@ struct blz_solver {
     float *df_r = nullptr, *df_b = nullptr, *dl_r = nullptr, *dl_b = nullptr;
     const float *sr_r = nullptr, *sr_b = nullptr;
     float *sx_r = nullptr, *sx_b = nullptr;
-    double *d_b2ref = nullptr;                  // ||b||^2 of the current defect solve (device)
     bool defect_valid = false;                  // dl holds the remainder of the last solve
     float *scratch = nullptr;                   // 6 T-sized arrays (vorticity)
     // sourcing: compacted particle records, per-field index boxes and the
@@ -178,7 +177,7 @@ static void release(blz_solver *s) {
     }
     cudaFree(s->pdens);
     cudaFree(s->p_r); cudaFree(s->p_b); cudaFree(s->rhs_r); cudaFree(s->rhs_b);
-    cudaFree(s->df_r); cudaFree(s->df_b); cudaFree(s->dl_r); cudaFree(s->dl_b); cudaFree(s->d_b2ref);
+    cudaFree(s->df_r); cudaFree(s->df_b); cudaFree(s->dl_r); cudaFree(s->dl_b);
     cudaFree(s->scratch);
     cudaFree(s->parts); cudaFree(s->boxes); cudaFree(s->bin_start); cudaFree(s->bin_list); cudaFree(s->active);
     cudaFree(s->partials); cudaFree(s->d_norm2);
@@ -238,7 +237,6 @@ int blz_create(const blz_params *p, blz_solver **out) {
     ok = ok && alloc(&s->p_r, nT / 2) && alloc(&s->p_b, nT / 2) && alloc(&s->rhs_r, nT / 2) && alloc(&s->rhs_b, nT / 2);
     if (p->defect_correction) {
         ok = ok && alloc(&s->df_r, nT / 2) && alloc(&s->df_b, nT / 2) && alloc(&s->dl_r, nT / 2) && alloc(&s->dl_b, nT / 2);
-        ok = ok && cudaMalloc(&s->d_b2ref, sizeof(double)) == cudaSuccess;
         s->sr_r = s->df_r; s->sr_b = s->df_b; s->sx_r = s->dl_r; s->sx_b = s->dl_b;
     } else {
         s->sr_r = s->rhs_r; s->sr_b = s->rhs_b; s->sx_r = s->p_r; s->sx_b = s->p_b;
@@ -525,15 +523,36 @@ static int residual_sync(blz_solver *s, double *r, double *b) {
     return residual_on(s, s->rhs_r, s->rhs_b, s->p_r, s->p_b, r, b);
 }
 
-// The residual the solve's stopping rule reads: of the system the sweeps
-// work on, relative to ||b|| of the frame (the defect solve's
-// ||b - A p - A delta|| equals the pressure's residual ||b - A (p + delta)||).
-static int solve_residual(blz_solver *s, double *r, double *b) {
-    int rc = residual_on(s, s->sr_r, s->sr_b, s->sx_r, s->sx_b, r, b);
-    if (rc != BLZ_OK || !s->P.defect_correction) return rc;
-    double b2 = 0.0;
-    CK(s, cudaMemcpy(&b2, s->d_b2ref, sizeof(double), cudaMemcpyDeviceToHost));
-    *b = std::sqrt(b2);
+static DefectArrays defect_arrays(blz_solver *s) {
+    return DefectArrays{s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->dl_r, s->dl_b, s->df_r, s->df_b};
+}
+
+// The defect of p (+ delta) into df with the norms of b - A (p + delta)
+// in d_norm2 (defect-correction solves).
+static int launch_defect_of(blz_solver *s) {
+    const DefectArrays a = defect_arrays(s);
+    s->launches += launch_defect(s->g, solve_params(s->P), a.rhs_r, a.rhs_b, a.p_r, a.p_b, a.d_r, a.d_b, a.df_r,
+                                 a.df_b, s->partials, s->n_partials, s->d_norm2, s->st);
+    CKL(s);
+    return BLZ_OK;
+}
+
+// The residual the solve's stopping rule reads, synchronised to the host.  A
+// defect-correction solve (after sweeps) first folds delta into p, then forms
+// a fresh FP64 defect, whose norms are those of the pressure p + delta.
+static int solve_residual(blz_solver *s, double *r, double *b, bool after_sweeps) {
+    if (!s->P.defect_correction) return residual_on(s, s->sr_r, s->sr_b, s->sx_r, s->sx_b, r, b);
+    if (after_sweeps) {
+        launch_fold(s->g, s->p_r, s->p_b, s->dl_r, s->dl_b, s->st);
+        CKL(s);
+        s->launches++;
+    }
+    int rc = launch_defect_of(s);
+    if (rc != BLZ_OK) return rc;
+    CK(s, cudaMemcpyAsync(s->h_norm2, s->d_norm2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(s, cudaStreamSynchronize(s->st));
+    *r = std::sqrt(s->h_norm2[0]);
+    *b = std::sqrt(s->h_norm2[1]);
     return BLZ_OK;
 }
 
@@ -747,6 +766,7 @@ static int solve_device_loop(blz_solver *s, blz_step_stats *st, int chunk) {
     blz_solver::SolveGraph *gr = nullptr;
     for (auto &x : s->graphs)
         if (x.exec && x.chunk == chunk) gr = &x;
+    const DefectArrays dfa = defect_arrays(s);
     if (!gr) {
         for (auto &x : s->graphs)
             if (!x.exec) { gr = &x; break; }
@@ -754,7 +774,7 @@ static int solve_device_loop(blz_solver *s, blz_step_stats *st, int chunk) {
         cudaError_t e = build_solve_graph(s->g, solve_params(P), s->sr_r, s->sr_b, s->sx_r, s->sx_b, s->partials,
                                           s->n_partials, s->d_norm2, s->ctl, chunk, P.max_iter, P.tol, s->variant,
                                           s->st, &gr->exec, &gr->body, &gr->prologue, q_r(s), q_b(s),
-                                          P.defect_correction ? s->d_b2ref : nullptr);
+                                          P.defect_correction ? &dfa : nullptr);
         if (e != cudaSuccess) return fail(s, BLZ_ERR_CUDA, "building the solve graph failed: %s", cudaGetErrorString(e));
         gr->chunk = chunk;
     }
@@ -842,10 +862,8 @@ int blz_solve(blz_solver *s, blz_step_stats *st) {
             CK(s, cudaMemsetAsync(s->dl_r, 0, half * sizeof(float), s->st));
             CK(s, cudaMemsetAsync(s->dl_b, 0, half * sizeof(float), s->st));
         }
-        s->launches += launch_defect(s->g, solve_params(P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, s->df_r, s->df_b,
-                                     s->partials, s->n_partials, s->d_norm2, s->st);
-        CKL(s);
-        CK(s, cudaMemcpyAsync(s->d_b2ref, s->d_norm2 + 1, sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+        const int rc0 = launch_defect_of(s);
+        if (rc0 != BLZ_OK) return rc0;
         s->defect_valid = false;
     }
     int pre = 0;                                 // sweeps of p before the solve proper
@@ -919,13 +937,13 @@ static int solve_body(blz_solver *s, blz_step_stats *st) {
         if ((rc = timed_sweeps(P.max_iter)) != BLZ_OK) return rc;
         done = P.max_iter;
     } else {
-        if ((rc = solve_residual(s, &r, &b)) != BLZ_OK) return rc;
+        if ((rc = solve_residual(s, &r, &b, false)) != BLZ_OK) return rc;
         ++checks;
         while (done < P.max_iter && !(b == 0.0 || r / b <= P.tol)) {
             const int n = std::min(chunk, P.max_iter - done);
             if ((rc = timed_sweeps(n)) != BLZ_OK) return rc;
             done += n;
-            if ((rc = solve_residual(s, &r, &b)) != BLZ_OK) return rc;
+            if ((rc = solve_residual(s, &r, &b, true)) != BLZ_OK) return rc;
             ++checks;
             add_elapsed();
         }
@@ -934,7 +952,7 @@ static int solve_body(blz_solver *s, blz_step_stats *st) {
     s->last_iters = done;
     if (st) {
         if (!have) {
-            if ((rc = solve_residual(s, &r, &b)) != BLZ_OK) return rc;
+            if ((rc = solve_residual(s, &r, &b, done > 0)) != BLZ_OK) return rc;
             ++checks;
             if (done > 0) add_elapsed();
         }

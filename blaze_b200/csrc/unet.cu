@@ -12,17 +12,18 @@
 //   2  p_prev / rms(p_prev)
 //   3  r / rms(r)                r = b - A p_prev, A the solver's 7-point operator
 // Output: delta = head(features) and the correction d = kappa*rms(r)*delta.
-// The solver then sweeps p and d alike k times (d with a zero right-hand
+// The solver may sweep p and d alike k times first (d with a zero right-hand
 // side; Gauss-Seidel is affine, so S^k(p + alpha d) = S^k(p) + alpha M^k d
-// for every alpha; default k = 40) and adds alpha M^k d.  By default alpha
-// minimises the residual norm ||b - A (S^k(p) + alpha M^k d)||: the
-// combination chosen on what the stopping rule measures, after the smoother
-// has removed the error it removes anyway.  The other choice
-// (blz_unet_set_step) minimises the error's energy norm, alpha =
-// <d, r> / <d, A d>, which weighs the smooth error Gauss-Seidel removes
-// slowest as the sweep count does.  A useless d gets alpha ~ 0.  rms() and
-// the inner products run over the whole grid in FP64; kappa is a constant of
-// the trained weights (the training set's mean rms(p* - p_prev) / rms(r)).
+// for every alpha; blz_unet_set_smoothing, default k = 0) and adds
+// alpha M^k d.  By default alpha minimises the error's energy norm,
+// alpha = <d, r> / <d, A d> (A symmetric positive definite), which weighs
+// the smooth error Gauss-Seidel removes slowest as the sweep count does, and
+// can never raise ||p* - p||_A.  The other choice (blz_unet_set_step)
+// minimises the residual norm ||b - A (S^k(p) + alpha M^k d)||, the
+// combination chosen on what the stopping rule measures.  A useless d gets
+// alpha ~ 0.  rms() and the inner products run over the whole grid in FP64;
+// kappa is a constant of the trained weights (the training set's mean
+// rms(p* - p_prev) / rms(r)).
 //
 // The 3x3x3 convolutions (forward and data gradient) run on the tcgen05 tensor
 // cores (unet_conv.cu).  Pooling, the transposed convolutions, weight gradients,
@@ -723,8 +724,8 @@ struct blz_unet {
     double *partials = nullptr, *sums = nullptr, *h_sums = nullptr;
     float *scales = nullptr;
     float *dpk = nullptr, *alpha = nullptr;     // warm start: packed correction + zero rhs; its step
-    int smooth = 40;                            // sweeps of p and d before the step is chosen
-    int step_mode = BLZ_WARM_STEP_RESIDUAL;     // how the step along d is chosen
+    int smooth = 0;                             // sweeps of p and d before the step is chosen
+    int step_mode = BLZ_WARM_STEP_ENERGY;       // how the step along d is chosen
     int *err = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;

@@ -354,11 +354,12 @@ int  blz_conv3d(const blz_conv_desc *d, const void *x, const void *w, const floa
  * accumulation.  It maps, per cell, b = rho dx^2/dt * rhs, a Neumann-ghost
  * indicator, the previous pressure p and the residual r = b - A p (each over
  * its FP64 rms on the whole grid) to delta, and d = kappa * rms(r) * delta.
- * The solve then sweeps p and d alike k times (blz_unet_set_smoothing,
- * default 40; d with a zero right-hand side) and adds alpha M^k d, alpha
+ * The solve may sweep p and d alike k times first (blz_unet_set_smoothing,
+ * default 0; d with a zero right-hand side) and adds alpha M^k d, alpha
  * chosen by blz_unet_set_step (FP64 over the grid; default: minimising the
- * residual norm of the sum, so the warm start's residual after smoothing is
- * never above that of the plain start).  Parameters are one
+ * energy norm of the error, which never rises above the plain start's;
+ * the residual-norm step keeps the smoothed residual at or below the plain
+ * start's).  Parameters are one
  * FP32 array; layer l's
  * weights start at info[4] and its bias at info[5] (blz_unet_layer_info).
  * Weights of a 3x3x3 layer are [27][cout][cin] (tap as in blz_conv3d), of a
@@ -379,10 +380,10 @@ long long blz_unet_num_params(const blz_unet *u);
 long long blz_unet_kernel_launches(const blz_unet *u);
 float blz_unet_last_alpha(const blz_unet *u);   /* alpha of the last warm start (synchronises) */
 int  blz_unet_set_smoothing(blz_unet *u, int sweeps);   /* k above (>= 0)                  */
-/* How alpha is chosen: RESIDUAL (default) minimises the residual norm of
- * the sum; ENERGY minimises the energy norm ||e - alpha M^k d||_A of the
- * error, alpha = <M^k d, r> / <M^k d, A M^k d> (A symmetric positive
- * definite: at least one Dirichlet face).                                  */
+/* How alpha is chosen: ENERGY (default) minimises the energy norm
+ * ||e - alpha M^k d||_A of the error, alpha = <M^k d, r> / <M^k d, A M^k d>
+ * (A symmetric positive definite: at least one Dirichlet face); RESIDUAL
+ * minimises the residual norm of the sum.                                  */
 #define BLZ_WARM_STEP_RESIDUAL 0
 #define BLZ_WARM_STEP_ENERGY   1
 int  blz_unet_set_step(blz_unet *u, int mode);

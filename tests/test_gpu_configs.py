@@ -166,15 +166,15 @@ def test_config1_64_against_reference_build():
     against two runs of the reference build (A, B), and beside them the FP64
     oracle running the same schedule race free.
 
-    After 1 frame the error against run A must stay within twice the larger
-    of the reference's run-to-run spread |A - B| and the per-stage floor
-    (1e-5 relative L2, 1e-4 scaled max: fast math and float atomics reorder
-    sums).  After 10 frames the race-free schedule itself has drifted from the
-    racing one (the races change which neighbour values each block reads, and
-    the flow amplifies it); there the bound is 1.5 times the larger of the
-    FP64 oracle's own distance from run A and twice the spread: the CUDA path
-    must be as close to the reference as the exact restatement of its
-    schedule is."""
+    The reference's Gauss-Seidel races between 16x16 blocks: which neighbour
+    values a block reads depends on timing, so its result differs from the
+    race-free schedule by far more than rounding (about 6e-4 relative in T
+    after one frame), and two of its own runs differ from each other by a
+    timing-dependent amount (measured 4e-5 to 4e-4).  The bar is therefore
+    set by the exact restatement of the schedule: the CUDA path must be within
+    2e-5 / 2e-4 (1 frame) and 2e-3 / 2e-2 (10 frames) of the FP64 oracle, and
+    no farther from run A than 1.5 times the larger of the oracle's distance
+    from A and twice the run-to-run spread."""
     from oracle import ref
     if not ref.available():
         pytest.skip("reference build not present")
@@ -188,18 +188,15 @@ def test_config1_64_against_reference_build():
         spread = errors(rb[n], ra[n])
         ours = errors(got[n], ra[n])
         exact = errors(orc[n], ra[n])
-        rows[n] = {"spread": fmt(spread), "ours": fmt(ours), "fp64_oracle": fmt(exact),
-                   "ours_vs_oracle": fmt(errors(got[n], orc[n]))}
-        errs[n] = (spread, ours, exact)
+        to_oracle = errors(got[n], orc[n])
+        rows[n] = {"spread": fmt(spread), "ours": fmt(ours), "fp64_oracle": fmt(exact), "ours_vs_oracle": fmt(to_oracle)}
+        errs[n] = (spread, ours, exact, to_oracle)
     report("config1_64_reference", after_1=rows[1], after_10=rows[10])
-    for n, (spread, ours, exact) in errs.items():
+    for n, (spread, ours, exact, to_oracle) in errs.items():
+        check(to_oracle, *((2e-5, 2e-4) if n == 1 else (2e-3, 2e-2)), f"after {n} frames against the oracle")
         for f in FIELDS:
-            if n == 1:
-                lim_rel = 2.0 * max(spread[f][0], 1e-5)
-                lim_abs = 2.0 * max(spread[f][1], 1e-4)
-            else:
-                lim_rel = 1.5 * max(exact[f][0], 2.0 * spread[f][0])
-                lim_abs = 1.5 * max(exact[f][1], 2.0 * spread[f][1])
+            lim_rel = 1.5 * max(exact[f][0], 2.0 * spread[f][0])
+            lim_abs = 1.5 * max(exact[f][1], 2.0 * spread[f][1])
             assert ours[f][0] <= lim_rel and ours[f][1] <= lim_abs, \
                 f"after {n} frames, {f}: ours {ours[f]}, reference spread {spread[f]}, oracle {exact[f]}"
 
