@@ -61,21 +61,16 @@ void launch_divergence(const Geom &g, const float *U, const float *V, const floa
     k_divergence<<<gr, b, 0, st>>>(g, U, V, W, o, rhs_r, rhs_b);
 }
 
-// Quotient num/den for the neighbour count den in {1..6} on the FMA pipe:
-// q0 = num*RN(1/den), then one remainder correction e = num - q0*den (exact
-// with an FMA) and q = q0 + e*RN(1/den) (Markstein's correction step).  An
-// IEEE division would put a reciprocal and an int-to-float conversion per
-// cell on the XU pipe, which bounds the sweep well below HBM speed.
+// Quotient num/den for the neighbour count den in {1..6}: one rounded
+// multiply by RN(1/den), within 1.5 ulp of the exact quotient (exact for
+// den = 1, 2, 4).  The reference build divides with fast math's approximate
+// division; an IEEE division (or a remainder-corrected product) would cost
+// the sweep, which is issue bound, two to three more instructions per cell.
 __device__ __forceinline__ float inv_count(float den) {
     return den == 6.0f ? 1.0f / 6.0f : den == 5.0f ? 0.2f : den == 4.0f ? 0.25f
          : den == 3.0f ? 1.0f / 3.0f : den == 2.0f ? 0.5f : 1.0f;
 }
-__device__ __forceinline__ float div_count(float num, float den) {
-    const float inv = inv_count(den);
-    const float q0 = __fmul_rn(num, inv);
-    const float e = __fmaf_rn(-q0, den, num);
-    return __fmaf_rn(e, inv, q0);
-}
+__device__ __forceinline__ float div_count(float num, float den) { return __fmul_rn(num, inv_count(den)); }
 
 // One Gauss-Seidel update p = (scale*rhs + sum p_nb)/n_nb (FluidSolver.cu:
 // 532-561), summed in the reference's neighbour order.  n_nb counts the
@@ -178,19 +173,15 @@ __device__ __forceinline__ float4 gs_quad(float scale, int s, float4 r, float4 o
         num = __fadd_rn(num, ypa[t]);
         num = __fadd_rn(num, zma[t]);
         num = __fadd_rn(num, zpa[t]);
-        const float den = t == 0 ? q.d0 : t == 3 ? q.d3 : q.db;
         const float inv = t == 0 ? q.i0 : t == 3 ? q.i3 : q.ib;
-        const float q0 = __fmul_rn(num, inv);
-        out[t] = __fmaf_rn(__fmaf_rn(-q0, den, num), inv, q0);
+        out[t] = __fmul_rn(num, inv);
     }
     return make_float4(out[0], out[1], out[2], out[3]);
 }
 
 // gs_quad on Blackwell's paired FP32 instructions: cells (0,1) and (2,3) of
 // the quad go through one fma/add/mul.rn.f32x2 each, every lane rounded as
-// IEEE FP32, in gs_quad's order, so the bits equal gs_quad's.  -q0 comes
-// from num times -inv (round to nearest is symmetric, so this is -RN(num
-// inv) exactly).
+// IEEE FP32, in gs_quad's order, so the bits equal gs_quad's.
 typedef unsigned long long f2_t;
 __device__ __forceinline__ f2_t f2(float lo, float hi) {
     f2_t r;
@@ -217,16 +208,14 @@ __device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
 }
 
 __device__ __forceinline__ f2_t gs_pair(f2_t scale2, f2_t r, f2_t xl, f2_t xr, f2_t ym, f2_t yp, f2_t zm, f2_t zp,
-                                        f2_t den, f2_t inv, f2_t ninv) {
+                                        f2_t inv) {
     f2_t num = f2_fma(scale2, r, xl);
     num = f2_add(num, xr);
     num = f2_add(num, ym);
     num = f2_add(num, yp);
     num = f2_add(num, zm);
     num = f2_add(num, zp);
-    const f2_t q0 = f2_mul(num, inv);
-    const f2_t nq0 = f2_mul(num, ninv);
-    return f2_fma(f2_fma(nq0, den, num), inv, q0);
+    return f2_mul(num, inv);
 }
 
 __device__ __forceinline__ float4 gs_quad_pk(float scale, int s, float4 r, float4 o, float xe, float4 ym, float4 yp,
@@ -235,9 +224,9 @@ __device__ __forceinline__ float4 gs_quad_pk(float scale, int s, float4 r, float
     const f2_t xl01 = s == 0 ? f2(xe, o.x) : f2(o.x, o.y), xl23 = s == 0 ? f2(o.y, o.z) : f2(o.z, o.w);
     const f2_t xr01 = s == 0 ? f2(o.x, o.y) : f2(o.y, o.z), xr23 = s == 0 ? f2(o.z, o.w) : f2(o.w, xe);
     const f2_t a = gs_pair(sc, f2(r.x, r.y), xl01, xr01, f2(ym.x, ym.y), f2(yp.x, yp.y), f2(zm.x, zm.y),
-                           f2(zp.x, zp.y), f2(q.d0, q.db), f2(q.i0, q.ib), f2(-q.i0, -q.ib));
+                           f2(zp.x, zp.y), f2(q.i0, q.ib));
     const f2_t b = gs_pair(sc, f2(r.z, r.w), xl23, xr23, f2(ym.z, ym.w), f2(yp.z, yp.w), f2(zm.z, zm.w),
-                           f2(zp.z, zp.w), f2(q.db, q.d3), f2(q.ib, q.i3), f2(-q.ib, -q.i3));
+                           f2(zp.z, zp.w), f2(q.ib, q.i3));
     float4 out;
     f2_split(a, out.x, out.y);
     f2_split(b, out.z, out.w);
