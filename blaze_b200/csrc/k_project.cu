@@ -61,16 +61,29 @@ void launch_divergence(const Geom &g, const float *U, const float *V, const floa
     k_divergence<<<gr, b, 0, st>>>(g, U, V, W, o, rhs_r, rhs_b);
 }
 
-// Quotient num/den for the neighbour count den in {1..6}: one rounded
-// multiply by RN(1/den), within 1.5 ulp of the exact quotient (exact for
-// den = 1, 2, 4).  The reference build divides with fast math's approximate
-// division; an IEEE division (or a remainder-corrected product) would cost
-// the sweep, which is issue bound, two to three more instructions per cell.
+// Quotient num/den for the neighbour count den in {1..6} as
+// RN(num * hi + RN(num * lo)), hi = RN(1/den) and lo = RN(1/den - hi): two
+// instructions on the FMA pipe instead of an IEEE division (a reciprocal and
+// an int-to-float conversion per cell on the XU pipe) or a remainder-
+// corrected product (three).  The result is within about half an ulp of the
+// quotient and, unlike num * RN(1/den) alone, carries no bias: RN(1/3),
+// RN(1/5) and RN(1/6) are all slightly large, and a sweep that scaled every
+// update by 1 + 3e-8 would converge to the solution of A - 1.8e-7 I, whose
+// smooth modes differ from A's by parts in 10^4 at 256^3.
 __device__ __forceinline__ float inv_count(float den) {
     return den == 6.0f ? 1.0f / 6.0f : den == 5.0f ? 0.2f : den == 4.0f ? 0.25f
          : den == 3.0f ? 1.0f / 3.0f : den == 2.0f ? 0.5f : 1.0f;
 }
-__device__ __forceinline__ float div_count(float num, float den) { return __fmul_rn(num, inv_count(den)); }
+__device__ __forceinline__ float inv_count_lo(float den) {
+    return den == 6.0f ? -4.967053879312289e-09f : den == 5.0f ? -2.9802322831784522e-09f
+         : den == 3.0f ? -9.934107758624577e-09f : 0.0f;
+}
+__device__ __forceinline__ float div_hl(float num, float hi, float lo) {
+    return __fmaf_rn(num, hi, __fmul_rn(num, lo));
+}
+__device__ __forceinline__ float div_count(float num, float den) {
+    return div_hl(num, inv_count(den), inv_count_lo(den));
+}
 
 // One Gauss-Seidel update p = (scale*rhs + sum p_nb)/n_nb (FluidSolver.cu:
 // 532-561), summed in the reference's neighbour order.  n_nb counts the
@@ -119,27 +132,30 @@ __global__ void k_rbgs_half(Geom g, SolveParams sp, const float *__restrict__ rh
 // that falls outside the segment; 128-bit store.
 __device__ __forceinline__ float4 ld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
 
-// Neighbour counts of a quad and their reciprocals: the count is the same
-// for every cell of the quad except the one at a row end (cell 0 when the
-// row's cells sit at even i and the quad starts the row, cell 3 when odd
-// and it ends the row), so it is formed three times per quad, not per cell.
+// Neighbour counts' reciprocals (hi, lo of div_hl) of a quad: the count is
+// the same for every cell of the quad except the one at a row end (cell 0
+// when the row's cells sit at even i and the quad starts the row, cell 3
+// when odd and it ends the row), so they are formed three times per quad.
 struct QuadDen {
-    float d0, i0, db, ib, d3, i3;
+    float l0, i0, lb, ib, l3, i3;
 };
 
 __device__ __forceinline__ QuadDen quad_den(const SolveParams &sp, int s, bool first, bool last, bool has_ym,
                                             bool has_yp, bool has_zm, bool has_zp) {
     const bool dir = sp.dirichlet;
     QuadDen q;
-    q.db = 2.0f + (has_ym ? 1.0f : (dir && sp.open.ylo ? 1.0f : 0.0f)) +
-           (has_yp ? 1.0f : (dir && sp.open.yhi ? 1.0f : 0.0f)) +
-           (has_zm ? 1.0f : (dir && sp.open.zlo ? 1.0f : 0.0f)) +
-           (has_zp ? 1.0f : (dir && sp.open.zhi ? 1.0f : 0.0f));
-    q.d0 = (s == 0 && first) ? q.db - 1.0f + (dir && sp.open.xlo ? 1.0f : 0.0f) : q.db;
-    q.d3 = (s == 1 && last) ? q.db - 1.0f + (dir && sp.open.xhi ? 1.0f : 0.0f) : q.db;
-    q.ib = inv_count(q.db);
-    q.i0 = inv_count(q.d0);
-    q.i3 = inv_count(q.d3);
+    const float db = 2.0f + (has_ym ? 1.0f : (dir && sp.open.ylo ? 1.0f : 0.0f)) +
+                     (has_yp ? 1.0f : (dir && sp.open.yhi ? 1.0f : 0.0f)) +
+                     (has_zm ? 1.0f : (dir && sp.open.zlo ? 1.0f : 0.0f)) +
+                     (has_zp ? 1.0f : (dir && sp.open.zhi ? 1.0f : 0.0f));
+    const float d0 = (s == 0 && first) ? db - 1.0f + (dir && sp.open.xlo ? 1.0f : 0.0f) : db;
+    const float d3 = (s == 1 && last) ? db - 1.0f + (dir && sp.open.xhi ? 1.0f : 0.0f) : db;
+    q.ib = inv_count(db);
+    q.i0 = inv_count(d0);
+    q.i3 = inv_count(d3);
+    q.lb = inv_count_lo(db);
+    q.l0 = inv_count_lo(d0);
+    q.l3 = inv_count_lo(d3);
     return q;
 }
 
@@ -173,8 +189,9 @@ __device__ __forceinline__ float4 gs_quad(float scale, int s, float4 r, float4 o
         num = __fadd_rn(num, ypa[t]);
         num = __fadd_rn(num, zma[t]);
         num = __fadd_rn(num, zpa[t]);
-        const float inv = t == 0 ? q.i0 : t == 3 ? q.i3 : q.ib;
-        out[t] = __fmul_rn(num, inv);
+        const float hi = t == 0 ? q.i0 : t == 3 ? q.i3 : q.ib;
+        const float lo = t == 0 ? q.l0 : t == 3 ? q.l3 : q.lb;
+        out[t] = div_hl(num, hi, lo);
     }
     return make_float4(out[0], out[1], out[2], out[3]);
 }
@@ -208,14 +225,14 @@ __device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
 }
 
 __device__ __forceinline__ f2_t gs_pair(f2_t scale2, f2_t r, f2_t xl, f2_t xr, f2_t ym, f2_t yp, f2_t zm, f2_t zp,
-                                        f2_t inv) {
+                                        f2_t hi, f2_t lo) {
     f2_t num = f2_fma(scale2, r, xl);
     num = f2_add(num, xr);
     num = f2_add(num, ym);
     num = f2_add(num, yp);
     num = f2_add(num, zm);
     num = f2_add(num, zp);
-    return f2_mul(num, inv);
+    return f2_fma(num, hi, f2_mul(num, lo));
 }
 
 __device__ __forceinline__ float4 gs_quad_pk(float scale, int s, float4 r, float4 o, float xe, float4 ym, float4 yp,
@@ -224,9 +241,9 @@ __device__ __forceinline__ float4 gs_quad_pk(float scale, int s, float4 r, float
     const f2_t xl01 = s == 0 ? f2(xe, o.x) : f2(o.x, o.y), xl23 = s == 0 ? f2(o.y, o.z) : f2(o.z, o.w);
     const f2_t xr01 = s == 0 ? f2(o.x, o.y) : f2(o.y, o.z), xr23 = s == 0 ? f2(o.z, o.w) : f2(o.w, xe);
     const f2_t a = gs_pair(sc, f2(r.x, r.y), xl01, xr01, f2(ym.x, ym.y), f2(yp.x, yp.y), f2(zm.x, zm.y),
-                           f2(zp.x, zp.y), f2(q.i0, q.ib));
+                           f2(zp.x, zp.y), f2(q.i0, q.ib), f2(q.l0, q.lb));
     const f2_t b = gs_pair(sc, f2(r.z, r.w), xl23, xr23, f2(ym.z, ym.w), f2(yp.z, yp.w), f2(zm.z, zm.w),
-                           f2(zp.z, zp.w), f2(q.ib, q.i3));
+                           f2(zp.z, zp.w), f2(q.ib, q.i3), f2(q.lb, q.l3));
     float4 out;
     f2_split(a, out.x, out.y);
     f2_split(b, out.z, out.w);
