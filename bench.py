@@ -13,11 +13,14 @@ Prints one JSON line (rank 0).
                   [--plain-only] [--weights PATH]
 
 --impl reference times the reference's own CUDA build (oracle/_ref) on the
-same scene and particles through its FluidSolver API, with maxIterSolve equal
-to the mean sweep count the plain RBGS step needs here (the reference has no
-residual control).  N > 1 runs independent replicas, one per GPU (the single
-grid does not shard); value is the sum over ranks, timed as the max over
-ranks.
+same scene and particles through its FluidSolver API, each frame with
+maxIterSolve equal to the sweeps the plain RBGS step needs on that frame
+(measured by a plain-only run of this script in a child process; the
+reference has no residual control).  N > 1 runs independent replicas, one
+per GPU (the single grid does not shard); value is the sum over ranks, timed
+as the max over ranks.  --workload fire384 runs the 384^3 large fire with
+moving emitters the same way; --workload batch splits one set of 64
+simulations across the ranks.
 """
 import argparse
 import json

@@ -428,10 +428,13 @@ int  blz_set_warm_start(blz_solver *s, blz_unet *u);
  * exactly as that grid's own device-loop solve would, whether it goes on; a
  * CUDA graph with a conditional WHILE node loops until no grid goes on.  Each
  * grid's pressure, sweep count and residual equal those of its own solve bit
- * for bit.  The sweep launch shape is autotuned per batch.  When no grid's
- * forces depend on time (no curl noise, no moving wind noise), every frame
- * is one graph launch.  Every solver needs width % 8 == 0, 3-D red-black
- * order, tol > 0, the same check_every, and max_iter a multiple of it.  The
+ * for bit.  A solver with a warm-start network attached (blz_set_warm_start)
+ * is warm-started inside the batch exactly as alone, before the batched
+ * loop; solvers of equal dims may share a network.  The sweep launch shape
+ * is autotuned per batch.  When no grid's forces depend on time (no curl
+ * noise, no moving wind noise), every frame is one graph launch.  Every
+ * solver needs width % 8 == 0, 3-D red-black order, tol > 0, the same
+ * check_every, max_iter a multiple of it, and defect_correction = 0.  The
  * batch puts all solvers on its own stream; while batched, step them only
  * through the batch (the solvers stay owned by the caller and must outlive
  * the batch, which returns them to their own streams when destroyed).      */

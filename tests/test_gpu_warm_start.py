@@ -12,8 +12,8 @@ Bars, from the measured trajectories: over the first 20 frames (frames
 5-24, the benchmark's window length) the warm-started frames of both seeds
 together need at most 0.7 of the plain sweeps (measured 0.60: 0.70 on 902,
 0.44 on 903); over all 50 frames the network makes neither trajectory slower
-and both together at most 0.95 of the plain sweeps (measured 0.91: 0.96 and
-0.86).  Later frames are harder for both: many stop at the cap in both runs,
+and both together at most 0.95 of the plain sweeps (measured 0.83: 0.86 and
+0.80).  Later frames are harder for both: many stop at the cap in both runs,
 which pulls the long-run ratio toward 1.  On the benchmark's own window
 (seed 3) the network needs 0.35 of the plain sweeps.  The numbers are
 printed.  The warm start runs with its defaults: the energy-norm step, no smoothing sweeps."""
