@@ -503,27 +503,29 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     auto wait_red = [&](int k) { return tb_wait(smem_addr(&tbar[k & 3]), ((k - (z0 - 3)) >> 2) & 1); };
     auto wait_black = [&](int k) { return tb_wait(smem_addr(&tbar[4 + (k & 3)]), ((k - (z0 - 2)) >> 2) & 1); };
     auto wait_in = [&](int k) { return tb_wait(smem_addr(&tbar[8 + (k & 1)]), ((k - (z0 - 2)) >> 1) & 1); };
-    auto prefetch = [&](int k_red, int k_black, int k_in) {
+    // ALL: every plane asked for is known to be in range (steady steps).
+    auto prefetch = [&](int k_red, int k_black, int k_in, auto all_c) __attribute__((always_inline)) {
+        constexpr bool ALL = decltype(all_c)::value;
         if constexpr (TMA) {
             if (!leader) return;
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (k_red >= z0 - 3 && k_red < z1 + 3) tma_fill(map_r, k_red & 3, k_red);
-            if (k_black >= z0 - 2 && k_black < z1 + 2) tma_fill(map_b, 4 + (k_black & 3), k_black);
-            if (k_in >= z0 - 2 && k_in < z1 + 4) tma_fill(map_in, 8 + (k_in & 1), k_in);
+            if (ALL || (k_red >= z0 - 3 && k_red < z1 + 3)) tma_fill(map_r, k_red & 3, k_red);
+            if (ALL || (k_black >= z0 - 2 && k_black < z1 + 2)) tma_fill(map_b, 4 + (k_black & 3), k_black);
+            if (ALL || (k_in >= z0 - 2 && k_in < z1 + 4)) tma_fill(map_in, 8 + (k_in & 1), k_in);
             return;
         }
         // red rhs: levels 0 and 2 cover planes [z0-3, z1+3); black rhs: levels 1 and 3 cover [z0-2, z1+2)
-        if (kin(k_red) && k_red >= z0 - 3 && k_red < z1 + 3) {
+        if (ALL || (kin(k_red) && k_red >= z0 - 3 && k_red < z1 + 3)) {
             const int o = RR + (k_red & 3) * slotb;
             if (okA) cp16(o + ownA, rhs_r + offA + k_red * pl);
             if (okB) cp16(o + ownB, rhs_r + offB + k_red * pl);
         }
-        if (kin(k_black) && k_black >= z0 - 2 && k_black < z1 + 2) {
+        if (ALL || (kin(k_black) && k_black >= z0 - 2 && k_black < z1 + 2)) {
             const int o = RB + (k_black & 3) * slotb;
             if (okA) cp16(o + ownA, rhs_b + offA + k_black * pl);
             if (okB) cp16(o + ownB, rhs_b + offB + k_black * pl);
         }
-        if (kin(k_in) && k_in < z1 + 4) {
+        if (ALL || (kin(k_in) && k_in < z1 + 4)) {
             const int o = STG + (k_in & 1) * slotb;
             if (okA) cp16(o + ownA, pin_b + offA + k_in * pl);
             if (okB) cp16(o + ownB, pin_b + offB + k_in * pl);
@@ -555,13 +557,15 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     sts4(slot(1, z0 - 3) + ownA, b0A);
     sts4(slot(1, z0 - 4) + ownB, bm1B);
     sts4(slot(1, z0 - 3) + ownB, b0B);
-    prefetch(z0 - 3, z0 - 4, z0 - 2);                 // what the first step reads
+    prefetch(z0 - 3, z0 - 4, z0 - 2, std::false_type{});   // what the first step reads
     // One quad update of row parity S: colour c on plane k, `own` the row's
     // element offset, o the other colour's own quad, ym/yp/zm/zp its
-    // neighbours.
-    auto update = [&](auto s_c, int c, int k, int own, int den, float4 o, float4 ym, float4 yp, float4 zm,
-                      float4 zp, const QuadDen &qi, bool hym, bool hyp) -> float4 {
+    // neighbours.  INNER: plane k is known to have both z neighbours.
+    auto update = [&](auto s_c, auto inner_c, int c, int k, int own, int den, float4 o, float4 ym, float4 yp,
+                      float4 zm, float4 zp, const QuadDen &qi, bool hym, bool hyp) __attribute__((always_inline))
+        -> float4 {
         constexpr int S = decltype(s_c)::value;
+        constexpr bool INNER = decltype(inner_c)::value;
         float xe;
         if constexpr (WARPROW) {
             const float v = S == 0 ? __shfl_up_sync(0xffffffffu, o.w, 1) : __shfl_down_sync(0xffffffffu, o.x, 1);
@@ -572,69 +576,81 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
         }
         const float4 rv = rhs_ld(c, k, own, den);
         if constexpr (PK) {
-            if (k > 0 && k < D - 1) return gs_quad_pk(sp.scale, S, rv, o, xe, ym, yp, zm, zp, qi);
+            if (INNER || (k > 0 && k < D - 1)) return gs_quad_pk(sp.scale, S, rv, o, xe, ym, yp, zm, zp, qi);
             return gs_quad_pk(sp.scale, S, rv, o, xe, ym, yp, zm, zp,
                               quad_den(sp, S, first, last, hym, hyp, k > 0, k < D - 1));
         }
-        if (k > 0 && k < D - 1) return gs_quad(sp.scale, S, rv, o, xe, ym, yp, zm, zp, qi);
+        if (INNER || (k > 0 && k < D - 1)) return gs_quad(sp.scale, S, rv, o, xe, ym, yp, zm, zp, qi);
         return gs_quad(sp.scale, S, rv, o, xe, ym, yp, zm, zp, quad_den(sp, S, first, last, hym, hyp, k > 0, k < D - 1));
     };
     // The four levels of step t.  Every level of a step has, in row A, row
     // parity (jA + t) & 1 (level h: plane t - h, colour h & 1), row B the
-    // other one.
-    auto levels = [&](int t, auto sa_c) {
+    // other one.  MODE 0 checks everything; in steady steps (every level
+    // active, every level's plane interior, t + 1 < D) MODE 1 checks only
+    // the row masks, and MODE 2 (both rows update on every level) nothing.
+    // The arithmetic is the same in every mode.
+    auto levels = [&](int t, auto sa_c, auto mode_c) __attribute__((always_inline)) {
         constexpr int SA = decltype(sa_c)::value, SB = 1 - SA;
+        constexpr int MODE = decltype(mode_c)::value;
+        constexpr bool STEADY = MODE > 0, ROWS = MODE == 2;
         const std::integral_constant<int, SA> sA{};
         const std::integral_constant<int, SB> sB{};
+        const std::integral_constant<bool, STEADY> in{};
         const QuadDen &qa = SA ? qA1 : qA0;
         const QuadDen &qb = SB ? qB1 : qB0;
-        if (kact(0, t)) {
+        if (STEADY || kact(0, t)) {
             const int b = slot(1, t);
-            if (mA & 1u) {
-                r0A = update(sA, 0, t, ownA, denA, b0A, lds4(b + ownA - rowb), b0B, bm1A, bp1A, qa, hymA, hypA);
+            if (ROWS || (mA & 1u)) {
+                r0A = update(sA, in, 0, t, ownA, denA, b0A, lds4(b + ownA - rowb), b0B, bm1A, bp1A, qa, hymA, hypA);
                 sts4(slot(0, t) + ownA, r0A);
             }
-            if (mB & 1u) {
-                r0B = update(sB, 0, t, ownB, denB, b0B, b0A, lds4(b + ownB + rowb), bm1B, bp1B, qb, hymB, hypB);
+            if (ROWS || (mB & 1u)) {
+                r0B = update(sB, in, 0, t, ownB, denB, b0B, b0A, lds4(b + ownB + rowb), bm1B, bp1B, qb, hymB, hypB);
                 sts4(slot(0, t) + ownB, r0B);
             }
         }
-        if (t >= D) { r0A = zero4; r0B = zero4; }
-        if (kact(1, t - 1)) {
+        if (!STEADY && t >= D) { r0A = zero4; r0B = zero4; }
+        if (STEADY || kact(1, t - 1)) {
             const int b = slot(0, t - 1), w = slot(1, t - 1);
-            if (mA & 2u) {
-                bm1A = update(sA, 1, t - 1, ownA, denA, rm1A, lds4(b + ownA - rowb), rm1B, rm2A, r0A, qa, hymA, hypA);
+            if (ROWS || (mA & 2u)) {
+                bm1A = update(sA, in, 1, t - 1, ownA, denA, rm1A, lds4(b + ownA - rowb), rm1B, rm2A, r0A, qa, hymA,
+                              hypA);
                 sts4(w + ownA, bm1A);
             }
-            if (mB & 2u) {
-                bm1B = update(sB, 1, t - 1, ownB, denB, rm1B, rm1A, lds4(b + ownB + rowb), rm2B, r0B, qb, hymB, hypB);
+            if (ROWS || (mB & 2u)) {
+                bm1B = update(sB, in, 1, t - 1, ownB, denB, rm1B, rm1A, lds4(b + ownB + rowb), rm2B, r0B, qb, hymB,
+                              hypB);
                 sts4(w + ownB, bm1B);
             }
         }
-        if (kact(2, t - 2)) {
+        if (STEADY || kact(2, t - 2)) {
             const int b = slot(1, t - 2), w = slot(0, t - 2);
-            if (mA & 4u) {
-                rm2A = update(sA, 0, t - 2, ownA, denA, bm2A, lds4(b + ownA - rowb), bm2B, bm3A, bm1A, qa, hymA, hypA);
+            if (ROWS || (mA & 4u)) {
+                rm2A = update(sA, in, 0, t - 2, ownA, denA, bm2A, lds4(b + ownA - rowb), bm2B, bm3A, bm1A, qa, hymA,
+                              hypA);
                 sts4(w + ownA, rm2A);
             }
-            if (mB & 4u) {
-                rm2B = update(sB, 0, t - 2, ownB, denB, bm2B, bm2A, lds4(b + ownB + rowb), bm3B, bm1B, qb, hymB, hypB);
+            if (ROWS || (mB & 4u)) {
+                rm2B = update(sB, in, 0, t - 2, ownB, denB, bm2B, bm2A, lds4(b + ownB + rowb), bm3B, bm1B, qb, hymB,
+                              hypB);
                 sts4(w + ownB, rm2B);
             }
         }
         const int k3 = t - 3;
-        if (kact(3, k3)) {
+        if (STEADY || kact(3, k3)) {
             const int b = slot(0, k3);
-            const bool outp = k3 >= z0;
-            if (mA & 8u) {
-                bm3A = update(sA, 1, k3, ownA, denA, rm3A, lds4(b + ownA - rowb), rm3B, rm4A, rm2A, qa, hymA, hypA);
+            const bool outp = STEADY || k3 >= z0;
+            if (ROWS || (mA & 8u)) {
+                bm3A = update(sA, in, 1, k3, ownA, denA, rm3A, lds4(b + ownA - rowb), rm3B, rm4A, rm2A, qa, hymA,
+                              hypA);
                 if (outp) {
                     *reinterpret_cast<float4 *>(pout_r + offA + k3 * pl) = rm3A;
                     *reinterpret_cast<float4 *>(pout_b + offA + k3 * pl) = bm3A;
                 }
             }
-            if (mB & 8u) {
-                bm3B = update(sB, 1, k3, ownB, denB, rm3B, rm3A, lds4(b + ownB + rowb), rm4B, rm2B, qb, hymB, hypB);
+            if (ROWS || (mB & 8u)) {
+                bm3B = update(sB, in, 1, k3, ownB, denB, rm3B, rm3A, lds4(b + ownB + rowb), rm4B, rm2B, qb, hymB,
+                              hypB);
                 if (outp) {
                     *reinterpret_cast<float4 *>(pout_r + offB + k3 * pl) = rm3B;
                     *reinterpret_cast<float4 *>(pout_b + offB + k3 * pl) = bm3B;
@@ -642,13 +658,19 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
             }
         }
     };
-    for (int t = z0 - 3; t < z1 + 3; ++t) {
+    // Both rows of this thread update on every level of a steady step.
+    const bool rows_full = mA == 15u && mB == 15u;
+    // One step of the wavefront; STEADY is CTA-uniform, so every thread
+    // meets the same barriers.
+    auto step = [&](int t, auto steady_c) __attribute__((always_inline)) -> bool {
+        constexpr bool STEADY = decltype(steady_c)::value;
+        const bool in1 = STEADY || kin(t + 1);
         if constexpr (TMA) {
             // this step's copies were issued in the previous one; slots are
             // overwritten only after the barrier (their last readers were in
             // the previous step)
             bool ok = wait_red(t);
-            if (t - 1 >= z0 - 2) ok = wait_black(t - 1) && ok;
+            if (STEADY || t - 1 >= z0 - 2) ok = wait_black(t - 1) && ok;
             ok = wait_in(t + 1) && ok;
             if (__syncthreads_or(!ok)) {
                 // CTA-uniform: stop the pass.  The copies issued in the
@@ -656,31 +678,52 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
                 // flight; wait for them once more before exiting.
                 if (leader) atomicAdd(&g_tb_timeouts, 1u);
                 wait_red(t);
-                if (t - 1 >= z0 - 2) wait_black(t - 1);
+                if (STEADY || t - 1 >= z0 - 2) wait_black(t - 1);
                 wait_in(t + 1);
-                return;
+                return false;
             }
             const int st = (int)(dbase - smc) + (8 + ((t + 1) & 1)) * dslot;
-            bp1A = okA && kin(t + 1) ? lds4(st + denA) : zero4;
-            bp1B = okB && kin(t + 1) ? lds4(st + denB) : zero4;
+            bp1A = okA && in1 ? lds4(st + denA) : zero4;
+            bp1B = okB && in1 ? lds4(st + denB) : zero4;
             __syncthreads();
-            prefetch(t + 1, t, t + 2);
+            prefetch(t + 1, t, t + 2, steady_c);
         } else {
-            prefetch(t + 1, t, t + 2);                // what the next step reads
+            prefetch(t + 1, t, t + 2, steady_c);      // what the next step reads
             asm volatile("cp.async.wait_group 1;" ::: "memory");
             const int st = STG + ((t + 1) & 1) * slotb;
-            bp1A = okA && kin(t + 1) ? lds4(st + ownA) : zero4;
-            bp1B = okB && kin(t + 1) ? lds4(st + ownB) : zero4;
+            bp1A = okA && in1 ? lds4(st + ownA) : zero4;
+            bp1B = okB && in1 ? lds4(st + ownB) : zero4;
             __syncthreads();
         }
         sts4(slot(1, t + 1) + ownA, bp1A);
         sts4(slot(1, t + 1) + ownB, bp1B);
-        if ((jA + t) & 1) levels(t, std::integral_constant<int, 1>{});
-        else levels(t, std::integral_constant<int, 0>{});
+        const bool odd = (jA + t) & 1;
+        if constexpr (STEADY) {
+            if (rows_full) {
+                if (odd) levels(t, std::integral_constant<int, 1>{}, std::integral_constant<int, 2>{});
+                else levels(t, std::integral_constant<int, 0>{}, std::integral_constant<int, 2>{});
+            } else {
+                if (odd) levels(t, std::integral_constant<int, 1>{}, std::integral_constant<int, 1>{});
+                else levels(t, std::integral_constant<int, 0>{}, std::integral_constant<int, 1>{});
+            }
+        } else {
+            if (odd) levels(t, std::integral_constant<int, 1>{}, std::integral_constant<int, 0>{});
+            else levels(t, std::integral_constant<int, 0>{}, std::integral_constant<int, 0>{});
+        }
         rm4A = rm3A; rm3A = rm2A; rm2A = rm1A; rm1A = r0A;
         bm3A = bm2A; bm2A = bm1A; bm1A = b0A; b0A = bp1A;
         rm4B = rm3B; rm3B = rm2B; rm2B = rm1B; rm1B = r0B;
         bm3B = bm2B; bm2B = bm1B; bm1B = b0B; b0B = bp1B;
+        return true;
+    };
+    // Steady steps: t in [ts, te).  From z0 + 3 every level is active; from
+    // 4 level 3's plane t - 3 has a z- neighbour; below z1 + 2 every level is
+    // active and every prefetch is in range; below D - 2 planes t + 1 and t + 2
+    // exist and level 0's plane t has a z+ neighbour.
+    const int ts = max(z0 + 3, 4), te = min(z1 + 2, D - 2);
+    for (int t = z0 - 3; t < z1 + 3; ++t) {
+        const bool ok = t >= ts && t < te ? step(t, std::true_type{}) : step(t, std::false_type{});
+        if (!ok) return;
     }
     if constexpr (!TMA) asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
