@@ -542,6 +542,7 @@ def run_batch(args, ws, rank, local):
                        "mean_sweeps_plain_sims": float(sweeps[:, ~learned_mask].mean()) if (~learned_mask).any() else None,
                        "mean_sweeps_learned_sims": float(sweeps[:, learned_mask].mean()) if learned_mask.any() else None,
                        "all_converged": all(x["converged"] for fr in stats for x in fr),
+                       "batch_sweep_kernel": _batch_kernel_name(stats[0][0]["sweep_variant"]),
                        "per_sim_agreement_with_unbatched": "bitwise, all fields of all sims" if agree else "DIFFERS",
                        "parallelism": f"simulations split over {ws} GPU(s) by cell count (parallel.shard_sims)"},
             "unbatched": {"value": total_cells * args.steps / (ms_alone * 1e-3), "ms_per_step": ms_alone / args.steps,
@@ -549,6 +550,13 @@ def run_batch(args, ws, rank, local):
                                  "with its own device-loop solve graph"},
             "batch_speedup": ms_alone / ms,
             "gpu_launches": int(launches), "clocks": clk.summary()}
+
+
+def _batch_kernel_name(v):
+    """The batch autotuner's choice as reported in the stats' sweep_variant."""
+    if v > 100:
+        return f"temporal blocking, two sweeps per pass, tiles of {v - 100} planes (autotuned)"
+    return f"segment kernel, one sweep per pass, {v} plane(s) per thread (autotuned)"
 
 
 def plain_sweeps_per_frame(args, local):

@@ -60,6 +60,7 @@ __global__ void k_batch_active(const BatchCtl *__restrict__ ctl, int n, const lo
 
 constexpr int kKZ[4] = {1, 2, 4, 8};
 constexpr int kBlocks[2] = {128, 256};
+constexpr int kTbZC[3] = {8, 16, 32};         // planes per temporal-blocking tile
 
 } // namespace
 
@@ -78,6 +79,14 @@ struct blz_batch {
     int total_blocks = 0;
     double *partials = nullptr;
     int kz = -1, block = 256, grid = 0;       // chosen launch shape (kz < 0: not tuned yet)
+    // temporal blocking (two sweeps per pass over HBM): planes per tile, 0
+    // when the segment kernel was chosen (or the batch does not allow it)
+    int tb_zc = 0;
+    int force_zc = -1;                        // blz_batch_set_sweep: -1 autotune, 0 segment, > 0 tiles of that many planes
+    bool tb_ok = false;                       // every grid's shape allows it and check_every % 4 == 0
+    BatchTile *d_tiles = nullptr;             // tiles of the current tb_zc, heaviest first
+    int ntiles = 0, tiles_cap = 0;
+    size_t tb_smem = 0;                       // largest dynamic shared memory of a tile
     bool time_free = false;                   // frame graphs allowed
     cudaGraphExec_t solve_exec = nullptr;
     cudaGraphExec_t frame_exec[2] = {nullptr, nullptr};
@@ -127,10 +136,42 @@ static void active_list(blz_batch *b, int kz, int set_cond, cudaGraphConditional
                                         set_cond, h);
 }
 
+// Tiles of every grid for zc planes per tile (rows per tile as the grid's own
+// pass), ordered heaviest first so the block scheduler ends with the small
+// ones; uploaded to b->d_tiles.
+static int build_tiles(blz_batch *b, const std::vector<BatchSim> &h, int zc) {
+    struct Item { BatchTile t; long long cost; };
+    std::vector<Item> items;
+    for (int i = 0; i < b->n; ++i) {
+        const Geom &g = h[i].g;
+        const int ty = batch_tb_rows(g), wq = g.W >> 3;
+        for (int j0 = 0; j0 < g.H; j0 += ty)
+            for (int z0 = 0; z0 < g.D; z0 += zc) {
+                const int z1 = std::min(z0 + zc, g.D);
+                items.push_back({BatchTile{i, j0, z0, z1, ty}, (long long)(ty + 8) * wq * (z1 - z0 + 6)});
+            }
+    }
+    std::stable_sort(items.begin(), items.end(), [](const Item &x, const Item &y) { return x.cost > y.cost; });
+    std::vector<BatchTile> t(items.size());
+    for (size_t i = 0; i < items.size(); ++i) t[i] = items[i].t;
+    if ((int)t.size() > b->tiles_cap) {
+        cudaFree(b->d_tiles);
+        b->d_tiles = nullptr;
+        b->tiles_cap = 0;
+        BCK(cudaMalloc(&b->d_tiles, sizeof(BatchTile) * t.size()));
+        b->tiles_cap = (int)t.size();
+    }
+    BCK(cudaMemcpyAsync(b->d_tiles, t.data(), sizeof(BatchTile) * t.size(), cudaMemcpyHostToDevice, b->st));
+    BCK(cudaStreamSynchronize(b->st));
+    b->ntiles = (int)t.size();
+    return BLZ_OK;
+}
+
 // Body of the batched solve, appended to the capture in progress on b->st:
 // check_every sweeps over the grids still running, their residual and decision.
 static void capture_body(blz_batch *b, cudaGraphConditionalHandle h) {
-    launch_batch_sweeps(b->d_sims, b->d_act, b->n, b->chunk, b->kz, b->grid, b->block, b->st);
+    if (b->tb_zc > 0) launch_batch_tb(b->d_sims, b->d_tiles, b->ntiles, b->d_ctl, b->chunk, b->tb_smem, b->st);
+    else launch_batch_sweeps(b->d_sims, b->d_act, b->n, b->chunk, b->kz, b->grid, b->block, b->st);
     launch_batch_check(b->d_sims, b->d_blk0, b->n, b->total_blocks, b->d_ctl, b->partials, 1, b->chunk, b->st);
     active_list(b, b->kz, 1, h);
 }
@@ -230,8 +271,10 @@ done:
     return rc;
 }
 
-// Autotuner: planes per thread x block size, two sweeps of the whole batch on
-// scratch copies of every pressure (all shapes give identical results).
+// Autotuner: the segment kernel's planes per thread x block size (two sweeps
+// of the whole batch timed) against temporal blocking with 8, 16 or 32
+// planes per tile (four sweeps timed), per sweep, on scratch copies of every
+// pressure (all shapes give identical results).
 static int tune(blz_batch *b) {
     if (b->kz >= 0) return BLZ_OK;
     std::vector<BatchSim> h(b->n), hs(b->n);
@@ -271,8 +314,31 @@ static int tune(blz_batch *b) {
             float ms = 0.0f;
             if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev0, b->ev1);
             b->launches += 7;
-            if (e == cudaSuccess && ms < best) { best = ms; b->kz = kz; b->block = blk; b->grid = grid; }
+            if (e == cudaSuccess && ms / 2.0f < best) { best = ms / 2.0f; b->kz = kz; b->block = blk; b->grid = grid; }
         }
+    b->tb_zc = 0;
+    int tb_best = b->force_zc > 0 ? b->force_zc : 0;
+    for (int zi = 0; zi < 3 && b->tb_ok && b->force_zc < 0 && e == cudaSuccess; ++zi) {
+        const int zc = kTbZC[zi];
+        const int rc = build_tiles(b, h, zc);
+        if (rc != BLZ_OK) { e = cudaErrorUnknown; break; }
+        launch_batch_tb(d_scr, b->d_tiles, b->ntiles, b->d_ctl, 4, b->tb_smem, b->st);
+        e = cudaEventRecord(b->ev0, b->st);
+        launch_batch_tb(d_scr, b->d_tiles, b->ntiles, b->d_ctl, 4, b->tb_smem, b->st);
+        if (e == cudaSuccess) e = cudaEventRecord(b->ev1, b->st);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventSynchronize(b->ev1);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+        b->launches += 4;
+        if (e == cudaSuccess && ms / 4.0f < best) { best = ms / 4.0f; tb_best = zc; }
+    }
+    if (e == cudaSuccess && tb_best > 0) {
+        b->tb_zc = tb_best;
+        if (build_tiles(b, h, tb_best) != BLZ_OK) e = cudaErrorUnknown;
+        // no sweeps: only the kernel's shared-memory limit, set outside the capture
+        launch_batch_tb(d_scr, b->d_tiles, b->ntiles, b->d_ctl, 0, b->tb_smem, b->st);
+    }
     cudaStreamSynchronize(b->st);
     cudaFree(scratch);
     cudaFree(d_scr);
@@ -287,7 +353,7 @@ static void release(blz_batch *b) {
     if (b->solve_exec) cudaGraphExecDestroy(b->solve_exec);
     for (auto &x : b->frame_exec) if (x) cudaGraphExecDestroy(x);
     cudaFree(b->d_sims); cudaFree(b->d_ctl); cudaFree(b->d_item0); cudaFree(b->d_blk0); cudaFree(b->partials);
-    cudaFree(b->d_act); cudaFree(b->d_act_sim); cudaFree(b->d_act_item0);
+    cudaFree(b->d_act); cudaFree(b->d_act_sim); cudaFree(b->d_act_item0); cudaFree(b->d_tiles);
     if (b->h_ctl) cudaFreeHost(b->h_ctl);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -319,7 +385,7 @@ static int read_stats(blz_batch *b, blz_step_stats *stats, int loop_ran) {
         st.rhs_norm = bn;
         st.rel_residual = bn > 0.0 ? r / bn : 0.0;
         st.residual_checks = c.checks;
-        st.sweep_variant = b->kz;
+        st.sweep_variant = b->tb_zc > 0 ? 100 + b->tb_zc : b->kz;
         st.device_loop = 1;
         if (solver_warm(b->sims[i])) {
             st.warm_started = 1;
@@ -372,6 +438,11 @@ int blz_batch_create(blz_solver *const *sims, int n, blz_batch **out) {
         b->params.push_back(P);
     }
     b->chunk = b->params[0]->check_every;
+    b->tb_ok = b->chunk % 4 == 0;
+    for (int i = 0; i < n; ++i) {
+        if (!batch_tb_supported(h[i].g)) b->tb_ok = false;
+        else b->tb_smem = std::max(b->tb_smem, batch_tb_smem(h[i].g));
+    }
     b->time_free = true;
     for (const blz_params *P : b->params)
         if (std::fabs(P->turbulence_amp) > 0.0f || (P->wind_amp > 0.0f && P->wind_speed != 0.0f && P->wind_turb_amp != 0.0f))
@@ -430,6 +501,21 @@ int blz_batch_destroy(blz_batch *b) {
 
 void *blz_batch_stream(blz_batch *b) { return b ? (void *)b->st : nullptr; }
 
+int blz_batch_set_sweep(blz_batch *b, int planes) {
+    if (!b) return bfail(BLZ_ERR_ARG, "null batch");
+    if (planes < -1) return bfail(BLZ_ERR_ARG, "planes must be -1 (autotune), 0 (segment kernel) or > 0");
+    if (planes > 0 && !b->tb_ok)
+        return bfail(BLZ_ERR_ARG, "temporal blocking needs check_every %% 4 == 0 and every grid with width %% 8 == 0, "
+                                  "width <= 384");
+    BCK(cudaStreamSynchronize(b->st));
+    b->force_zc = planes;
+    b->kz = -1;                               // tune again at the next solve
+    if (b->solve_exec) { cudaGraphExecDestroy(b->solve_exec); b->solve_exec = nullptr; }
+    for (auto &x : b->frame_exec)
+        if (x) { cudaGraphExecDestroy(x); x = nullptr; }
+    return BLZ_OK;
+}
+
 long long blz_batch_kernel_launches(const blz_batch *b) { return b ? b->launches : 0; }
 
 float blz_batch_last_ms(const blz_batch *b) { return b ? b->last_ms : 0.0f; }
@@ -450,7 +536,7 @@ int blz_batch_solve(blz_batch *b, blz_step_stats *stats) {
     if (!b) return bfail(BLZ_ERR_ARG, "null batch");
     int rc = tune(b);
     if (rc != BLZ_OK) return rc;
-    b->body = 2 * b->chunk + 2 + 1;
+    b->body = (b->tb_zc > 0 ? b->chunk / 2 : 2 * b->chunk) + 2 + 1;
     if (!b->solve_exec && (rc = build_solve_graph_of(b)) != BLZ_OK) return rc;
     BCK(cudaEventRecord(b->ev0, b->st));
     BCK(cudaGraphLaunch(b->solve_exec, b->st));
@@ -465,7 +551,7 @@ int blz_batch_step(blz_batch *b, const float *times, blz_step_stats *stats) {
     if (!b) return bfail(BLZ_ERR_ARG, "null batch");
     int rc = tune(b);
     if (rc != BLZ_OK) return rc;
-    b->body = 2 * b->chunk + 2 + 1;
+    b->body = (b->tb_zc > 0 ? b->chunk / 2 : 2 * b->chunk) + 2 + 1;
     if (b->time_free) {
         const int par = b->parity;
         if (!b->frame_exec[par]) {

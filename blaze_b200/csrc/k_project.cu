@@ -405,13 +405,19 @@ __host__ __device__ inline int tb_dense_slot_bytes(int Wq, int rows_alloc) {
     return (rows_alloc * Wq * 16 + 127) & ~127;
 }
 
-template <bool WARPROW, bool TMA, bool PK = false>
-__global__ void __launch_bounds__(kTbThreads, 1)
-k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float *__restrict__ rhs_b,
-           const float *__restrict__ pin_b, float *__restrict__ pout_r, float *__restrict__ pout_b, int TY, int ZC,
-           const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_b,
-           const __grid_constant__ CUtensorMap map_in) {
-    // Shared memory, in units of one plane slot (2*blockDim.y rows of
+// One tile of a temporal-blocking pass: output rows [j0, j0 + TY) and planes
+// [z0, z1) of one grid, by a CTA of nrp row pairs x Wq quads (thread (mq, rp)
+// owns quad mq of rows 2 rp and 2 rp + 1; `live` is false for threads of the
+// CTA beyond that shape, which only meet the barriers).  `leader` is one
+// thread of the CTA (TMA issue).  The tensor maps are used with TMA only.
+template <bool WARPROW, bool TMA, bool PK>
+__device__ __forceinline__ void tb2_tile(const Geom &g, const SolveParams &sp, const float *__restrict__ rhs_r,
+                                         const float *__restrict__ rhs_b, const float *__restrict__ pin_b,
+                                         float *__restrict__ pout_r, float *__restrict__ pout_b, int TY, int j0,
+                                         int z0, int z1, int mq, int rp, int nrp, bool live, bool leader,
+                                         const CUtensorMap *map_r, const CUtensorMap *map_b,
+                                         const CUtensorMap *map_in) {
+    // Shared memory, in units of one plane slot (2*nrp rows of
     // Wq + 1 float4; the last float4 of each row is a zero pad), addressed
     // by 32-bit byte offsets:
     //   [0, 8)   p, colour c and plane k at slot c*4 + (k & 3)
@@ -428,25 +434,23 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     extern __shared__ __align__(128) float4 sm4[];
     __shared__ __align__(8) uint64_t tbar[kTbDenseSlots];
     const int Wh = g.W >> 1, Wq = Wh >> 2, D = g.D;
-    const int rows_alloc = 2 * (int)blockDim.y;
+    const int rows_alloc = 2 * nrp;
     const int dslot = TMA ? tb_dense_slot_bytes(Wq, rows_alloc) : 0;
     char *const raw = reinterpret_cast<char *>(sm4);
     char *const dbase = TMA ? raw + ((128u - (smem_addr(raw) & 127u)) & 127u) : raw;
     char *const smc = dbase + (TMA ? kTbDenseSlots * dslot : 0);
     const uint32_t sm_base = static_cast<uint32_t>(__cvta_generic_to_shared(smc));
     const int rows = TY + 8;
-    const int mq = threadIdx.x, rA = 2 * threadIdx.y, rB = rA + 1;
-    const int j0 = blockIdx.x * TY, z0 = blockIdx.y * ZC;
-    const int z1 = z0 + ZC < D ? z0 + ZC : D;
+    const int rA = 2 * rp, rB = rA + 1;
     const int jA = j0 - 4 + rA, jB = jA + 1;
-    const bool okA = jA >= 0 && jA < g.H, okB = rB < rows && jB >= 0 && jB < g.H;
+    const bool okA = live && jA >= 0 && jA < g.H, okB = live && rB < rows && jB >= 0 && jB < g.H;
     const int m0 = 4 * mq;
     const long long pl = (long long)Wh * g.H;
     const long long offA = (long long)m0 + (long long)Wh * (okA ? jA : 0);
     const long long offB = (long long)m0 + (long long)Wh * (okB ? jB : 0);
     const bool first = m0 == 0, last = m0 + 4 == Wh;
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int rowb = (Wq + 1) * 16, slotb = 2 * (int)blockDim.y * rowb;
+    const int rowb = (Wq + 1) * 16, slotb = rows_alloc * rowb;
     const int ownA = rA * rowb + mq * 16, ownB = ownA + rowb;
     const int denA = (rA * Wq + mq) * 16, denB = denA + Wq * 16;       // dense-slot offsets (TMA)
     auto slot = [&](int c, int k) { return (c * 4 + (k & 3)) * slotb; };
@@ -457,13 +461,15 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sm_base + (uint32_t)off), "l"(src)
                      : "memory");
     };
+    if (live) {
 #pragma unroll
-    for (int sl = 0; sl < 8; ++sl) {
-        sts4(sl * slotb + ownA, zero4);
-        sts4(sl * slotb + ownB, zero4);
-        if (last) {                                   // the rows' pads
-            sts4(sl * slotb + ownA + 16, zero4);
-            sts4(sl * slotb + ownB + 16, zero4);
+        for (int sl = 0; sl < 8; ++sl) {
+            sts4(sl * slotb + ownA, zero4);
+            sts4(sl * slotb + ownB, zero4);
+            if (last) {                               // the rows' pads
+                sts4(sl * slotb + ownA + 16, zero4);
+                sts4(sl * slotb + ownB + 16, zero4);
+            }
         }
     }
     // Rows on which level h updates: bit h (the halo shrinks by one row per
@@ -484,16 +490,15 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     const QuadDen qB0 = quad_den(sp, 0, first, last, hymB, hypB, true, true);
     const QuadDen qB1 = quad_den(sp, 1, first, last, hymB, hypB, true, true);
     const int RR = 8 * slotb, RB = 12 * slotb, STG = 16 * slotb;
-    const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
     const uint32_t dbase_u = smem_addr(dbase);
     // TMA: one bulk tensor copy of plane k into dense slot ds.
-    auto tma_fill = [&](const CUtensorMap &m, int ds, int k) {
+    auto tma_fill = [&](const CUtensorMap *m, int ds, int k) {
         const uint32_t bar = smem_addr(&tbar[ds]);
         const uint32_t bytes = (uint32_t)(rows_alloc * Wh * 4);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
         asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
                      " [%0], [%1, {%2, %3, %4}], [%5];"
-                     ::"r"(dbase_u + (uint32_t)(ds * dslot)), "l"(reinterpret_cast<uint64_t>(&m)), "r"(0),
+                     ::"r"(dbase_u + (uint32_t)(ds * dslot)), "l"(reinterpret_cast<uint64_t>(m)), "r"(0),
                        "r"(j0 - 4), "r"(k), "r"(bar)
                      : "memory");
     };
@@ -553,10 +558,12 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
     float4 b0A = okA && kin(z0 - 3) ? ld4(pin_b + offA + (z0 - 3) * pl) : zero4;
     float4 bm1B = okB && kin(z0 - 4) ? ld4(pin_b + offB + (z0 - 4) * pl) : zero4;
     float4 b0B = okB && kin(z0 - 3) ? ld4(pin_b + offB + (z0 - 3) * pl) : zero4;
-    sts4(slot(1, z0 - 4) + ownA, bm1A);
-    sts4(slot(1, z0 - 3) + ownA, b0A);
-    sts4(slot(1, z0 - 4) + ownB, bm1B);
-    sts4(slot(1, z0 - 3) + ownB, b0B);
+    if (live) {
+        sts4(slot(1, z0 - 4) + ownA, bm1A);
+        sts4(slot(1, z0 - 3) + ownA, b0A);
+        sts4(slot(1, z0 - 4) + ownB, bm1B);
+        sts4(slot(1, z0 - 3) + ownB, b0B);
+    }
     prefetch(z0 - 3, z0 - 4, z0 - 2, std::false_type{});   // what the first step reads
     // One quad update of row parity S: colour c on plane k, `own` the row's
     // element offset, o the other colour's own quad, ym/yp/zm/zp its
@@ -695,8 +702,10 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
             bp1B = okB && in1 ? lds4(st + ownB) : zero4;
             __syncthreads();
         }
-        sts4(slot(1, t + 1) + ownA, bp1A);
-        sts4(slot(1, t + 1) + ownB, bp1B);
+        if (live) {
+            sts4(slot(1, t + 1) + ownA, bp1A);
+            sts4(slot(1, t + 1) + ownB, bp1B);
+        }
         const bool odd = (jA + t) & 1;
         if constexpr (STEADY) {
             if (rows_full) {
@@ -726,6 +735,18 @@ k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float 
         if (!ok) return;
     }
     if constexpr (!TMA) asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+template <bool WARPROW, bool TMA, bool PK = false>
+__global__ void __launch_bounds__(kTbThreads, 1)
+k_rbgs_tb2(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float *__restrict__ rhs_b,
+           const float *__restrict__ pin_b, float *__restrict__ pout_r, float *__restrict__ pout_b, int TY, int ZC,
+           const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_b,
+           const __grid_constant__ CUtensorMap map_in) {
+    const int z0 = blockIdx.y * ZC, z1 = z0 + ZC < g.D ? z0 + ZC : g.D;
+    tb2_tile<WARPROW, TMA, PK>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, blockIdx.x * TY, z0, z1, threadIdx.x,
+                               threadIdx.y, blockDim.y, true, threadIdx.x == 0 && threadIdx.y == 0, &map_r, &map_b,
+                               &map_in);
 }
 
 static bool tb_supported(const Geom &g) {
@@ -1550,6 +1571,47 @@ void launch_batch_sweeps(const BatchSim *sims, const BatchActive *act, int nsims
             default: k_batch_sweep<8><<<grid, block, smem, st>>>(sims, act, c); break;
             }
         }
+}
+
+// Temporal blocking over a batch: one CTA per tile (grid, row band, z chunk)
+// of every grid, each tile exactly a tile of that grid's own pass, so a
+// grid's pressure equals two of its own sweeps bit for bit.  The CTA's 384
+// threads map onto the tile's Wq x nrp shape; threads beyond it only meet
+// the barriers.  Tiles of a grid whose solve has finished return at once.
+// Phase 0 reads p (black) and writes the grid's scratch q; phase 1 reads q
+// and writes p, so an even number of passes leaves the result in p.
+__global__ void __launch_bounds__(kTbThreads, 1)
+k_batch_tb2(const BatchSim *__restrict__ sims, const BatchTile *__restrict__ tiles,
+            const BatchCtl *__restrict__ ctl, int phase) {
+    const BatchTile T = tiles[blockIdx.x];
+    if (!ctl[T.sim].active) return;
+    const BatchSim &S = sims[T.sim];
+    const Geom g = S.g;
+    const SolveParams sp = S.sp;
+    const int Wq = g.W >> 3, nrp = (T.ty + 9) >> 1;
+    const int mq = (int)threadIdx.x % Wq, rp = (int)threadIdx.x / Wq;
+    const float *pin_b = phase ? S.q_b : S.p_b;
+    float *out_r = phase ? S.p_r : S.q_r;
+    float *out_b = phase ? S.p_b : S.q_b;
+    tb2_tile<false, false, false>(g, sp, S.rhs_r, S.rhs_b, pin_b, out_r, out_b, T.ty, T.j0, T.z0, T.z1, mq, rp, nrp,
+                                  rp < nrp, threadIdx.x == 0, nullptr, nullptr, nullptr);
+}
+
+bool batch_tb_supported(const Geom &g) { return tb_supported(g); }
+
+int batch_tb_rows(const Geom &g) { return tb_rows_tile(g.W >> 3, g.H); }
+
+size_t batch_tb_smem(const Geom &g) { return tb_smem(g, batch_tb_rows(g)); }
+
+void launch_batch_tb(const BatchSim *sims, const BatchTile *tiles, int ntiles, const BatchCtl *ctl, int sweeps,
+                     size_t smem, cudaStream_t st) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_batch_tb2, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        attr_set = true;
+    }
+    for (int pass = 0; pass < sweeps / 2; ++pass)
+        k_batch_tb2<<<ntiles, kTbThreads, smem, st>>>(sims, tiles, ctl, pass & 1);
 }
 
 __device__ __forceinline__ int find_sim(const int *__restrict__ start, int nsims, int b) {

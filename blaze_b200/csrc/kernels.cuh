@@ -142,8 +142,14 @@ struct BatchSim {
     SolveParams sp;
     const float *rhs_r, *rhs_b;
     float *p_r, *p_b;
+    float *q_r, *q_b;                   // the solver's temporal-blocking scratch pressure
     int max_iter;
     double tol;
+};
+// One temporal-blocking tile of a batch: grid `sim`, output rows
+// [j0, j0 + ty) and planes [z0, z1); ty = batch_tb_rows(grid).
+struct BatchTile {
+    int sim, j0, z0, z1, ty;
 };
 struct BatchCtl {
     int iters, checks, converged, active;
@@ -164,6 +170,14 @@ int  batch_sweep_grid(int kz, int block);
 // kz); nsims bounds its size.
 void launch_batch_sweeps(const BatchSim *sims, const BatchActive *act, int nsims, int sweeps, int kz, int grid,
                          int block, cudaStream_t st);
+// Temporal blocking in a batch: whether a grid's shape allows it, its tile
+// rows and the dynamic shared memory of its tiles; `sweeps` (a multiple of
+// 4) sweeps of every active grid as sweeps / 2 passes over the tiles.
+bool batch_tb_supported(const Geom &g);
+int  batch_tb_rows(const Geom &g);
+size_t batch_tb_smem(const Geom &g);
+void launch_batch_tb(const BatchSim *sims, const BatchTile *tiles, int ntiles, const BatchCtl *ctl, int sweeps,
+                     size_t smem, cudaStream_t st);
 // FP64 residual of every active grid (grid s owns partial blocks
 // [blk0[s], blk0[s+1]), residual_blocks(g_s) of them) and the per-grid
 // continue/stop decision.  2 launches.

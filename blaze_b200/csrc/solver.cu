@@ -1142,6 +1142,8 @@ void solver_batch_view(blz_solver *s, BatchSim *out, const blz_params **P) {
     out->rhs_b = s->rhs_b;
     out->p_r = s->p_r;
     out->p_b = s->p_b;
+    out->q_r = q_r(s);
+    out->q_b = q_b(s);
     out->max_iter = s->P.max_iter;
     out->tol = s->P.tol;
     if (P) *P = &s->P;

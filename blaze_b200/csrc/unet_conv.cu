@@ -54,14 +54,28 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
 
+__device__ __forceinline__ unsigned long long conv_now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// A commit group of one tile's MMAs completes in microseconds.
+constexpr unsigned long long kConvWaitNs = 10ull * 1000ull * 1000ull;
+
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, int *err) {
-    // Bounded: gives up after ~2^26 polls, records the timeout and returns.
-    for (int it = 0; it < (1 << 26); ++it) {
-        uint32_t done;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                     " selp.u32 %0, 1, 0, p;\n}\n"
-                     : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
-        if (done) return true;
+    // Bounded in time (device global timer): gives up after kConvWaitNs,
+    // records the timeout and returns.
+    const unsigned long long t0 = conv_now_ns();
+    for (;;) {
+        for (int it = 0; it < 64; ++it) {
+            uint32_t done;
+            asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                         " selp.u32 %0, 1, 0, p;\n}\n"
+                         : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
+            if (done) return true;
+        }
+        if (conv_now_ns() - t0 > kConvWaitNs) break;
     }
     if (err) atomicExch(err, 1);
     return false;
@@ -70,7 +84,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, int *e
 } // namespace
 
 template <int N, bool RELU, bool OUT_F32>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 1)
 k_conv3d_tc(int W, int H, int D, int cin, int out_stride, int out_offset, const __nv_bfloat16 *__restrict__ x,
             const __nv_bfloat16 *__restrict__ w, const float *__restrict__ bias, void *__restrict__ y,
             const __nv_bfloat16 *__restrict__ aux, int *err) {
@@ -104,13 +118,18 @@ k_conv3d_tc(int W, int H, int D, int cin, int out_stride, int out_offset, const 
     const int chunks = cin / 16;
     bool ok = true;
     for (int c = 0; c < chunks && ok; ++c) {
-        // Stage the 9 input rows of this 16-channel chunk ...
-        for (int e = tid; e < 9 * kRowVox * 2; e += 128) {
-            const int r = e / (kRowVox * 2), rem = e % (kRowVox * 2);
-            const int v = rem >> 1, kg = rem & 1;
+        // Stage the 9 input rows (dz, dy) of this 16-channel chunk: row r =
+        // (dz + 1) * 3 + (dy + 1) holds 16-byte chunks (kg, v) at kg *
+        // kKgBytes + v * 16, from voxel v of that row ...
+#pragma unroll
+        for (int r = 0; r < 9; ++r) {
             const int dz = r / 3 - 1, dy = r % 3 - 1;
-            const long long g = (long long)(z + 1 + dz) * plane + P0 - 1 + (long long)dy * Wp + v;
-            cp_async16(aS + r * kRowBytes + kg * kKgBytes + v * 16, x + g * cin + c * 16 + kg * 8);
+            const __nv_bfloat16 *rs =
+                x + ((long long)(z + 1 + dz) * plane + P0 - 1 + (long long)dy * Wp) * cin + c * 16;
+            for (int e = tid; e < 2 * kRowVox; e += 128) {
+                const int kg = e & 1, v = e >> 1;
+                cp_async16(aS + r * kRowBytes + kg * kKgBytes + v * 16, rs + (long long)v * cin + kg * 8);
+            }
         }
         // ... and the 27 taps' weights of the chunk (B: N x 16, K-major).
         for (int e = tid; e < 27 * N * 2; e += 128) {
@@ -209,29 +228,49 @@ int conv3d_smem_bytes(int cout) { return kABytes + 27 * cout * 32; }
 // half-resolution layers, which carry most of the network's voxels).  A CTA
 // keeps the layer's weights resident in shared memory and walks one 128-voxel
 // tile through `zs` consecutive planes.  Output plane z needs input planes
-// z-1, z, z+1 (padded planes z, z+1, z+2), 3 rows each; a ring of 5 plane
-// slots is filled by cp.async one plane ahead, so each plane's rows are
-// staged once per tile instead of three times, and the TMEM accumulator is
-// double buffered: the MMAs of plane z run while the epilogue of plane z-1
-// drains the other buffer and the rows of plane z+3 arrive.
-//   iteration z: issue loads of padded plane z+3 (slot (z+3)%5, whose last
+// z-1, z, z+1 (padded planes z, z+1, z+2), 3 rows each; a ring of S plane
+// slots is filled by cp.async S - 4 planes ahead, so each plane's rows are
+// staged once per tile instead of three times and their latency is hidden
+// behind S - 4 iterations, and the TMEM accumulator is double buffered: the
+// MMAs of plane z run while the epilogue of plane z-1 drains the other
+// buffer and the rows of planes up to z+S-2 arrive.
+//   iteration z: issue loads of padded plane z+S-2 (slot (z-2)%S, whose last
 //   reader, plane z-2's MMAs, completed in iteration z-1) | wait for planes
 //   <= z+2 | one thread issues 27 x cin/16 MMAs into buffer z&1 and commits to
 //   mbarrier z&1 | all threads wait for plane z-1's commit and store it.
+// S is as many slots as fit, at most 8: with two CTAs per SM when at least 6
+// fit in half the SM's shared memory (two independent pipelines), else with
+// one CTA.
 // ---------------------------------------------------------------------------
-constexpr int kZmSlots = 5;
+constexpr int kZmSmemOne = 227 * 1024 - 1024;            // dynamic bytes, one CTA per SM
+constexpr int kZmSmemTwo = 228 * 1024 / 2 - 1024 - 128;  // dynamic bytes, two CTAs per SM
 
 template <int CIN> __host__ __device__ constexpr int zm_slot_bytes() { return (CIN / 16) * 3 * kRowBytes; }
 template <int N, int CIN> __host__ __device__ constexpr int zm_w_bytes() { return 27 * (CIN / 16) * N * 32; }
-template <int N, int CIN> __host__ __device__ constexpr int zm_smem_bytes() { return zm_w_bytes<N, CIN>() + kZmSlots * zm_slot_bytes<CIN>(); }
+template <int N, int CIN> __host__ __device__ constexpr int zm_slots() {
+    return (kZmSmemTwo - zm_w_bytes<N, CIN>()) / zm_slot_bytes<CIN>() >= 6
+               ? ((kZmSmemTwo - zm_w_bytes<N, CIN>()) / zm_slot_bytes<CIN>() > 8
+                      ? 8 : (kZmSmemTwo - zm_w_bytes<N, CIN>()) / zm_slot_bytes<CIN>())
+               : ((kZmSmemOne - zm_w_bytes<N, CIN>()) / zm_slot_bytes<CIN>() > 8
+                      ? 8 : (kZmSmemOne - zm_w_bytes<N, CIN>()) / zm_slot_bytes<CIN>());
+}
+template <int N, int CIN> __host__ __device__ constexpr int zm_smem_bytes() {
+    return zm_w_bytes<N, CIN>() + zm_slots<N, CIN>() * zm_slot_bytes<CIN>();
+}
+static_assert(zm_slots<16, 16>() == 8 && zm_slots<32, 16>() == 7 && zm_slots<16, 32>() == 8 &&
+                  zm_slots<32, 32>() == 7, "ring slots of the z-marching convolution");
+static_assert(zm_smem_bytes<16, 16>() <= kZmSmemTwo && zm_smem_bytes<32, 16>() <= kZmSmemTwo &&
+                  zm_smem_bytes<16, 32>() <= kZmSmemOne && zm_smem_bytes<32, 32>() <= kZmSmemOne,
+              "shared memory of the z-marching convolution");
 
 template <int N, int CIN, bool RELU>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 1)
 k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const __nv_bfloat16 *__restrict__ x,
             const __nv_bfloat16 *__restrict__ w, const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y,
             const __nv_bfloat16 *__restrict__ aux, int *err) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int CH = CIN / 16;
+    constexpr int S = zm_slots<N, CIN>();
     constexpr int kSlot = zm_slot_bytes<CIN>();
     constexpr int kCols = 2 * N < 32 ? 32 : 2 * N;
     unsigned char *sB = smem;
@@ -268,26 +307,30 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
         cp_async16(bS + ct * N * 32 + kg * N * 16 + n * 16, w + ((size_t)t * N + n) * CIN + ch * 16 + kg * 8);
     }
     // Rows dy = -1, 0, 1 of padded plane pz (130 voxels each, the tile's row
-    // segment and one voxel either side), per chunk and 8-channel half.
+    // segment and one voxel either side), per chunk and 8-channel half: row
+    // (ch, dy) of the slot holds 16-byte chunks (kg, v) at kg * kKgBytes +
+    // v * 16, read from voxel v of that row, channels ch * 16 + kg * 8.
     auto load_plane = [&](int pz) {
-        const uint32_t dst = aS + (uint32_t)((pz % kZmSlots) * kSlot);
-        for (int e = tid; e < CH * 3 * kRowVox * 2; e += 128) {
-            const int kg = e & 1;
-            int rest = e >> 1;
-            const int v = rest % kRowVox;
-            rest /= kRowVox;
-            const int dy = rest % 3, ch = rest / 3;
-            const long long g = (long long)pz * plane + P0 - 1 + (long long)(dy - 1) * Wp + v;
-            cp_async16(dst + ch * 3 * kRowBytes + dy * kRowBytes + kg * kKgBytes + v * 16,
-                       x + g * CIN + ch * 16 + kg * 8);
+        const uint32_t dst = aS + (uint32_t)((pz % S) * kSlot);
+        const __nv_bfloat16 *src = x + ((long long)pz * plane + P0 - 1 - Wp) * CIN;
+#pragma unroll
+        for (int row = 0; row < CH * 3; ++row) {
+            const int ch = row / 3, dy = row % 3;
+            const __nv_bfloat16 *rs = src + (long long)dy * Wp * CIN + ch * 16;
+            const uint32_t rd = dst + (uint32_t)(row * kRowBytes);
+            for (int e = tid; e < 2 * kRowVox; e += 128) {
+                const int kg = e & 1, v = e >> 1;
+                cp_async16(rd + kg * kKgBytes + v * 16, rs + (long long)v * CIN + kg * 8);
+            }
         }
     };
-    if (nz > 0) {
-        load_plane(z0);
-        load_plane(z0 + 1);
-        load_plane(z0 + 2);
+    // Prologue: padded planes z0 .. z0+S-3, one commit group each (the
+    // weights join the first), so commit group q holds padded plane z0 + q.
+#pragma unroll 1
+    for (int p = 0; p < S - 2; ++p) {
+        if (p < nz + 2) load_plane(z0 + p);
+        asm volatile("cp.async.commit_group;" ::: "memory");
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
     constexpr uint32_t idesc = umma_idesc_bf16(kConvM, N);
 
     auto epilogue = [&](int it) -> bool {
@@ -344,17 +387,20 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
     int issued = 0;                                     // MMA groups committed
     for (int it = 0; it < nz && ok; ++it) {
         const int z = z0 + it;
-        if (it + 1 < nz) load_plane(z + 3);
-        asm volatile("cp.async.commit_group;\ncp.async.wait_group 1;" ::: "memory");
+        if (it + S - 2 < nz + 2) load_plane(z + S - 2);
+        // groups committed: S - 2 + it + 1; all but the newest S - 4 done
+        // means padded planes <= z0 + it + 2 = z + 2 have landed
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group %0;" ::"n"(S - 4) : "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t acc = tmem + (uint32_t)((it & 1) * N);
             // slots of padded planes z, z+1, z+2 (taps dz = -1, 0, +1)
-            const uint32_t sz[3] = {aS + (uint32_t)((z % kZmSlots) * kSlot),
-                                    aS + (uint32_t)(((z + 1) % kZmSlots) * kSlot),
-                                    aS + (uint32_t)(((z + 2) % kZmSlots) * kSlot)};
+            const uint32_t sz[3] = {aS + (uint32_t)((z % S) * kSlot),
+                                    aS + (uint32_t)(((z + 1) % S) * kSlot),
+                                    aS + (uint32_t)(((z + 2) % S) * kSlot)};
 #pragma unroll
             for (int ch = 0; ch < CH; ++ch) {
 #pragma unroll

@@ -140,3 +140,75 @@ def test_batch_with_warm_start_equals_single(turbulence):
             assert np.array_equal(fa[i][name], fb[i][name]), (i, name)
     for n in nets.values():
         n.close()
+
+
+# Temporal blocking in a batch: one band (16^2 rows), two bands with a ragged
+# second one (96 rows of 80 per tile), 8-row tiles of 48 quads (width 384),
+# an odd depth, and a small grid.
+TB_DIMS = [(16, 16, 16), (64, 96, 40), (384, 20, 12), (48, 40, 31), (32, 24, 16)]
+
+
+def _tb_scenes():
+    from blaze_b200.scenes import batch_scenes
+    return [batch_scenes(1, seed=20 + i, tol=1e-4, max_iter=4000, check_every=20, dims=[d])[0]
+            for i, d in enumerate(TB_DIMS)]
+
+
+def _run_frames(sims, frames, batch_planes=None):
+    from blaze_b200.batch import Batch
+    stats = []
+    if batch_planes is None:
+        for f in range(frames):
+            row = []
+            for s in sims:
+                s.addSource()
+                row.append(s.step(f / 24.0))
+            stats.append(row)
+        return stats
+    batch = Batch(sims)
+    batch.set_sweep(batch_planes)
+    for f in range(frames):
+        batch.add_source()
+        stats.append(batch.step([f / 24.0] * len(sims)))
+    batch.close()
+    return stats
+
+
+@pytest.mark.parametrize("planes", [-1, 0, 8, 16, 32])
+def test_batch_sweep_kernels_equal_single(planes):
+    """Every sweep kernel of the batch (autotuned, segment, temporal blocking
+    with 8, 16 or 32 planes per tile) gives each grid the sweeps, residuals
+    and fields of its own solve, bit for bit."""
+    frames = 3
+    single = _make(_tb_scenes())
+    sa = _run_frames(single, frames)
+    batched = _make(_tb_scenes())
+    sb = _run_frames(batched, frames, planes)
+    for f in range(frames):
+        for i in range(len(single)):
+            a, b = sa[f][i], sb[f][i]
+            assert a["iterations"] > 0 and a["iterations"] == b["iterations"], (planes, f, i, a, b)
+            assert a["residual"] == b["residual"] and a["converged"] == b["converged"], (planes, f, i)
+            if planes > 0:
+                assert b["sweep_variant"] == 100 + planes
+            elif planes == 0:
+                assert b["sweep_variant"] in (1, 2, 4, 8)
+    for i in range(len(single)):
+        for name in FIELDS:
+            assert np.array_equal(single[i].get(name), batched[i].get(name)), (planes, i, name)
+    for s in single + batched:
+        s.close()
+
+
+def test_batch_temporal_blocking_needs_four_sweep_checks():
+    """check_every = 10 (not a multiple of 4) leaves only the segment kernel."""
+    from blaze_b200.batch import Batch
+    from blaze_b200.scenes import batch_scenes
+    sims = _make(batch_scenes(2, seed=3, tol=1e-4, max_iter=400, check_every=10, dims=[(16, 16, 16)]))
+    batch = Batch(sims)
+    with pytest.raises(RuntimeError):
+        batch.set_sweep(16)
+    batch.set_sweep(0)
+    batch.close()
+    for s in sims:
+        s.close()
