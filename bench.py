@@ -554,6 +554,8 @@ def run_batch(args, ws, rank, local):
 
 def _batch_kernel_name(v):
     """The batch autotuner's choice as reported in the stats' sweep_variant."""
+    if v > 200:
+        return f"temporal blocking, two sweeps per pass, tiles of {v - 200} planes, paired-FP32 stencil (autotuned)"
     if v > 100:
         return f"temporal blocking, two sweeps per pass, tiles of {v - 100} planes (autotuned)"
     return f"segment kernel, one sweep per pass, {v} plane(s) per thread (autotuned)"

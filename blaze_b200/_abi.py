@@ -206,7 +206,7 @@ EXPORTS = {
     "blz_batch_create": (C.c_int, [_P(C.c_void_p), C.c_int, _P(C.c_void_p)]),
     "blz_batch_destroy": (C.c_int, [C.c_void_p]),
     "blz_batch_stream": (C.c_void_p, [C.c_void_p]),
-    "blz_batch_set_sweep": (C.c_int, [C.c_void_p, C.c_int]),
+    "blz_batch_set_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "blz_batch_add_source": (C.c_int, [C.c_void_p]),
     "blz_batch_step": (C.c_int, [C.c_void_p, _P(C.c_float), _P(BlzStepStats)]),
     "blz_batch_solve": (C.c_int, [C.c_void_p, _P(BlzStepStats)]),

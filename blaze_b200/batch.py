@@ -54,12 +54,13 @@ class Batch:
         check(self._lib.blz_batch_solve(self._h, self._stats))
         return [s.as_dict() for s in self._stats]
 
-    def set_sweep(self, planes):
+    def set_sweep(self, planes, paired=False):
         """-1: autotune (default); 0: the segment kernel; planes > 0: temporal
-        blocking with tiles of that many planes.  Every choice gives the
-        same bits; the stats' sweep_variant reports the one in use (1, 2, 4, 8
-        planes per thread, or 100 + planes per tile)."""
-        check(self._lib.blz_batch_set_sweep(self._h, int(planes)))
+        blocking with tiles of that many planes (paired: the paired-FP32
+        stencil).  Every choice gives the same bits; the stats' sweep_variant
+        reports the one in use (1, 2, 4, 8 planes per thread, or 100 (scalar)
+        or 200 (paired) + planes per tile)."""
+        check(self._lib.blz_batch_set_sweep(self._h, int(planes), 1 if paired else 0))
 
     def last_ms(self):
         return float(self._lib.blz_batch_last_ms(self._h))

@@ -82,7 +82,9 @@ struct blz_batch {
     // temporal blocking (two sweeps per pass over HBM): planes per tile, 0
     // when the segment kernel was chosen (or the batch does not allow it)
     int tb_zc = 0;
+    bool tb_pk = false;                       // paired-FP32 stencil in the tiles
     int force_zc = -1;                        // blz_batch_set_sweep: -1 autotune, 0 segment, > 0 tiles of that many planes
+    bool force_pk = false;                    // ... with the paired-FP32 stencil
     bool tb_ok = false;                       // every grid's shape allows it and check_every % 4 == 0
     BatchTile *d_tiles = nullptr;             // tiles of the current tb_zc, heaviest first
     int ntiles = 0, tiles_cap = 0;
@@ -170,7 +172,8 @@ static int build_tiles(blz_batch *b, const std::vector<BatchSim> &h, int zc) {
 // Body of the batched solve, appended to the capture in progress on b->st:
 // check_every sweeps over the grids still running, their residual and decision.
 static void capture_body(blz_batch *b, cudaGraphConditionalHandle h) {
-    if (b->tb_zc > 0) launch_batch_tb(b->d_sims, b->d_tiles, b->ntiles, b->d_ctl, b->chunk, b->tb_smem, b->st);
+    if (b->tb_zc > 0)
+        launch_batch_tb(b->d_sims, b->d_tiles, b->ntiles, b->d_ctl, b->chunk, b->tb_smem, b->tb_pk, b->st);
     else launch_batch_sweeps(b->d_sims, b->d_act, b->n, b->chunk, b->kz, b->grid, b->block, b->st);
     launch_batch_check(b->d_sims, b->d_blk0, b->n, b->total_blocks, b->d_ctl, b->partials, 1, b->chunk, b->st);
     active_list(b, b->kz, 1, h);
@@ -273,8 +276,9 @@ done:
 
 // Autotuner: the segment kernel's planes per thread x block size (two sweeps
 // of the whole batch timed) against temporal blocking with 8, 16 or 32
-// planes per tile (four sweeps timed), per sweep, on scratch copies of every
-// pressure (all shapes give identical results).
+// planes per tile, scalar or paired-FP32 stencil (four sweeps timed), per
+// sweep, on scratch copies of every pressure (all shapes give identical
+// results).
 static int tune(blz_batch *b) {
     if (b->kz >= 0) return BLZ_OK;
     std::vector<BatchSim> h(b->n), hs(b->n);
@@ -317,27 +321,32 @@ static int tune(blz_batch *b) {
             if (e == cudaSuccess && ms / 2.0f < best) { best = ms / 2.0f; b->kz = kz; b->block = blk; b->grid = grid; }
         }
     b->tb_zc = 0;
+    b->tb_pk = false;
     int tb_best = b->force_zc > 0 ? b->force_zc : 0;
+    bool pk_best = b->force_zc > 0 && b->force_pk;
     for (int zi = 0; zi < 3 && b->tb_ok && b->force_zc < 0 && e == cudaSuccess; ++zi) {
         const int zc = kTbZC[zi];
         const int rc = build_tiles(b, h, zc);
         if (rc != BLZ_OK) { e = cudaErrorUnknown; break; }
-        launch_batch_tb(d_scr, b->d_tiles, b->ntiles, b->d_ctl, 4, b->tb_smem, b->st);
-        e = cudaEventRecord(b->ev0, b->st);
-        launch_batch_tb(d_scr, b->d_tiles, b->ntiles, b->d_ctl, 4, b->tb_smem, b->st);
-        if (e == cudaSuccess) e = cudaEventRecord(b->ev1, b->st);
-        if (e == cudaSuccess) e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaEventSynchronize(b->ev1);
-        float ms = 0.0f;
-        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-        b->launches += 4;
-        if (e == cudaSuccess && ms / 4.0f < best) { best = ms / 4.0f; tb_best = zc; }
+        for (int pk = 0; pk < 2 && e == cudaSuccess; ++pk) {
+            launch_batch_tb(d_scr, b->d_tiles, b->ntiles, b->d_ctl, 4, b->tb_smem, pk != 0, b->st);
+            e = cudaEventRecord(b->ev0, b->st);
+            launch_batch_tb(d_scr, b->d_tiles, b->ntiles, b->d_ctl, 4, b->tb_smem, pk != 0, b->st);
+            if (e == cudaSuccess) e = cudaEventRecord(b->ev1, b->st);
+            if (e == cudaSuccess) e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaEventSynchronize(b->ev1);
+            float ms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+            b->launches += 4;
+            if (e == cudaSuccess && ms / 4.0f < best) { best = ms / 4.0f; tb_best = zc; pk_best = pk != 0; }
+        }
     }
     if (e == cudaSuccess && tb_best > 0) {
         b->tb_zc = tb_best;
+        b->tb_pk = pk_best;
         if (build_tiles(b, h, tb_best) != BLZ_OK) e = cudaErrorUnknown;
-        // no sweeps: only the kernel's shared-memory limit, set outside the capture
-        launch_batch_tb(d_scr, b->d_tiles, b->ntiles, b->d_ctl, 0, b->tb_smem, b->st);
+        // no sweeps: only the kernels' shared-memory limit, set outside the capture
+        launch_batch_tb(d_scr, b->d_tiles, b->ntiles, b->d_ctl, 0, b->tb_smem, false, b->st);
     }
     cudaStreamSynchronize(b->st);
     cudaFree(scratch);
@@ -385,7 +394,7 @@ static int read_stats(blz_batch *b, blz_step_stats *stats, int loop_ran) {
         st.rhs_norm = bn;
         st.rel_residual = bn > 0.0 ? r / bn : 0.0;
         st.residual_checks = c.checks;
-        st.sweep_variant = b->tb_zc > 0 ? 100 + b->tb_zc : b->kz;
+        st.sweep_variant = b->tb_zc > 0 ? (b->tb_pk ? 200 : 100) + b->tb_zc : b->kz;
         st.device_loop = 1;
         if (solver_warm(b->sims[i])) {
             st.warm_started = 1;
@@ -501,7 +510,7 @@ int blz_batch_destroy(blz_batch *b) {
 
 void *blz_batch_stream(blz_batch *b) { return b ? (void *)b->st : nullptr; }
 
-int blz_batch_set_sweep(blz_batch *b, int planes) {
+int blz_batch_set_sweep(blz_batch *b, int planes, int paired) {
     if (!b) return bfail(BLZ_ERR_ARG, "null batch");
     if (planes < -1) return bfail(BLZ_ERR_ARG, "planes must be -1 (autotune), 0 (segment kernel) or > 0");
     if (planes > 0 && !b->tb_ok)
@@ -509,6 +518,7 @@ int blz_batch_set_sweep(blz_batch *b, int planes) {
                                   "width <= 384");
     BCK(cudaStreamSynchronize(b->st));
     b->force_zc = planes;
+    b->force_pk = paired != 0;
     b->kz = -1;                               // tune again at the next solve
     if (b->solve_exec) { cudaGraphExecDestroy(b->solve_exec); b->solve_exec = nullptr; }
     for (auto &x : b->frame_exec)

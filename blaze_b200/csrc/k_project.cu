@@ -1579,7 +1579,9 @@ void launch_batch_sweeps(const BatchSim *sims, const BatchActive *act, int nsims
 // threads map onto the tile's Wq x nrp shape; threads beyond it only meet
 // the barriers.  Tiles of a grid whose solve has finished return at once.
 // Phase 0 reads p (black) and writes the grid's scratch q; phase 1 reads q
-// and writes p, so an even number of passes leaves the result in p.
+// and writes p, so an even number of passes leaves the result in p.  PK: the
+// stencil on paired FP32 instructions (the same bits).
+template <bool PK>
 __global__ void __launch_bounds__(kTbThreads, 1)
 k_batch_tb2(const BatchSim *__restrict__ sims, const BatchTile *__restrict__ tiles,
             const BatchCtl *__restrict__ ctl, int phase) {
@@ -1593,8 +1595,8 @@ k_batch_tb2(const BatchSim *__restrict__ sims, const BatchTile *__restrict__ til
     const float *pin_b = phase ? S.q_b : S.p_b;
     float *out_r = phase ? S.p_r : S.q_r;
     float *out_b = phase ? S.p_b : S.q_b;
-    tb2_tile<false, false, false>(g, sp, S.rhs_r, S.rhs_b, pin_b, out_r, out_b, T.ty, T.j0, T.z0, T.z1, mq, rp, nrp,
-                                  rp < nrp, threadIdx.x == 0, nullptr, nullptr, nullptr);
+    tb2_tile<false, false, PK>(g, sp, S.rhs_r, S.rhs_b, pin_b, out_r, out_b, T.ty, T.j0, T.z0, T.z1, mq, rp, nrp,
+                               rp < nrp, threadIdx.x == 0, nullptr, nullptr, nullptr);
 }
 
 bool batch_tb_supported(const Geom &g) { return tb_supported(g); }
@@ -1604,14 +1606,17 @@ int batch_tb_rows(const Geom &g) { return tb_rows_tile(g.W >> 3, g.H); }
 size_t batch_tb_smem(const Geom &g) { return tb_smem(g, batch_tb_rows(g)); }
 
 void launch_batch_tb(const BatchSim *sims, const BatchTile *tiles, int ntiles, const BatchCtl *ctl, int sweeps,
-                     size_t smem, cudaStream_t st) {
+                     size_t smem, bool pk, cudaStream_t st) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_batch_tb2, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_batch_tb2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_batch_tb2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
         attr_set = true;
     }
-    for (int pass = 0; pass < sweeps / 2; ++pass)
-        k_batch_tb2<<<ntiles, kTbThreads, smem, st>>>(sims, tiles, ctl, pass & 1);
+    for (int pass = 0; pass < sweeps / 2; ++pass) {
+        if (pk) k_batch_tb2<true><<<ntiles, kTbThreads, smem, st>>>(sims, tiles, ctl, pass & 1);
+        else k_batch_tb2<false><<<ntiles, kTbThreads, smem, st>>>(sims, tiles, ctl, pass & 1);
+    }
 }
 
 __device__ __forceinline__ int find_sim(const int *__restrict__ start, int nsims, int b) {

@@ -172,12 +172,13 @@ void launch_batch_sweeps(const BatchSim *sims, const BatchActive *act, int nsims
                          int block, cudaStream_t st);
 // Temporal blocking in a batch: whether a grid's shape allows it, its tile
 // rows and the dynamic shared memory of its tiles; `sweeps` (a multiple of
-// 4) sweeps of every active grid as sweeps / 2 passes over the tiles.
+// 4) sweeps of every active grid as sweeps / 2 passes over the tiles (pk: the
+// paired-FP32 stencil; the same bits).
 bool batch_tb_supported(const Geom &g);
 int  batch_tb_rows(const Geom &g);
 size_t batch_tb_smem(const Geom &g);
 void launch_batch_tb(const BatchSim *sims, const BatchTile *tiles, int ntiles, const BatchCtl *ctl, int sweeps,
-                     size_t smem, cudaStream_t st);
+                     size_t smem, bool pk, cudaStream_t st);
 // FP64 residual of every active grid (grid s owns partial blocks
 // [blk0[s], blk0[s+1]), residual_blocks(g_s) of them) and the per-grid
 // continue/stop decision.  2 launches.

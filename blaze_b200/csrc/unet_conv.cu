@@ -231,17 +231,27 @@ int conv3d_smem_bytes(int cout) { return kABytes + 27 * cout * 32; }
 // z-1, z, z+1 (padded planes z, z+1, z+2), 3 rows each; a ring of S plane
 // slots is filled by cp.async S - 4 planes ahead, so each plane's rows are
 // staged once per tile instead of three times and their latency is hidden
-// behind S - 4 iterations, and the TMEM accumulator is double buffered: the
-// MMAs of plane z run while the epilogue of plane z-1 drains the other
-// buffer and the rows of planes up to z+S-2 arrive.
-//   iteration z: issue loads of padded plane z+S-2 (slot (z-2)%S, whose last
-//   reader, plane z-2's MMAs, completed in iteration z-1) | wait for planes
-//   <= z+2 | one thread issues 27 x cin/16 MMAs into buffer z&1 and commits to
-//   mbarrier z&1 | all threads wait for plane z-1's commit and store it.
+// behind S - 4 iterations, and the TMEM accumulator is double buffered.  The
+// CTA is warp specialised and its warps hand over through mbarriers only:
+//   workers (warps 0-3), iteration z: issue the loads of padded plane z+S-2
+//   (into the slot of plane z-2, whose last reader, plane z-2's MMAs,
+//   completed before they read that plane out) | wait for their own copies
+//   of planes <= z+2, fence them to the async proxy and arrive on full[] of
+//   plane z+2 | wait for plane z-1's MMAs (accf), read its accumulator from
+//   TMEM, add bias / ReLU, store, arrive on acce (buffer free);
+//   MMA warp (warp 4), iteration z: wait full[] of plane z+2 and acce of
+//   buffer z&1 (read out by iteration z-2) | lane 0 issues 27 x cin/16 MMAs
+//   into buffer z&1 and commits to accf[z&1].
+// So the MMAs of plane z run while the workers drain plane z-1 and stage
+// plane z+S-2.  Every wait is bounded in time; a wait that gives up sets
+// the error flag and ends that warp's loop, which ends the others' at their
+// next (bounded) wait.
 // S is as many slots as fit, at most 8: with two CTAs per SM when at least 6
 // fit in half the SM's shared memory (two independent pipelines), else with
 // one CTA.
 // ---------------------------------------------------------------------------
+constexpr int kZmWorkers = 128;                           // staging + epilogue warps 0-3
+constexpr int kZmThreads = kZmWorkers + 32;               // + the MMA warp
 constexpr int kZmSmemOne = 227 * 1024 - 1024;            // dynamic bytes, one CTA per SM
 constexpr int kZmSmemTwo = 228 * 1024 / 2 - 1024 - 128;  // dynamic bytes, two CTAs per SM
 
@@ -264,7 +274,7 @@ static_assert(zm_smem_bytes<16, 16>() <= kZmSmemTwo && zm_smem_bytes<32, 16>() <
               "shared memory of the z-marching convolution");
 
 template <int N, int CIN, bool RELU>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kZmThreads, 1)
 k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const __nv_bfloat16 *__restrict__ x,
             const __nv_bfloat16 *__restrict__ w, const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y,
             const __nv_bfloat16 *__restrict__ aux, int *err) {
@@ -273,11 +283,16 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
     constexpr int S = zm_slots<N, CIN>();
     constexpr int kSlot = zm_slot_bytes<CIN>();
     constexpr int kCols = 2 * N < 32 ? 32 : 2 * N;
+    constexpr uint32_t idesc = umma_idesc_bf16(kConvM, N);
     unsigned char *sB = smem;
     unsigned char *sA = smem + zm_w_bytes<N, CIN>();
-    __shared__ __align__(8) uint64_t mbar[2];
+    // full[s]: the plane in ring slot s has landed (one arrival per worker
+    // thread); accf[b]: the MMAs into accumulator buffer b completed (their
+    // commit); acce[b]: buffer b has been read out (one arrival per worker).
+    __shared__ __align__(8) uint64_t full[S], accf[2], acce[2];
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool worker = warp < 4;
     const int Wp = W + 2, Hp = H + 2;
     const long long plane = (long long)Wp * Hp;
     const long long P0 = (long long)Wp + (long long)kConvM * blockIdx.x;
@@ -290,8 +305,12 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])) : "memory");
+        for (int s = 0; s < S; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(kZmWorkers) : "memory");
+        for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&accf[b])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acce[b])), "r"(kZmWorkers) : "memory");
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -299,135 +318,175 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base;
     const uint32_t aS = smem_u32(sA), bS = smem_u32(sB);
+    // Ring slot of padded plane pz: (pz - z0) % S, so the n-th fill of a slot
+    // is the plane z0 + s + n S and completes phase n of full[s].
+    auto slot_of = [&](int pz) { return (pz - z0) % S; };
+    auto fill_parity = [&](int pz) { return (uint32_t)(((pz - z0) / S) & 1); };
 
-    // Weights of every 16-channel chunk: block (ch, tap) = N rows x 32 B, K-major.
-    for (int e = tid; e < 27 * CH * N * 2; e += 128) {
-        const int kg = e & 1, n = (e >> 1) % N, ct = (e >> 1) / N;          // ct = ch * 27 + tap
-        const int ch = ct / 27, t = ct % 27;
-        cp_async16(bS + ct * N * 32 + kg * N * 16 + n * 16, w + ((size_t)t * N + n) * CIN + ch * 16 + kg * 8);
-    }
-    // Rows dy = -1, 0, 1 of padded plane pz (130 voxels each, the tile's row
-    // segment and one voxel either side), per chunk and 8-channel half: row
-    // (ch, dy) of the slot holds 16-byte chunks (kg, v) at kg * kKgBytes +
-    // v * 16, read from voxel v of that row, channels ch * 16 + kg * 8.
-    auto load_plane = [&](int pz) {
-        const uint32_t dst = aS + (uint32_t)((pz % S) * kSlot);
-        const __nv_bfloat16 *src = x + ((long long)pz * plane + P0 - 1 - Wp) * CIN;
-#pragma unroll
-        for (int row = 0; row < CH * 3; ++row) {
-            const int ch = row / 3, dy = row % 3;
-            const __nv_bfloat16 *rs = src + (long long)dy * Wp * CIN + ch * 16;
-            const uint32_t rd = dst + (uint32_t)(row * kRowBytes);
-            for (int e = tid; e < 2 * kRowVox; e += 128) {
-                const int kg = e & 1, v = e >> 1;
-                cp_async16(rd + kg * kKgBytes + v * 16, rs + (long long)v * CIN + kg * 8);
-            }
+    if (worker) {
+        // ---- workers: stage planes, drain the accumulators ----
+        // Weights of every 16-channel chunk: block (ch, tap) = N rows x 32 B,
+        // K-major; they join the first plane's commit group.
+        for (int e = tid; e < 27 * CH * N * 2; e += kZmWorkers) {
+            const int kg = e & 1, n = (e >> 1) % N, ct = (e >> 1) / N;      // ct = ch * 27 + tap
+            const int ch = ct / 27, t = ct % 27;
+            cp_async16(bS + ct * N * 32 + kg * N * 16 + n * 16, w + ((size_t)t * N + n) * CIN + ch * 16 + kg * 8);
         }
-    };
-    // Prologue: padded planes z0 .. z0+S-3, one commit group each (the
-    // weights join the first), so commit group q holds padded plane z0 + q.
-#pragma unroll 1
-    for (int p = 0; p < S - 2; ++p) {
-        if (p < nz + 2) load_plane(z0 + p);
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    }
-    constexpr uint32_t idesc = umma_idesc_bf16(kConvM, N);
-
-    auto epilogue = [&](int it) -> bool {
-        const bool done = mbar_wait(smem_u32(&mbar[it & 1]), (uint32_t)((it >> 1) & 1), err);
-        const bool ok = __syncthreads_and(done) != 0;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (!ok) return false;
-        const long long P = P0 + 32 * warp + lane;
-        const int xp = (int)(P % Wp), yp = (int)(P / Wp);
-        const bool inside = xp >= 1 && xp <= W && yp >= 1 && yp <= H;
-        const long long outv = (long long)(z0 + it + 1) * plane + P;
+        // Rows dy = -1, 0, 1 of padded plane pz (130 voxels each, the tile's
+        // row segment and one voxel either side): row (ch, dy) of the slot
+        // holds 16-byte chunks (kg, v) at kg * kKgBytes + v * 16, read from
+        // voxel v of that row, channels ch * 16 + kg * 8.
+        auto load_plane = [&](int pz) {
+            const uint32_t dst = aS + (uint32_t)(slot_of(pz) * kSlot);
+            const __nv_bfloat16 *src = x + ((long long)pz * plane + P0 - 1 - Wp) * CIN;
 #pragma unroll
-        for (int n0 = 0; n0 < N; n0 += 16) {
-            uint32_t r[16];
-            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)((it & 1) * N + n0);
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-                           "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                         : "r"(taddr) : "memory");
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (inside) {
-                float v[16];
-#pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    v[q] = __uint_as_float(r[q]) + (bias ? __ldg(bias + n0 + q) : 0.0f);
-                    if (RELU) v[q] = fmaxf(v[q], 0.0f);
+            for (int row = 0; row < CH * 3; ++row) {
+                const int ch = row / 3, dy = row % 3;
+                const __nv_bfloat16 *rs = src + (long long)dy * Wp * CIN + ch * 16;
+                const uint32_t rd = dst + (uint32_t)(row * kRowBytes);
+                for (int e = tid; e < 2 * kRowVox; e += kZmWorkers) {
+                    const int kg = e & 1, v = e >> 1;
+                    cp_async16(rd + kg * kKgBytes + v * 16, rs + (long long)v * CIN + kg * 8);
                 }
-                const long long o = outv * out_stride + out_offset + n0;
-                if (aux) {
-                    const uint4 a0 = __ldg(reinterpret_cast<const uint4 *>(aux + o));
-                    const uint4 a1 = __ldg(reinterpret_cast<const uint4 *>(aux + o) + 1);
-                    const __nv_bfloat16 *ah0 = reinterpret_cast<const __nv_bfloat16 *>(&a0);
-                    const __nv_bfloat16 *ah1 = reinterpret_cast<const __nv_bfloat16 *>(&a1);
+            }
+        };
+        // This thread's voxel of the tile (TMEM lane 32 * warp + lane) and
+        // the bias, the same on every plane.
+        const long long Pv = P0 + 32 * warp + lane;
+        const int yv = (int)(Pv / Wp), xv = (int)(Pv - (long long)yv * Wp);
+        const bool inside = xv >= 1 && xv <= W && yv >= 1 && yv <= H;
+        float bv[N];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        if (!(__bfloat162float(ah0[q]) > 0.0f)) v[q] = 0.0f;
-                        if (!(__bfloat162float(ah1[q]) > 0.0f)) v[8 + q] = 0.0f;
+        for (int q = 0; q < N; ++q) bv[q] = bias ? __ldg(bias + q) : 0.0f;
+        // Reads accumulator buffer it & 1 (output plane z0 + it) and stores
+        // it; false (the whole warp alike) when its wait gave up.
+        auto epilogue = [&](int it) -> bool {
+            const bool done = mbar_wait(smem_u32(&accf[it & 1]), (uint32_t)((it >> 1) & 1), err);
+            if (!__all_sync(0xffffffffu, done)) return false;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const long long outv = (long long)(z0 + it + 1) * plane + Pv;
+#pragma unroll
+            for (int n0 = 0; n0 < N; n0 += 16) {
+                uint32_t r[16];
+                const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)((it & 1) * N + n0);
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                               "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+                               "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                             : "r"(taddr) : "memory");
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (inside) {
+                    float v[16];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        v[q] = __uint_as_float(r[q]) + bv[n0 + q];
+                        if (RELU) v[q] = fmaxf(v[q], 0.0f);
+                    }
+                    const long long o = outv * out_stride + out_offset + n0;
+                    if (aux) {
+                        const uint4 a0 = __ldg(reinterpret_cast<const uint4 *>(aux + o));
+                        const uint4 a1 = __ldg(reinterpret_cast<const uint4 *>(aux + o) + 1);
+                        const __nv_bfloat16 *ah0 = reinterpret_cast<const __nv_bfloat16 *>(&a0);
+                        const __nv_bfloat16 *ah1 = reinterpret_cast<const __nv_bfloat16 *>(&a1);
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            if (!(__bfloat162float(ah0[q]) > 0.0f)) v[q] = 0.0f;
+                            if (!(__bfloat162float(ah1[q]) > 0.0f)) v[8 + q] = 0.0f;
+                        }
+                    }
+                    __nv_bfloat162 h[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                    uint4 *dst = reinterpret_cast<uint4 *>(y + o);
+                    dst[0] = *reinterpret_cast<uint4 *>(&h[0]);
+                    dst[1] = *reinterpret_cast<uint4 *>(&h[4]);
+                }
+            }
+            // buffer it & 1 may be overwritten by the MMAs of iteration it + 2
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acce[it & 1])) : "memory");
+            return true;
+        };
+        auto arrive_full = [&](int pz) {
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[slot_of(pz)])) : "memory");
+        };
+        // Prologue: padded planes z0 .. z0+S-3, one commit group each, so
+        // commit group q holds padded plane z0 + q.
+#pragma unroll 1
+        for (int p = 0; p < S - 2; ++p) {
+            if (p < nz + 2) load_plane(z0 + p);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        }
+        bool ok = true;
+#pragma unroll 1
+        for (int it = 0; it < nz && ok; ++it) {
+            const int z = z0 + it;
+            // plane z+S-2 goes into the slot of plane z-2, whose last reader
+            // (the MMAs of iteration it-2) completed before epilogue(it-2)
+            if (it + S - 2 < nz + 2) load_plane(z + S - 2);
+            // groups committed: S - 2 + it + 1; all but the newest S - 4
+            // done means this thread's copies of planes <= z + 2 landed
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            asm volatile("cp.async.wait_group %0;" ::"n"(S - 4) : "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (it == 0) {
+                arrive_full(z);
+                arrive_full(z + 1);
+            }
+            arrive_full(z + 2);
+            if (it > 0) ok = epilogue(it - 1);
+        }
+        if (ok && nz > 0) ok = epilogue(nz - 1);
+        if (!ok && err) atomicExch(err, 1);
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+    } else {
+        // ---- MMA warp: lane 0 issues each plane's 27 x cin/16 MMAs ----
+        int issued = 0;
+        bool ok = true;
+#pragma unroll 1
+        for (int it = 0; it < nz && ok; ++it) {
+            const int z = z0 + it;
+            bool done = true;
+            if (it == 0) {
+                done = mbar_wait(smem_u32(&full[slot_of(z)]), fill_parity(z), err) && done;
+                done = mbar_wait(smem_u32(&full[slot_of(z + 1)]), fill_parity(z + 1), err) && done;
+            }
+            done = mbar_wait(smem_u32(&full[slot_of(z + 2)]), fill_parity(z + 2), err) && done;
+            // accumulator buffer it & 1 was last read out by epilogue(it - 2)
+            if (it >= 2) done = mbar_wait(smem_u32(&acce[it & 1]), (uint32_t)(((it - 2) >> 1) & 1), err) && done;
+            if (!__all_sync(0xffffffffu, done)) { ok = false; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (lane == 0) {
+                const uint32_t acc = tmem + (uint32_t)((it & 1) * N);
+                // slots of padded planes z, z+1, z+2 (taps dz = -1, 0, +1)
+                const uint32_t sz[3] = {aS + (uint32_t)(slot_of(z) * kSlot), aS + (uint32_t)(slot_of(z + 1) * kSlot),
+                                        aS + (uint32_t)(slot_of(z + 2) * kSlot)};
+#pragma unroll
+                for (int ch = 0; ch < CH; ++ch) {
+#pragma unroll
+                    for (int t = 0; t < 27; ++t) {
+                        const int dzi = t / 9, dyi = (t / 3) % 3, dxi = t % 3;
+                        const uint64_t ad = umma_desc(sz[dzi] + ch * 3 * kRowBytes + dyi * kRowBytes + dxi * 16,
+                                                      kKgBytes, 128);
+                        const uint64_t bd = umma_desc(bS + (ch * 27 + t) * N * 32, N * 16, 128);
+                        const uint32_t accum = (ch > 0 || t > 0) ? 1u : 0u;
+                        asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                                     ::"r"(acc), "l"(ad), "l"(bd), "r"(idesc), "r"(accum) : "memory");
                     }
                 }
-                __nv_bfloat162 h[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
-                uint4 *dst = reinterpret_cast<uint4 *>(y + o);
-                dst[0] = *reinterpret_cast<uint4 *>(&h[0]);
-                dst[1] = *reinterpret_cast<uint4 *>(&h[4]);
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                             ::"r"(smem_u32(&accf[it & 1])) : "memory");
             }
+            __syncwarp();
+            issued = it + 1;
         }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        return true;
-    };
-
-    bool ok = true;
-    int issued = 0;                                     // MMA groups committed
-    for (int it = 0; it < nz && ok; ++it) {
-        const int z = z0 + it;
-        if (it + S - 2 < nz + 2) load_plane(z + S - 2);
-        // groups committed: S - 2 + it + 1; all but the newest S - 4 done
-        // means padded planes <= z0 + it + 2 = z + 2 have landed
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        asm volatile("cp.async.wait_group %0;" ::"n"(S - 4) : "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t acc = tmem + (uint32_t)((it & 1) * N);
-            // slots of padded planes z, z+1, z+2 (taps dz = -1, 0, +1)
-            const uint32_t sz[3] = {aS + (uint32_t)((z % S) * kSlot),
-                                    aS + (uint32_t)(((z + 1) % S) * kSlot),
-                                    aS + (uint32_t)(((z + 2) % S) * kSlot)};
-#pragma unroll
-            for (int ch = 0; ch < CH; ++ch) {
-#pragma unroll
-                for (int t = 0; t < 27; ++t) {
-                    const int dzi = t / 9, dyi = (t / 3) % 3, dxi = t % 3;
-                    const uint64_t ad = umma_desc(sz[dzi] + ch * 3 * kRowBytes + dyi * kRowBytes + dxi * 16,
-                                                  kKgBytes, 128);
-                    const uint64_t bd = umma_desc(bS + (ch * 27 + t) * N * 32, N * 16, 128);
-                    const uint32_t accum = (ch > 0 || t > 0) ? 1u : 0u;
-                    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                                 " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-                                 ::"r"(acc), "l"(ad), "l"(bd), "r"(idesc), "r"(accum) : "memory");
-                }
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         ::"r"(smem_u32(&mbar[it & 1])) : "memory");
-        }
-        issued = it + 1;
-        if (it > 0) ok = epilogue(it - 1);
+        // The last committed MMAs complete before the accumulator columns are
+        // released, also when a worker's wait gave up (bounded wait).
+        if (issued > 0)
+            mbar_wait(smem_u32(&accf[(issued - 1) & 1]), (uint32_t)(((issued - 1) >> 1) & 1), nullptr);
+        (void)ok;
     }
-    if (ok && nz > 0) ok = epilogue(nz - 1);
-    if (!ok && issued > 0) {
-        // A wait gave up: give the last committed MMAs one more bounded wait
-        // before the accumulator columns are released.
-        mbar_wait(smem_u32(&mbar[(issued - 1) & 1]), (uint32_t)(((issued - 1) >> 1) & 1), nullptr);
-    }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
@@ -445,7 +504,7 @@ static cudaError_t launch_zm(const ConvDesc &cd, const __nv_bfloat16 *x, const _
     const long long interior = (long long)(cd.W + 2) * cd.H;
     const dim3 grid((unsigned)((interior + kConvM - 1) / kConvM), (unsigned)((cd.D + kZmPlanes - 1) / kZmPlanes));
     const int os = cd.out_stride > 0 ? cd.out_stride : cd.cout;
-    k_conv3d_zm<N, CIN, RELU><<<grid, 128, smem, st>>>(cd.W, cd.H, cd.D, kZmPlanes, os, cd.out_offset, x, w, bias,
+    k_conv3d_zm<N, CIN, RELU><<<grid, kZmThreads, smem, st>>>(cd.W, cd.H, cd.D, kZmPlanes, os, cd.out_offset, x, w, bias,
                                                        static_cast<__nv_bfloat16 *>(y), aux, err);
     return cudaGetLastError();
 }

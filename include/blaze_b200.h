@@ -442,15 +442,16 @@ typedef struct blz_batch blz_batch;
 int  blz_batch_create(blz_solver *const *solvers, int n, blz_batch **out);
 int  blz_batch_destroy(blz_batch *b);
 void *blz_batch_stream(blz_batch *b);                      /* the batch's cudaStream_t */
-/* Sweep kernel of the batched solve: -1 (default) autotunes between the
- * segment kernel (one sweep per pass over HBM) and temporal blocking (two
- * sweeps per pass, tiles of 8, 16 or 32 planes); 0 forces the segment
- * kernel; planes > 0 forces temporal blocking with tiles of that many planes
+/* Sweep kernel of the batched solve: planes = -1 (default) autotunes between
+ * the segment kernel (one sweep per pass over HBM) and temporal blocking (two
+ * sweeps per pass, tiles of 8, 16 or 32 planes, scalar or paired-FP32
+ * stencil); 0 forces the segment kernel; planes > 0 forces temporal blocking
+ * with tiles of that many planes, paired != 0 with the paired-FP32 stencil
  * (BLZ_ERR_ARG unless check_every % 4 == 0 and every grid has width % 8 == 0
  * and width <= 384).  Every choice gives the same bits.  The stats'
  * sweep_variant reports the choice: the segment kernel's planes per thread
- * (1, 2, 4, 8), or 100 + planes per tile for temporal blocking.            */
-int  blz_batch_set_sweep(blz_batch *b, int planes);
+ * (1, 2, 4, 8), or 100 (scalar) or 200 (paired) + planes per tile.         */
+int  blz_batch_set_sweep(blz_batch *b, int planes, int paired);
 int  blz_batch_add_source(blz_batch *b);                   /* blz_add_source of every solver */
 /* One frame of every solver: forces at times[i] (NULL: 0), divergence, the
  * batched solve, gradient, advection; stats[i] (may be NULL) gets solver i's

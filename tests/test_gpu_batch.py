@@ -154,7 +154,7 @@ def _tb_scenes():
             for i, d in enumerate(TB_DIMS)]
 
 
-def _run_frames(sims, frames, batch_planes=None):
+def _run_frames(sims, frames, batch_planes=None, paired=False):
     from blaze_b200.batch import Batch
     stats = []
     if batch_planes is None:
@@ -166,7 +166,7 @@ def _run_frames(sims, frames, batch_planes=None):
             stats.append(row)
         return stats
     batch = Batch(sims)
-    batch.set_sweep(batch_planes)
+    batch.set_sweep(batch_planes, paired)
     for f in range(frames):
         batch.add_source()
         stats.append(batch.step([f / 24.0] * len(sims)))
@@ -174,23 +174,25 @@ def _run_frames(sims, frames, batch_planes=None):
     return stats
 
 
-@pytest.mark.parametrize("planes", [-1, 0, 8, 16, 32])
-def test_batch_sweep_kernels_equal_single(planes):
+@pytest.mark.parametrize("planes,paired", [(-1, False), (0, False), (8, False), (16, False), (32, False),
+                                           (8, True), (32, True)])
+def test_batch_sweep_kernels_equal_single(planes, paired):
     """Every sweep kernel of the batch (autotuned, segment, temporal blocking
-    with 8, 16 or 32 planes per tile) gives each grid the sweeps, residuals
-    and fields of its own solve, bit for bit."""
+    with 8, 16 or 32 planes per tile, scalar or paired-FP32 stencil) gives
+    each grid the sweeps, residuals and fields of its own solve, bit for
+    bit."""
     frames = 3
     single = _make(_tb_scenes())
     sa = _run_frames(single, frames)
     batched = _make(_tb_scenes())
-    sb = _run_frames(batched, frames, planes)
+    sb = _run_frames(batched, frames, planes, paired)
     for f in range(frames):
         for i in range(len(single)):
             a, b = sa[f][i], sb[f][i]
             assert a["iterations"] > 0 and a["iterations"] == b["iterations"], (planes, f, i, a, b)
             assert a["residual"] == b["residual"] and a["converged"] == b["converged"], (planes, f, i)
             if planes > 0:
-                assert b["sweep_variant"] == 100 + planes
+                assert b["sweep_variant"] == (200 if paired else 100) + planes
             elif planes == 0:
                 assert b["sweep_variant"] in (1, 2, 4, 8)
     for i in range(len(single)):

@@ -314,12 +314,14 @@ def test_sweep_variants_identical_full_width_rows():
 
 
 @pytest.mark.parametrize("dims,bc", [((64, 200, 70), BLZ_BC_FREE_SURFACE), ((256, 40, 40), BLZ_BC_FREE_SURFACE),
-                                     ((384, 20, 12), BLZ_BC_REF_COMPAT), ((128, 48, 33), BLZ_BC_FREE_SURFACE)])
+                                     ((384, 20, 12), BLZ_BC_REF_COMPAT), ((128, 48, 33), BLZ_BC_FREE_SURFACE),
+                                     ((256, 512, 64), BLZ_BC_FREE_SURFACE)])
 def test_temporal_blocking_equals_plain_sweeps(dims, bc):
     """The two-sweeps-per-pass kernels (variants 6-10, 9 with TMA-staged rhs
     and input planes, 10 with the stencil on paired FP32 instructions:
-    several row bands and z chunks here) give the plain segment kernel's
-    bits."""
+    several row bands and z chunks here; 256 x 512 x 64 has 32 row bands and
+    chunks of 16 planes, so its steady steps run in long stretches) give the
+    plain segment kernel's bits."""
     out = {}
     for v in (0, 6, 7, 8, 9, 10):
         gpu, _ = pair(scene(dims=dims, bc_mode=bc, sweep_variant=v), 68)
