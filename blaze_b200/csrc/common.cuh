@@ -42,14 +42,16 @@ __device__ __forceinline__ float clamp_coord(float g, int n) {
 __device__ __forceinline__ float ldg(const float *p) { return __ldg(p); }
 
 // Clamped trilinear sample at an object-space position (src/Grid.h:94-108).
+// Offsets within a field are 32-bit: the solver refuses grids whose
+// (W + 1)(H + 1)(D + 1) reaches 2^31.
 __device__ __forceinline__ float trilinear(const FieldRef &f, float inv_dx, float px, float py, float pz) {
     const float gX = clamp_coord(px * inv_dx - f.ox, f.w);
     const float gY = clamp_coord(py * inv_dx - f.oy, f.h);
     const float gZ = clamp_coord(pz * inv_dx - f.oz, f.d);
     const int x0 = (int)gX, y0 = (int)gY, z0 = (int)gZ;
     const float fx = gX - (float)x0, fy = gY - (float)y0, fz = gZ - (float)z0;
-    const size_t sy = (size_t)f.w, sz = (size_t)f.w * f.h;
-    const float *p = f.a + lin(x0, y0, z0, f.w, f.h);
+    const int sy = f.w, sz = f.w * f.h;
+    const float *p = f.a + (x0 + sy * y0 + sz * z0);
     const float a000 = ldg(p), a100 = ldg(p + 1);
     const float a010 = ldg(p + sy), a110 = ldg(p + sy + 1);
     const float a001 = ldg(p + sz), a101 = ldg(p + sz + 1);
@@ -77,7 +79,7 @@ __device__ __forceinline__ float tricubic(const FieldRef &f, float inv_dx, float
     const int i1 = (int)gX, j1 = (int)gY, k1 = (int)gZ;
     const int i0 = max(i1 - 1, 0), i2 = i1 + 1, i3 = min(i1 + 2, f.w - 1);
     const float sx = gX - (float)i1, sy = gY - (float)j1, sz = gZ - (float)k1;
-    const size_t rs = (size_t)f.w, ps = (size_t)f.w * f.h;
+    const int rs = f.w, ps = f.w * f.h;             // 32-bit offsets, as in trilinear
     float zs[4];
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) {
@@ -86,7 +88,7 @@ __device__ __forceinline__ float tricubic(const FieldRef &f, float inv_dx, float
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
             const int jy = jj == 0 ? max(j1 - 1, 0) : jj == 3 ? min(j1 + 2, f.h - 1) : j1 + jj - 1;
-            const float *row = f.a + rs * (size_t)jy + ps * (size_t)kz;
+            const float *row = f.a + (rs * jy + ps * kz);
             float v = cerp(ldg(row + i0), ldg(row + i1), ldg(row + i2), ldg(row + i3), sx);
             ys[jj] = CLAMP ? fmaxf(v, 0.0f) : v;
         }

@@ -197,8 +197,8 @@ int blz_create(const blz_params *p, blz_solver **out) {
         return fail(nullptr, BLZ_ERR_ARG, "grid dims must be >= 4 (got %d x %d x %d)", p->width, p->height, p->depth);
     if (p->width & 1)
         return fail(nullptr, BLZ_ERR_ARG, "width must be even for the colour-packed solve (got %d)", p->width);
-    if ((long long)p->width * p->height * p->depth > (1LL << 31))
-        return fail(nullptr, BLZ_ERR_ARG, "grid too large for 32-bit packed indexing");
+    if ((long long)(p->width + 1) * (p->height + 1) * (p->depth + 1) >= (1LL << 31))
+        return fail(nullptr, BLZ_ERR_ARG, "grid too large for 32-bit field offsets");
     if (!(p->dx > 0.0f) || !(p->dt > 0.0f) || !(p->density > 0.0f))
         return fail(nullptr, BLZ_ERR_ARG, "dx, dt and density must be positive");
     if (p->max_iter < 0 || p->max_particles < 0)

@@ -102,6 +102,15 @@ __device__ __forceinline__ float warp_sum_f(float v) {
     return v;
 }
 
+// x, y, z of index v of a W x H x D box in 32-bit arithmetic (every index
+// here is below 2^32: blz_unet_create caps the grid at 2^28 cells).
+__device__ __forceinline__ void split3(long long v, int W, int H, int &x, int &y, int &z) {
+    const unsigned u = (unsigned)v, q = u / (unsigned)W, zq = q / (unsigned)H;
+    x = (int)(u - q * (unsigned)W);
+    y = (int)(q - zq * (unsigned)H);
+    z = (int)zq;
+}
+
 constexpr int kNormThreads = 256;
 constexpr int kNormBlocks = 1024;
 
@@ -111,9 +120,8 @@ k_unet_norms(GridInfo g, CellArr rhs, CellArr p, double *partials) {
     const long long n = (long long)g.W * g.H * g.D;
     double sb = 0.0, sp = 0.0, sr = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % g.W);
-        const long long jk = t / g.W;
-        const int j = (int)(jk % g.H), k = (int)(jk / g.H);
+        int i, j, k;
+        split3(t, g.W, g.H, i, j, k);
         float b, pc, r;
         cell_brp(g, rhs, p, i, j, k, b, pc, r);
         sb += (double)b * b;
@@ -173,7 +181,8 @@ __global__ void k_unet_input(GridInfo g, CellArr rhs, CellArr p, int ox, int oy,
     const long long n = Wp * Hp * (d.D + 2);
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int xp = (int)(t % Wp), yp = (int)((t / Wp) % Hp), zp = (int)(t / (Wp * Hp));
+    int xp, yp, zp;
+    split3(t, (int)Wp, (int)Hp, xp, yp, zp);
     const int i = ox + xp - 1, j = oy + yp - 1, k = oz + zp - 1;
     float v[kInCh];
 #pragma unroll
@@ -230,9 +239,10 @@ __global__ void k_pool2(const bf16 *__restrict__ x, int xs, int xoff, LDims df, 
     const long long n = (long long)dc.W * dc.H * dc.D * g8;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int c = (int)(t % g8) * 8;
-    const long long v = t / g8;
-    const int cx = (int)(v % dc.W), cy = (int)((v / dc.W) % dc.H), cz = (int)(v / ((long long)dc.W * dc.H));
+    const int c = (int)((unsigned)t % (unsigned)g8) * 8;
+    const long long v = (unsigned)t / (unsigned)g8;
+    int cx, cy, cz;
+    split3(v, dc.W, dc.H, cx, cy, cz);
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -256,9 +266,10 @@ __global__ void k_skip_grad(const bf16 *__restrict__ dcat, const bf16 *__restric
     const long long n = (long long)df.W * df.H * df.D * g8;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int c = (int)(t % g8) * 8;
-    const long long v = t / g8;
-    const int x = (int)(v % df.W), y = (int)((v / df.W) % df.H), z = (int)(v / ((long long)df.W * df.H));
+    const int c = (int)((unsigned)t % (unsigned)g8) * 8;
+    const long long v = (unsigned)t / (unsigned)g8;
+    int x, y, z;
+    split3(v, df.W, df.H, x, y, z);
     const long long f = pvox(df, x, y, z);
     float a[8], s[8], p[8], o[8];
     unpack8(ld8(dcat + f * 2 * C + C + c), a);
@@ -287,7 +298,8 @@ k_upconv_t(const bf16 *__restrict__ x, LDims dc, const float *__restrict__ w, co
     const long long n = (long long)dc.W * dc.H * dc.D;
     const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (v >= n) return;
-    const int cx = (int)(v % dc.W), cy = (int)((v / dc.W) % dc.H), cz = (int)(v / ((long long)dc.W * dc.H));
+    int cx, cy, cz;
+    split3(v, dc.W, dc.H, cx, cy, cz);
     const LDims df{dc.W * 2, dc.H * 2, dc.D * 2};
     float acc[COUT];
 #pragma unroll
@@ -325,7 +337,8 @@ k_upconv(const bf16 *__restrict__ x, LDims dc, int cin, int cout, const float *_
     const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (v >= n) return;
     const int par = blockIdx.y, co0 = blockIdx.z * 8;
-    const int cx = (int)(v % dc.W), cy = (int)((v / dc.W) % dc.H), cz = (int)(v / ((long long)dc.W * dc.H));
+    int cx, cy, cz;
+    split3(v, dc.W, dc.H, cx, cy, cz);
     const LDims df{dc.W * 2, dc.H * 2, dc.D * 2};
     float acc[8];
 #pragma unroll
@@ -359,7 +372,8 @@ k_upconv_bwd(const bf16 *__restrict__ g, int gs, LDims dc, int cin, int cout, co
     const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (v >= n) return;
     const int ci0 = blockIdx.y * 8;
-    const int cx = (int)(v % dc.W), cy = (int)((v / dc.W) % dc.H), cz = (int)(v / ((long long)dc.W * dc.H));
+    int cx, cy, cz;
+    split3(v, dc.W, dc.H, cx, cy, cz);
     const LDims df{dc.W * 2, dc.H * 2, dc.D * 2};
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int par = 0; par < 8; ++par) {
@@ -444,8 +458,8 @@ __global__ void __launch_bounds__(256) k_wgrad(WgArgs a) {
             const long long n = nb + vv;
             float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             if (n < n1) {
-                const int x = (int)(n % a.d.W), y = (int)((n / a.d.W) % a.d.H);
-                const int z = (int)(n / ((long long)a.d.W * a.d.H));
+                int x, y, z;
+                split3(n, a.d.W, a.d.H, x, y, z);
                 const long long P = pvox(a.d, x, y, z);
                 if (isA) {
                     const long long Pa = MODE == kModeConv ? P : pvox(df, 2 * x + px, 2 * y + py, 2 * z + pz);
@@ -502,7 +516,8 @@ __global__ void k_unet_delta(const bf16 *__restrict__ d0b, LDims d, const float 
     const long long n = (long long)d.W * d.H * d.D;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int i = (int)(t % d.W), j = (int)((t / d.W) % d.H), k = (int)(t / ((long long)d.W * d.H));
+    int i, j, k;
+    split3(t, d.W, d.H, i, j, k);
     float f[16];
     (((i + j + k) & 1) ? db : dr)[pidx(i, j, k, d.W >> 1, d.H)] = __ldg(scales + 3) * head_out(d0b, pvox(d, i, j, k), head, f);
 }
@@ -515,9 +530,8 @@ k_unet_project(GridInfo g, CellArr rhs, CellArr p, CellArr dl, double *partials)
     const GridInfo g0{g.W, g.H, g.D, g.open, g.dirichlet, 0.0f};
     double rq = 0.0, qq = 0.0, dr = 0.0, dq = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % g.W);
-        const long long jk = t / g.W;
-        const int j = (int)(jk % g.H), k = (int)(jk / g.H);
+        int i, j, k;
+        split3(t, g.W, g.H, i, j, k);
         float b, pc, r, zb, dc, mq;
         cell_brp(g, rhs, p, i, j, k, b, pc, r);
         cell_brp(g0, rhs, dl, i, j, k, zb, dc, mq);      // with b = 0: mq = -(A d)
@@ -585,7 +599,8 @@ __global__ void k_unet_out(const bf16 *__restrict__ d0b, LDims d, const float *_
     const long long n = (long long)d.W * d.H * d.D;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int i = (int)(t % d.W), j = (int)((t / d.W) % d.H), k = (int)(t / ((long long)d.W * d.H));
+    int i, j, k;
+    split3(t, d.W, d.H, i, j, k);
     float f[16];
     out[t] = head_out(d0b, pvox(d, i, j, k), head, f);
 }
@@ -605,7 +620,8 @@ k_unet_loss(const bf16 *__restrict__ d0b, LDims d, int ox, int oy, int oz, GridI
     for (int c = 0; c < 17; ++c) gw[c] = 0.0f;
     double l2 = 0.0, t2 = 0.0;
     if (t < n) {
-        const int x = (int)(t % d.W), y = (int)((t / d.W) % d.H), z = (int)(t / ((long long)d.W * d.H));
+        int x, y, z;
+        split3(t, d.W, d.H, x, y, z);
         const long long P = pvox(d, x, y, z);
         float f[16];
         const float o = head_out(d0b, P, head, f);
@@ -1120,6 +1136,8 @@ int blz_unet_create(int width, int height, int depth, blz_unet **out) {
     if (width < 8 || height < 8 || depth < 8 || width % 8 || height % 8 || depth % 8)
         return ufail(BLZ_ERR_ARG, "network dims must be positive multiples of 8 (got %d x %d x %d)", width, height,
                      depth);
+    if ((long long)width * height * depth > (1LL << 28))
+        return ufail(BLZ_ERR_ARG, "network grid above 2^28 cells (%d x %d x %d)", width, height, depth);
     blz_unet *u = new blz_unet();
     for (int l = 0; l < 4; ++l) u->L[l] = {width >> l, height >> l, depth >> l};
     cudaGetDevice(&u->device);

@@ -142,12 +142,16 @@ k_conv3d_tc(int W, int H, int D, int cin, int out_stride, int out_offset, const 
         __syncthreads();
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll 1
+            // a tap's operands: the block's descriptors plus constant offsets
+            // in the 16-byte address field (addresses below 2^18 bytes, so
+            // the field never carries)
+            const uint64_t a_desc0 = umma_desc(aS, kKgBytes, 128), b_desc0 = umma_desc(bS, N * 16, 128);
+#pragma unroll
             for (int t = 0; t < 27; ++t) {
                 const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
                 const int r = (dz + 1) * 3 + (dy + 1);
-                const uint64_t ad = umma_desc(aS + r * kRowBytes + (dx + 1) * 16, kKgBytes, 128);
-                const uint64_t bd = umma_desc(bS + t * N * 32, N * 16, 128);
+                const uint64_t ad = a_desc0 + (uint64_t)((r * kRowBytes + (dx + 1) * 16) >> 4);
+                const uint64_t bd = b_desc0 + (uint64_t)((t * N * 32) >> 4);
                 const uint32_t acc = (c > 0 || t > 0) ? 1u : 0u;
                 asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
@@ -441,6 +445,11 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
         asm volatile("cp.async.wait_group 0;" ::: "memory");
     } else {
         // ---- MMA warp: lane 0 issues each plane's 27 x cin/16 MMAs ----
+        // Operand descriptors at the start of the plane ring and of the
+        // weights.  Every operand address stays below 2^18 bytes, so adding an
+        // offset's 16-byte units to the 14-bit address field never carries.
+        const uint64_t a_desc0 = umma_desc(aS, kKgBytes, 128);
+        const uint64_t b_desc0 = umma_desc(bS, N * 16, 128);
         int issued = 0;
         bool ok = true;
 #pragma unroll 1
@@ -458,17 +467,19 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (lane == 0) {
                 const uint32_t acc = tmem + (uint32_t)((it & 1) * N);
-                // slots of padded planes z, z+1, z+2 (taps dz = -1, 0, +1)
-                const uint32_t sz[3] = {aS + (uint32_t)(slot_of(z) * kSlot), aS + (uint32_t)(slot_of(z + 1) * kSlot),
-                                        aS + (uint32_t)(slot_of(z + 2) * kSlot)};
+                // descriptors of the slots of padded planes z, z+1, z+2 (taps
+                // dz = -1, 0, +1); a tap's operand is its slot's descriptor
+                // plus a constant offset in the 16-byte address field
+                const uint64_t sz[3] = {a_desc0 + (uint64_t)((slot_of(z) * kSlot) >> 4),
+                                        a_desc0 + (uint64_t)((slot_of(z + 1) * kSlot) >> 4),
+                                        a_desc0 + (uint64_t)((slot_of(z + 2) * kSlot) >> 4)};
 #pragma unroll
                 for (int ch = 0; ch < CH; ++ch) {
 #pragma unroll
                     for (int t = 0; t < 27; ++t) {
                         const int dzi = t / 9, dyi = (t / 3) % 3, dxi = t % 3;
-                        const uint64_t ad = umma_desc(sz[dzi] + ch * 3 * kRowBytes + dyi * kRowBytes + dxi * 16,
-                                                      kKgBytes, 128);
-                        const uint64_t bd = umma_desc(bS + (ch * 27 + t) * N * 32, N * 16, 128);
+                        const uint64_t ad = sz[dzi] + (uint64_t)((ch * 3 * kRowBytes + dyi * kRowBytes + dxi * 16) >> 4);
+                        const uint64_t bd = b_desc0 + (uint64_t)(((ch * 27 + t) * N * 32) >> 4);
                         const uint32_t accum = (ch > 0 || t > 0) ? 1u : 0u;
                         asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                                      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
