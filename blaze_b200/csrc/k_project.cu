@@ -766,11 +766,7 @@ static size_t tb_smem_tma(const Geom &g, int TY) {
     return 128 + (size_t)kTbDenseSlots * tb_dense_slot_bytes(Wq, ra) + sizeof(float4) * 8 * (size_t)ra * (Wq + 1);
 }
 
-typedef CUresult (*TensorMapEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                      const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static TensorMapEncodeFn tensor_map_encoder() {
+TensorMapEncodeFn tensor_map_encoder() {
     static TensorMapEncodeFn fn = nullptr;
     static bool tried = false;
     if (!tried) {

@@ -1,5 +1,6 @@
 // kernels.cuh — host-side launchers of the fluid-step kernels.
 #pragma once
+#include <cuda.h>   // CUtensorMap and its enums (the encoder comes from cudaGetDriverEntryPoint)
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -60,6 +61,13 @@ void launch_turb_noise(const Geom &g, const float *T, const float *U, const floa
                        cudaStream_t st);
 void launch_turb_apply(const Geom &g, float *U, float *V, float *W, const float *nU,
                        const float *nV, const float *nW, const ForceParams &fp, cudaStream_t st);
+
+// cuTensorMapEncodeTiled, looked up once through the runtime's driver entry
+// point (nullptr when the driver has none).
+typedef CUresult (*TensorMapEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                      const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+TensorMapEncodeFn tensor_map_encoder();
 
 // -- projection ---------------------------------------------------------------
 void launch_divergence(const Geom &g, const float *U, const float *V, const float *W,

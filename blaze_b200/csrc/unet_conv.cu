@@ -259,19 +259,28 @@ constexpr int kZmThreads = kZmWorkers + 32;               // + the MMA warp
 constexpr int kZmSmemOne = 227 * 1024 - 1024;            // dynamic bytes, one CTA per SM
 constexpr int kZmSmemTwo = 228 * 1024 / 2 - 1024 - 128;  // dynamic bytes, two CTAs per SM
 
-template <int CIN> __host__ __device__ constexpr int zm_slot_bytes() { return (CIN / 16) * 3 * kRowBytes; }
+// A slot holds the rows dy = -1, 0, 1 of one padded plane, each row block
+// [ch][kg][v][8 channels] (CIN/16 chunks of two 8-channel halves of 130
+// voxels) as one TMA box, the blocks 128-byte aligned.
+template <int CIN> __host__ __device__ constexpr int zm_dy_bytes() { return ((CIN / 16) * kRowBytes + 127) & ~127; }
+template <int CIN> __host__ __device__ constexpr int zm_slot_bytes() { return 3 * zm_dy_bytes<CIN>(); }
 template <int N, int CIN> __host__ __device__ constexpr int zm_w_bytes() { return 27 * (CIN / 16) * N * 32; }
+// dynamic shared memory besides the slots: the weights and 128 bytes of
+// alignment slack
+template <int N, int CIN> __host__ __device__ constexpr int zm_fixed_bytes() { return zm_w_bytes<N, CIN>() + 128; }
 template <int N, int CIN> __host__ __device__ constexpr int zm_slots() {
-    return (kZmSmemTwo - zm_w_bytes<N, CIN>()) / zm_slot_bytes<CIN>() >= 6
-               ? ((kZmSmemTwo - zm_w_bytes<N, CIN>()) / zm_slot_bytes<CIN>() > 8
-                      ? 8 : (kZmSmemTwo - zm_w_bytes<N, CIN>()) / zm_slot_bytes<CIN>())
-               : ((kZmSmemOne - zm_w_bytes<N, CIN>()) / zm_slot_bytes<CIN>() > 8
-                      ? 8 : (kZmSmemOne - zm_w_bytes<N, CIN>()) / zm_slot_bytes<CIN>());
+    return (kZmSmemTwo - zm_fixed_bytes<N, CIN>()) / zm_slot_bytes<CIN>() >= 6
+               ? ((kZmSmemTwo - zm_fixed_bytes<N, CIN>()) / zm_slot_bytes<CIN>() > 8
+                      ? 8 : (kZmSmemTwo - zm_fixed_bytes<N, CIN>()) / zm_slot_bytes<CIN>())
+               : ((kZmSmemOne - zm_fixed_bytes<N, CIN>()) / zm_slot_bytes<CIN>() > 8
+                      ? 8 : (kZmSmemOne - zm_fixed_bytes<N, CIN>()) / zm_slot_bytes<CIN>());
 }
 template <int N, int CIN> __host__ __device__ constexpr int zm_smem_bytes() {
-    return zm_w_bytes<N, CIN>() + zm_slots<N, CIN>() * zm_slot_bytes<CIN>();
+    return zm_fixed_bytes<N, CIN>() + zm_slots<N, CIN>() * zm_slot_bytes<CIN>();
 }
-static_assert(zm_slots<16, 16>() == 8 && zm_slots<32, 16>() == 7 && zm_slots<16, 32>() == 8 &&
+static_assert(zm_w_bytes<16, 16>() % 128 == 0 && zm_w_bytes<32, 32>() % 128 == 0 && zm_dy_bytes<16>() == 4224 &&
+                  zm_dy_bytes<32>() == 8320, "128-byte aligned slots");
+static_assert(zm_slots<16, 16>() == 8 && zm_slots<32, 16>() == 6 && zm_slots<16, 32>() == 8 &&
                   zm_slots<32, 32>() == 7, "ring slots of the z-marching convolution");
 static_assert(zm_smem_bytes<16, 16>() <= kZmSmemTwo && zm_smem_bytes<32, 16>() <= kZmSmemTwo &&
                   zm_smem_bytes<16, 32>() <= kZmSmemOne && zm_smem_bytes<32, 32>() <= kZmSmemOne,
@@ -279,20 +288,20 @@ static_assert(zm_smem_bytes<16, 16>() <= kZmSmemTwo && zm_smem_bytes<32, 16>() <
 
 template <int N, int CIN, bool RELU>
 __global__ void __launch_bounds__(kZmThreads, 1)
-k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const __nv_bfloat16 *__restrict__ x,
+k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const __grid_constant__ CUtensorMap xmap,
             const __nv_bfloat16 *__restrict__ w, const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y,
             const __nv_bfloat16 *__restrict__ aux, int *err) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int CH = CIN / 16;
     constexpr int S = zm_slots<N, CIN>();
     constexpr int kSlot = zm_slot_bytes<CIN>();
+    constexpr int kDy = zm_dy_bytes<CIN>();
+    constexpr uint32_t kSlotTx = 3u * CH * kRowBytes;       // bytes the three row boxes of a plane bring
     constexpr int kCols = 2 * N < 32 ? 32 : 2 * N;
     constexpr uint32_t idesc = umma_idesc_bf16(kConvM, N);
-    unsigned char *sB = smem;
-    unsigned char *sA = smem + zm_w_bytes<N, CIN>();
-    // full[s]: the plane in ring slot s has landed (one arrival per worker
-    // thread); accf[b]: the MMAs into accumulator buffer b completed (their
-    // commit); acce[b]: buffer b has been read out (one arrival per worker).
+    // full[s]: the plane in ring slot s has landed (the TMA copies' bytes);
+    // accf[b]: the MMAs into accumulator buffer b completed (their commit);
+    // acce[b]: buffer b has been read out (one arrival per worker).
     __shared__ __align__(8) uint64_t full[S], accf[2], acce[2];
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -310,7 +319,7 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
     }
     if (tid == 0) {
         for (int s = 0; s < S; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(kZmWorkers) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[s])) : "memory");
         for (int b = 0; b < 2; ++b) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&accf[b])) : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acce[b])), "r"(kZmWorkers) : "memory");
@@ -321,39 +330,47 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base;
-    const uint32_t aS = smem_u32(sA), bS = smem_u32(sB);
+    const uint32_t bS = (smem_u32(smem) + 127u) & ~127u;       // weights, then the ring, 128-byte aligned
+    const uint32_t aS = bS + (uint32_t)zm_w_bytes<N, CIN>();
     // Ring slot of padded plane pz: (pz - z0) % S, so the n-th fill of a slot
     // is the plane z0 + s + n S and completes phase n of full[s].
     auto slot_of = [&](int pz) { return (pz - z0) % S; };
     auto fill_parity = [&](int pz) { return (uint32_t)(((pz - z0) / S) & 1); };
-
+    // Weights of every 16-channel chunk: block (ch, tap) = N rows x 32 B,
+    // K-major (cp.async by the workers, fenced to the async proxy before the
+    // barrier that starts the pipeline).
     if (worker) {
-        // ---- workers: stage planes, drain the accumulators ----
-        // Weights of every 16-channel chunk: block (ch, tap) = N rows x 32 B,
-        // K-major; they join the first plane's commit group.
         for (int e = tid; e < 27 * CH * N * 2; e += kZmWorkers) {
             const int kg = e & 1, n = (e >> 1) % N, ct = (e >> 1) / N;      // ct = ch * 27 + tap
             const int ch = ct / 27, t = ct % 27;
             cp_async16(bS + ct * N * 32 + kg * N * 16 + n * 16, w + ((size_t)t * N + n) * CIN + ch * 16 + kg * 8);
         }
-        // Rows dy = -1, 0, 1 of padded plane pz (130 voxels each, the tile's
-        // row segment and one voxel either side): row (ch, dy) of the slot
-        // holds 16-byte chunks (kg, v) at kg * kKgBytes + v * 16, read from
-        // voxel v of that row, channels ch * 16 + kg * 8.
-        auto load_plane = [&](int pz) {
-            const uint32_t dst = aS + (uint32_t)(slot_of(pz) * kSlot);
-            const __nv_bfloat16 *src = x + ((long long)pz * plane + P0 - 1 - Wp) * CIN;
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    // Padded plane pz by TMA: rows dy = -1, 0, 1 of the tile (130 voxels
+    // each: its 128 and one either side, flattened in-plane index P0 - 1 +
+    // (dy - 1) Wp on), one box per row of 8 channels x 130 voxels x 2
+    // halves x 1 plane x CIN/16 chunks, landing as [ch][kg][v][8] at
+    // dy * kDy in the slot; voxels outside the plane read as zeros.
+    auto tma_plane = [&](int pz) {
+        const uint32_t bar = smem_u32(&full[slot_of(pz)]);
+        const uint32_t dst = aS + (uint32_t)(slot_of(pz) * kSlot);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kSlotTx) : "memory");
 #pragma unroll
-            for (int row = 0; row < CH * 3; ++row) {
-                const int ch = row / 3, dy = row % 3;
-                const __nv_bfloat16 *rs = src + (long long)dy * Wp * CIN + ch * 16;
-                const uint32_t rd = dst + (uint32_t)(row * kRowBytes);
-                for (int e = tid; e < 2 * kRowVox; e += kZmWorkers) {
-                    const int kg = e & 1, v = e >> 1;
-                    cp_async16(rd + kg * kKgBytes + v * 16, rs + (long long)v * CIN + kg * 8);
-                }
-            }
-        };
+        for (int dy = 0; dy < 3; ++dy)
+            asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                         " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+                         ::"r"(dst + (uint32_t)(dy * kDy)), "l"(reinterpret_cast<uint64_t>(&xmap)), "r"(0),
+                           "r"((int)(P0 - 1) + (dy - 1) * Wp), "r"(0), "r"(pz), "r"(0), "r"(bar)
+                         : "memory");
+    };
+    int last_plane = z0 - 1;                             // last plane thread 0 asked for
+
+    if (worker) {
+        // ---- workers: thread 0 issues the plane copies; all drain the
+        // accumulators ----
         // This thread's voxel of the tile (TMEM lane 32 * warp + lane) and
         // the bias, the same on every plane.
         const long long Pv = P0 + 32 * warp + lane;
@@ -411,38 +428,33 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acce[it & 1])) : "memory");
             return true;
         };
-        auto arrive_full = [&](int pz) {
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[slot_of(pz)])) : "memory");
-        };
-        // Prologue: padded planes z0 .. z0+S-3, one commit group each, so
-        // commit group q holds padded plane z0 + q.
-#pragma unroll 1
-        for (int p = 0; p < S - 2; ++p) {
-            if (p < nz + 2) load_plane(z0 + p);
-            asm volatile("cp.async.commit_group;" ::: "memory");
-        }
+        // Prologue: padded planes z0 .. z0+S-3 (those the tile needs).
+        if (tid == 0)
+            for (int p = 0; p < S - 2 && p < nz + 2; ++p) {
+                tma_plane(z0 + p);
+                last_plane = z0 + p;
+            }
         bool ok = true;
 #pragma unroll 1
         for (int it = 0; it < nz && ok; ++it) {
             const int z = z0 + it;
             // plane z+S-2 goes into the slot of plane z-2, whose last reader
-            // (the MMAs of iteration it-2) completed before epilogue(it-2)
-            if (it + S - 2 < nz + 2) load_plane(z + S - 2);
-            // groups committed: S - 2 + it + 1; all but the newest S - 4
-            // done means this thread's copies of planes <= z + 2 landed
-            asm volatile("cp.async.commit_group;" ::: "memory");
-            asm volatile("cp.async.wait_group %0;" ::"n"(S - 4) : "memory");
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (it == 0) {
-                arrive_full(z);
-                arrive_full(z + 1);
+            // (the MMAs of iteration it-2) completed before this thread's
+            // epilogue(it-2) returned
+            if (tid == 0 && it + S - 2 < nz + 2) {
+                tma_plane(z + S - 2);
+                last_plane = z + S - 2;
             }
-            arrive_full(z + 2);
             if (it > 0) ok = epilogue(it - 1);
         }
         if (ok && nz > 0) ok = epilogue(nz - 1);
         if (!ok && err) atomicExch(err, 1);
-        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        // No copy may land after the CTA ends: thread 0 waits (bounded) for
+        // the latest fill of every slot it issued (done already unless a
+        // wait gave up).
+        if (tid == 0)
+            for (int p = last_plane; p >= z0 && p > last_plane - S; --p)
+                mbar_wait(smem_u32(&full[slot_of(p)]), fill_parity(p), nullptr);
     } else {
         // ---- MMA warp: lane 0 issues each plane's 27 x cin/16 MMAs ----
         // Operand descriptors at the start of the plane ring and of the
@@ -478,7 +490,7 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
 #pragma unroll
                     for (int t = 0; t < 27; ++t) {
                         const int dzi = t / 9, dyi = (t / 3) % 3, dxi = t % 3;
-                        const uint64_t ad = sz[dzi] + (uint64_t)((ch * 3 * kRowBytes + dyi * kRowBytes + dxi * 16) >> 4);
+                        const uint64_t ad = sz[dzi] + (uint64_t)((dyi * kDy + ch * kRowBytes + dxi * 16) >> 4);
                         const uint64_t bd = b_desc0 + (uint64_t)(((ch * 27 + t) * N * 32) >> 4);
                         const uint32_t accum = (ch > 0 || t > 0) ? 1u : 0u;
                         asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
@@ -506,16 +518,38 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
 
 constexpr int kZmPlanes = 16;
 
+// Tensor map of a padded channels-last activation x (CIN channels, W+2 x
+// H+2 x D+2 voxels from x) for the z-marching convolution's row boxes:
+// dims (8 channels, in-plane voxel, 8-channel half, plane, 16-channel chunk)
+// with byte strides (2 CIN, 16, plane, 32), box (8, 130, 2, 1, CIN/16).  The
+// innermost coordinate of every copy is 0, so every copy starts 16-byte
+// aligned.
+static bool zm_tensor_map(CUtensorMap *m, const __nv_bfloat16 *x, const ConvDesc &cd) {
+    TensorMapEncodeFn enc = tensor_map_encoder();
+    if (!enc || (reinterpret_cast<uintptr_t>(x) & 15) != 0) return false;
+    const cuuint64_t Wp = (cuuint64_t)cd.W + 2, Hp = (cuuint64_t)cd.H + 2, Dp = (cuuint64_t)cd.D + 2;
+    const cuuint64_t C = (cuuint64_t)cd.cin;
+    const cuuint64_t dims[5] = {8, Wp * Hp, 2, Dp, C / 16};
+    const cuuint64_t strides[4] = {C * 2, 16, Wp * Hp * C * 2, 32};
+    const cuuint32_t box[5] = {8, (cuuint32_t)kRowVox, 2, 1, (cuuint32_t)(C / 16)};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16 *>(x), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int N, int CIN, bool RELU>
 static cudaError_t launch_zm(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
                              void *y, const __nv_bfloat16 *aux, int *err, cudaStream_t st) {
     constexpr int smem = zm_smem_bytes<N, CIN>();
     cudaError_t e = cudaFuncSetAttribute(k_conv3d_zm<N, CIN, RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
+    CUtensorMap xm;
+    if (!zm_tensor_map(&xm, x, cd)) return cudaErrorNotSupported;
     const long long interior = (long long)(cd.W + 2) * cd.H;
     const dim3 grid((unsigned)((interior + kConvM - 1) / kConvM), (unsigned)((cd.D + kZmPlanes - 1) / kZmPlanes));
     const int os = cd.out_stride > 0 ? cd.out_stride : cd.cout;
-    k_conv3d_zm<N, CIN, RELU><<<grid, kZmThreads, smem, st>>>(cd.W, cd.H, cd.D, kZmPlanes, os, cd.out_offset, x, w, bias,
+    k_conv3d_zm<N, CIN, RELU><<<grid, kZmThreads, smem, st>>>(cd.W, cd.H, cd.D, kZmPlanes, os, cd.out_offset, xm, w, bias,
                                                        static_cast<__nv_bfloat16 *>(y), aux, err);
     return cudaGetLastError();
 }

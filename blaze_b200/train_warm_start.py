@@ -26,6 +26,11 @@
    trajectory and a learned one (each frame warm-started by the network,
    then RBGS to the same residual, continuing from its own solutions);
    reports sweeps and solve time per frame.
+
+Evaluation alone, of given weights (no training, nothing saved):
+
+    python -m blaze_b200.train_warm_start --eval-only --init blaze_b200/weights/plume256.npz \
+        --eval-seeds 902-905 --eval-frames 50 --report eval.json
 """
 import argparse
 import json
@@ -225,9 +230,15 @@ def main(argv=None):
     ap.add_argument("--keep-kappa", action="store_true", help="keep the --init weights' kappa")
     ap.add_argument("--init", default=None, help="start from these weights (npz)")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--out", required=True)
+    ap.add_argument("--out", default=None, help="where the trained weights go (required unless --eval-only)")
+    ap.add_argument("--eval-only", action="store_true",
+                    help="evaluate the --init weights on --eval-seeds for --eval-frames frames; no training")
     ap.add_argument("--report", default=None, help="JSON summary path")
     args = ap.parse_args(argv)
+    if args.eval_only and not args.init:
+        ap.error("--eval-only needs --init")
+    if not args.eval_only and not args.out:
+        ap.error("--out is required")
 
     import torch
     from .unet import WarmStartUNet, init_params
@@ -251,6 +262,24 @@ def main(argv=None):
     rounds = []
     plain_seeds = _seed_list(args.plain_seeds)
     policy_seeds = _seed_list(args.policy_seeds)
+    if args.eval_only:
+        rows = evaluate(full, n, _seed_list(args.eval_seeds), args.eval_frames, args.warmup, args.tol,
+                        args.max_iter, args.check_every, log)
+        sweep_ratio, time_ratio, conv = _ratios(rows)
+        per_seed = {}
+        for seed in _seed_list(args.eval_seeds):
+            sub = [r for r in rows if r["seed"] == seed]
+            per_seed[str(seed)] = dict(zip(("sweep_ratio", "time_ratio", "all_converged"), _ratios(sub)))
+        summary = {"grid": n, "weights": args.init, "kappa": kappa, "eval_seeds": args.eval_seeds,
+                   "eval_frames": args.eval_frames, "warmup": args.warmup, "tol": args.tol, "max_iter": args.max_iter,
+                   "steps_per_arm": len(rows) // 2, "sweep_ratio": sweep_ratio, "time_ratio": time_ratio,
+                   "eval_all_converged": conv, "per_seed": per_seed, "eval": rows}
+        full.close()
+        log(json.dumps({k: v for k, v in summary.items() if k != "eval"}))
+        if args.report:
+            with open(args.report, "w") as f:
+                json.dump(summary, f, indent=1)
+        return
     if args.harvest:
         # one round that trains on every harvested group
         groups = []
