@@ -232,30 +232,32 @@ int conv3d_smem_bytes(int cout) { return kABytes + 27 * cout * 32; }
 // half-resolution layers, which carry most of the network's voxels).  A CTA
 // keeps the layer's weights resident in shared memory and walks one 128-voxel
 // tile through `zs` consecutive planes.  Output plane z needs input planes
-// z-1, z, z+1 (padded planes z, z+1, z+2), 3 rows each; a ring of S plane
-// slots is filled by cp.async S - 4 planes ahead, so each plane's rows are
-// staged once per tile instead of three times and their latency is hidden
-// behind S - 4 iterations, and the TMEM accumulator is double buffered.  The
-// CTA is warp specialised and its warps hand over through mbarriers only:
-//   workers (warps 0-3), iteration z: issue the loads of padded plane z+S-2
-//   (into the slot of plane z-2, whose last reader, plane z-2's MMAs,
-//   completed before they read that plane out) | wait for their own copies
-//   of planes <= z+2, fence them to the async proxy and arrive on full[] of
-//   plane z+2 | wait for plane z-1's MMAs (accf), read its accumulator from
-//   TMEM, add bias / ReLU, store, arrive on acce (buffer free);
+// z-1, z, z+1 (padded planes z, z+1, z+2), 3 rows each.  They arrive by TMA
+// (one tensor-map box per row, completing on the slot's mbarrier by
+// transaction count) in a ring of S plane slots, S - 2 planes ahead, so each
+// plane's rows are staged once per tile and their latency is hidden behind
+// several planes; the TMEM accumulator has kZmAcc buffers.  The CTA is warp
+// specialised and its warps hand over through mbarriers only:
+//   workers (warps 0-3), iteration z: thread 0 issues the copies of padded
+//   plane z+S-2 (into the slot of plane z-2, whose last reader, plane z-2's
+//   MMAs, completed before the workers read that plane out) | all wait for
+//   plane z-1's MMAs (accf), read its accumulator from TMEM, add bias /
+//   ReLU, store, arrive on acce (buffer free);
 //   MMA warp (warp 4), iteration z: wait full[] of plane z+2 and acce of
-//   buffer z&1 (read out by iteration z-2) | lane 0 issues 27 x cin/16 MMAs
-//   into buffer z&1 and commits to accf[z&1].
-// So the MMAs of plane z run while the workers drain plane z-1 and stage
-// plane z+S-2.  Every wait is bounded in time; a wait that gives up sets
-// the error flag and ends that warp's loop, which ends the others' at their
-// next (bounded) wait.
+//   buffer z % kZmAcc (read out by iteration z-kZmAcc) | lane 0 issues
+//   27 x cin/16 MMAs into that buffer and commits to its accf.
+// So the MMA warp runs up to kZmAcc - 1 planes ahead of the workers.  Every
+// wait is bounded in time; a wait that gives up sets the error flag and ends
+// that warp's loop, which ends the others' at their next (bounded) wait;
+// before the CTA ends, the MMA warp waits for its last commit and thread 0
+// for the latest copy into every slot.
 // S is as many slots as fit, at most 8: with two CTAs per SM when at least 6
 // fit in half the SM's shared memory (two independent pipelines), else with
 // one CTA.
 // ---------------------------------------------------------------------------
 constexpr int kZmWorkers = 128;                           // staging + epilogue warps 0-3
 constexpr int kZmThreads = kZmWorkers + 32;               // + the MMA warp
+constexpr int kZmAcc = 4;                                 // accumulator buffers in TMEM
 constexpr int kZmSmemOne = 227 * 1024 - 1024;            // dynamic bytes, one CTA per SM
 constexpr int kZmSmemTwo = 228 * 1024 / 2 - 1024 - 128;  // dynamic bytes, two CTAs per SM
 
@@ -297,12 +299,13 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
     constexpr int kSlot = zm_slot_bytes<CIN>();
     constexpr int kDy = zm_dy_bytes<CIN>();
     constexpr uint32_t kSlotTx = 3u * CH * kRowBytes;       // bytes the three row boxes of a plane bring
-    constexpr int kCols = 2 * N < 32 ? 32 : 2 * N;
+    constexpr int kCols = kZmAcc * N < 32 ? 32 : kZmAcc * N;   // a power of two
     constexpr uint32_t idesc = umma_idesc_bf16(kConvM, N);
     // full[s]: the plane in ring slot s has landed (the TMA copies' bytes);
     // accf[b]: the MMAs into accumulator buffer b completed (their commit);
-    // acce[b]: buffer b has been read out (one arrival per worker).
-    __shared__ __align__(8) uint64_t full[S], accf[2], acce[2];
+    // acce[b]: buffer b has been read out (one arrival per worker).  Plane
+    // iteration it uses buffer it % kZmAcc, the n-th time for n = it / kZmAcc.
+    __shared__ __align__(8) uint64_t full[S], accf[kZmAcc], acce[kZmAcc];
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool worker = warp < 4;
@@ -320,7 +323,7 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
     if (tid == 0) {
         for (int s = 0; s < S; ++s)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[s])) : "memory");
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < kZmAcc; ++b) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&accf[b])) : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acce[b])), "r"(kZmWorkers) : "memory");
         }
@@ -379,17 +382,17 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
         float bv[N];
 #pragma unroll
         for (int q = 0; q < N; ++q) bv[q] = bias ? __ldg(bias + q) : 0.0f;
-        // Reads accumulator buffer it & 1 (output plane z0 + it) and stores
+        // Reads accumulator buffer it % kZmAcc (output plane z0 + it) and stores
         // it; false (the whole warp alike) when its wait gave up.
         auto epilogue = [&](int it) -> bool {
-            const bool done = mbar_wait(smem_u32(&accf[it & 1]), (uint32_t)((it >> 1) & 1), err);
+            const bool done = mbar_wait(smem_u32(&accf[it % kZmAcc]), (uint32_t)((it / kZmAcc) & 1), err);
             if (!__all_sync(0xffffffffu, done)) return false;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const long long outv = (long long)(z0 + it + 1) * plane + Pv;
 #pragma unroll
             for (int n0 = 0; n0 < N; n0 += 16) {
                 uint32_t r[16];
-                const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)((it & 1) * N + n0);
+                const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)((it % kZmAcc) * N + n0);
                 asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
                              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
                                "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
@@ -423,9 +426,9 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
                     dst[1] = *reinterpret_cast<uint4 *>(&h[4]);
                 }
             }
-            // buffer it & 1 may be overwritten by the MMAs of iteration it + 2
+            // the buffer may be overwritten by the MMAs of iteration it + kZmAcc
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acce[it & 1])) : "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acce[it % kZmAcc])) : "memory");
             return true;
         };
         // Prologue: padded planes z0 .. z0+S-3 (those the tile needs).
@@ -473,12 +476,13 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
                 done = mbar_wait(smem_u32(&full[slot_of(z + 1)]), fill_parity(z + 1), err) && done;
             }
             done = mbar_wait(smem_u32(&full[slot_of(z + 2)]), fill_parity(z + 2), err) && done;
-            // accumulator buffer it & 1 was last read out by epilogue(it - 2)
-            if (it >= 2) done = mbar_wait(smem_u32(&acce[it & 1]), (uint32_t)(((it - 2) >> 1) & 1), err) && done;
+            // accumulator buffer it % kZmAcc was last read out by epilogue(it - kZmAcc)
+            if (it >= kZmAcc)
+                done = mbar_wait(smem_u32(&acce[it % kZmAcc]), (uint32_t)(((it - kZmAcc) / kZmAcc) & 1), err) && done;
             if (!__all_sync(0xffffffffu, done)) { ok = false; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (lane == 0) {
-                const uint32_t acc = tmem + (uint32_t)((it & 1) * N);
+                const uint32_t acc = tmem + (uint32_t)((it % kZmAcc) * N);
                 // descriptors of the slots of padded planes z, z+1, z+2 (taps
                 // dz = -1, 0, +1); a tap's operand is its slot's descriptor
                 // plus a constant offset in the 16-byte address field
@@ -499,7 +503,7 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
                     }
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                             ::"r"(smem_u32(&accf[it & 1])) : "memory");
+                             ::"r"(smem_u32(&accf[it % kZmAcc])) : "memory");
             }
             __syncwarp();
             issued = it + 1;
@@ -507,7 +511,7 @@ k_conv3d_zm(int W, int H, int D, int zs, int out_stride, int out_offset, const _
         // The last committed MMAs complete before the accumulator columns are
         // released, also when a worker's wait gave up (bounded wait).
         if (issued > 0)
-            mbar_wait(smem_u32(&accf[(issued - 1) & 1]), (uint32_t)(((issued - 1) >> 1) & 1), nullptr);
+            mbar_wait(smem_u32(&accf[(issued - 1) % kZmAcc]), (uint32_t)(((issued - 1) / kZmAcc) & 1), nullptr);
         (void)ok;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

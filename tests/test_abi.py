@@ -79,7 +79,9 @@ def test_argument_checks_need_no_gpu(lib):
     assert lib.blz_default_params(C.byref(p)) == 0
     assert p.density == pytest.approx(0.1) and p.max_iter == 200
     h = C.c_void_p()
-    for bad in (dict(width=3), dict(width=15), dict(dx=0.0), dict(bc_mode=7), dict(max_iter=-1)):
+    # 1290^3: (W + 1)(H + 1)(D + 1) reaches 2^31, past 32-bit field offsets
+    for bad in (dict(width=3), dict(width=15), dict(dx=0.0), dict(bc_mode=7), dict(max_iter=-1),
+                dict(width=1290, height=1290, depth=1290)):
         q = p.copy()
         for k, v in bad.items():
             setattr(q, k, v)
@@ -123,6 +125,10 @@ def test_warm_start_and_batch_argument_checks_need_no_gpu(lib):
     assert lib.blz_batch_solve(None, None) == _abi.BLZ_ERR_ARG
     assert lib.blz_batch_step(None, None, None) == _abi.BLZ_ERR_ARG
     assert "null batch" in _err(lib)
+    assert lib.blz_batch_set_sweep(None, 16, 0) == _abi.BLZ_ERR_ARG
+    assert "null batch" in _err(lib)
+    assert lib.blz_unet_create(648, 648, 648, C.byref(h)) == _abi.BLZ_ERR_ARG
+    assert "2^28" in _err(lib)
 
 
 def test_noalloc_residual_argument_checks_need_no_gpu(lib):
