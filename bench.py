@@ -55,12 +55,18 @@ REF_SWEEPS_ENV = "BLZ_REF_SWEEPS"
 
 
 def load_peaks():
+    return _peak("hbm_gbs", 6650.0)
+
+
+def _peak(key, fallback):
+    """A measured peak of this pool's B200s (MEASURED_PEAKS.json), else the
+    earlier measurement given as fallback."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        return float(d[key]), "measured"
     except Exception:
-        return 6650.0, "fallback"
+        return fallback, "fallback"
 
 
 class ClockSampler:
@@ -150,6 +156,53 @@ def cpu_baseline(scn, parts, mean_sweeps):
             "sample": f"one {scn.gridRes[0]}^3 frame of the FP64 oracle: non-solver stages timed once, "
                       f"{n_s} GS sweeps timed and scaled to {mean_sweeps:.0f} sweeps "
                       f"({per_sweep * 1e3:.1f} ms/sweep, {per_step:.1f} s/step)"}
+
+
+def unet_flops(dims):
+    """Multiply-add FLOPs (x2) of one forward pass of the warm-start network
+    at grid dims (W, H, D): 3x3x3 convolutions at their level, 2x2x2
+    transposed convolutions at their output level, the 1x1 head."""
+    from blaze_b200.unet import layers, KIND_CONV3, KIND_UP
+    W, H, D = dims
+    vox = [(W >> l) * (H >> l) * (D >> l) for l in range(4)]
+    total = 0
+    for L in layers():
+        name = L["name"]
+        if L["kind"] == KIND_CONV3:
+            total += 2 * 27 * L["cin"] * L["cout"] * vox[int(name[1])]
+        elif L["kind"] == KIND_UP:
+            total += 2 * L["cin"] * L["cout"] * vox[int(name[1])]
+        else:
+            total += 2 * L["cin"] * L["cout"] * vox[0]
+    return total
+
+
+def unet_roofline(net, scn, solver, stream, reps=3):
+    """The forward pass on the solver's current rhs and pressure: mean of
+    `reps` runs after one untimed, CUDA events on `stream`."""
+    import torch
+    W, H, D = scn.gridRes
+    rhs = torch.from_numpy(np.ascontiguousarray(solver.get("RHS"))).cuda()
+    p = torch.from_numpy(np.ascontiguousarray(solver.get("P"))).cuda()
+    out = torch.empty((D, H, W), dtype=torch.float32, device="cuda")
+    params = scn.to_params()
+    net.forward(params, rhs, p, out=out, stream=stream.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        net.forward(params, rhs, p, out=out, stream=stream.cuda_stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    flops = unet_flops((W, H, D))
+    peak, kind = _peak("bf16_tflops", 1590.0)             # burst: the forward timed on its own
+    achieved = flops / (ms * 1e-3) / 1e12
+    return {"bound": "tensor", "kernel": "warm-start network forward (k_conv3d_zm / k_conv3d_tc on tcgen05, "
+                                          "BF16 in, FP32 accumulate; pooling, transposed convolutions, head on SIMT)",
+            "ms": ms, "tflop": flops / 1e12, "achieved": achieved, "peak": peak, "peak_kind": kind,
+            "unit": "TFLOP/s", "frac": achieved / peak,
+            "timing": f"CUDA events around {reps} forward passes on the bench stream, outside the timed region"}
 
 
 def _load_net(args, W, H, D):
@@ -284,6 +337,13 @@ def run_ours(args, ws, rank, local):
     torch.cuda.synchronize()
     sweep_ms_events = m0.elapsed_time(m1) / n_meas
 
+    # The network's forward pass alone (its convolutions run on the tcgen05
+    # tensor cores), timed with CUDA events on this stream, against the
+    # measured BF16 peak: the tensor-core roofline of the warm start.
+    unet_line = None
+    if head_learned:
+        unet_line = unet_roofline(net, scn, solver, stream)
+
     e2e_s = None
     # e2e through the public API with host buffers: per frame the particle
     # records go host->device (the reference re-reads an animated source every
@@ -400,6 +460,7 @@ def run_ours(args, ws, rank, local):
                      "timing": f"CUDA events around {n_meas} sweeps on the bench stream after the timed passes; "
                                "in-region figure from the device global timer around each sweep batch",
                      "sweep_variant": variant},
+        "roofline_warm_start": unet_line,
         "e2e": None if e2e_s is None else
                {"value": ws * args.steps / e2e_s, "unit": "steps/s",
                 "h2d_bytes_per_step": int(parts.nbytes), "d2h_bytes_per_step": int(n_cells * 4)},
