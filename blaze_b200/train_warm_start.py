@@ -51,12 +51,27 @@ def _seed_list(spec):
     return out
 
 
+# Which scene family harvest and evaluation run: "plume" (the plume family,
+# scenes.family_scene) or "fire" (the large fire with moving emitters,
+# scenes.large_fire_scene, whose particles are re-uploaded every frame).
+SCENE = "plume"
+
+
 def _solver(n, seed, tol, max_iter, check_every):
-    from .scenes import Timer, family_scene
+    """(solver, scene, timer, per-frame particle hook)."""
+    from .scenes import Timer, family_scene, large_fire_scene
     from .solver import FluidSolver
-    scn, parts = family_scene(n=n, seed=seed, tol=tol, max_iter=max_iter, check_every=check_every)
     tmr = Timer()
-    return FluidSolver(tmr, scn, particles=parts), scn, tmr
+    if SCENE == "fire":
+        scn, frame_parts = large_fire_scene(n=n, seed=seed)
+        scn.tol, scn.maxIterSolve = tol, max_iter
+        solver = FluidSolver(tmr, scn, particles=frame_parts(0))
+
+        def hook():
+            solver.setParticles(frame_parts(tmr.iter))
+        return solver, scn, tmr, hook
+    scn, parts = family_scene(n=n, seed=seed, tol=tol, max_iter=max_iter, check_every=check_every)
+    return FluidSolver(tmr, scn, particles=parts), scn, tmr, (lambda: None)
 
 
 def _field(solver, name, shape):
@@ -82,10 +97,11 @@ def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, lo
     it, as deployed."""
     pairs, ratios = [], []
     for seed in seeds:
-        solver, scn, tmr = _solver(n, seed, tol, max_iter, check_every)
+        solver, scn, tmr, hook = _solver(n, seed, tol, max_iter, check_every)
         shape = scn.to_params().field_shape("P")
         t0 = time.time()
         for f in range(warmup + frames):
+            hook()
             solver.addSource()
             solver.forces(tmr.time)
             solver.divergence()
@@ -173,8 +189,9 @@ def evaluate(net, n, seeds, frames, warmup, tol, max_iter, check_every, log=prin
     rows = []
     for seed in seeds:
         for learned in (False, True):
-            solver, scn, tmr = _solver(n, seed, tol, max_iter, check_every)
+            solver, scn, tmr, hook = _solver(n, seed, tol, max_iter, check_every)
             for f in range(warmup + frames):
+                hook()
                 solver.addSource()
                 solver.forces(tmr.time)
                 solver.divergence()
@@ -206,6 +223,8 @@ def _ratios(rows):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--grid", type=int, default=256)
+    ap.add_argument("--scene", choices=("plume", "fire"), default="plume",
+                    help="scene family harvested and evaluated: the plume family or the large fire")
     ap.add_argument("--plain-seeds", default="100-107", help="seeds harvested with plain solves ('' for none)")
     ap.add_argument("--policy-seeds", default="108-115", help="seeds harvested on policy in each round")
     ap.add_argument("--rounds", type=int, default=1, help="on-policy harvest + training rounds")
@@ -248,6 +267,8 @@ def main(argv=None):
         print(msg, flush=True)
 
     torch.cuda.set_device(0)
+    global SCENE
+    SCENE = args.scene
     n = args.grid
     crop = (min(args.crop, n),) * 3
     grid = family_scene(n=n, seed=0)[0].to_params()
@@ -270,7 +291,7 @@ def main(argv=None):
         for seed in _seed_list(args.eval_seeds):
             sub = [r for r in rows if r["seed"] == seed]
             per_seed[str(seed)] = dict(zip(("sweep_ratio", "time_ratio", "all_converged"), _ratios(sub)))
-        summary = {"grid": n, "weights": args.init, "kappa": kappa, "eval_seeds": args.eval_seeds,
+        summary = {"grid": n, "scene": args.scene, "weights": args.init, "kappa": kappa, "eval_seeds": args.eval_seeds,
                    "eval_frames": args.eval_frames, "warmup": args.warmup, "tol": args.tol, "max_iter": args.max_iter,
                    "steps_per_arm": len(rows) // 2, "sweep_ratio": sweep_ratio, "time_ratio": time_ratio,
                    "eval_all_converged": conv, "per_seed": per_seed, "eval": rows}
@@ -326,7 +347,8 @@ def main(argv=None):
                     args.check_every, log)
     sweep_ratio, time_ratio, conv = _ratios(rows)
     summary = {
-        "grid": n, "plain_seeds": args.plain_seeds, "policy_seeds": args.policy_seeds, "rounds": rounds,
+        "grid": n, "scene": args.scene, "plain_seeds": args.plain_seeds, "policy_seeds": args.policy_seeds,
+        "rounds": rounds,
         "harvest": args.harvest, "keep_kappa": args.keep_kappa,
         "eval_seeds": args.eval_seeds, "frames": args.frames, "stride": args.stride, "warmup": args.warmup,
         "tol": args.tol,
