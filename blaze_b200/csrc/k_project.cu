@@ -978,7 +978,10 @@ constexpr int kResThreads = 256;
 
 // Tiles of the z-marching residual (W % 8 == 0 and W <= 2048): a block of
 // kResThreads threads covers kResThreads / Wq rows of quads and kResKZ planes.
-constexpr int kResKZ = 8;
+// 16 planes and at most 64 registers (four blocks per SM): at 256^3 the 512
+// tiles are one wave, with 32 warps per SM waiting on DRAM.
+constexpr int kResKZ = 16;
+constexpr int kResBlocksPerSM = 4;
 
 __host__ __device__ inline bool residual_tiled(const Geom &g) { return (g.W & 7) == 0 && (g.W >> 3) <= kResThreads; }
 __host__ __device__ inline int residual_tile_rows(const Geom &g) { return kResThreads / (g.W >> 3); }
@@ -1166,7 +1169,7 @@ __device__ __forceinline__ void residual_block(const Geom &g, const SolveParams 
 }
 
 // One block per tile when residual_tiled(g), else grid-stride segments.
-__global__ void __launch_bounds__(kResThreads)
+__global__ void __launch_bounds__(kResThreads, kResBlocksPerSM)
 k_residual_seg(Geom g, SolveParams sp, double scale, const float *__restrict__ rr,
                const float *__restrict__ rb, const float *__restrict__ pr, const float *__restrict__ pb,
                double *__restrict__ partials) {

@@ -217,6 +217,14 @@ namespace blz {
 cudaError_t launch_conv3d(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
                           void *y, int *err, cudaStream_t st, const __nv_bfloat16 *aux = nullptr);
 
+// 2x2x2 stride-2 transposed convolution on the tensor cores: x coarse W x H x
+// D (padded channels-last, cin channels), w BF16 [8][cout][cin], output into
+// channels [0, cout) of the fine tensor y (channel stride ys).  (cin, cout)
+// in {(32, 16), (64, 32), (128, 64)}, else cudaErrorNotSupported.
+cudaError_t launch_upconv_tc(int W, int H, int D, int cin, int cout, const __nv_bfloat16 *x,
+                             const __nv_bfloat16 *w, const float *bias, __nv_bfloat16 *y, int ys, int *err,
+                             cudaStream_t st);
+
 // Sets the calling thread's error text (what blz_last_error(NULL) returns).
 void set_thread_error(const char *msg);
 

@@ -29,6 +29,7 @@
 // cores (unet_conv.cu).  Pooling, the transposed convolutions, weight gradients,
 // the loss and Adam are SIMT kernels: together they are a small share of the
 // FLOPs, and weight gradients only run in training.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -112,7 +113,19 @@ __device__ __forceinline__ void split3(long long v, int W, int H, int &x, int &y
 }
 
 constexpr int kNormThreads = 256;
-constexpr int kNormBlocks = 1024;
+constexpr int kNormBlocks = 1024;                  // partials capacity (blocks of the reductions)
+
+// Grid of a grid-stride reduction kernel: one wave of as many blocks as are
+// resident on the device's SMs (at most kNormBlocks), so no block waits for a
+// second wave.
+template <typename K>
+static int one_wave(K kernel) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kNormThreads, 0);
+    return std::max(1, std::min(kNormBlocks, sms * std::max(1, per)));
+}
 
 // Sums of b^2, p^2, r^2 over the grid (FP64), one triple per block.
 __global__ void __launch_bounds__(kNormThreads)
@@ -280,93 +293,15 @@ __global__ void k_skip_grad(const bf16 *__restrict__ dcat, const bf16 *__restric
     st8(out + f * C + c, o);
 }
 
-// 2x2x2 stride-2 transposed convolution: fine voxel (2x+a, 2y+b, 2z+c)
-// = bias + W[a + 2b + 4c] . x[x, y, z].  W: FP32 [8][cout][cin].  Output into
-// channels [0, cout) of a tensor with channel stride ys.  A block covers 128
-// coarse voxels and one parity (blockIdx.y), whose COUT x CIN weights sit in
-// shared memory and are read as uniform broadcasts; each thread computes all
-// COUT outputs of its fine voxel from its coarse voxel's CIN inputs, 32 at a
-// time in registers.
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(128)
-k_upconv_t(const bf16 *__restrict__ x, LDims dc, const float *__restrict__ w, const float *__restrict__ bias,
-           bf16 *__restrict__ y, int ys) {
-    __shared__ __align__(16) float sw[COUT * CIN];
-    const int par = blockIdx.y;
-    for (int e = threadIdx.x; e < COUT * CIN; e += blockDim.x) sw[e] = __ldg(w + (size_t)par * COUT * CIN + e);
-    __syncthreads();
-    const long long n = (long long)dc.W * dc.H * dc.D;
-    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    int cx, cy, cz;
-    split3(v, dc.W, dc.H, cx, cy, cz);
-    const LDims df{dc.W * 2, dc.H * 2, dc.D * 2};
-    float acc[COUT];
-#pragma unroll
-    for (int o = 0; o < COUT; ++o) acc[o] = __ldg(bias + o);
-    const bf16 *xp = x + pvox(dc, cx, cy, cz) * CIN;
-#pragma unroll 1
-    for (int c0 = 0; c0 < CIN; c0 += 32) {
-        float xv[32];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) unpack8(ld8(xp + c0 + 8 * q), xv + 8 * q);
-#pragma unroll
-        for (int o = 0; o < COUT; ++o) {
-            const float4 *wr = reinterpret_cast<const float4 *>(sw + o * CIN + c0);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const float4 ww = wr[q];
-                acc[o] = fmaf(ww.x, xv[4 * q], acc[o]);
-                acc[o] = fmaf(ww.y, xv[4 * q + 1], acc[o]);
-                acc[o] = fmaf(ww.z, xv[4 * q + 2], acc[o]);
-                acc[o] = fmaf(ww.w, xv[4 * q + 3], acc[o]);
-            }
-        }
-    }
-    const long long f = pvox(df, 2 * cx + (par & 1), 2 * cy + ((par >> 1) & 1), 2 * cz + (par >> 2));
-#pragma unroll
-    for (int o = 0; o < COUT; o += 8) st8(y + f * ys + o, acc + o);
-}
-
-// Generic transposed convolution (any cin, cout multiple of 8): one thread
-// per coarse voxel, parity (blockIdx.y) and 8 output channels (blockIdx.z).
-__global__ void __launch_bounds__(128)
-k_upconv(const bf16 *__restrict__ x, LDims dc, int cin, int cout, const float *__restrict__ w,
-         const float *__restrict__ bias, bf16 *__restrict__ y, int ys) {
-    const long long n = (long long)dc.W * dc.H * dc.D;
-    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const int par = blockIdx.y, co0 = blockIdx.z * 8;
-    int cx, cy, cz;
-    split3(v, dc.W, dc.H, cx, cy, cz);
-    const LDims df{dc.W * 2, dc.H * 2, dc.D * 2};
-    float acc[8];
-#pragma unroll
-    for (int o = 0; o < 8; ++o) acc[o] = __ldg(bias + co0 + o);
-    const bf16 *xp = x + pvox(dc, cx, cy, cz) * cin;
-    const float *wp = w + ((size_t)par * cout + co0) * cin;
-    for (int ci = 0; ci < cin; ci += 8) {
-        float xv[8];
-        unpack8(ld8(xp + ci), xv);
-#pragma unroll
-        for (int o = 0; o < 8; ++o) {
-            const float4 w0 = __ldg(reinterpret_cast<const float4 *>(wp + (size_t)o * cin + ci));
-            const float4 w1 = __ldg(reinterpret_cast<const float4 *>(wp + (size_t)o * cin + ci + 4));
-            acc[o] = fmaf(w0.x, xv[0], acc[o]); acc[o] = fmaf(w0.y, xv[1], acc[o]);
-            acc[o] = fmaf(w0.z, xv[2], acc[o]); acc[o] = fmaf(w0.w, xv[3], acc[o]);
-            acc[o] = fmaf(w1.x, xv[4], acc[o]); acc[o] = fmaf(w1.y, xv[5], acc[o]);
-            acc[o] = fmaf(w1.z, xv[6], acc[o]); acc[o] = fmaf(w1.w, xv[7], acc[o]);
-        }
-    }
-    const long long f = pvox(df, 2 * cx + (par & 1), 2 * cy + ((par >> 1) & 1), 2 * cz + (par >> 2));
-    st8(y + f * ys + co0, acc);
-}
-
+// The forward pass of the transposed convolutions runs on the tensor cores
+// (launch_upconv_tc, unet_conv.cu) with the BF16 copy of the weights.
+//
 // Data gradient of the transposed convolution, masked by the coarse input's
-// ReLU: gx[v][ci] = (sum_par sum_co W[par][co][ci] g[fine(v, par)][co]) * (act[v][ci] > 0).
+// ReLU: gx[v][ci] = (sum_par sum_co W[par][co][ci] g[fine(v, par)][co]) * (act[v][ci] > 0),
+// with the same BF16 weights as the forward pass.
 // g: fine tensor, channels [0, cout) of channel stride gs.
 __global__ void __launch_bounds__(128)
-k_upconv_bwd(const bf16 *__restrict__ g, int gs, LDims dc, int cin, int cout, const float *__restrict__ w,
+k_upconv_bwd(const bf16 *__restrict__ g, int gs, LDims dc, int cin, int cout, const bf16 *__restrict__ w,
              const bf16 *__restrict__ act, bf16 *__restrict__ gx) {
     const long long n = (long long)dc.W * dc.H * dc.D;
     const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -378,18 +313,16 @@ k_upconv_bwd(const bf16 *__restrict__ g, int gs, LDims dc, int cin, int cout, co
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int par = 0; par < 8; ++par) {
         const long long f = pvox(df, 2 * cx + (par & 1), 2 * cy + ((par >> 1) & 1), 2 * cz + (par >> 2));
-        const float *wp = w + (size_t)par * cout * cin + ci0;
+        const bf16 *wp = w + (size_t)par * cout * cin + ci0;
         for (int co = 0; co < cout; co += 8) {
             float gv[8];
             unpack8(ld8(g + f * gs + co), gv);
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                const float4 w0 = __ldg(reinterpret_cast<const float4 *>(wp + (size_t)(co + q) * cin));
-                const float4 w1 = __ldg(reinterpret_cast<const float4 *>(wp + (size_t)(co + q) * cin + 4));
-                acc[0] = fmaf(w0.x, gv[q], acc[0]); acc[1] = fmaf(w0.y, gv[q], acc[1]);
-                acc[2] = fmaf(w0.z, gv[q], acc[2]); acc[3] = fmaf(w0.w, gv[q], acc[3]);
-                acc[4] = fmaf(w1.x, gv[q], acc[4]); acc[5] = fmaf(w1.y, gv[q], acc[5]);
-                acc[6] = fmaf(w1.z, gv[q], acc[6]); acc[7] = fmaf(w1.w, gv[q], acc[7]);
+                float wv[8];
+                unpack8(ld8(wp + (size_t)(co + q) * cin), wv);
+#pragma unroll
+                for (int e = 0; e < 8; ++e) acc[e] = fmaf(wv[e], gv[q], acc[e]);
             }
         }
     }
@@ -693,6 +626,12 @@ __global__ void k_export_conv(const float *__restrict__ w, int co, int ci, bf16 
     wd[((size_t)(26 - t) * ci + i) * co + o] = h;
 }
 
+// BF16 copy of a transposed convolution's weights, same [8][cout][cin] order.
+__global__ void k_export_up(const float *__restrict__ w, long long n, bf16 *__restrict__ wf) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e < n) wf[e] = __float2bfloat16_rn(w[e]);
+}
+
 inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // ---------------------------------------------------------------------------
@@ -731,6 +670,7 @@ struct blz_unet {
     bool bf_dirty = true;
     int adam_t = 0;
     float kappa = 1.0f;
+    int nb_norms = kNormBlocks, nb_project = kNormBlocks;   // one-wave grids of the reductions
     // forward activations
     Ten X0, e0a, cat0, d0a, d0b, p1, e1a, cat1, d1a, d1b, p2, e2a, cat2, d2a, d2b, p3, e3a, e3b;
     // gradients (allocated by the first training call)
@@ -802,6 +742,11 @@ GridInfo grid_info(const blz_params &P) {
 int refresh_bf16(blz_unet *u, cudaStream_t st) {
     if (!u->bf_dirty) return BLZ_OK;
     for (int l = 0; l < NLAYERS; ++l) {
+        if (kLayers[l].kind == kUp) {
+            const long long n = 8LL * kLayers[l].cout * kLayers[l].cin;
+            k_export_up<<<nblk(n, 256), 256, 0, st>>>(u->params + u->w_off[l], n, u->wf + u->bf_off[l]);
+            ++u->launches;
+        }
         if (kLayers[l].kind != kConv3) continue;
         const long long n = 27LL * kLayers[l].cout * kLayers[l].cin;
         k_export_conv<<<nblk(n, 256), 256, 0, st>>>(u->params + u->w_off[l], kLayers[l].cout, kLayers[l].cin,
@@ -867,16 +812,10 @@ int conv_wgrad(blz_unet *u, int l, const Ten &gy, const Ten &x, cudaStream_t st)
 int up_fwd(blz_unet *u, int l, const Ten &x, const Ten &y, cudaStream_t st) {
     const LayerDef &L = kLayers[l];
     const LDims &dc = u->L[L.level + 1];
-    const long long n = (long long)dc.W * dc.H * dc.D;
-    const float *w = u->params + u->w_off[l], *b = u->params + u->b_off[l];
-    const dim3 g2(nblk(n, 128), 8);
-    if (L.cin == 32 && L.cout == 16) k_upconv_t<32, 16><<<g2, 128, 0, st>>>(x.base(), dc, w, b, y.base(), y.C);
-    else if (L.cin == 64 && L.cout == 32) k_upconv_t<64, 32><<<g2, 128, 0, st>>>(x.base(), dc, w, b, y.base(), y.C);
-    else if (L.cin == 128 && L.cout == 64) k_upconv_t<128, 64><<<g2, 128, 0, st>>>(x.base(), dc, w, b, y.base(), y.C);
-    else {
-        const dim3 grid(nblk(n, 128), 8, L.cout / 8);
-        k_upconv<<<grid, 128, 0, st>>>(x.base(), dc, L.cin, L.cout, w, b, y.base(), y.C);
-    }
+    const cudaError_t e = launch_upconv_tc(dc.W, dc.H, dc.D, L.cin, L.cout, x.base(), u->wf + u->bf_off[l],
+                                           u->params + u->b_off[l], y.base(), y.C, u->err, st);
+    if (e != cudaSuccess)
+        return ufail(BLZ_ERR_CUDA, "transposed convolution %d (%d -> %d): %s", l, L.cin, L.cout, cudaGetErrorString(e));
     ++u->launches;
     UCKL();
     return BLZ_OK;
@@ -893,7 +832,7 @@ int up_bwd(blz_unet *u, int l, const Ten &gy, const Ten &x, const Ten &gx, cudaS
              u->grads + u->b_off[l]};
     launch_wgrad<kModeUp>(a, 8, st);
     const dim3 grid(nblk(n, 128), L.cin / 8);
-    k_upconv_bwd<<<grid, 128, 0, st>>>(gy.base(), gy.C, dc, L.cin, L.cout, u->params + u->w_off[l], x.base(),
+    k_upconv_bwd<<<grid, 128, 0, st>>>(gy.base(), gy.C, dc, L.cin, L.cout, u->wf + u->bf_off[l], x.base(),
                                        gx.base());
     u->launches += 2;
     UCKL();
@@ -920,8 +859,8 @@ int skip_grad(blz_unet *u, const Ten &gcat, const Ten &cat, const Ten &gpool, co
 
 int prepare_input(blz_unet *u, const GridInfo &g, const CellArr &rhs, const CellArr &p, const int org[3],
                   cudaStream_t st) {
-    k_unet_norms<<<kNormBlocks, kNormThreads, 0, st>>>(g, rhs, p, u->partials);
-    k_unet_scales<<<1, 256, 0, st>>>(u->partials, kNormBlocks, (double)g.W * g.H * g.D, u->kappa, u->scales);
+    k_unet_norms<<<u->nb_norms, kNormThreads, 0, st>>>(g, rhs, p, u->partials);
+    k_unet_scales<<<1, 256, 0, st>>>(u->partials, u->nb_norms, (double)g.W * g.H * g.D, u->kappa, u->scales);
     const LDims &d = u->L[0];
     const long long n = (long long)(d.W + 2) * (d.H + 2) * (d.D + 2);
     k_unet_input<<<nblk(n, 256), 256, 0, st>>>(g, rhs, p, org[0], org[1], org[2], d, u->scales, u->X0.base());
@@ -1099,9 +1038,9 @@ int unet_combine(blz_unet *u, const blz_params &P, const float *rhs_r, const flo
     const LDims &d = u->L[0];
     const long long n = (long long)d.W * d.H * d.D;
     const float *dr = u->dpk, *db = u->dpk + n / 2;
-    k_unet_project<<<kNormBlocks, kNormThreads, 0, st>>>(g, CellArr{rhs_r, rhs_b}, CellArr{p_r, p_b},
+    k_unet_project<<<u->nb_project, kNormThreads, 0, st>>>(g, CellArr{rhs_r, rhs_b}, CellArr{p_r, p_b},
                                                          CellArr{dr, db}, u->partials);
-    k_unet_alpha<<<1, 256, 0, st>>>(u->partials, kNormBlocks, u->step_mode, u->alpha);
+    k_unet_alpha<<<1, 256, 0, st>>>(u->partials, u->nb_project, u->step_mode, u->alpha);
     k_unet_update<<<nblk(n / 2, 256), 256, 0, st>>>(n / 2, dr, db, u->alpha, p_r, p_b);
     u->launches += 3;
     if (launches) *launches += 3;
@@ -1141,6 +1080,8 @@ int blz_unet_create(int width, int height, int depth, blz_unet **out) {
     blz_unet *u = new blz_unet();
     for (int l = 0; l < 4; ++l) u->L[l] = {width >> l, height >> l, depth >> l};
     cudaGetDevice(&u->device);
+    u->nb_norms = one_wave(k_unet_norms);
+    u->nb_project = one_wave(k_unet_project);
     size_t off = 0, bf = 0;
     for (int l = 0; l < NLAYERS; ++l) {
         const LayerDef &L = kLayers[l];
@@ -1148,7 +1089,7 @@ int blz_unet_create(int width, int height, int depth, blz_unet **out) {
         u->w_off[l] = off;
         u->b_off[l] = off + wn;
         off += wn + L.cout;
-        if (L.kind == kConv3) { u->bf_off[l] = bf; bf += wn; }
+        if (L.kind == kConv3 || L.kind == kUp) { u->bf_off[l] = bf; bf += wn; }
     }
     u->n_params = off;
     u->n_bf = bf;

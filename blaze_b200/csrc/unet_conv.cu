@@ -612,6 +612,151 @@ cudaError_t launch_conv3d(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv
     return cudaErrorInvalidValue;
 }
 
+// ---------------------------------------------------------------------------
+// 2x2x2 stride-2 transposed convolution on the tensor cores.  Fine voxel
+// (2x+a, 2y+b, 2z+c) = bias + W[a + 2b + 4c] . x[x, y, z], so the 8 parities
+// of a coarse voxel are one GEMM row: one CTA takes M = 128 consecutive
+// padded coarse voxels of interior plane z (its interior rows, as the 3x3x3
+// kernels tile a plane) and computes D[128 x 8 COUT] = X[128 x CIN] W^T with
+// W in BF16 [8][COUT][CIN] (GEMM row n = par * COUT + co), K = 16 per MMA,
+// N = 8 COUT split into MMAs of at most 256 columns.  Operands are staged
+// once by cp.async in the canonical K-major layouts of the 3x3x3 kernels
+// (A: [chunk][kg][voxel][8], B: [chunk][kg][n][8]); one thread issues the
+// MMAs and commits them to an mbarrier (bounded wait); the epilogue reads
+// each parity's COUT columns from TMEM, adds the bias and stores BF16 into
+// the fine voxel's channels [0, COUT) of a tensor with channel stride ys.
+// ---------------------------------------------------------------------------
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128, 1)
+k_upconv_tc(int W, int H, int D, const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ w,
+            const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y, int ys, int *err) {
+    constexpr int N = 8 * COUT, CH = CIN / 16;
+    constexpr int NMMA = N > 256 ? 256 : N;              // columns per MMA
+    constexpr int kCols = N;                              // 128, 256 or 512: a power of two
+    constexpr int kAChunk = 2 * kConvM * 16;              // [kg][voxel][8] of one 16-channel chunk
+    constexpr int kBChunk = 2 * N * 16;                   // [kg][n][8] of one 16-channel chunk
+    constexpr uint32_t idesc = umma_idesc_bf16(kConvM, NMMA);
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Wp = W + 2, Hp = H + 2;
+    const long long plane = (long long)Wp * Hp;
+    const int z = blockIdx.y;                                              // interior coarse plane
+    const long long P0 = (long long)Wp + (long long)kConvM * blockIdx.x;   // first voxel of the tile
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base)), "r"(kCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const uint32_t aS = smem_u32(smem), bS = aS + (uint32_t)(CH * kAChunk);
+    // A: 16-byte chunk (c, kg) of voxel v at aS + c kAChunk + kg 2048 + v 16.
+    const __nv_bfloat16 *xs = x + ((long long)(z + 1) * plane + P0) * CIN;
+    for (int e = tid; e < CH * 2 * kConvM; e += 128) {
+        const int c = e / (2 * kConvM), r = e % (2 * kConvM), kg = r & 1, v = r >> 1;
+        cp_async16(aS + c * kAChunk + kg * (kConvM * 16) + v * 16, xs + (long long)v * CIN + c * 16 + kg * 8);
+    }
+    // B: 16-byte chunk (c, kg) of row n at bS + c kBChunk + kg N 16 + n 16.
+    for (int e = tid; e < CH * 2 * N; e += 128) {
+        const int c = e / (2 * N), r = e % (2 * N), kg = r & 1, n = r >> 1;
+        cp_async16(bS + c * kBChunk + kg * (N * 16) + n * 16, w + (size_t)n * CIN + c * 16 + kg * 8);
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+#pragma unroll
+            for (int h = 0; h < N / NMMA; ++h) {
+                const uint64_t ad = umma_desc(aS + c * kAChunk, kConvM * 16, 128);
+                const uint64_t bd = umma_desc(bS + c * kBChunk + h * NMMA * 16, N * 16, 128);
+                const uint32_t accum = c > 0 ? 1u : 0u;
+                asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                             ::"r"(tmem + (uint32_t)(h * NMMA)), "l"(ad), "l"(bd), "r"(idesc), "r"(accum)
+                             : "memory");
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     ::"r"(smem_u32(&mbar)) : "memory");
+    }
+    // CTA-uniform outcome, so the .sync.aligned TMEM loads never run in a
+    // divergent warp.
+    const bool ok = __syncthreads_and(mbar_wait(smem_u32(&mbar), 0u, err)) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+        // warp w owns TMEM lanes 32w..32w+31 = voxels of the tile
+        const long long Pv = P0 + 32 * warp + lane;
+        const int yv = (int)(Pv / Wp), xv = (int)(Pv - (long long)yv * Wp);
+        const bool inside = xv >= 1 && xv <= W && yv >= 1 && yv <= H;
+        const int cx = xv - 1, cy = yv - 1;
+        const long long Wf = 2LL * W + 2, Hf = 2LL * H + 2;
+#pragma unroll 1
+        for (int par = 0; par < 8; ++par) {
+            const long long f = ((long long)(2 * z + (par >> 2) + 1) * Hf + (2 * cy + ((par >> 1) & 1) + 1)) * Wf +
+                                (2 * cx + (par & 1) + 1);
+#pragma unroll
+            for (int n0 = 0; n0 < COUT; n0 += 16) {
+                uint32_t r[16];
+                const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(par * COUT + n0);
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                               "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+                               "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                             : "r"(taddr) : "memory");
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (inside) {
+                    __nv_bfloat162 hv[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        hv[q] = __floats2bfloat162_rn(__uint_as_float(r[2 * q]) + __ldg(bias + n0 + 2 * q),
+                                                      __uint_as_float(r[2 * q + 1]) + __ldg(bias + n0 + 2 * q + 1));
+                    uint4 *dst = reinterpret_cast<uint4 *>(y + f * ys + n0);
+                    dst[0] = *reinterpret_cast<uint4 *>(&hv[0]);
+                    dst[1] = *reinterpret_cast<uint4 *>(&hv[4]);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+}
+
+template <int CIN, int COUT>
+static cudaError_t launch_up_tc(int W, int H, int D, const __nv_bfloat16 *x, const __nv_bfloat16 *w,
+                                const float *bias, __nv_bfloat16 *y, int ys, int *err, cudaStream_t st) {
+    constexpr int smem = (CIN / 16) * 2 * kConvM * 16 + (CIN / 16) * 2 * (8 * COUT) * 16;
+    cudaError_t e = cudaFuncSetAttribute(k_upconv_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const long long interior = (long long)(W + 2) * H;
+    const dim3 grid((unsigned)((interior + kConvM - 1) / kConvM), (unsigned)D);
+    k_upconv_tc<CIN, COUT><<<grid, 128, smem, st>>>(W, H, D, x, w, bias, y, ys, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_upconv_tc(int W, int H, int D, int cin, int cout, const __nv_bfloat16 *x,
+                             const __nv_bfloat16 *w, const float *bias, __nv_bfloat16 *y, int ys, int *err,
+                             cudaStream_t st) {
+    if (ys % 8 != 0) return cudaErrorInvalidValue;
+    if (cin == 32 && cout == 16) return launch_up_tc<32, 16>(W, H, D, x, w, bias, y, ys, err, st);
+    if (cin == 64 && cout == 32) return launch_up_tc<64, 32>(W, H, D, x, w, bias, y, ys, err, st);
+    if (cin == 128 && cout == 64) return launch_up_tc<128, 64>(W, H, D, x, w, bias, y, ys, err, st);
+    return cudaErrorNotSupported;
+}
+
 } // namespace blz
 
 namespace {

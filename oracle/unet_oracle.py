@@ -12,9 +12,10 @@ the reference's Gauss-Seidel solve (src/FluidSolver.cu:517-599) with the
 boundary handling of blz_params (walls; free-surface p = 0 ghosts).
 
 With ``bf16=True`` every tensor the GPU stores in BF16 (input, activations,
-activation gradients) and the 3x3x3 weights are rounded to BF16 (round to
-nearest even) at the same points, so the only remaining difference to the
-GPU is the FP32-vs-FP64 accumulation order.  With ``bf16=False`` it is the
+activation gradients) and the 3x3x3 and transposed-convolution weights (the
+GPU's forward passes and data gradients read BF16 copies of them) are
+rounded to BF16 (round to nearest even) at the same points, so the only
+remaining difference to the GPU is the FP32-vs-FP64 accumulation order.  With ``bf16=False`` it is the
 plain FP64 network, used for the finite-difference check of the backward
 pass.  Arrays are numpy (z, y, x[, c]).
 """
@@ -196,7 +197,7 @@ class Net:
         self.bf16 = bf16
         if bf16:
             for name, kind, *_ in LAYERS:
-                if kind == CONV3:
+                if kind in (CONV3, UP):
                     self.W[name] = bf16_round(self.W[name])
 
     def r(self, a):

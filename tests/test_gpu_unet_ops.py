@@ -60,7 +60,7 @@ def _weights(params):
     from oracle import unet_oracle as uo
     W, B = uo.unpack(params)
     for name, kind, *_ in uo.LAYERS:
-        if kind == uo.CONV3:
+        if kind in (uo.CONV3, uo.UP):
             W[name] = uo.bf16_round(W[name])
     return W, B
 
