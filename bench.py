@@ -198,8 +198,9 @@ def unet_roofline(net, scn, solver, stream, reps=3):
     flops = unet_flops((W, H, D))
     peak, kind = _peak("bf16_tflops", 1590.0)             # burst: the forward timed on its own
     achieved = flops / (ms * 1e-3) / 1e12
-    return {"bound": "tensor", "kernel": "warm-start network forward (k_conv3d_zm / k_conv3d_tc on tcgen05, "
-                                          "BF16 in, FP32 accumulate; pooling, transposed convolutions, head on SIMT)",
+    return {"bound": "tensor", "kernel": "warm-start network forward (k_conv3d_zm / k_conv3d_tc / k_upconv_tc "
+                                          "on tcgen05, BF16 in, FP32 accumulate; pooling, input, norms and head "
+                                          "on SIMT)",
             "ms": ms, "tflop": flops / 1e12, "achieved": achieved, "peak": peak, "peak_kind": kind,
             "unit": "TFLOP/s", "frac": achieved / peak,
             "timing": f"CUDA events around {reps} forward passes on the bench stream, outside the timed region"}
