@@ -224,6 +224,13 @@ cudaError_t launch_conv3d(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv
 cudaError_t launch_upconv_tc(int W, int H, int D, int cin, int cout, const __nv_bfloat16 *x,
                              const __nv_bfloat16 *w, const float *bias, __nv_bfloat16 *y, int ys, int *err,
                              cudaStream_t st);
+// Weight gradient (no bias) of a 3x3x3 convolution (up = 0: x and gy at level
+// W x H x D, dw [27][cout][cin]) or of a 2x2x2 transposed convolution (up = 1:
+// x coarse at W x H x D, gy fine, dw [8][cout][cin]) on the tensor cores,
+// added to dw.  Tensors are padded channels-last, passed at padded voxel 0,
+// with BLZ_CONV_SLACK zero voxels on either side; gy zero on its halo.
+cudaError_t launch_wgrad_tc(int up, int W, int H, int D, int cin, int cout, const __nv_bfloat16 *x, int xs,
+                            const __nv_bfloat16 *gy, int gys, int gyoff, float *dw, int *err, cudaStream_t st);
 
 // Sets the calling thread's error text (what blz_last_error(NULL) returns).
 void set_thread_error(const char *msg);

@@ -25,10 +25,11 @@
 // kappa is a constant of the trained weights (the training set's mean
 // rms(p* - p_prev) / rms(r)).
 //
-// The 3x3x3 convolutions (forward and data gradient) run on the tcgen05 tensor
-// cores (unet_conv.cu).  Pooling, the transposed convolutions, weight gradients,
-// the loss and Adam are SIMT kernels: together they are a small share of the
-// FLOPs, and weight gradients only run in training.
+// The 3x3x3 convolutions (forward, data and weight gradients) and the
+// transposed convolutions (forward and weight gradient) run on the tcgen05
+// tensor cores (unet_conv.cu).  Pooling, the transposed convolution's data
+// gradient, bias gradients, the loss and Adam are SIMT kernels: together they
+// are a small share of the FLOPs.
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -334,102 +335,31 @@ k_upconv_bwd(const bf16 *__restrict__ g, int gs, LDims dc, int cin, int cout, co
     st8(gx + c, acc);
 }
 
-// Weight (and bias) gradients as a sum over voxels of outer products,
-// dW[tap][co][ci] += sum_v A(v)[co] * B(v, tap)[ci]:
-//   conv (27 taps): A = output gradient at voxel v, B = input at v + offset(tap)
-//   up   (8 parities): A = fine output gradient at (2v + parity), B = coarse input at v
-// One block: one tap, a TCO x TCI tile of (co, ci) and a chunk of voxels,
-// staged 64 voxels at a time in shared memory; 256 threads in NG groups
-// that split the staged voxels, reduced in shared memory, then added to dW
-// with FP32 atomics.
-struct WgArgs {
-    const bf16 *a; int as, aoff;      // gradient tensor, channel stride and first channel
-    const bf16 *b; int bs;            // input tensor and its channel stride
-    LDims d;                          // dims of the voxel loop (the conv's level, or the coarse level)
-    int co, ci;
-    long long n, chunk;               // voxels, voxels per block
-    float *dw, *db;
-};
-
-enum { kModeConv = 0, kModeUp = 1 };
-
-template <int TCO, int TCI, int MODE>
-__global__ void __launch_bounds__(256) k_wgrad(WgArgs a) {
-    constexpr int TY = TCO / 4, TX = TCI / 4, TPG = TY * TX, NG = 256 / TPG, SV = 64;
-    __shared__ __align__(16) float sA[SV][TCO + 4];
-    __shared__ __align__(16) float sB[SV][TCI + 4];
-    __shared__ __align__(16) float sR[NG * TCO * TCI];
-    const int tid = threadIdx.x, grp = tid / TPG, lt = tid % TPG, ty = lt / TX, tx = lt % TX;
-    const int tap = blockIdx.y;
-    const int nco = a.co / TCO;
-    const int cot = (int)(blockIdx.z % nco) * TCO, cit = (int)(blockIdx.z / nco) * TCI;
-    const long long Wp = a.d.W + 2, Hp = a.d.H + 2;
-    long long boff = 0;
-    int px = 0, py = 0, pz = 0;
-    if (MODE == kModeConv) {
-        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-        boff = ((long long)dz * Hp + dy) * Wp + dx;
-    } else {
-        px = tap & 1; py = (tap >> 1) & 1; pz = tap >> 2;
-    }
-    const LDims df{a.d.W * 2, a.d.H * 2, a.d.D * 2};
-    const bool bias_block = a.db && cit == 0 && (MODE == kModeUp || tap == 0);
-    const long long n0 = (long long)blockIdx.x * a.chunk;
-    const long long n1 = n0 + a.chunk < a.n ? n0 + a.chunk : a.n;
-    float acc[4][4];
+// Bias gradient: db[c] += sum over the voxels of g[P][goff + c] (C channels,
+// channel stride gs), the whole padded tensor (its halo is zero).  Thread t
+// sums 8 channels (group t % (C / 8)) over a strided set of voxels; the
+// block reduces them in shared memory and adds one FP32 atomic per channel.
+template <int C>
+__global__ void __launch_bounds__(256) k_bias_grad(const bf16 *__restrict__ g, int gs, int goff, long long nvox,
+                                                   float *__restrict__ db) {
+    constexpr int NG = C / 8, VPB = 256 / NG;
+    __shared__ float red[256][9];
+    const int tid = threadIdx.x, grp = tid % NG;
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (long long v = (long long)blockIdx.x * VPB + tid / NG; v < nvox; v += (long long)gridDim.x * VPB) {
+        float f[8];
+        unpack8(ld8(g + v * gs + goff + grp * 8), f);
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
-    float bacc = 0.0f;
-    for (long long nb = n0; nb < n1; nb += SV) {
-        for (int e = tid; e < SV * (TCO / 8) + SV * (TCI / 8); e += 256) {
-            const bool isA = e < SV * (TCO / 8);
-            const int ee = isA ? e : e - SV * (TCO / 8);
-            const int c8 = isA ? ee % (TCO / 8) : ee % (TCI / 8);
-            const int vv = isA ? ee / (TCO / 8) : ee / (TCI / 8);
-            const long long n = nb + vv;
-            float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            if (n < n1) {
-                int x, y, z;
-                split3(n, a.d.W, a.d.H, x, y, z);
-                const long long P = pvox(a.d, x, y, z);
-                if (isA) {
-                    const long long Pa = MODE == kModeConv ? P : pvox(df, 2 * x + px, 2 * y + py, 2 * z + pz);
-                    unpack8(ld8(a.a + Pa * a.as + a.aoff + cot + c8 * 8), f);
-                } else {
-                    unpack8(ld8(a.b + (P + boff) * a.bs + cit + c8 * 8), f);
-                }
-            }
-            float *dst = isA ? &sA[vv][c8 * 8] : &sB[vv][c8 * 8];
-            *reinterpret_cast<float4 *>(dst) = make_float4(f[0], f[1], f[2], f[3]);
-            *reinterpret_cast<float4 *>(dst + 4) = make_float4(f[4], f[5], f[6], f[7]);
-        }
-        __syncthreads();
-        for (int v = grp; v < SV; v += NG) {
-            const float4 av = *reinterpret_cast<const float4 *>(&sA[v][ty * 4]);
-            const float4 bv = *reinterpret_cast<const float4 *>(&sB[v][tx * 4]);
-            const float ar[4] = {av.x, av.y, av.z, av.w}, br[4] = {bv.x, bv.y, bv.z, bv.w};
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(ar[i], br[j], acc[i][j]);
-        }
-        if (bias_block && tid < TCO)
-            for (int v = 0; v < SV; ++v) bacc += sA[v][tid];
-        __syncthreads();
+        for (int e = 0; e < 8; ++e) acc[e] += f[e];
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) sR[grp * TCO * TCI + (ty * 4 + i) * TCI + tx * 4 + j] = acc[i][j];
+    for (int e = 0; e < 8; ++e) red[tid][e] = acc[e];
     __syncthreads();
-    for (int e = tid; e < TCO * TCI; e += 256) {
-        float s = 0.0f;
-        for (int gq = 0; gq < NG; ++gq) s += sR[gq * TCO * TCI + e];
-        atomicAdd(a.dw + ((size_t)tap * a.co + cot + e / TCI) * a.ci + cit + e % TCI, s);
+    if (tid < C) {
+        float t = 0.0f;
+        for (int r = tid / 8; r < 256; r += NG) t += red[r][tid % 8];
+        atomicAdd(db + tid, t);
     }
-    if (bias_block && tid < TCO) atomicAdd(a.db + cot + tid, bacc);
 }
 
 // Head: out = b + w . d0b[v] (16 channels).
@@ -780,31 +710,28 @@ int conv_dgrad(blz_unet *u, int l, const Ten &gy, const Ten &gx, const Ten *aux,
     return BLZ_OK;
 }
 
-template <int MODE>
-void launch_wgrad(const WgArgs &a, int taps, cudaStream_t st) {
-    const int tco = a.co >= 32 ? 32 : 16, tci = a.ci >= 32 ? 32 : 16;
-    const int tiles = (a.co / tco) * (a.ci / tci);
-    long long want = (4 * 148 + taps * tiles - 1) / (taps * tiles);
-    long long chunks = (a.n + 255) / 256;
-    if (chunks > want) chunks = want;
-    if (chunks < 1) chunks = 1;
-    WgArgs b = a;
-    b.chunk = ((a.n + chunks - 1) / chunks + 63) / 64 * 64;
-    chunks = (a.n + b.chunk - 1) / b.chunk;
-    const dim3 grid((unsigned)chunks, (unsigned)taps, (unsigned)tiles);
-    if (tco == 16 && tci == 16) k_wgrad<16, 16, MODE><<<grid, 256, 0, st>>>(b);
-    else if (tco == 16) k_wgrad<16, 32, MODE><<<grid, 256, 0, st>>>(b);
-    else if (tci == 16) k_wgrad<32, 16, MODE><<<grid, 256, 0, st>>>(b);
-    else k_wgrad<32, 32, MODE><<<grid, 256, 0, st>>>(b);
+void launch_bias_grad(const bf16 *g, int gs, int goff, int C, const LDims &d, float *db, cudaStream_t st) {
+    const long long nvox = (long long)(d.W + 2) * (d.H + 2) * (d.D + 2);
+    const int vpb = 256 / (C / 8);
+    const unsigned blocks = (unsigned)std::min<long long>(8 * 148, (nvox + vpb - 1) / vpb);
+    switch (C) {
+    case 16: k_bias_grad<16><<<blocks, 256, 0, st>>>(g, gs, goff, nvox, db); break;
+    case 32: k_bias_grad<32><<<blocks, 256, 0, st>>>(g, gs, goff, nvox, db); break;
+    case 64: k_bias_grad<64><<<blocks, 256, 0, st>>>(g, gs, goff, nvox, db); break;
+    default: k_bias_grad<128><<<blocks, 256, 0, st>>>(g, gs, goff, nvox, db); break;
+    }
 }
 
 int conv_wgrad(blz_unet *u, int l, const Ten &gy, const Ten &x, cudaStream_t st) {
     const LayerDef &L = kLayers[l];
     const LDims &d = u->L[L.level];
-    WgArgs a{gy.base(), gy.C, 0, x.base(), x.C, d, L.cout, L.cin, (long long)d.W * d.H * d.D, 0,
-             u->grads + u->w_off[l], u->grads + u->b_off[l]};
-    launch_wgrad<kModeConv>(a, 27, st);
-    ++u->launches;
+    const cudaError_t e = launch_wgrad_tc(0, d.W, d.H, d.D, L.cin, L.cout, x.base(), x.C, gy.base(), gy.C, 0,
+                                          u->grads + u->w_off[l], u->err, st);
+    if (e != cudaSuccess)
+        return ufail(BLZ_ERR_CUDA, "conv weight gradient layer %d (%d -> %d): %s", l, L.cin, L.cout,
+                     cudaGetErrorString(e));
+    launch_bias_grad(gy.base(), gy.C, 0, L.cout, d, u->grads + u->b_off[l], st);
+    u->launches += 2;
     UCKL();
     return BLZ_OK;
 }
@@ -828,13 +755,16 @@ int up_bwd(blz_unet *u, int l, const Ten &gy, const Ten &x, const Ten &gx, cudaS
     const LayerDef &L = kLayers[l];
     const LDims &dc = u->L[L.level + 1];
     const long long n = (long long)dc.W * dc.H * dc.D;
-    WgArgs a{gy.base(), gy.C, 0, x.base(), x.C, dc, L.cout, L.cin, n, 0, u->grads + u->w_off[l],
-             u->grads + u->b_off[l]};
-    launch_wgrad<kModeUp>(a, 8, st);
+    const cudaError_t e = launch_wgrad_tc(1, dc.W, dc.H, dc.D, L.cin, L.cout, x.base(), x.C, gy.base(), gy.C, 0,
+                                          u->grads + u->w_off[l], u->err, st);
+    if (e != cudaSuccess)
+        return ufail(BLZ_ERR_CUDA, "transposed convolution %d weight gradient (%d -> %d): %s", l, L.cin, L.cout,
+                     cudaGetErrorString(e));
+    launch_bias_grad(gy.base(), gy.C, 0, L.cout, u->L[L.level], u->grads + u->b_off[l], st);
     const dim3 grid(nblk(n, 128), L.cin / 8);
     k_upconv_bwd<<<grid, 128, 0, st>>>(gy.base(), gy.C, dc, L.cin, L.cout, u->wf + u->bf_off[l], x.base(),
                                        gx.base());
-    u->launches += 2;
+    u->launches += 3;
     UCKL();
     return BLZ_OK;
 }

@@ -757,6 +757,272 @@ cudaError_t launch_upconv_tc(int W, int H, int D, int cin, int cout, const __nv_
     return cudaErrorNotSupported;
 }
 
+// ---------------------------------------------------------------------------
+// Weight gradients on the tensor cores.  For the 3x3x3 convolution
+//   dW[tap][co][ci] = sum over voxels P of gy[P][co] * x[P + off(tap)][ci],
+// a GEMM whose reduction (K) runs over voxels.  Both tensors are channels
+// last, so 8 channels of one voxel are one 16-byte row, and a block of
+// voxels staged row by row is already an operand in the MN-major, no-swizzle
+// layout: core matrices of 8 voxels (K) x 8 channels (M or N), 8-voxel groups
+// LBO = 128 B apart, 8-channel groups SBO apart.  With K blocks of KB voxels:
+//   A (M = 128): 16 eight-channel groups (r, g) of x over the 9 row offsets
+//     r = (dz, dy), each a window of KB + 2 voxels staged from one voxel
+//     early; tap dx reads the same window 16 * (dx + 1) bytes further on;
+//   B (N = Cout): gy over the KB voxels;
+//   three accumulators (dx) of Cout columns in TMEM.
+// The K range is the padded voxels from the first interior row to the last;
+// gy is zero on the halo, so halo voxels add nothing.  For the 2x2x2
+// transposed convolution (8 parities)
+//   dW[par][co][ci] = sum over coarse voxels v of gy[fine(v, par)][co] * x[v][ci]:
+//   A (M = 128): 16 groups (par, co group) of gy gathered at the fine voxels
+//     (zero for halo voxels), B (N = Cin): x over the KB coarse voxels.
+// A CTA owns one M tile (blockIdx.y) and a run of K blocks (blockIdx.x),
+// double buffered: block i + 1 is staged by cp.async before the MMAs of block
+// i are issued, so its loads are in flight while they run (issuing the MMAs
+// first exposes every block's load latency and measured 10 % slower).  One
+// thread issues the MMAs; each buffer's commit arrives on its own mbarrier,
+// waited on (bounded in time) before the buffer is restaged.  The CTA's sums
+// are added to dW with FP32 atomics.
+// ---------------------------------------------------------------------------
+constexpr int kWgKB = 128;                 // voxels per K block; the up gather has one per thread
+static_assert(kWgKB + 2 <= BLZ_CONV_SLACK, "the last K block's window must stay inside the slack");
+
+struct WgTcArgs {
+    const __nv_bfloat16 *x;
+    int xs;                                // layer input (conv) / coarse input (up), channel stride
+    const __nv_bfloat16 *gy;
+    int gys, gyoff;                        // output gradient: channel stride, first channel
+    int W, H, D;                           // dims of the K loop's level (up: the coarse one)
+    long long pbeg;                        // first padded voxel of the K range
+    int nkb, kb_per;                       // K blocks in all, per CTA
+    float *dw;
+    int *err;
+};
+
+__device__ __forceinline__ void st_shared_zero16(uint32_t dst) {
+    asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(dst), "r"(0u) : "memory");
+}
+
+template <int MODE, int CIN, int CO>
+struct WgShape {
+    static constexpr int AW = MODE == 0 ? kWgKB + 2 : kWgKB;   // staged voxels per A group
+    static constexpr int GA = AW * 16;                         // bytes per A group
+    static constexpr int NGA = (MODE == 0 ? CIN : CO) / 8;     // A groups per row offset / parity
+    static constexpr int NGALL = (MODE == 0 ? 9 : 8) * NGA;
+    static constexpr int MTILES = (NGALL + 15) / 16;
+    static constexpr int N = MODE == 0 ? CO : CIN;
+    static constexpr int NGB = N / 8;
+    static constexpr int GB = kWgKB * 16;
+    static constexpr int ABYTES = 16 * GA, BUF = ABYTES + NGB * GB;
+    static constexpr int NACC = MODE == 0 ? 3 : 1;
+    static constexpr int COLS = NACC * N <= 32 ? 32 : NACC * N <= 64 ? 64 : NACC * N <= 128 ? 128
+                                                    : NACC * N <= 256 ? 256 : 512;
+    static_assert(NACC * N <= 512, "accumulators exceed tensor memory");
+    static_assert(N % 16 == 0 && N <= 256, "MN-major B needs N a multiple of 16, at most 256");
+};
+
+template <int MODE, int CIN, int CO>
+__global__ void __launch_bounds__(128, 1) k_wgrad_tc(WgTcArgs a) {
+    using S = WgShape<MODE, CIN, CO>;
+    constexpr int KB = kWgKB, N = S::N, NGA = S::NGA;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int mt = blockIdx.y;
+    const long long Wp = a.W + 2, Hp = a.H + 2, plane = Wp * Hp;
+    const int kb0 = blockIdx.x * a.kb_per;
+    const int nk = min(a.kb_per, a.nkb - kb0);
+    const uint32_t s0 = smem_u32(smem);
+    const uint32_t mb0 = smem_u32(&mbar[0]);
+    auto mb = [&](int b) { return mb0 + 8u * (uint32_t)b; };
+
+    // A groups that hold no row (conv tiles past the 9th row offset) stay zero.
+    for (int e = tid; e < 2 * S::BUF / 16; e += 128) st_shared_zero16(s0 + e * 16);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base)), "r"(S::COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb(0)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb(1)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+
+    auto stage = [&](int kb, int buf) {
+        const uint32_t sa = s0 + buf * S::BUF, sb = sa + S::ABYTES;
+        const long long P0 = a.pbeg + (long long)kb * KB;
+        if constexpr (MODE == 0) {
+            // local row offset lr holds groups lr * NGA .. lr * NGA + NGA - 1;
+            // element e of its window is voxel e / NGA, group e % NGA
+            constexpr int NR = 16 / NGA, PER = S::AW * NGA;
+#pragma unroll
+            for (int lr = 0; lr < NR; ++lr) {
+                const int r = mt * NR + lr;
+                if (r >= 9) break;
+                const __nv_bfloat16 *src =
+                    a.x + (P0 - 1 + (long long)(r / 3 - 1) * plane + (long long)(r % 3 - 1) * Wp) * a.xs;
+                for (int e = tid; e < PER; e += 128) {
+                    const int v = e / NGA, g = e & (NGA - 1);
+                    cp_async16(sa + (lr * NGA + g) * S::GA + v * 16, src + v * a.xs + g * 8);
+                }
+            }
+            const __nv_bfloat16 *gb = a.gy + P0 * a.gys + a.gyoff;
+            for (int e = tid; e < S::NGB * KB; e += 128) {
+                const int g = e & (S::NGB - 1), v = e / S::NGB;
+                cp_async16(sb + g * S::GB + v * 16, gb + v * a.gys + g * 8);
+            }
+        } else {
+            // thread tid gathers coarse voxel P0 + tid's 16 groups
+            const long long P = P0 + tid;
+            const long long zc = P / plane, rem = P - zc * plane;
+            const long long yc = rem / Wp, xc = rem - yc * Wp;
+            const bool inside = zc >= 1 && zc <= a.D && yc >= 1 && yc <= a.H && xc >= 1 && xc <= a.W;
+            const long long Wf = 2LL * a.W + 2, Hf = 2LL * a.H + 2;
+#pragma unroll 4
+            for (int lg = 0; lg < 16; ++lg) {
+                const int grp = mt * 16 + lg, par = grp / NGA, g = grp % NGA;
+                const uint32_t dst = sa + lg * S::GA + tid * 16;
+                if (inside) {
+                    const long long f = ((2 * zc - 1 + (par >> 2)) * Hf + (2 * yc - 1 + ((par >> 1) & 1))) * Wf +
+                                        (2 * xc - 1 + (par & 1));
+                    cp_async16(dst, a.gy + f * a.gys + a.gyoff + g * 8);
+                } else {
+                    st_shared_zero16(dst);
+                }
+            }
+            for (int e = tid; e < S::NGB * KB; e += 128) {
+                const int g = e % S::NGB, v = e / S::NGB;
+                cp_async16(sb + g * S::GB + v * 16, a.x + (P0 + v) * a.xs + g * 8);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+
+    // kind::f16, D FP32, A and B BF16, both MN-major
+    constexpr uint32_t idesc = umma_idesc_bf16(128, N) | (1u << 15) | (1u << 16);
+    bool ok = true;
+    int issued = 0;                                      // MMA batches committed
+    if (nk > 0) stage(kb0, 0);
+    for (int i = 0; i < nk; ++i) {
+        const int buf = i & 1;
+        if (i + 1 < nk) {
+            // buffer buf ^ 1 was last read by the MMAs of block i - 1
+            if (i >= 1) ok = __syncthreads_and(mbar_wait(mb(buf ^ 1), ((i - 1) >> 1) & 1, a.err)) != 0;
+            if (!ok) break;
+            stage(kb0 + i + 1, buf ^ 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = s0 + buf * S::BUF, sb = sa + S::ABYTES;
+            const uint64_t ad0 = umma_desc(sa, 128, S::GA), bd0 = umma_desc(sb, 128, S::GB);
+#pragma unroll
+            for (int kk = 0; kk < KB / 16; ++kk) {
+                const uint64_t bd = bd0 + (uint64_t)((kk * 256) >> 4);
+#pragma unroll
+                for (int d = 0; d < S::NACC; ++d) {
+                    const uint64_t ad = ad0 + (uint64_t)((kk * 256 + (MODE == 0 ? d * 16 : 0)) >> 4);
+                    const uint32_t acc = (i > 0 || kk > 0) ? 1u : 0u;
+                    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                                 " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                                 ::"r"(tmem + (uint32_t)(d * N)), "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                                 : "memory");
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(mb(buf)) : "memory");
+        }
+        ++issued;
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // The last commit completes after every MMA issued before it.
+    if (issued > 0)
+        ok = __syncthreads_and(mbar_wait(mb((issued - 1) & 1), ((issued - 1) >> 1) & 1, a.err) && ok) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok && issued == nk && nk > 0) {
+        // TMEM lane m = A row: group m / 8, channel m % 8 of it.
+        const int m = 32 * warp + lane, grp = mt * 16 + (m >> 3), c8 = m & 7;
+        const bool valid = grp < S::NGALL;
+        const int hi = grp / NGA, ch = (grp % NGA) * 8 + c8;   // conv: (row offset, ci); up: (parity, co)
+#pragma unroll 1
+        for (int d = 0; d < S::NACC; ++d) {
+#pragma unroll 1
+            for (int n0 = 0; n0 < N; n0 += 16) {
+                uint32_t r[16];
+                const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * N + n0);
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                               "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+                               "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                             : "r"(taddr) : "memory");
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (valid) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const int n = n0 + q;
+                        const size_t o = MODE == 0 ? ((size_t)(3 * hi + d) * CO + n) * CIN + ch
+                                                   : ((size_t)hi * CO + ch) * CIN + n;
+                        atomicAdd(a.dw + o, __uint_as_float(r[q]));
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::COLS) : "memory");
+}
+
+template <int MODE, int CIN, int CO>
+static cudaError_t launch_wg_tc(WgTcArgs a, cudaStream_t st) {
+    using S = WgShape<MODE, CIN, CO>;
+    constexpr int smem = 2 * S::BUF;
+    cudaError_t e = cudaFuncSetAttribute(k_wgrad_tc<MODE, CIN, CO>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const long long Wp = a.W + 2, plane = Wp * (a.H + 2);
+    a.pbeg = plane + Wp;                                  // first interior row
+    const long long pend = (long long)(a.D + 1) * plane - Wp;   // past the last interior row
+    const long long nkb = (pend - a.pbeg + kWgKB - 1) / kWgKB;
+    if (nkb >= (1LL << 30)) return cudaErrorInvalidValue;
+    // about two CTAs per SM, at least four K blocks each
+    const long long want = (2 * 148 + S::MTILES - 1) / S::MTILES;
+    long long per = (nkb + want - 1) / want;
+    if (per < 4) per = 4;
+    a.nkb = (int)nkb;
+    a.kb_per = (int)per;
+    const dim3 grid((unsigned)((nkb + per - 1) / per), (unsigned)S::MTILES);
+    k_wgrad_tc<MODE, CIN, CO><<<grid, 128, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wgrad_tc(int up, int W, int H, int D, int cin, int cout, const __nv_bfloat16 *x, int xs,
+                            const __nv_bfloat16 *gy, int gys, int gyoff, float *dw, int *err, cudaStream_t st) {
+    if (xs % 8 != 0 || gys % 8 != 0 || gyoff % 8 != 0) return cudaErrorInvalidValue;
+    WgTcArgs a{x, xs, gy, gys, gyoff, W, H, D, 0, 0, 0, dw, err};
+    if (up) {
+        if (cin == 32 && cout == 16) return launch_wg_tc<1, 32, 16>(a, st);
+        if (cin == 64 && cout == 32) return launch_wg_tc<1, 64, 32>(a, st);
+        if (cin == 128 && cout == 64) return launch_wg_tc<1, 128, 64>(a, st);
+        return cudaErrorNotSupported;
+    }
+#define BLZ_WG(ci, co) if (cin == ci && cout == co) return launch_wg_tc<0, ci, co>(a, st)
+    BLZ_WG(16, 16); BLZ_WG(16, 32); BLZ_WG(32, 16); BLZ_WG(32, 32); BLZ_WG(32, 64);
+    BLZ_WG(64, 32); BLZ_WG(64, 64); BLZ_WG(64, 128); BLZ_WG(128, 64); BLZ_WG(128, 128);
+#undef BLZ_WG
+    return cudaErrorNotSupported;
+}
+
 } // namespace blz
 
 namespace {

@@ -202,8 +202,10 @@ def weights_path(name):
 
 
 def _main(argv=None):
-    """Times the network's forward pass on a random n^3 grid:
-    python -m blaze_b200.unet --forward 256 --reps 5"""
+    """Times the network's forward pass on a random n^3 grid, or one training
+    step (forward, loss and every gradient) with --train-step:
+    python -m blaze_b200.unet --forward 256 --reps 5
+    python -m blaze_b200.unet --forward 128 --train-step --reps 5"""
     import argparse
     import time
     import torch
@@ -211,6 +213,7 @@ def _main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--forward", type=int, default=128, help="grid edge (multiple of 8)")
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--train-step", action="store_true", help="time blz_unet_loss_grad instead")
     args = ap.parse_args(argv)
     n = args.forward
     g = SceneSettings(gridRes=(n, n, n), dx=1.0 / n, closedBounds=(1, 1, 1, 0, 1, 1), bc_mode=1).to_params()
@@ -219,16 +222,20 @@ def _main(argv=None):
     p = 0.1 * torch.randn((n, n, n), device="cuda", generator=gen)
     net = WarmStartUNet((n, n, n), init_params(0))
     out = torch.empty((n, n, n), device="cuda")
-    net.forward(g, rhs, p, out=out)
+    pt = p + 0.05 * torch.randn((n, n, n), device="cuda", generator=gen)
+    run = (lambda: net.loss_grad(g, rhs, p, pt)) if args.train_step else (lambda: net.forward(g, rhs, p, out=out))
+    run()
     torch.cuda.synchronize()
+    launches0 = net.kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.reps):
-        net.forward(g, rhs, p, out=out)
+        run()
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.reps
-    print(json.dumps({"grid": n, "forward_ms": ms, "launches_per_forward": net.kernel_launches() // (args.reps + 1)}))
+    key = "train_step_ms" if args.train_step else "forward_ms"
+    print(json.dumps({"grid": n, key: ms, "launches_per_call": (net.kernel_launches() - launches0) // args.reps}))
     net.close()
 
 
