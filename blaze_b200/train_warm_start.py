@@ -90,11 +90,13 @@ def sor_omega(dims):
 
 
 def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, log=print, policy=None,
-            extra_cap=6000, stride=1):
+            extra_cap=6000, stride=1, omega=None):
     """List of dicts {rhs, p_prev, p_star} (device FP32, (D, H, W)) and the
     rms(p* - p_prev) / rms(r) ratios.  With `policy` (a full-grid
     WarmStartUNet) the frames after the warm-up are solved warm-started by
-    it, as deployed."""
+    it, as deployed.  `omega` is the target solve's relaxation factor (None:
+    Young's optimum, sor_omega; 1: FP64 Gauss-Seidel, whose targets after
+    `extra_cap` sweeps keep the smooth error Gauss-Seidel removes slowest)."""
     pairs, ratios = [], []
     for seed in seeds:
         solver, scn, tmr, hook = _solver(n, seed, tol, max_iter, check_every)
@@ -116,7 +118,7 @@ def harvest(n, seeds, frames, warmup, tol, target_tol, max_iter, check_every, lo
             solver.set_warm_start(None)
             if keep:
                 p_tol = _field(solver, "P", shape)
-                extra, rel = solver.tight_solve(target_tol, extra_cap, sor_omega((n, n, n)))
+                extra, rel = solver.tight_solve(target_tol, extra_cap, omega or sor_omega((n, n, n)))
                 p_star = _field(solver, "P", shape)
                 solver.set_device("P", p_tol.data_ptr())
                 d = (p_star - p_prev).double()
@@ -236,6 +238,8 @@ def main(argv=None):
     ap.add_argument("--tol", type=float, default=1e-4)
     ap.add_argument("--target-tol", type=float, default=1e-8)
     ap.add_argument("--extra-cap", type=int, default=6000, help="FP64 SOR sweeps spent tightening each target")
+    ap.add_argument("--target-omega", type=float, default=0.0,
+                    help="relaxation factor of the target solve (0: Young's optimum; 1: Gauss-Seidel)")
     ap.add_argument("--max-iter", type=int, default=40000)
     ap.add_argument("--check-every", type=int, default=20)
     ap.add_argument("--iters", type=int, default=1500, help="Adam steps per training round")
@@ -320,7 +324,7 @@ def main(argv=None):
             t0 = time.time()
             got, rat = harvest(n, seeds, frames, args.warmup, args.tol, args.target_tol, args.max_iter,
                                args.check_every, log, policy=full if kind == "policy" else None,
-                               extra_cap=args.extra_cap, stride=stride)
+                               extra_cap=args.extra_cap, stride=stride, omega=args.target_omega or None)
             t_harvest += time.time() - t0
             new += got
             ratios += rat
@@ -352,7 +356,7 @@ def main(argv=None):
         "harvest": args.harvest, "keep_kappa": args.keep_kappa,
         "eval_seeds": args.eval_seeds, "frames": args.frames, "stride": args.stride, "warmup": args.warmup,
         "tol": args.tol,
-        "target_tol": args.target_tol, "extra_cap": args.extra_cap, "iters": args.iters, "crop": crop[0],
+        "target_tol": args.target_tol, "extra_cap": args.extra_cap, "target_omega": args.target_omega or "sor", "iters": args.iters, "crop": crop[0],
         "perturb": args.perturb, "init": args.init, "kappa": kappa, "harvest_s": t_harvest, "train_s": t_train,
         "eval": rows, "sweep_ratio": sweep_ratio, "time_ratio": time_ratio, "eval_all_converged": conv}
     full.meta = {k: v for k, v in summary.items() if k != "eval"}
