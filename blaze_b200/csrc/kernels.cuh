@@ -224,6 +224,12 @@ cudaError_t launch_conv3d(const ConvDesc &cd, const __nv_bfloat16 *x, const __nv
 cudaError_t launch_upconv_tc(int W, int H, int D, int cin, int cout, const __nv_bfloat16 *x,
                              const __nv_bfloat16 *w, const float *bias, __nv_bfloat16 *y, int ys, int *err,
                              cudaStream_t st);
+// Data gradient of a 2x2x2 transposed convolution on the tensor cores: gx
+// (coarse, channel stride cin) = (act > 0) * sum over parities of gy (fine,
+// channel stride gs, channels [0, cout)) times the BF16 weights [8][cout][cin].
+cudaError_t launch_upconv_dgrad_tc(int W, int H, int D, int cin, int cout, const __nv_bfloat16 *gy, int gs,
+                                   const __nv_bfloat16 *w, const __nv_bfloat16 *act, __nv_bfloat16 *gx, int *err,
+                                   cudaStream_t st);
 // Weight gradient (no bias) of a 3x3x3 convolution (up = 0: x and gy at level
 // W x H x D, dw [27][cout][cin]) or of a 2x2x2 transposed convolution (up = 1:
 // x coarse at W x H x D, gy fine, dw [8][cout][cin]) on the tensor cores,

@@ -25,11 +25,10 @@
 // kappa is a constant of the trained weights (the training set's mean
 // rms(p* - p_prev) / rms(r)).
 //
-// The 3x3x3 convolutions (forward, data and weight gradients) and the
-// transposed convolutions (forward and weight gradient) run on the tcgen05
-// tensor cores (unet_conv.cu).  Pooling, the transposed convolution's data
-// gradient, bias gradients, the loss and Adam are SIMT kernels: together they
-// are a small share of the FLOPs.
+// The 3x3x3 and the transposed convolutions (forward, data and weight
+// gradients) run on the tcgen05 tensor cores (unet_conv.cu).  Pooling, bias
+// gradients, the loss and Adam are SIMT kernels: together they are a small
+// share of the FLOPs.
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -292,47 +291,6 @@ __global__ void k_skip_grad(const bf16 *__restrict__ dcat, const bf16 *__restric
 #pragma unroll
     for (int e = 0; e < 8; ++e) o[e] = s[e] > 0.0f ? a[e] + 0.125f * p[e] : 0.0f;
     st8(out + f * C + c, o);
-}
-
-// The forward pass of the transposed convolutions runs on the tensor cores
-// (launch_upconv_tc, unet_conv.cu) with the BF16 copy of the weights.
-//
-// Data gradient of the transposed convolution, masked by the coarse input's
-// ReLU: gx[v][ci] = (sum_par sum_co W[par][co][ci] g[fine(v, par)][co]) * (act[v][ci] > 0),
-// with the same BF16 weights as the forward pass.
-// g: fine tensor, channels [0, cout) of channel stride gs.
-__global__ void __launch_bounds__(128)
-k_upconv_bwd(const bf16 *__restrict__ g, int gs, LDims dc, int cin, int cout, const bf16 *__restrict__ w,
-             const bf16 *__restrict__ act, bf16 *__restrict__ gx) {
-    const long long n = (long long)dc.W * dc.H * dc.D;
-    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const int ci0 = blockIdx.y * 8;
-    int cx, cy, cz;
-    split3(v, dc.W, dc.H, cx, cy, cz);
-    const LDims df{dc.W * 2, dc.H * 2, dc.D * 2};
-    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int par = 0; par < 8; ++par) {
-        const long long f = pvox(df, 2 * cx + (par & 1), 2 * cy + ((par >> 1) & 1), 2 * cz + (par >> 2));
-        const bf16 *wp = w + (size_t)par * cout * cin + ci0;
-        for (int co = 0; co < cout; co += 8) {
-            float gv[8];
-            unpack8(ld8(g + f * gs + co), gv);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                float wv[8];
-                unpack8(ld8(wp + (size_t)(co + q) * cin), wv);
-#pragma unroll
-                for (int e = 0; e < 8; ++e) acc[e] = fmaf(wv[e], gv[q], acc[e]);
-            }
-        }
-    }
-    const long long c = pvox(dc, cx, cy, cz) * cin + ci0;
-    float a[8];
-    unpack8(ld8(act + c), a);
-#pragma unroll
-    for (int e = 0; e < 8; ++e) if (!(a[e] > 0.0f)) acc[e] = 0.0f;
-    st8(gx + c, acc);
 }
 
 // Bias gradient: db[c] += sum over the voxels of g[P][goff + c] (C channels,
@@ -754,16 +712,19 @@ int up_fwd(blz_unet *u, int l, const Ten &x, const Ten &y, cudaStream_t st) {
 int up_bwd(blz_unet *u, int l, const Ten &gy, const Ten &x, const Ten &gx, cudaStream_t st) {
     const LayerDef &L = kLayers[l];
     const LDims &dc = u->L[L.level + 1];
-    const long long n = (long long)dc.W * dc.H * dc.D;
+    if (x.C != L.cin || gx.C != L.cin)
+        return ufail(BLZ_ERR_ARG, "transposed convolution %d: coarse tensors need %d channels", l, L.cin);
     const cudaError_t e = launch_wgrad_tc(1, dc.W, dc.H, dc.D, L.cin, L.cout, x.base(), x.C, gy.base(), gy.C, 0,
                                           u->grads + u->w_off[l], u->err, st);
     if (e != cudaSuccess)
         return ufail(BLZ_ERR_CUDA, "transposed convolution %d weight gradient (%d -> %d): %s", l, L.cin, L.cout,
                      cudaGetErrorString(e));
     launch_bias_grad(gy.base(), gy.C, 0, L.cout, u->L[L.level], u->grads + u->b_off[l], st);
-    const dim3 grid(nblk(n, 128), L.cin / 8);
-    k_upconv_bwd<<<grid, 128, 0, st>>>(gy.base(), gy.C, dc, L.cin, L.cout, u->wf + u->bf_off[l], x.base(),
-                                       gx.base());
+    const cudaError_t e2 = launch_upconv_dgrad_tc(dc.W, dc.H, dc.D, L.cin, L.cout, gy.base(), gy.C,
+                                                  u->wf + u->bf_off[l], x.base(), gx.base(), u->err, st);
+    if (e2 != cudaSuccess)
+        return ufail(BLZ_ERR_CUDA, "transposed convolution %d data gradient (%d -> %d): %s", l, L.cin, L.cout,
+                     cudaGetErrorString(e2));
     u->launches += 3;
     UCKL();
     return BLZ_OK;

@@ -54,6 +54,10 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
 
+__device__ __forceinline__ void st_shared_zero16(uint32_t dst) {
+    asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(dst), "r"(0u) : "memory");
+}
+
 __device__ __forceinline__ unsigned long long conv_now_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -758,6 +762,174 @@ cudaError_t launch_upconv_tc(int W, int H, int D, int cin, int cout, const __nv_
 }
 
 // ---------------------------------------------------------------------------
+// Data gradient of the transposed convolution on the tensor cores:
+//   gx[v][ci] = (x[v][ci] > 0) * sum over (par, co) of gy[fine(v, par)][co] * W[par][co][ci],
+// a GEMM of M = 128 padded coarse voxels (the tile of k_upconv_tc), K =
+// 8 COUT (parity, channel) and N = CIN.  A is gy gathered at the fine voxels
+// in the K-major layout of the 3x3x3 kernels ([k group][voxel][8], zero for
+// halo voxels); B is the BF16 weights in the MN-major layout ([ci group]
+// [k][8], k rows 16 B apart), re-laid from [8][COUT][CIN] while staging.
+// The parities go in chunks of PC (all 8, or 4 for 128 -> 64, so that a
+// chunk fits in shared memory), each chunk's MMAs committed to the mbarrier
+// and waited on (bounded) before the next chunk is staged.  The epilogue
+// masks by the forward activation and stores BF16.
+// ---------------------------------------------------------------------------
+template <int CIN, int COUT>
+struct UpDgradShape {
+    static constexpr int PC = CIN == 128 ? 4 : 8;         // parities per chunk
+    static constexpr int KC = PC * COUT;                   // K per chunk
+    static constexpr int ABYTES = KC * kConvM * 2;         // KC / 8 slabs of 128 voxels x 16 B
+    static constexpr int BBYTES = KC * CIN * 2;
+    static constexpr int SMEM = ABYTES + BBYTES;
+    static_assert(SMEM <= 227 * 1024, "chunk exceeds shared memory");
+    static_assert(CIN % 16 == 0 && CIN <= 256, "N = CIN must be a multiple of 16, at most 256");
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128, 1)
+k_upconv_dgrad_tc(int W, int H, int D, const __nv_bfloat16 *__restrict__ gy, int gs,
+                  const __nv_bfloat16 *__restrict__ w, const __nv_bfloat16 *__restrict__ act,
+                  __nv_bfloat16 *__restrict__ gx, int *err) {
+    using S = UpDgradShape<CIN, COUT>;
+    constexpr int KC = S::KC, NG = COUT / 8;
+    // kind::f16, D FP32, A and B BF16, A K-major, B MN-major
+    constexpr uint32_t idesc = umma_idesc_bf16(kConvM, CIN) | (1u << 16);
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int Wp = W + 2, Hp = H + 2;
+    const long long plane = (long long)Wp * Hp;
+    const int z = blockIdx.y;                                              // interior coarse plane
+    const long long P0 = (long long)Wp + (long long)kConvM * blockIdx.x;   // first voxel of the tile
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base)), "r"(CIN < 32 ? 32 : CIN) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const uint32_t aS = smem_u32(smem), bS = aS + (uint32_t)S::ABYTES;
+    // thread tid gathers voxel P0 + tid of the tile
+    const long long P = P0 + tid;
+    const int yv = (int)(P / Wp), xv = (int)(P - (long long)yv * Wp);
+    const bool inside = xv >= 1 && xv <= W && yv >= 1 && yv <= H;
+    const long long Wf = 2LL * W + 2, Hf = 2LL * H + 2;
+    bool ok = true;
+    constexpr int NCH = 8 / S::PC;
+#pragma unroll 1
+    for (int c = 0; c < NCH && ok; ++c) {
+        // A: k group kg = (parity, 8 channels) of voxel tid at aS + kg 2048 + tid 16
+#pragma unroll 4
+        for (int kg = 0; kg < KC / 8; ++kg) {
+            const int par = c * S::PC + kg / NG, g = kg % NG;
+            const uint32_t dst = aS + kg * (kConvM * 16) + tid * 16;
+            if (inside) {
+                const long long f = ((long long)(2 * z + (par >> 2) + 1) * Hf + (2 * (yv - 1) + ((par >> 1) & 1) + 1)) * Wf +
+                                    (2 * (xv - 1) + (par & 1) + 1);
+                cp_async16(dst, gy + f * gs + g * 8);
+            } else {
+                st_shared_zero16(dst);
+            }
+        }
+        // B: chunk (k, ci group ng) of W row c KC + k at bS + (ng KC + k) 16
+        for (int e = tid; e < KC * (CIN / 8); e += 128) {
+            const int k = e / (CIN / 8), ng = e % (CIN / 8);
+            cp_async16(bS + (ng * KC + k) * 16, w + (size_t)(c * KC + k) * CIN + ng * 8);
+        }
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint64_t ad0 = umma_desc(aS, kConvM * 16, 128), bd0 = umma_desc(bS, 128, KC * 16);
+#pragma unroll
+            for (int s = 0; s < KC / 16; ++s) {
+                const uint64_t ad = ad0 + (uint64_t)((2 * s * kConvM * 16) >> 4);
+                const uint64_t bd = bd0 + (uint64_t)((s * 256) >> 4);
+                const uint32_t accum = (c > 0 || s > 0) ? 1u : 0u;
+                asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                             ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(accum) : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(&mbar)) : "memory");
+        }
+        // The staged chunk is overwritten only once its MMAs completed.
+        ok = __syncthreads_and(mbar_wait(smem_u32(&mbar), (uint32_t)(c & 1), err)) != 0;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+        // TMEM lane tid = 32 warp + lane is this thread's own voxel P
+        const long long vc = (long long)(z + 1) * plane + P;
+#pragma unroll 1
+        for (int n0 = 0; n0 < CIN; n0 += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)n0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+                           "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                         : "r"(taddr) : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (inside) {
+                const uint4 a0 = __ldg(reinterpret_cast<const uint4 *>(act + vc * CIN + n0));
+                const uint4 a1 = __ldg(reinterpret_cast<const uint4 *>(act + vc * CIN + n0) + 1);
+                const __nv_bfloat16 *ah0 = reinterpret_cast<const __nv_bfloat16 *>(&a0);
+                const __nv_bfloat16 *ah1 = reinterpret_cast<const __nv_bfloat16 *>(&a1);
+                __nv_bfloat162 hv[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const float a = __bfloat162float(q < 4 ? ah0[2 * q] : ah1[2 * q - 8]) > 0.0f
+                                        ? __uint_as_float(r[2 * q]) : 0.0f;
+                    const float b = __bfloat162float(q < 4 ? ah0[2 * q + 1] : ah1[2 * q - 7]) > 0.0f
+                                        ? __uint_as_float(r[2 * q + 1]) : 0.0f;
+                    hv[q] = __floats2bfloat162_rn(a, b);
+                }
+                uint4 *dst = reinterpret_cast<uint4 *>(gx + vc * CIN + n0);
+                dst[0] = *reinterpret_cast<uint4 *>(&hv[0]);
+                dst[1] = *reinterpret_cast<uint4 *>(&hv[4]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(CIN < 32 ? 32 : CIN)
+                     : "memory");
+}
+
+template <int CIN, int COUT>
+static cudaError_t launch_up_dgrad(int W, int H, int D, const __nv_bfloat16 *gy, int gs, const __nv_bfloat16 *w,
+                                   const __nv_bfloat16 *act, __nv_bfloat16 *gx, int *err, cudaStream_t st) {
+    constexpr int smem = UpDgradShape<CIN, COUT>::SMEM;
+    cudaError_t e = cudaFuncSetAttribute(k_upconv_dgrad_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem);
+    if (e != cudaSuccess) return e;
+    const long long interior = (long long)(W + 2) * H;
+    const dim3 grid((unsigned)((interior + kConvM - 1) / kConvM), (unsigned)D);
+    k_upconv_dgrad_tc<CIN, COUT><<<grid, 128, smem, st>>>(W, H, D, gy, gs, w, act, gx, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_upconv_dgrad_tc(int W, int H, int D, int cin, int cout, const __nv_bfloat16 *gy, int gs,
+                                   const __nv_bfloat16 *w, const __nv_bfloat16 *act, __nv_bfloat16 *gx, int *err,
+                                   cudaStream_t st) {
+    if (gs % 8 != 0) return cudaErrorInvalidValue;
+    if (cin == 32 && cout == 16) return launch_up_dgrad<32, 16>(W, H, D, gy, gs, w, act, gx, err, st);
+    if (cin == 64 && cout == 32) return launch_up_dgrad<64, 32>(W, H, D, gy, gs, w, act, gx, err, st);
+    if (cin == 128 && cout == 64) return launch_up_dgrad<128, 64>(W, H, D, gy, gs, w, act, gx, err, st);
+    return cudaErrorNotSupported;
+}
+
+// ---------------------------------------------------------------------------
 // Weight gradients on the tensor cores.  For the 3x3x3 convolution
 //   dW[tap][co][ci] = sum over voxels P of gy[P][co] * x[P + off(tap)][ci],
 // a GEMM whose reduction (K) runs over voxels.  Both tensors are channels
@@ -798,10 +970,6 @@ struct WgTcArgs {
     float *dw;
     int *err;
 };
-
-__device__ __forceinline__ void st_shared_zero16(uint32_t dst) {
-    asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(dst), "r"(0u) : "memory");
-}
 
 template <int MODE, int CIN, int CO>
 struct WgShape {
