@@ -89,6 +89,8 @@ class BlzStepStats(C.Structure):
 
 
 BLZ_CONV_SLACK = 256
+BLZ_SLAB_ALIGN = 16
+BLZ_SLAB_HALO = 4
 
 
 class BlzConvDesc(C.Structure):
@@ -175,6 +177,12 @@ EXPORTS = {
     "blz_sweeps": (C.c_int, [C.c_void_p, C.c_int]),
     "blz_tight_solve": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_double, _P(C.c_int), _P(C.c_double)]),
     "blz_residual": (C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double)]),
+    "blz_slab_info": (C.c_int, [C.c_void_p, _P(C.c_int), _P(C.c_int), _P(C.c_longlong)]),
+    "blz_slab_get_planes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "blz_slab_set_planes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "blz_slab_pass": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "blz_slab_residual": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, _P(C.c_int), _P(C.c_int)]),
+    "blz_reduce_partials": (C.c_int, [C.c_void_p, C.c_void_p, _P(C.c_double), _P(C.c_double)]),
     "blz_get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "blz_set_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "blz_field_size": (C.c_size_t, [C.c_void_p, C.c_int]),

@@ -868,6 +868,62 @@ static void launch_tb_pass(const Geom &g, const SolveParams &sp, const float *rh
     }
 }
 
+// A pass restricted to planes [zlo, zhi) of the grid (one z slab of a grid
+// decomposed over ranks): chunk blockIdx.y covers ZC planes from zlo.  A tile
+// reads the black input on planes [z0 - 4, z1 + 4) and writes planes
+// [z0, z1) only, so on the slab the result is bitwise that of a whole-grid
+// pass given the same input on [zlo - 4, zhi + 4).  Loads by cp.async (no
+// TMA).
+template <bool WARPROW, bool PK>
+__global__ void __launch_bounds__(kTbThreads, 1)
+k_rbgs_tb2_slab(Geom g, SolveParams sp, const float *__restrict__ rhs_r, const float *__restrict__ rhs_b,
+                const float *__restrict__ pin_b, float *__restrict__ pout_r, float *__restrict__ pout_b, int TY,
+                int ZC, int zlo, int zhi) {
+    const int z0 = zlo + blockIdx.y * ZC, z1 = z0 + ZC < zhi ? z0 + ZC : zhi;
+    tb2_tile<WARPROW, false, PK>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, blockIdx.x * TY, z0, z1,
+                                 threadIdx.x, threadIdx.y, blockDim.y, true, threadIdx.x == 0 && threadIdx.y == 0,
+                                 nullptr, nullptr, nullptr);
+}
+
+bool slab_pass_supported(const Geom &g) { return tb_supported(g); }
+
+void launch_tb_pass_slab(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
+                         const float *pin_b, float *pout_r, float *pout_b, int zlo, int zhi, bool pk,
+                         cudaStream_t st) {
+    const int Wq = g.W >> 3, TY = tb_rows_tile(Wq, g.H);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_rbgs_tb2_slab<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_rbgs_tb2_slab<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_rbgs_tb2_slab<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        cudaFuncSetAttribute(k_rbgs_tb2_slab<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmemMax);
+        attr_set = true;
+    }
+    const int ra = tb_rows_alloc(TY);
+    const size_t smem = tb_smem(g, TY);
+    // z chunks so that the row bands times the chunks fill the SMs, at least 8 planes
+    const int bands = (g.H + TY - 1) / TY, depth = zhi - zlo;
+    const int chunks = std::max(1, device_sm_count() / bands);
+    const int ZC = std::max(8, (depth + chunks - 1) / chunks);
+    const dim3 b(Wq, ra / 2, 1);
+    const dim3 gr(bands, (depth + ZC - 1) / ZC, 1);
+    if (pk) {
+        if (Wq == 32)
+            k_rbgs_tb2_slab<true, true><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC,
+                                                             zlo, zhi);
+        else
+            k_rbgs_tb2_slab<false, true><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC,
+                                                              zlo, zhi);
+    } else {
+        if (Wq == 32)
+            k_rbgs_tb2_slab<true, false><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC,
+                                                              zlo, zhi);
+        else
+            k_rbgs_tb2_slab<false, false><<<gr, b, smem, st>>>(g, sp, rhs_r, rhs_b, pin_b, pout_r, pout_b, TY, ZC,
+                                                               zlo, zhi);
+    }
+}
+
 // (planes per thread, rows per block) of each segment-kernel variant; the
 // variants after them are the temporal-blocking pass with ZC planes per CTA
 // (0: sized to fill the SMs): 9 with its rhs and input planes staged by TMA,
@@ -1261,6 +1317,37 @@ int launch_residual(const Geom &g, const SolveParams &sp, const float *rhs_r, co
     }
     k_reduce_pairs<<<1, 1024, 0, st>>>(partials, parts, out2);
     return 2;
+}
+
+// The residual tiles blk0 .. blk0 + gridDim.x - 1 of a tiled grid (the
+// tiles of a z slab), partial sums at their whole-grid indices.
+__global__ void __launch_bounds__(kResThreads, kResBlocksPerSM)
+k_residual_tiles(Geom g, SolveParams sp, double scale, const float *__restrict__ rr,
+                 const float *__restrict__ rb, const float *__restrict__ pr, const float *__restrict__ pb, int blk0,
+                 double *__restrict__ partials) {
+    residual_tile_block(g, sp, scale, rr, rb, pr, pb, blk0 + (int)blockIdx.x, partials);
+}
+
+int residual_slab_tiles(const Geom &g, int z0, int z1, int *first, int *count) {
+    if (!residual_tiled(g) || z0 < 0 || z1 > g.D || z0 >= z1 || z0 % kResKZ != 0 || (z1 % kResKZ != 0 && z1 != g.D))
+        return -1;
+    const int ty = residual_tiles_y(g);
+    *first = (z0 / kResKZ) * ty;
+    *count = ((z1 + kResKZ - 1) / kResKZ - z0 / kResKZ) * ty;
+    return 0;
+}
+
+int launch_residual_slab(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
+                         const float *p_r, const float *p_b, int z0, int z1, double *partials, cudaStream_t st) {
+    int first = 0, count = 0;
+    if (residual_slab_tiles(g, z0, z1, &first, &count) != 0) return -1;
+    k_residual_tiles<<<count, kResThreads, 0, st>>>(g, sp, (double)sp.scale_d, rhs_r, rhs_b, p_r, p_b, first,
+                                                     partials);
+    return 1;
+}
+
+void launch_reduce_pairs(const double *partials, int n, double *out2, cudaStream_t st) {
+    k_reduce_pairs<<<1, 1024, 0, st>>>(partials, n, out2);
 }
 
 // pressure_gradient_update_kernel (FluidSolver.cu:601-669).  Interior faces

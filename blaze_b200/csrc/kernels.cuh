@@ -105,6 +105,22 @@ int  launch_residual(const Geom &g, const SolveParams &sp, const float *rhs_r, c
                      const float *p_r, const float *p_b, double *partials, int max_partials,
                      double *out2, cudaStream_t st);
 int  residual_blocks(const Geom &g);
+// z-slab decomposition of a solve.  slab_pass_supported: the temporal-blocking
+// pass applies to g.  launch_tb_pass_slab: one pass (two sweeps) over planes
+// [zlo, zhi), black input pin_b (read on [zlo - 4, zhi + 4)), both colours out.
+// residual_slab_tiles: the residual partials (whole-grid indices [first,
+// first + count)) of planes [z0, z1), z0 and z1 multiples of the tiles'
+// depth (z1 may be D); -1 when g's residual is not tiled or the range is
+// not aligned.  launch_residual_slab writes them (reads p planes z0 - 1 and
+// z1); launch_reduce_pairs sums n pairs in the whole-grid residual's order.
+bool slab_pass_supported(const Geom &g);
+void launch_tb_pass_slab(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
+                         const float *pin_b, float *pout_r, float *pout_b, int zlo, int zhi, bool pk,
+                         cudaStream_t st);
+int  residual_slab_tiles(const Geom &g, int z0, int z1, int *first, int *count);
+int  launch_residual_slab(const Geom &g, const SolveParams &sp, const float *rhs_r, const float *rhs_b,
+                          const float *p_r, const float *p_b, int z0, int z1, double *partials, cudaStream_t st);
+void launch_reduce_pairs(const double *partials, int n, double *out2, cudaStream_t st);
 // d_r/d_b (may be null): the correction of a defect-correction solve, the
 // pressure being p + d.
 void launch_gradient(const Geom &g, const SolveParams &sp, float dt_over_rho_dx, const float *p_r,

@@ -1128,6 +1128,98 @@ int blz_set_field(blz_solver *s, int f, const float *src, int on_device) {
     return BLZ_OK;
 }
 
+// ---- z-slab decomposition of the solve ------------------------------------
+// Every rank holds the whole grid and updates only its slab of planes; the
+// caller moves halo planes between ranks (blaze_b200/slab.py).
+
+int blz_slab_info(blz_solver *s, int *supported, int *n_partials, long long *plane_floats) {
+    if (!s || !supported || !n_partials || !plane_floats) return fail(s, BLZ_ERR_ARG, "null argument");
+    int first = 0, count = 0;
+    *supported = slab_pass_supported(s->g) && residual_slab_tiles(s->g, 0, s->g.D, &first, &count) == 0 &&
+                 s->P.gs_order == BLZ_GS_RB3D && !s->P.defect_correction;
+    *n_partials = residual_blocks(s->g);
+    *plane_floats = (long long)(s->g.W / 2) * s->g.H;
+    return BLZ_OK;
+}
+
+// The colour-packed array of (buffer, colour): p or the pass scratch q.
+static float *slab_array(blz_solver *s, int buf, int colour) {
+    if (buf == 0) return colour ? s->p_b : s->p_r;
+    return colour ? q_b(s) : q_r(s);
+}
+
+static int slab_planes_arg(blz_solver *s, int buf, int colour, int z0, int z1, const void *dev) {
+    if (!dev) return fail(s, BLZ_ERR_ARG, "null device buffer");
+    if ((buf != 0 && buf != 1) || (colour != 0 && colour != 1) || z0 < 0 || z1 > s->g.D || z0 > z1)
+        return fail(s, BLZ_ERR_ARG, "slab planes: buffer %d colour %d planes [%d, %d) of %d", buf, colour, z0, z1,
+                    s->g.D);
+    return BLZ_OK;
+}
+
+int blz_slab_get_planes(blz_solver *s, int buf, int colour, int z0, int z1, void *dst) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    int rc = slab_planes_arg(s, buf, colour, z0, z1, dst);
+    if (rc != BLZ_OK) return rc;
+    const size_t pl = (size_t)(s->g.W / 2) * s->g.H;
+    if (z1 > z0)
+        CK(s, cudaMemcpyAsync(dst, slab_array(s, buf, colour) + pl * z0, pl * (z1 - z0) * sizeof(float),
+                              cudaMemcpyDeviceToDevice, s->st));
+    return BLZ_OK;
+}
+
+int blz_slab_set_planes(blz_solver *s, int buf, int colour, int z0, int z1, const void *src) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    int rc = slab_planes_arg(s, buf, colour, z0, z1, src);
+    if (rc != BLZ_OK) return rc;
+    const size_t pl = (size_t)(s->g.W / 2) * s->g.H;
+    s->defect_valid = false;
+    if (z1 > z0)
+        CK(s, cudaMemcpyAsync(slab_array(s, buf, colour) + pl * z0, src, pl * (z1 - z0) * sizeof(float),
+                              cudaMemcpyDeviceToDevice, s->st));
+    return BLZ_OK;
+}
+
+int blz_slab_pass(blz_solver *s, int z0, int z1, int from_q) {
+    if (!s) return fail(nullptr, BLZ_ERR_ARG, "null solver");
+    int ok = 0, np = 0;
+    long long pf = 0;
+    blz_slab_info(s, &ok, &np, &pf);
+    if (!ok) return fail(s, BLZ_ERR_STATE, "slab pass: needs W %% 8 == 0, the temporal-blocking pass, "
+                                           "RB3D order and no defect correction");
+    if (z0 < 0 || z1 > s->g.D || z0 >= z1 || (from_q != 0 && from_q != 1))
+        return fail(s, BLZ_ERR_ARG, "slab pass: planes [%d, %d) of %d, from_q %d", z0, z1, s->g.D, from_q);
+    s->defect_valid = false;
+    const SolveParams sp = solve_params(s->P);
+    if (from_q) launch_tb_pass_slab(s->g, sp, s->rhs_r, s->rhs_b, q_b(s), s->p_r, s->p_b, z0, z1, true, s->st);
+    else launch_tb_pass_slab(s->g, sp, s->rhs_r, s->rhs_b, s->p_b, q_r(s), q_b(s), z0, z1, true, s->st);
+    CKL(s);
+    s->launches++;
+    return BLZ_OK;
+}
+
+int blz_slab_residual(blz_solver *s, int z0, int z1, double *partials, int *first, int *count) {
+    if (!s || !partials || !first || !count) return fail(s, BLZ_ERR_ARG, "null argument");
+    if (residual_slab_tiles(s->g, z0, z1, first, count) != 0)
+        return fail(s, BLZ_ERR_ARG, "slab residual: planes [%d, %d) of %d must be whole residual tiles of %d planes",
+                    z0, z1, s->g.D, BLZ_SLAB_ALIGN);
+    launch_residual_slab(s->g, solve_params(s->P), s->rhs_r, s->rhs_b, s->p_r, s->p_b, z0, z1, partials, s->st);
+    CKL(s);
+    s->launches++;
+    return BLZ_OK;
+}
+
+int blz_reduce_partials(blz_solver *s, const double *partials, double *res, double *bn) {
+    if (!s || !partials || !res || !bn) return fail(s, BLZ_ERR_ARG, "null argument");
+    launch_reduce_pairs(partials, residual_blocks(s->g), s->d_norm2, s->st);
+    CKL(s);
+    s->launches++;
+    CK(s, cudaMemcpyAsync(s->h_norm2, s->d_norm2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(s, cudaStreamSynchronize(s->st));
+    *res = std::sqrt(s->h_norm2[0]);
+    *bn = std::sqrt(s->h_norm2[1]);
+    return BLZ_OK;
+}
+
 } // extern "C"
 
 namespace blz {

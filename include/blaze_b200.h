@@ -235,6 +235,44 @@ int  blz_tight_solve(blz_solver *s, double tol, int max_sweeps, double omega, in
 /* FP64 ||b - A p||_2 and ||b||_2 of the current rhs and p.                  */
 int  blz_residual(blz_solver *s, double *res_norm, double *rhs_norm);
 
+/* ---- z-slab decomposition of one grid's pressure solve --------------------
+ * No counterpart in the reference (one GPU, FluidSolver.cu:517-599 solves
+ * the whole grid).  Ranks (one process per GPU) each hold a solver of the
+ * whole grid, run the step's other stages on the whole grid, and split the
+ * solve into z slabs: each rank updates planes [z0, z1) only, and the caller
+ * moves halo planes between ranks (blaze_b200/slab.py does both).  Slab
+ * bounds are multiples of BLZ_SLAB_ALIGN (or D).  A pass over a slab reads
+ * the black pressure on [z0 - BLZ_SLAB_HALO, z1 + BLZ_SLAB_HALO); the
+ * residual of a slab reads p on planes z0 - 1 and z1.  The residual's
+ * partial sums of all slabs, gathered into one array, reduce in the
+ * whole-grid order, so the decomposed solve takes the same sweeps and gives
+ * the same pressure, bit for bit, as blz_solve on one GPU (RB3D order, check
+ * interval a multiple of 4, no defect correction).  All calls are
+ * asynchronous on the solver's stream except blz_reduce_partials.           */
+#define BLZ_SLAB_ALIGN 16
+#define BLZ_SLAB_HALO  4
+/* supported: the slab entry points apply to this solver (W % 8 == 0 with
+ * the temporal-blocking pass, tiled residual, RB3D, no defect correction);
+ * n_partials: FP64 pairs of the whole grid's residual; plane_floats: floats
+ * per colour plane of the packed pressure (W/2 * H).                        */
+int  blz_slab_info(blz_solver *s, int *supported, int *n_partials, long long *plane_floats);
+/* Copies planes [z0, z1) of one colour (0 red, 1 black) of the pressure
+ * (buf 0) or of the pass scratch (buf 1) to / from device memory of
+ * (z1 - z0) * plane_floats floats.                                          */
+int  blz_slab_get_planes(blz_solver *s, int buf, int colour, int z0, int z1, void *dst_dev);
+int  blz_slab_set_planes(blz_solver *s, int buf, int colour, int z0, int z1, const void *src_dev);
+/* One temporal-blocking pass (two red-black sweeps) over planes [z0, z1):
+ * black input from the scratch (from_q = 1) or the pressure, both colours
+ * written to the other buffer on [z0, z1) only.                             */
+int  blz_slab_pass(blz_solver *s, int z0, int z1, int from_q);
+/* The residual's FP64 partial sums over the tiles of planes [z0, z1) of p,
+ * written to partials (device, n_partials pairs) at their whole-grid
+ * indices [first, first + count).                                           */
+int  blz_slab_residual(blz_solver *s, int z0, int z1, double *partials, int *first, int *count);
+/* ||b - A p|| and ||b|| from a full array of partials (device), summed in
+ * the whole-grid residual's order.  Synchronises the solver's stream.       */
+int  blz_reduce_partials(blz_solver *s, const double *partials, double *res_norm, double *rhs_norm);
+
 /* Field access in the reference layout.  on_device != 0: dst/src is a device
  * pointer of the field's size; otherwise host memory.                       */
 int  blz_get_field(blz_solver *s, int field, float *dst, int on_device);

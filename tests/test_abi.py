@@ -131,6 +131,22 @@ def test_warm_start_and_batch_argument_checks_need_no_gpu(lib):
     assert "2^28" in _err(lib)
 
 
+def test_slab_entry_points_refuse_null_arguments(lib):
+    """The z-slab solve's entry points reject a null solver or null outputs
+    before any device call."""
+    _abi.bind(lib)
+    ok, n, pf = C.c_int(), C.c_int(), C.c_longlong()
+    assert lib.blz_slab_info(None, C.byref(ok), C.byref(n), C.byref(pf)) == _abi.BLZ_ERR_ARG
+    assert lib.blz_slab_get_planes(None, 0, 0, 0, 1, None) == _abi.BLZ_ERR_ARG
+    assert lib.blz_slab_set_planes(None, 0, 0, 0, 1, None) == _abi.BLZ_ERR_ARG
+    assert lib.blz_slab_pass(None, 0, 16, 0) == _abi.BLZ_ERR_ARG
+    first, count = C.c_int(), C.c_int()
+    assert lib.blz_slab_residual(None, 0, 16, None, C.byref(first), C.byref(count)) == _abi.BLZ_ERR_ARG
+    r, b = C.c_double(), C.c_double()
+    assert lib.blz_reduce_partials(None, None, C.byref(r), C.byref(b)) == _abi.BLZ_ERR_ARG
+    assert _abi.BLZ_SLAB_ALIGN == 16 and _abi.BLZ_SLAB_HALO == 4
+
+
 def test_noalloc_residual_argument_checks_need_no_gpu(lib):
     """The allocation-free residual refuses what blz_create refuses (an
     unknown bc_mode, bad dims, non-positive dx/dt/density) and grids deeper
