@@ -864,4 +864,13 @@ int orc_num_threads(void) {
 #endif
 }
 
+// Threads of the oracle's later parallel loops (the single-core baseline).
+void orc_set_num_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
 } // extern "C"
