@@ -64,8 +64,9 @@ def load():
         lib.orc_noise_set_lattice_patterns.argtypes = [C.POINTER(C.c_ulonglong), C.c_int]
         lib.orc_noise.argtypes = [C.POINTER(_abi.BlzNoiseArgs), C.c_void_p, C.c_longlong, C.c_void_p]
         lib.orc_num_threads.restype = C.c_int
-        lib.orc_set_num_threads.restype = None
-        lib.orc_set_num_threads.argtypes = [C.c_int]
+        if hasattr(lib, "orc_set_num_threads"):
+            lib.orc_set_num_threads.restype = None
+            lib.orc_set_num_threads.argtypes = [C.c_int]
         _lib = lib
     return _lib
 
@@ -188,8 +189,13 @@ def num_threads():
 
 
 def set_num_threads(n):
-    """Threads of the oracle's later parallel loops (OpenMP)."""
-    load().orc_set_num_threads(int(n))
+    """Threads of the oracle's later parallel loops (OpenMP); False when the
+    built library predates this call."""
+    lib = load()
+    if not hasattr(lib, "orc_set_num_threads"):
+        return False
+    lib.orc_set_num_threads(int(n))
+    return True
 
 
 def tex_sample(T, pos3, quant=3):
